@@ -1,0 +1,151 @@
+"""ctypes wrapper around the CPU oracle (oracle/build/libhw_oracle.so).
+
+Test infrastructure: imported only by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, always as the checker.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+LIB_PATH = os.path.join(ORACLE_DIR, "build", "libhw_oracle.so")
+
+_lib = None
+
+
+class OrOpts(ctypes.Structure):
+    _fields_ = [
+        ("eps_abs", ctypes.c_double),
+        ("eps_rel", ctypes.c_double),
+        ("h0", ctypes.c_double),
+        ("t_stop", ctypes.c_double),
+        ("seed", ctypes.c_ulonglong),
+        ("nref", ctypes.c_int),
+        ("write_fields", ctypes.c_int),
+        ("outdir", ctypes.c_char_p),
+    ]
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        vp, dp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int
+        L.or_create.restype = vp
+        L.or_create.argtypes = [ctypes.c_char_p, ctypes.POINTER(OrOpts)]
+        L.or_destroy.argtypes = [vp]
+        L.or_last_error.restype = ctypes.c_char_p
+        L.or_nx.argtypes = [vp]
+        L.or_nt.argtypes = [vp]
+        L.or_scalar.restype = ctypes.c_double
+        L.or_scalar.argtypes = [vp, ctypes.c_char_p]
+        L.or_table.argtypes = [vp, ctypes.c_char_p, dp, ip]
+        L.or_initial_state.argtypes = [vp, dp]
+        L.or_rhs.argtypes = [vp, ctypes.c_double, dp, dp]
+        L.or_evolve_apply.argtypes = [vp, dp, ctypes.c_double, dp, dp]
+        L.or_run.argtypes = [vp, dp, dp, dp, ip]
+        L.or_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)] * 1 + [ctypes.POINTER(ctypes.c_longlong)] * 2
+        L.or_breaking_log.restype = ctypes.c_char_p
+        L.or_breaking_log.argtypes = [vp]
+        L.or_reset.argtypes = [vp]
+        L.or_fft.argtypes = [ip, dp, dp, dp, dp, ip]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Oracle:
+    def __init__(self, workdir, eps_abs=0.0, eps_rel=0.0, h0=0.0, t_stop=0.0, seed=0,
+                 nref=0, outdir=None, write_fields=0):
+        L = lib()
+        self._outdir = outdir.encode() if outdir else None
+        o = OrOpts(eps_abs, eps_rel, h0, t_stop, seed, nref, write_fields, self._outdir)
+        self.h = L.or_create(str(workdir).encode(), ctypes.byref(o))
+        if not self.h:
+            raise RuntimeError("oracle: " + L.or_last_error().decode())
+        self.nx = L.or_nx(self.h)
+        self.n = L.or_nt(self.h)
+
+    def close(self):
+        if self.h:
+            lib().or_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def scalar(self, name):
+        return lib().or_scalar(self.h, name.encode())
+
+    def table(self, name):
+        cap = 4 * max(self.nx, self.n) + 16
+        out = np.zeros(cap)
+        m = lib().or_table(self.h, name.encode(), _p(out), cap)
+        if m < 0:
+            raise KeyError(name)
+        return out[:m].copy()
+
+    def initial_state(self):
+        y = np.zeros(4 * self.nx)
+        lib().or_initial_state(self.h, _p(y))
+        return y
+
+    def rhs(self, t, y):
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        dz = np.zeros_like(y)
+        lib().or_rhs(self.h, float(t), _p(y), _p(dz))
+        return dz
+
+    def evolve_apply(self, t, t1, h, y):
+        tt = np.array([t], dtype=np.float64)
+        hh = np.array([h], dtype=np.float64)
+        st = lib().or_evolve_apply(self.h, _p(tt), float(t1), _p(hh), _p(y))
+        if st:
+            raise RuntimeError("oracle evolve failed")
+        return float(tt[0]), float(hh[0])
+
+    def run(self, cap_rows=None):
+        cap = cap_rows if cap_rows else self.n
+        ng = max(int(self.scalar("ngauge")), 1)
+        ge = np.zeros(cap * ng)
+        gd = np.zeros(cap * ng)
+        tim = np.zeros(cap)
+        rows = lib().or_run(self.h, _p(ge), _p(gd), _p(tim), cap)
+        return tim[:rows], ge[: rows * ng].reshape(rows, ng), gd[: rows * ng].reshape(rows, ng)
+
+    def stats(self):
+        a, b, c = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        lib().or_stats(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+        return a.value, b.value, c.value
+
+    def breaking_log(self):
+        return lib().or_breaking_log(self.h).decode()
+
+    def reset(self):
+        lib().or_reset(self.h)
+
+
+def fft(x, sign=-1):
+    x = np.asarray(x, dtype=np.complex128)
+    n = x.size
+    re = np.ascontiguousarray(x.real)
+    im = np.ascontiguousarray(x.imag)
+    ro = np.zeros(n)
+    io = np.zeros(n)
+    lib().or_fft(n, _p(re), _p(im), _p(ro), _p(io), sign)
+    return ro + 1j * io
