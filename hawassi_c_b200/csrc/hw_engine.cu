@@ -1,0 +1,716 @@
+// hw_engine.cu -- kernels, host engine and C ABI of the B200 HAWASSI 1D engine.
+//
+// One member (tank realisation) is advanced by one thread-block cluster of C
+// CTAs (C = N / M, slice M <= 2048 points, M / 8 threads per CTA).  One launch
+// per (M, C) class advances every member of that class through its output
+// samples, the whole RKF45 loop (stages, error norm, step control, retries)
+// staying on the device.  Classes run concurrently on forked streams.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/hawassi_b200.h"
+#include "hw_kernels.h"
+#include "hw_setup.hpp"
+
+using namespace hwdev;
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+// reference layout (4N doubles) -> internal (2N double2, spectral permuted)
+__global__ void k_to_internal(const double* __restrict__ ref, double2* __restrict__ dst, int N, int logC, int M) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= N) return;
+  const int C = 1 << logC;
+  const int p = (q & (C - 1)) * M + (q >> logC);
+  dst[p] = make_double2(ref[q], ref[N + q]);
+  dst[N + p] = make_double2(ref[2 * N + q], ref[3 * N + q]);
+}
+
+__global__ void k_to_reference(const double2* __restrict__ src, double* __restrict__ ref, int N, int logC, int M) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= N) return;
+  const int C = 1 << logC;
+  const int p = (q & (C - 1)) * M + (q >> logC);
+  const double2 e = src[p], u = src[N + p];
+  ref[q] = e.x;
+  ref[N + q] = e.y;
+  ref[2 * N + q] = u.x;
+  ref[3 * N + q] = u.y;
+}
+
+// ---------------------------------------------------------------------------
+// host engine
+// ---------------------------------------------------------------------------
+#define HW_CUDA(call)                                                                       \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess) {                                                                \
+      err = std::string(#call) + ": " + cudaGetErrorString(e_);                             \
+      return false;                                                                         \
+    }                                                                                       \
+  } while (0)
+
+struct Arena {
+  char* base = nullptr;
+  size_t used = 0, cap = 0;
+  template <class T>
+  T* take(size_t n) {
+    size_t off = (used + 255) & ~size_t(255);
+    used = off + n * sizeof(T);
+    return reinterpret_cast<T*>(base + off);
+  }
+};
+
+struct HostMember {
+  hw::Member m;
+  int N = 0, C = 1, M = 0, logC = 0;
+  DevMember d{};
+  void* dev = nullptr;       // arena base
+  size_t dev_bytes = 0;
+  double t0 = 0, h0 = 0;
+};
+
+struct Class {
+  int M, C;
+  std::vector<int> members;
+  int* d_list = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+};
+
+}  // namespace
+
+struct hw_ctx {
+  std::vector<HostMember> mem;
+  std::vector<Class> classes;
+  DevMember* d_mems = nullptr;
+  std::vector<std::pair<int, double2*>> tw;   // twiddle tables per N
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr;
+  int* d_single = nullptr;    // one-member list for single-member launches
+  double* d_ref = nullptr;    // 4*maxN staging for reference-layout transfers
+  int maxN = 0;
+  int device = 0;
+  std::string err;
+
+  bool init(const std::vector<std::string>& dirs, const hw_opts* o);
+  bool upload_member(HostMember& h);
+  bool launch_class(const Class& c, const int* list, int nblocks_members, int mode, cudaStream_t s);
+  bool launch_member(int mi, int mode, double t_rhs);
+  bool run(int i_stop_all, double t_end, bool by_time);
+  bool sync_desc();
+  bool reset();
+  ~hw_ctx();
+};
+
+static std::string g_create_err;
+
+namespace {
+
+std::vector<double> permute(const std::vector<double>& v, int N, int C, int M) {
+  std::vector<double> r(N);
+  for (int q = 0; q < N; ++q) r[(q % C) * M + q / C] = v[q];
+  return r;
+}
+
+cudaError_t launch_any(int M, int mode, DevMember* mems, const int* list, int nmem, int C, double t, cudaStream_t s) {
+  switch (M) {
+    case 256: return hw_launch_256(mode, mems, list, nmem, C, t, s);
+    case 512: return hw_launch_512(mode, mems, list, nmem, C, t, s);
+    case 1024: return hw_launch_1024(mode, mems, list, nmem, C, t, s);
+    case 2048: return hw_launch_2048(mode, mems, list, nmem, C, t, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace
+
+bool hw_ctx::upload_member(HostMember& h) {
+  const hw::Member& m = h.m;
+  const int N = h.N, C = h.C, M = h.M, K = m.flat ? 0 : m.nref, n = m.n;
+  // size the arena
+  size_t bytes = 0;
+  auto add = [&](size_t b) { bytes += ((b + 255) / 256) * 256; };
+  for (int i = 0; i < 10 + 2; ++i) add(sizeof(double) * N);                 // real tables
+  add(sizeof(double2) * N * 2);                                              // gamX, gamXs
+  add(sizeof(double) * size_t(N) * std::max(K, 1) * 2);                      // Csq, gam
+  for (int i = 0; i < 5; ++i) add(sizeof(double) * std::max(n, 2));          // splines
+  add(sizeof(double2) * size_t(2 * N) * 10);                                 // y, ynew, kb[7], zs
+  add(sizeof(double2) * size_t(N) * kScratch);
+  const int cap = std::max(N / 4, 4);
+  add(sizeof(BrkDev));
+  add(sizeof(Crest) * cap * 3);
+  add(sizeof(int) * (cap + 3 * N + 8));
+  add(sizeof(double) * N);
+  const long long log_cap = m.breaking ? (1LL << 22) : 16;
+  add(sizeof(double) * log_cap);
+  bytes += 4096;
+  HW_CUDA(cudaMalloc(&h.dev, bytes));
+  HW_CUDA(cudaMemset(h.dev, 0, bytes));
+  h.dev_bytes = bytes;
+  Arena a;
+  a.base = static_cast<char*>(h.dev);
+  a.cap = bytes;
+  DevMember& d = h.d;
+  std::memset(&d, 0, sizeof d);
+  d.N = N; d.C = C; d.M = M; d.logC = h.logC;
+  d.model = m.model; d.flat = m.flat ? 1 : 0; d.nref = K; d.brk = m.breaking ? 1 : 0;
+  d.has_influx = m.has_influx ? 1 : 0; d.prop_mode = m.prop_mode; d.n_in = n;
+  d.invN = 1.0 / N; d.dx = m.dx; d.eps_abs = m.eps_abs; d.eps_rel = m.eps_rel;
+  auto up = [&](const std::vector<double>& v, size_t cnt) -> double* {
+    double* p = a.take<double>(cnt);
+    if (!v.empty()) cudaMemcpy(p, v.data(), sizeof(double) * std::min(cnt, v.size()), cudaMemcpyHostToDevice);
+    return p;
+  };
+  std::vector<double> c1(N), gk(N);
+  for (int i = 0; i < N; ++i) {
+    c1[i] = (m.Csqr[i] / hwdev::kG) * m.k[i];
+    gk[i] = hwdev::kG * m.k[i];
+  }
+  d.k = up(permute(m.k, N, C, M), N);
+  d.aal = up(permute(m.aal, N, C, M), N);
+  d.c1 = up(permute(c1, N, C, M), N);
+  d.gk = up(permute(gk, N, C, M), N);
+  d.M0im = up(permute(m.M0im, N, C, M), N);
+  d.L = up(permute(m.L, N, C, M), N);
+  {
+    std::vector<double> g(2 * N), s(2 * N);
+    std::vector<double> pr = permute(m.gamX_re, N, C, M), pi = permute(m.gamX_im, N, C, M);
+    std::vector<double> qr = permute(m.gamXs_re, N, C, M), qi = permute(m.gamXs_im, N, C, M);
+    for (int i = 0; i < N; ++i) { g[2 * i] = pr[i]; g[2 * i + 1] = pi[i]; s[2 * i] = qr[i]; s[2 * i + 1] = qi[i]; }
+    d.gamX = reinterpret_cast<const double2*>(up(g, 2 * N));
+    d.gamXs = reinterpret_cast<const double2*>(up(s, 2 * N));
+  }
+  {
+    std::vector<double> cs(size_t(N) * std::max(K, 1), 0.0), gm(size_t(N) * std::max(K, 1), 0.0);
+    for (int j = 0; j < K; ++j) {
+      std::vector<double> pc = permute(m.Csq_ref[j], N, C, M);
+      std::copy(pc.begin(), pc.end(), cs.begin() + size_t(j) * N);
+      std::copy(m.gam_ref[j].begin(), m.gam_ref[j].end(), gm.begin() + size_t(j) * N);
+    }
+    d.Csq = up(cs, cs.size());
+    d.gam = up(gm, gm.size());
+  }
+  d.dcoef = up(m.dampcoef, N);
+  d.dchar = up(m.dampchar, N);
+  d.chi = up(m.ChiAdj, N);
+  d.depth = up(m.depth, N);
+  const size_t ns = size_t(std::max(n, 2));
+  d.tt = up(m.ttrace, ns);
+  d.ins = up(m.insig, ns);
+  d.insc = up(m.sp_c_in.empty() ? std::vector<double>(ns, 0.0) : m.sp_c_in, ns);
+  d.skw = up(m.insig_skew, ns);
+  d.skwc = up(m.sp_c_skew.empty() ? std::vector<double>(ns, 0.0) : m.sp_c_skew, ns);
+  double2* twp = nullptr;
+  for (auto& e : tw)
+    if (e.first == N) twp = e.second;
+  if (!twp) {
+    std::vector<double2> t(N);
+    for (int q = 0; q < N; ++q) {
+      // exp(-2 pi i q / N), argument reduced to the first octant for accuracy
+      const double a = 2.0 * M_PI * double(q) / double(N);
+      t[q] = make_double2(std::cos(a), -std::sin(a));
+    }
+    HW_CUDA(cudaMalloc(&twp, sizeof(double2) * N));
+    HW_CUDA(cudaMemcpy(twp, t.data(), sizeof(double2) * N, cudaMemcpyHostToDevice));
+    tw.emplace_back(N, twp);
+  }
+  d.tw = twp;
+  d.KBC = m.KBC; d.TC = m.TC; d.Tstar = m.Tstar; d.MaxEtaInit = m.MaxEtaInit; d.dt_in = m.dt;
+  d.xbstart = m.xbstart; d.xbend = m.xbend; d.xbendL = m.xbendL; d.xbstartR = m.xbstartR;
+  d.lenIF = m.lenIF; d.ILL = m.ILL; d.IFF = m.IFF;
+  d.y = a.take<double2>(2 * N);
+  d.ynew = a.take<double2>(2 * N);
+  for (int i = 0; i < 7; ++i) d.kb[i] = a.take<double2>(2 * N);
+  d.zs = a.take<double2>(2 * N);
+  for (int i = 0; i < kScratch; ++i) d.sc[i] = a.take<double2>(N);
+  // breaking state
+  BrkDev bk{};
+  bk.cap = cap;
+  BrkDev* dbk = a.take<BrkDev>(1);
+  bk.cb = a.take<Crest>(cap);
+  bk.cbn = a.take<Crest>(cap);
+  bk.cbp = a.take<Crest>(cap);
+  bk.id_node_end = a.take<int>(cap);
+  bk.nodes = a.take<int>(N);
+  bk.touched = a.take<int>(N);
+  bk.pk = a.take<int>(N);
+  bk.B = a.take<double>(N);
+  bk.log = a.take<double>(size_t(log_cap));
+  bk.log_cap = log_cap;
+  HW_CUDA(cudaMemcpy(dbk, &bk, sizeof bk, cudaMemcpyHostToDevice));
+  d.bk = dbk;
+  if (a.used > a.cap) { err = "internal: arena overflow"; return false; }
+  // initial state
+  d.t = m.ttrace[0];
+  d.h = m.h0;
+  h.t0 = d.t;
+  h.h0 = d.h;
+  d.i_out = 0;
+  d.i_stop = 0;
+  d.status = kOk;
+  d.exact = m.breaking ? 1 : 0;
+  double* tmp = nullptr;
+  HW_CUDA(cudaMalloc(&tmp, sizeof(double) * 4 * N));
+  HW_CUDA(cudaMemcpy(tmp, m.y0.data(), sizeof(double) * 4 * N, cudaMemcpyHostToDevice));
+  k_to_internal<<<(N + 255) / 256, 256>>>(tmp, d.y, N, h.logC, M);
+  HW_CUDA(cudaGetLastError());
+  HW_CUDA(cudaDeviceSynchronize());
+  cudaFree(tmp);
+  return true;
+}
+
+bool hw_ctx::init(const std::vector<std::string>& dirs, const hw_opts* o) {
+  hw_opts opt{};
+  if (o) opt = *o;
+  device = opt.device;
+  HW_CUDA(cudaSetDevice(device));
+  int ndev = 0;
+  HW_CUDA(cudaGetDeviceCount(&ndev));
+  for (cudaError_t e : {hw_attr_256(), hw_attr_512(), hw_attr_1024(), hw_attr_2048()})
+    if (e != cudaSuccess) { err = std::string("kernel attributes: ") + cudaGetErrorString(e); return false; }
+  hw::SetupOptions so;
+  so.eps_abs = opt.eps_abs;
+  so.eps_rel = opt.eps_rel;
+  so.h0 = opt.h0;
+  so.seed = opt.seed;
+  so.nref = opt.nref;
+  mem.resize(dirs.size());
+  for (size_t i = 0; i < dirs.size(); ++i) {
+    HostMember& h = mem[i];
+    if (!hw::build_member(dirs[i], so, h.m, err)) {
+      err = dirs[i] + ": " + err;
+      return false;
+    }
+    const int N = h.m.Nx;
+    if (N < 256 || (N & (N - 1)) != 0 || N > 32768) {
+      err = dirs[i] + ": the device engine needs a power-of-two grid with 256 <= Nx <= 32768 (Nx=" +
+            std::to_string(N) + ")";
+      return false;
+    }
+    if (h.m.breaking && h.m.prop_mode == 2) {
+      err = dirs[i] + ": bidirectional breaking windows are not supported on the device";
+      return false;
+    }
+    h.N = N;
+    int C = opt.cluster > 0 ? opt.cluster : std::max(1, N / 2048);
+    if ((C & (C - 1)) != 0 || N / C < 256 || N / C > 2048 || C > 16) {
+      err = "invalid cluster size " + std::to_string(C) + " for Nx=" + std::to_string(N);
+      return false;
+    }
+    h.C = C;
+    h.M = N / C;
+    h.logC = 0;
+    while ((1 << h.logC) < C) ++h.logC;
+    maxN = std::max(maxN, N);
+    if (!upload_member(h)) return false;
+    if (opt.exact_sequence) h.d.exact = 1;
+  }
+  HW_CUDA(cudaMalloc(&d_mems, sizeof(DevMember) * mem.size()));
+  for (size_t i = 0; i < mem.size(); ++i)
+    HW_CUDA(cudaMemcpy(d_mems + i, &mem[i].d, sizeof(DevMember), cudaMemcpyHostToDevice));
+  HW_CUDA(cudaMalloc(&d_single, sizeof(int) * mem.size()));
+  std::vector<int> ids(mem.size());
+  for (size_t i = 0; i < mem.size(); ++i) ids[i] = int(i);
+  HW_CUDA(cudaMemcpy(d_single, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice));
+  HW_CUDA(cudaMalloc(&d_ref, sizeof(double) * 4 * maxN));
+  HW_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
+  stream = own_stream;
+  HW_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+  // group members by (M, C); heavier members first inside each class
+  for (size_t i = 0; i < mem.size(); ++i) {
+    Class* cls = nullptr;
+    for (auto& c : classes)
+      if (c.M == mem[i].M && c.C == mem[i].C) cls = &c;
+    if (!cls) {
+      classes.push_back(Class{mem[i].M, mem[i].C, {}, nullptr, nullptr, nullptr});
+      cls = &classes.back();
+    }
+    cls->members.push_back(int(i));
+  }
+  for (auto& c : classes) {
+    HW_CUDA(cudaMalloc(&c.d_list, sizeof(int) * c.members.size()));
+    HW_CUDA(cudaMemcpy(c.d_list, c.members.data(), sizeof(int) * c.members.size(), cudaMemcpyHostToDevice));
+    HW_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    HW_CUDA(cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming));
+  }
+  return true;
+}
+
+bool hw_ctx::launch_member(int mi, int mode, double t_rhs) {
+  const HostMember& h = mem[size_t(mi)];
+  cudaError_t e = launch_any(h.M, mode, d_mems, d_single + mi, 1, h.C, t_rhs, stream);
+  if (e != cudaSuccess) { err = std::string("launch: ") + cudaGetErrorString(e); return false; }
+  return true;
+}
+
+bool hw_ctx::run(int i_stop_all, double t_end, bool by_time) {
+  // set stop indices on the device descriptors
+  for (size_t i = 0; i < mem.size(); ++i) {
+    const hw::Member& m = mem[i].m;
+    int stop = m.n;
+    if (by_time) {
+      stop = 0;
+      while (stop < m.n && m.ttrace[size_t(stop)] <= t_end) ++stop;
+    } else if (i_stop_all >= 0) {
+      stop = std::min(i_stop_all, m.n);
+    }
+    HW_CUDA(cudaMemcpyAsync(&d_mems[i].i_stop, &stop, sizeof(int), cudaMemcpyHostToDevice, stream));
+  }
+  HW_CUDA(cudaEventRecord(fork, stream));
+  for (auto& c : classes) {
+    HW_CUDA(cudaStreamWaitEvent(c.stream, fork, 0));
+    cudaError_t e = launch_any(c.M, 0, d_mems, c.d_list, int(c.members.size()), c.C, 0.0, c.stream);
+    if (e != cudaSuccess) { err = std::string("launch: ") + cudaGetErrorString(e); return false; }
+    HW_CUDA(cudaEventRecord(c.done, c.stream));
+    HW_CUDA(cudaStreamWaitEvent(stream, c.done, 0));
+  }
+  return true;
+}
+
+bool hw_ctx::sync_desc() {
+  HW_CUDA(cudaStreamSynchronize(stream));
+  for (size_t i = 0; i < mem.size(); ++i)
+    HW_CUDA(cudaMemcpy(&mem[i].d, d_mems + i, sizeof(DevMember), cudaMemcpyDeviceToHost));
+  return true;
+}
+
+bool hw_ctx::reset() {
+  HW_CUDA(cudaStreamSynchronize(stream));
+  for (size_t i = 0; i < mem.size(); ++i) {
+    HostMember& h = mem[i];
+    HW_CUDA(cudaMemcpy(&h.d, d_mems + i, sizeof(DevMember), cudaMemcpyDeviceToHost));
+    h.d.t = h.t0;
+    h.d.h = h.h0;
+    h.d.i_out = 0;
+    h.d.status = kOk;
+    h.d.k1_valid = 0;
+    h.d.rhs_calls = h.d.accepted = h.d.rejected = 0;
+    HW_CUDA(cudaMemcpy(d_ref, h.m.y0.data(), sizeof(double) * 4 * h.N, cudaMemcpyHostToDevice));
+    k_to_internal<<<(h.N + 255) / 256, 256, 0, stream>>>(d_ref, h.d.y, h.N, h.logC, h.M);
+    HW_CUDA(cudaGetLastError());
+    // breaking state
+    BrkDev bk;
+    HW_CUDA(cudaMemcpy(&bk, h.d.bk, sizeof bk, cudaMemcpyDeviceToHost));
+    bk.flag = bk.ITERbdt = bk.ITERbn = bk.n_touched = bk.npk = bk.any_above = 0;
+    bk.log_len = 0;
+    HW_CUDA(cudaMemset(bk.cb, 0, sizeof(Crest) * bk.cap));
+    HW_CUDA(cudaMemset(bk.cbn, 0, sizeof(Crest) * bk.cap));
+    HW_CUDA(cudaMemset(bk.cbp, 0, sizeof(Crest) * bk.cap));
+    HW_CUDA(cudaMemset(bk.id_node_end, 0, sizeof(int) * bk.cap));
+    HW_CUDA(cudaMemset(bk.B, 0, sizeof(double) * h.N));
+    HW_CUDA(cudaMemcpy(h.d.bk, &bk, sizeof bk, cudaMemcpyHostToDevice));
+    HW_CUDA(cudaMemcpy(d_mems + i, &h.d, sizeof(DevMember), cudaMemcpyHostToDevice));
+  }
+  HW_CUDA(cudaStreamSynchronize(stream));
+  return true;
+}
+
+hw_ctx::~hw_ctx() {
+  if (stream) cudaStreamSynchronize(stream);
+  for (auto& h : mem)
+    if (h.dev) cudaFree(h.dev);
+  for (auto& e : tw) cudaFree(e.second);
+  for (auto& c : classes) {
+    if (c.d_list) cudaFree(c.d_list);
+    if (c.stream) cudaStreamDestroy(c.stream);
+    if (c.done) cudaEventDestroy(c.done);
+  }
+  if (d_mems) cudaFree(d_mems);
+  if (d_single) cudaFree(d_single);
+  if (d_ref) cudaFree(d_ref);
+  if (fork) cudaEventDestroy(fork);
+  if (own_stream) cudaStreamDestroy(own_stream);
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+namespace {
+bool valid_member(hw_ctx* c, int m) {
+  if (!c) return false;
+  if (m < 0 || m >= int(c->mem.size())) {
+    c->err = "member index out of range";
+    return false;
+  }
+  return true;
+}
+}  // namespace
+
+extern "C" {
+
+hw_ctx* hw_create(const char* workdir, const hw_opts* opts) {
+  if (!workdir) { g_create_err = "workdir is NULL"; return nullptr; }
+  return hw_ensemble_create(&workdir, 1, opts);
+}
+
+hw_ctx* hw_ensemble_create(const char* const* workdirs, int n, const hw_opts* opts) {
+  if (!workdirs || n <= 0) { g_create_err = "no member decks given"; return nullptr; }
+  std::unique_ptr<hw_ctx> c(new hw_ctx());
+  std::vector<std::string> dirs;
+  for (int i = 0; i < n; ++i) dirs.emplace_back(workdirs[i] ? workdirs[i] : "");
+  if (!c->init(dirs, opts)) {
+    g_create_err = c->err;
+    return nullptr;
+  }
+  return c.release();
+}
+
+void hw_destroy(hw_ctx* ctx) { delete ctx; }
+
+const char* hw_last_error(const hw_ctx* ctx) { return ctx ? ctx->err.c_str() : g_create_err.c_str(); }
+
+int hw_members(const hw_ctx* ctx) { return ctx ? int(ctx->mem.size()) : 0; }
+
+int hw_nx(const hw_ctx* ctx, int m) {
+  if (!ctx || m < 0 || m >= int(ctx->mem.size())) return -1;
+  return ctx->mem[size_t(m)].N;
+}
+
+int hw_nt(const hw_ctx* ctx, int m) {
+  if (!ctx || m < 0 || m >= int(ctx->mem.size())) return -1;
+  return ctx->mem[size_t(m)].m.n;
+}
+
+int hw_initial_state(hw_ctx* ctx, int m, double* y) {
+  if (!valid_member(ctx, m) || !y) return 1;
+  const auto& v = ctx->mem[size_t(m)].m.y0;
+  std::memcpy(y, v.data(), sizeof(double) * v.size());
+  return 0;
+}
+
+int hw_rhs(hw_ctx* ctx, int m, double t, const double* y, double* dydt) {
+  if (!valid_member(ctx, m) || !y || !dydt) return 1;
+  std::string& err = ctx->err;
+  auto body = [&]() -> bool {
+    HostMember& h = ctx->mem[size_t(m)];
+    const int N = h.N;
+    HW_CUDA(cudaMemcpyAsync(ctx->d_ref, y, sizeof(double) * 4 * N, cudaMemcpyHostToDevice, ctx->stream));
+    k_to_internal<<<(N + 255) / 256, 256, 0, ctx->stream>>>(ctx->d_ref, h.d.zs, N, h.logC, h.M);
+    HW_CUDA(cudaGetLastError());
+    if (!ctx->launch_member(m, 2, t)) return false;
+    DevMember cur;
+    HW_CUDA(cudaMemcpyAsync(&cur, ctx->d_mems + m, sizeof cur, cudaMemcpyDeviceToHost, ctx->stream));
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    k_to_reference<<<(N + 255) / 256, 256, 0, ctx->stream>>>(cur.kb[6], ctx->d_ref, N, h.logC, h.M);
+    HW_CUDA(cudaGetLastError());
+    HW_CUDA(cudaMemcpyAsync(dydt, ctx->d_ref, sizeof(double) * 4 * N, cudaMemcpyDeviceToHost, ctx->stream));
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    return true;
+  };
+  return body() ? 0 : 1;
+}
+
+int hw_gsl_rhs(double t, const double* y, double* dydt, void* params) {
+  return hw_rhs(static_cast<hw_ctx*>(params), 0, t, y, dydt);
+}
+
+int hw_set_state(hw_ctx* ctx, int m, double t, double h, const double* y, int i_out) {
+  if (!valid_member(ctx, m)) return 1;
+  std::string& err = ctx->err;
+  auto body = [&]() -> bool {
+    HostMember& hm = ctx->mem[size_t(m)];
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    HW_CUDA(cudaMemcpy(&hm.d, ctx->d_mems + m, sizeof(DevMember), cudaMemcpyDeviceToHost));
+    if (y) {
+      HW_CUDA(cudaMemcpyAsync(ctx->d_ref, y, sizeof(double) * 4 * hm.N, cudaMemcpyHostToDevice, ctx->stream));
+      k_to_internal<<<(hm.N + 255) / 256, 256, 0, ctx->stream>>>(ctx->d_ref, hm.d.y, hm.N, hm.logC, hm.M);
+      HW_CUDA(cudaGetLastError());
+    }
+    hm.d.t = t;
+    hm.d.h = h;
+    hm.d.i_out = i_out;
+    hm.d.k1_valid = 0;
+    hm.d.status = kOk;
+    HW_CUDA(cudaMemcpyAsync(ctx->d_mems + m, &hm.d, sizeof(DevMember), cudaMemcpyHostToDevice, ctx->stream));
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    return true;
+  };
+  return body() ? 0 : 1;
+}
+
+int hw_evolve_apply(hw_ctx* ctx, int m, double* t, double t1, double* h, double* y) {
+  if (!valid_member(ctx, m) || !t || !h || !y) return 1;
+  std::string& err = ctx->err;
+  auto body = [&]() -> bool {
+    HostMember& hm = ctx->mem[size_t(m)];
+    const int N = hm.N;
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    HW_CUDA(cudaMemcpy(&hm.d, ctx->d_mems + m, sizeof(DevMember), cudaMemcpyDeviceToHost));
+    HW_CUDA(cudaMemcpyAsync(ctx->d_ref, y, sizeof(double) * 4 * N, cudaMemcpyHostToDevice, ctx->stream));
+    k_to_internal<<<(N + 255) / 256, 256, 0, ctx->stream>>>(ctx->d_ref, hm.d.y, N, hm.logC, hm.M);
+    HW_CUDA(cudaGetLastError());
+    hm.d.t = *t;
+    hm.d.h = *h;
+    hm.d.t1 = t1;
+    hm.d.k1_valid = 0;
+    hm.d.status = kOk;
+    HW_CUDA(cudaMemcpyAsync(ctx->d_mems + m, &hm.d, sizeof(DevMember), cudaMemcpyHostToDevice, ctx->stream));
+    if (!ctx->launch_member(m, 1, 0.0)) return false;
+    HW_CUDA(cudaMemcpyAsync(&hm.d, ctx->d_mems + m, sizeof(DevMember), cudaMemcpyDeviceToHost, ctx->stream));
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    k_to_reference<<<(N + 255) / 256, 256, 0, ctx->stream>>>(hm.d.y, ctx->d_ref, N, hm.logC, hm.M);
+    HW_CUDA(cudaGetLastError());
+    HW_CUDA(cudaMemcpyAsync(y, ctx->d_ref, sizeof(double) * 4 * N, cudaMemcpyDeviceToHost, ctx->stream));
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    *t = hm.d.t;
+    *h = hm.d.h;
+    return true;
+  };
+  if (!body()) return 1;
+  const int st = ctx->mem[size_t(m)].d.status;
+  if (st != kOk) {
+    ctx->err = "time integration failed (status " + std::to_string(st) + ")";
+    return 100 + st;
+  }
+  return 0;
+}
+
+int hw_run(hw_ctx* ctx, int i_stop) {
+  if (!ctx) return 1;
+  return ctx->run(i_stop, 0.0, false) ? 0 : 1;
+}
+
+int hw_run_to_time(hw_ctx* ctx, double t_end) {
+  if (!ctx) return 1;
+  return ctx->run(-1, t_end, true) ? 0 : 1;
+}
+
+int hw_get_state(hw_ctx* ctx, int m, double* t, double* h, double* y) {
+  if (!valid_member(ctx, m)) return 1;
+  std::string& err = ctx->err;
+  auto body = [&]() -> bool {
+    HostMember& hm = ctx->mem[size_t(m)];
+    HW_CUDA(cudaMemcpyAsync(&hm.d, ctx->d_mems + m, sizeof(DevMember), cudaMemcpyDeviceToHost, ctx->stream));
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (t) *t = hm.d.t;
+    if (h) *h = hm.d.h;
+    if (y) {
+      k_to_reference<<<(hm.N + 255) / 256, 256, 0, ctx->stream>>>(hm.d.y, ctx->d_ref, hm.N, hm.logC, hm.M);
+      HW_CUDA(cudaGetLastError());
+      HW_CUDA(cudaMemcpyAsync(y, ctx->d_ref, sizeof(double) * 4 * hm.N, cudaMemcpyDeviceToHost, ctx->stream));
+      HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    return true;
+  };
+  return body() ? 0 : 1;
+}
+
+int hw_reset(hw_ctx* ctx) { return ctx && ctx->reset() ? 0 : 1; }
+
+int hw_member_stats(hw_ctx* ctx, int m, long long* rhs, long long* acc, long long* rej, int* status) {
+  if (!valid_member(ctx, m)) return 1;
+  std::string& err = ctx->err;
+  auto body = [&]() -> bool {
+    HostMember& hm = ctx->mem[size_t(m)];
+    HW_CUDA(cudaMemcpyAsync(&hm.d, ctx->d_mems + m, sizeof(DevMember), cudaMemcpyDeviceToHost, ctx->stream));
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (rhs) *rhs = hm.d.rhs_calls;
+    if (acc) *acc = hm.d.accepted;
+    if (rej) *rej = hm.d.rejected;
+    if (status) *status = hm.d.status;
+    return true;
+  };
+  return body() ? 0 : 1;
+}
+
+int hw_last_dydt(hw_ctx* ctx, int m, double* dydt) {
+  if (!valid_member(ctx, m) || !dydt) return 1;
+  std::string& err = ctx->err;
+  auto body = [&]() -> bool {
+    HostMember& hm = ctx->mem[size_t(m)];
+    HW_CUDA(cudaMemcpyAsync(&hm.d, ctx->d_mems + m, sizeof(DevMember), cudaMemcpyDeviceToHost, ctx->stream));
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    // the last evaluation is kout in the exact sequence, k1 after a reuse in the pure one
+    const double2* src = hm.d.k1_valid ? hm.d.kb[0] : hm.d.kb[6];
+    k_to_reference<<<(hm.N + 255) / 256, 256, 0, ctx->stream>>>(src, ctx->d_ref, hm.N, hm.logC, hm.M);
+    HW_CUDA(cudaGetLastError());
+    HW_CUDA(cudaMemcpyAsync(dydt, ctx->d_ref, sizeof(double) * 4 * hm.N, cudaMemcpyDeviceToHost, ctx->stream));
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    return true;
+  };
+  return body() ? 0 : 1;
+}
+
+int hw_breaking_log(hw_ctx* ctx, int m, double* out, long long cap, long long* len) {
+  if (!valid_member(ctx, m)) return -1;
+  std::string& err = ctx->err;
+  long long recs = 0;
+  auto body = [&]() -> bool {
+    HostMember& hm = ctx->mem[size_t(m)];
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    BrkDev bk;
+    HW_CUDA(cudaMemcpy(&bk, hm.d.bk, sizeof bk, cudaMemcpyDeviceToHost));
+    const long long n = std::min(bk.log_len, cap);
+    if (len) *len = bk.log_len;
+    if (out && n > 0) HW_CUDA(cudaMemcpy(out, bk.log, sizeof(double) * size_t(n), cudaMemcpyDeviceToHost));
+    recs = bk.ITERbn;
+    return true;
+  };
+  return body() ? int(recs) : -1;
+}
+
+int hw_deck_table(const char* workdir, const hw_opts* opts, const char* name, double* out, int cap) {
+  if (!workdir || !name) { g_create_err = "NULL argument"; return -1; }
+  hw_opts o{};
+  if (opts) o = *opts;
+  hw::SetupOptions so;
+  so.eps_abs = o.eps_abs; so.eps_rel = o.eps_rel; so.h0 = o.h0; so.seed = o.seed; so.nref = o.nref;
+  hw::Member m;
+  if (!hw::build_member(workdir, so, m, g_create_err)) return -1;
+  const std::string nm(name);
+  std::vector<double> v;
+  if (nm == "x") v = m.x; else if (nm == "k") v = m.k; else if (nm == "depth") v = m.depth;
+  else if (nm == "dampchar") v = m.dampchar; else if (nm == "dampcoef") v = m.dampcoef;
+  else if (nm == "aal") v = m.aal; else if (nm == "ChiAdj") v = m.ChiAdj; else if (nm == "Csqr") v = m.Csqr;
+  else if (nm == "L") v = m.L; else if (nm == "M0im") v = m.M0im; else if (nm == "insig") v = m.insig;
+  else if (nm == "insig_skew") v = m.insig_skew; else if (nm == "ttrace") v = m.ttrace; else if (nm == "y0") v = m.y0;
+  else if (nm == "gamX") { v = m.gamX_re; v.insert(v.end(), m.gamX_im.begin(), m.gamX_im.end()); }
+  else if (nm == "gamX_skew") { v = m.gamXs_re; v.insert(v.end(), m.gamXs_im.begin(), m.gamXs_im.end()); }
+  else if (nm.rfind("gam_", 0) == 0 || nm.rfind("Csq_", 0) == 0) {
+    // gam_min / gam_plus / gam_mid and Csq_* in the reference's naming (ref order min, plus, mid)
+    const int j = nm.find("min") != std::string::npos ? 0 : nm.find("plus") != std::string::npos ? 1 : 2;
+    const auto& src = nm[0] == 'g' ? m.gam_ref : m.Csq_ref;
+    if (j < int(src.size())) v = src[size_t(j)];
+  } else {
+    const double s = nm == "Nx" ? m.Nx : nm == "n" ? m.n : nm == "dx" ? m.dx : nm == "dt" ? m.dt
+                   : nm == "nu_peak" ? m.nu_peak : nm == "kp" ? m.kp : nm == "lambda_p" ? m.lambda_p
+                   : nm == "Hs_in" ? m.Hs_in : nm == "MaxEtaInit" ? m.MaxEtaInit : nm == "depthinf" ? m.depthinf
+                   : nm == "Tstar" ? m.Tstar : nm == "xbstart" ? m.xbstart : nm == "xbend" ? m.xbend
+                   : nm == "cutfracwn" ? m.cutfracwn : nm == "Tp_peak" ? m.Tp_peak : std::nan("");
+    if (std::isnan(s)) { g_create_err = "unknown table " + nm; return -1; }
+    v.assign(1, s);
+  }
+  const int n = std::min(cap, int(v.size()));
+  if (out) std::memcpy(out, v.data(), sizeof(double) * size_t(n));
+  return int(v.size());
+}
+
+int hw_set_stream(hw_ctx* ctx, void* s) {
+  if (!ctx) return 1;
+  ctx->stream = s ? static_cast<cudaStream_t>(s) : ctx->own_stream;
+  return 0;
+}
+
+int hw_synchronize(hw_ctx* ctx) {
+  if (!ctx) return 1;
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    ctx->err = cudaGetErrorString(e);
+    return 1;
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,111 @@
+// hw_kernels.cuh -- the persistent evolve kernel and the single-RHS kernel of one
+// slice size M (instantiated once per M in hw_inst_<M>.cu).
+#pragma once
+
+#include "hw_breaking.cuh"
+#include "hw_kernels.h"
+#include "hw_stepper.cuh"
+
+namespace hwdev {
+
+template <int M>
+__global__ void __launch_bounds__(M / kPts) k_evolve(DevMember* mems, const int* list, int mode) {
+  extern __shared__ double2 smem_buf[];
+  __shared__ DevMember sd;
+  __shared__ double red[48];
+  cg::cluster_group cl = cg::this_cluster();
+  const int C = int(cl.num_blocks());
+  const int rank = int(cl.block_rank());
+  const int mi = list[blockIdx.x / C];
+  if (threadIdx.x == 0) sd = mems[mi];
+  __syncthreads();
+  Ctx<M> X{sd, smem_buf, red, rank, int(threadIdx.x)};
+  Bufs B;
+  B.y = sd.y;
+  B.yn = sd.ynew;
+  for (int i = 0; i < 7; ++i) B.k[i] = sd.kb[i];
+  StepState S{sd.t, sd.h, sd.status, sd.k1_valid, 0, 0, 0};
+  int iout = sd.i_out;
+  if (S.status == kOk) {
+    if (mode == 1) {
+      evolve_apply<M>(X, B, S, sd.t1);
+    } else {
+      while (iout < sd.i_stop && S.status == kOk) {
+        const double ti = sd.tt[iout];
+        while (S.t < ti && S.status == kOk) evolve_apply<M>(X, B, S, ti);
+        if (S.status == kOk) ++iout;
+      }
+    }
+  }
+  member_sync(C);
+  if (rank == 0 && threadIdx.x == 0) {
+    DevMember& g = mems[mi];
+    g.t = S.t;
+    g.h = S.h;
+    g.status = S.status;
+    g.k1_valid = S.k1_valid;
+    g.i_out = iout;
+    g.rhs_calls += S.rhs;
+    g.accepted += S.acc;
+    g.rejected += S.rej;
+    g.y = B.y;
+    g.ynew = B.yn;
+    for (int i = 0; i < 7; ++i) g.kb[i] = B.k[i];
+  }
+}
+
+// single RHS evaluation of member mi: kout = f(t, zs)
+template <int M>
+__global__ void __launch_bounds__(M / kPts) k_rhs(DevMember* mems, const int* list, double t) {
+  extern __shared__ double2 smem_buf[];
+  __shared__ DevMember sd;
+  __shared__ double red[48];
+  cg::cluster_group cl = cg::this_cluster();
+  const int C = int(cl.num_blocks());
+  const int rank = int(cl.block_rank());
+  const int mi = list[blockIdx.x / C];
+  if (threadIdx.x == 0) sd = mems[mi];
+  __syncthreads();
+  Ctx<M> X{sd, smem_buf, red, rank, int(threadIdx.x)};
+  rhs_eval<M>(X, t, sd.kb[6]);
+  member_sync(C);
+  if (rank == 0 && threadIdx.x == 0) mems[mi].rhs_calls += 1;
+}
+
+
+template <int M>
+cudaError_t set_attrs() {
+  const int bytes = padded(M) * int(sizeof(double2));
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(k_evolve<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_rhs<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_evolve<M>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_rhs<M>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+}
+
+template <int M>
+cudaError_t launch(int mode, DevMember* mems, const int* list, int nmem, int C, double t, cudaStream_t s) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(unsigned(nmem * C));
+  cfg.blockDim = dim3(M / kPts);
+  cfg.dynamicSmemBytes = size_t(padded(M)) * sizeof(double2);
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = unsigned(C);
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  if (mode == 2) return cudaLaunchKernelEx(&cfg, k_rhs<M>, mems, list, t);
+  return cudaLaunchKernelEx(&cfg, k_evolve<M>, mems, list, mode);
+}
+
+}  // namespace hwdev
+
+#define HW_INSTANTIATE(MM)                                                                          \
+  cudaError_t hw_attr_##MM() { return hwdev::set_attrs<MM>(); }                                    \
+  cudaError_t hw_launch_##MM(int mode, hwdev::DevMember* mems, const int* list, int nmem, int C,  \
+                             double t, cudaStream_t s) {                                            \
+    return hwdev::launch<MM>(mode, mems, list, nmem, C, t, s);                                      \
+  }

@@ -1,0 +1,218 @@
+"""ctypes binding of the C ABI in include/hawassi_b200.h."""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "lib", "libhawassi_b200.so")
+_lib = None
+
+
+class EngineError(RuntimeError):
+    pass
+
+
+class HwOpts(ctypes.Structure):
+    _fields_ = [
+        ("eps_abs", ctypes.c_double),
+        ("eps_rel", ctypes.c_double),
+        ("h0", ctypes.c_double),
+        ("seed", ctypes.c_ulonglong),
+        ("nref", ctypes.c_int),
+        ("exact_sequence", ctypes.c_int),
+        ("cluster", ctypes.c_int),
+        ("device", ctypes.c_int),
+    ]
+
+
+def library_path():
+    return _LIB_PATH
+
+
+EXPORTS = [
+    "hw_create", "hw_ensemble_create", "hw_destroy", "hw_last_error", "hw_members", "hw_nx", "hw_nt",
+    "hw_initial_state", "hw_rhs", "hw_gsl_rhs", "hw_evolve_apply", "hw_run", "hw_run_to_time",
+    "hw_get_state", "hw_set_state", "hw_reset", "hw_member_stats", "hw_last_dydt", "hw_breaking_log",
+    "hw_set_stream", "hw_synchronize", "hw_deck_table",
+]
+
+
+def load_library():
+    """Load the CUDA engine; raises EngineError if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        raise EngineError(f"CUDA engine not built: {_LIB_PATH} is missing (python -m hawassi_c_b200.build)")
+    L = ctypes.CDLL(_LIB_PATH)
+    vp, dp, ip, dd = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_double
+    llp = ctypes.POINTER(ctypes.c_longlong)
+    L.hw_create.restype = vp
+    L.hw_create.argtypes = [ctypes.c_char_p, ctypes.POINTER(HwOpts)]
+    L.hw_ensemble_create.restype = vp
+    L.hw_ensemble_create.argtypes = [ctypes.POINTER(ctypes.c_char_p), ip, ctypes.POINTER(HwOpts)]
+    L.hw_destroy.argtypes = [vp]
+    L.hw_last_error.restype = ctypes.c_char_p
+    L.hw_last_error.argtypes = [vp]
+    L.hw_members.argtypes = [vp]
+    L.hw_nx.argtypes = [vp, ip]
+    L.hw_nt.argtypes = [vp, ip]
+    L.hw_initial_state.argtypes = [vp, ip, dp]
+    L.hw_rhs.argtypes = [vp, ip, dd, dp, dp]
+    L.hw_gsl_rhs.argtypes = [dd, dp, dp, vp]
+    L.hw_evolve_apply.argtypes = [vp, ip, dp, dd, dp, dp]
+    L.hw_run.argtypes = [vp, ip]
+    L.hw_run_to_time.argtypes = [vp, dd]
+    L.hw_get_state.argtypes = [vp, ip, dp, dp, dp]
+    L.hw_set_state.argtypes = [vp, ip, dd, dd, dp, ip]
+    L.hw_reset.argtypes = [vp]
+    L.hw_member_stats.argtypes = [vp, ip, llp, llp, llp, ctypes.POINTER(ctypes.c_int)]
+    L.hw_last_dydt.argtypes = [vp, ip, dp]
+    L.hw_breaking_log.argtypes = [vp, ip, dp, ctypes.c_longlong, llp]
+    L.hw_set_stream.argtypes = [vp, vp]
+    L.hw_synchronize.argtypes = [vp]
+    L.hw_deck_table.argtypes = [ctypes.c_char_p, ctypes.POINTER(HwOpts), ctypes.c_char_p, dp, ip]
+    _lib = L
+    return L
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Engine:
+    """One deck directory (``Engine("deck")``) or a ragged ensemble
+    (``Engine(["deck0", "deck1", ...])``) on one GPU."""
+
+    def __init__(self, decks, eps_abs=0.0, eps_rel=0.0, h0=0.0, seed=0, nref=0, exact_sequence=False,
+                 cluster=0, device=0):
+        L = load_library()
+        if isinstance(decks, (str, os.PathLike)):
+            decks = [decks]
+        self.decks = [os.fspath(d) for d in decks]
+        opts = HwOpts(eps_abs, eps_rel, h0, seed, nref, int(bool(exact_sequence)), cluster, device)
+        arr = (ctypes.c_char_p * len(self.decks))(*[d.encode() for d in self.decks])
+        self._h = L.hw_ensemble_create(arr, len(self.decks), ctypes.byref(opts))
+        if not self._h:
+            raise EngineError(L.hw_last_error(None).decode())
+        self.members = L.hw_members(self._h)
+        self.nx = [L.hw_nx(self._h, i) for i in range(self.members)]
+        self.nt = [L.hw_nt(self._h, i) for i in range(self.members)]
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().hw_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise EngineError(f"{what}: " + load_library().hw_last_error(self._h).decode())
+
+    # -- reference call surface ----------------------------------------------
+    def initial_state(self, member=0):
+        y = np.zeros(4 * self.nx[member])
+        self._check(load_library().hw_initial_state(self._h, member, _dp(y)), "initial_state")
+        return y
+
+    def rhs(self, t, y, member=0):
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        dz = np.empty_like(y)
+        self._check(load_library().hw_rhs(self._h, member, float(t), _dp(y), _dp(dz)), "rhs")
+        return dz
+
+    def evolve_apply(self, t, t1, h, y, member=0):
+        """In place on y; returns (t, h) like gsl_odeiv_evolve_apply's outputs."""
+        tt = np.array([t], dtype=np.float64)
+        hh = np.array([h], dtype=np.float64)
+        rc = load_library().hw_evolve_apply(self._h, member, _dp(tt), float(t1), _dp(hh), _dp(y))
+        self._check(rc, "evolve_apply")
+        return float(tt[0]), float(hh[0])
+
+    def run(self, i_stop=-1, sync=True):
+        self._check(load_library().hw_run(self._h, int(i_stop)), "run")
+        if sync:
+            self.synchronize()
+
+    def run_to_time(self, t_end, sync=True):
+        self._check(load_library().hw_run_to_time(self._h, float(t_end)), "run_to_time")
+        if sync:
+            self.synchronize()
+
+    def state(self, member=0):
+        y = np.zeros(4 * self.nx[member])
+        t = np.zeros(1)
+        h = np.zeros(1)
+        self._check(load_library().hw_get_state(self._h, member, _dp(t), _dp(h), _dp(y)), "get_state")
+        return float(t[0]), float(h[0]), y
+
+    def set_state(self, t, h, y, member=0, i_out=0):
+        y = np.ascontiguousarray(y, dtype=np.float64) if y is not None else None
+        rc = load_library().hw_set_state(self._h, member, float(t), float(h),
+                                         _dp(y) if y is not None else None, int(i_out))
+        self._check(rc, "set_state")
+
+    def reset(self):
+        self._check(load_library().hw_reset(self._h), "reset")
+
+    def stats(self, member=0):
+        a, b, c = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        s = ctypes.c_int()
+        self._check(load_library().hw_member_stats(self._h, member, ctypes.byref(a), ctypes.byref(b),
+                                                   ctypes.byref(c), ctypes.byref(s)), "stats")
+        return {"rhs_calls": a.value, "accepted": b.value, "rejected": c.value, "status": s.value}
+
+    def last_dydt(self, member=0):
+        y = np.zeros(4 * self.nx[member])
+        self._check(load_library().hw_last_dydt(self._h, member, _dp(y)), "last_dydt")
+        return y
+
+    def breaking_log(self, member=0):
+        """breaking.dat records [(t, [nodes...]), ...] of the member."""
+        L = load_library()
+        n = ctypes.c_longlong()
+        if L.hw_breaking_log(self._h, member, None, 0, ctypes.byref(n)) < 0:
+            raise EngineError(L.hw_last_error(self._h).decode())
+        buf = np.zeros(max(n.value, 1))
+        L.hw_breaking_log(self._h, member, _dp(buf), n.value, ctypes.byref(n))
+        out, i = [], 0
+        while i < n.value:
+            t, cnt = buf[i], int(buf[i + 1])
+            out.append((t, [int(v) for v in buf[i + 2:i + 2 + cnt]]))
+            i += 2 + cnt
+        return out
+
+    def set_stream(self, stream_ptr):
+        self._check(load_library().hw_set_stream(self._h, ctypes.c_void_p(stream_ptr)), "set_stream")
+
+    def synchronize(self):
+        self._check(load_library().hw_synchronize(self._h), "synchronize")
+
+
+def deck_table(deck, name, seed=0, nref=0):
+    """Host-side set-up table of a deck (no GPU involved)."""
+    L = load_library()
+    opts = HwOpts(0.0, 0.0, 0.0, seed, nref, 0, 0, 0)
+    n = L.hw_deck_table(os.fspath(deck).encode(), ctypes.byref(opts), name.encode(), None, 0)
+    if n < 0:
+        raise EngineError(L.hw_last_error(None).decode())
+    out = np.zeros(max(n, 1))
+    L.hw_deck_table(os.fspath(deck).encode(), ctypes.byref(opts), name.encode(), _dp(out), n)
+    return out[:n]

@@ -1,0 +1,100 @@
+/*
+ * hawassi_b200.h -- C ABI of the B200 engine for HAWASSI's 1D pseudo-spectral
+ * Hamiltonian RHS and its RKF45 time stepping.
+ *
+ * Plain C linkage, plain pointers and sizes.  State vectors use the
+ * reference's layout: 4*Nx doubles [Re eta^ | Im eta^ | Re u^ | Im u^] in FFTW
+ * order (1d/rhs.c:33-38).  All pointers passed in are HOST pointers; device
+ * memory is owned by the context.  Every call returns 0 on success (GSL_SUCCESS)
+ * and a nonzero code otherwise, with a message in hw_last_error().  A context
+ * is used by one host thread at a time (the reference's RHS is not re-entrant
+ * either).
+ */
+#ifndef HAWASSI_B200_H
+#define HAWASSI_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct hw_ctx hw_ctx;
+
+typedef struct hw_opts {
+    double eps_abs;          /* <= 0: the reference's 1e-5 (1d/functions.c:529) */
+    double eps_rel;          /* <= 0: the reference's 1e-4 (1d/functions.c:530) */
+    double h0;               /* <= 0: the reference's first step 1e-4 (1d/functions.c:541) */
+    unsigned long long seed; /* phase seed for wavename = jonswap (reference: srand(time(0))) */
+    int nref;                /* varying depth: 0 or 3 = three reference depths (Up3IP), 2 = Up2IP */
+    int exact_sequence;      /* 1: evaluate the RHS exactly where GSL does even when it is stateless */
+    int cluster;             /* CTAs per member, power of two (0 = automatic) */
+    int device;              /* CUDA device ordinal */
+} hw_opts;
+
+/* Replaces the reference's set-up (1d/main.cc:42-226): parse <workdir>/input.txt and
+ * the files it names, build the tables on the host, upload them. NULL on error. */
+hw_ctx* hw_create(const char* workdir, const hw_opts* opts);
+
+/* Batched ragged ensemble: one member per deck directory, uneven grid sizes allowed;
+ * all members advance together in one launch per grid-size class. */
+hw_ctx* hw_ensemble_create(const char* const* workdirs, int n_members, const hw_opts* opts);
+
+void        hw_destroy(hw_ctx* ctx);
+const char* hw_last_error(const hw_ctx* ctx);   /* ctx may be NULL (last create error) */
+int         hw_members(const hw_ctx* ctx);
+int         hw_nx(const hw_ctx* ctx, int member);
+int         hw_nt(const hw_ctx* ctx, int member); /* output/influx samples of the member */
+
+/* Initial spectral state of set_initial_ode (1d/functions.c:314). */
+int hw_initial_state(hw_ctx* ctx, int member, double* y);
+
+/* One RHS evaluation; replaces rhs_HsF1/2/3 (1d/rhs.c:1,96,243) including their side
+ * effects (breaking state machine, breaking log, the global dy copy). */
+int hw_rhs(hw_ctx* ctx, int member, double t, const double* y, double* dydt);
+
+/* gsl_odeiv_system.function-compatible entry point (member 0, params = hw_ctx*):
+ *   gsl_odeiv_system sys = {hw_gsl_rhs, NULL, 4 * Nx, ctx};   (1d/functions.c:71-89) */
+int hw_gsl_rhs(double t, const double* y, double* dydt, void* params);
+
+/* Replaces gsl_odeiv_evolve_apply(e, c, s, &sys, &t, t1, &h, y) with rkf45 and
+ * control_y (1d/functions.c:550): one accepted step, whole step on the device. */
+int hw_evolve_apply(hw_ctx* ctx, int member, double* t, double t1, double* h, double* y);
+
+/* The time loop of ode_solver_Ham (1d/functions.c:546-553) for every member at once:
+ * integrate through the member's output samples [i_out, i_stop), clipping steps at
+ * each sample time like the reference. i_stop < 0 means all samples. Asynchronous on
+ * the context's stream. */
+int hw_run(hw_ctx* ctx, int i_stop);
+/* Same, stopping at the last output sample whose time is <= t_end. */
+int hw_run_to_time(hw_ctx* ctx, double t_end);
+
+/* Current state of a member (synchronises the context's stream). */
+int hw_get_state(hw_ctx* ctx, int member, double* t, double* h, double* y);
+/* Overwrite the state of a member (t, h, y in the reference layout, output index i_out). */
+int hw_set_state(hw_ctx* ctx, int member, double t, double h, const double* y, int i_out);
+/* Back to t0, h0 and the initial state, breaking state and counters cleared. */
+int hw_reset(hw_ctx* ctx);
+
+/* Counters of a member: RHS evaluations, accepted / rejected steps, status (0 ok). */
+int hw_member_stats(hw_ctx* ctx, int member, long long* rhs_calls, long long* accepted,
+                    long long* rejected, int* status);
+/* The last RHS output (the reference's global dy, 1d/rhs.c:224-227), reference layout. */
+int hw_last_dydt(hw_ctx* ctx, int member, double* dydt);
+/* Breaking log records (t, node count, nodes...) as doubles; returns the record count
+ * written, *len receives the number of doubles. */
+int hw_breaking_log(hw_ctx* ctx, int member, double* out, long long cap, long long* len);
+
+/* Host-only (no GPU needed): build the set-up of <workdir> and copy the named table
+ * (x, k, depth, dampchar, dampcoef, aal, ChiAdj, Csqr, L, M0im, gamX, gamX_skew, insig,
+ * insig_skew, ttrace, y0, gam_min/plus/mid, Csq_min/plus/mid) or scalar (Nx, n, dx, dt,
+ * nu_peak, kp, lambda_p, Hs_in, MaxEtaInit, depthinf, Tstar, xbstart, xbend, cutfracwn,
+ * Tp_peak) into out.  Returns the full length, -1 on error. */
+int hw_deck_table(const char* workdir, const hw_opts* opts, const char* name, double* out, int cap);
+
+/* Run on a caller-provided cudaStream_t (NULL: the context's own stream). */
+int hw_set_stream(hw_ctx* ctx, void* cuda_stream);
+int hw_synchronize(hw_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,93 @@
+"""GPU parity: the CUDA engine (through the C ABI) against the CPU oracle.
+
+Tolerances (floating point, FP64 both sides; the FFT algorithms differ):
+  * one RHS evaluation: relative L2 <= 1e-12;
+  * one evolve_apply step: t, h within 1e-12 relative, y relative L2 <= 1e-12;
+  * a non-breaking run to t_end: eta and u relative L2 <= 1e-9.
+"""
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+from decks_util import random_state, rel_l2, small_deck
+
+pytestmark = pytest.mark.gpu
+
+hw = pytest.importorskip("hawassi_c_b200")
+
+CASES = [
+    # name, nx, model, varying, cluster
+    ("hs2_flat_1024", 1024, "HS2", False, 1),
+    ("hs1_flat_1024", 1024, "HS1", False, 1),
+    ("hs3_flat_1024", 1024, "HS3", False, 1),
+    ("hs2_flat_2048_c2", 2048, "HS2", False, 2),
+    ("hs2_flat_4096_c4", 4096, "HS2", False, 4),
+    ("hs3_flat_2048_c8", 2048, "HS3", False, 8),
+    ("hs2_vary_1024", 1024, "HS2", True, 1),
+    ("hs3_vary_1024", 1024, "HS3", True, 1),
+    ("hs3_vary_2048_c2", 2048, "HS3", True, 2),
+    ("hs2_flat_512", 512, "HS2", False, 1),
+    ("hs2_flat_256", 256, "HS2", False, 1),
+]
+
+
+@pytest.mark.parametrize("name,nx,model,varying,cluster", CASES)
+def test_rhs_parity(tmp_path, name, nx, model, varying, cluster):
+    deck = small_deck(tmp_path, name, nx=nx, model=model, varying=varying)
+    o = ol.Oracle(deck)
+    e = hw.Engine(deck, cluster=cluster)
+    for i, t in enumerate([0.0, 2.37, 5.1]):
+        y = random_state(nx, 11 + i)
+        ref = o.rhs(t, y)
+        got = e.rhs(t, y)
+        assert rel_l2(got, ref) < 1e-12, (name, t, rel_l2(got, ref))
+    e.close()
+
+
+@pytest.mark.parametrize("name,nx,model,varying,cluster", CASES[:6])
+def test_evolve_apply_parity(tmp_path, name, nx, model, varying, cluster):
+    deck = small_deck(tmp_path, name, nx=nx, model=model, varying=varying)
+    o = ol.Oracle(deck, eps_abs=1e-8, eps_rel=1e-6)
+    e = hw.Engine(deck, cluster=cluster, eps_abs=1e-8, eps_rel=1e-6)
+    y0 = random_state(nx, 5)
+    ya, yb = y0.copy(), y0.copy()
+    ta, ha = 1.0, 1e-3
+    tb, hb = 1.0, 1e-3
+    for _ in range(4):
+        ta, ha = o.evolve_apply(ta, 1.5, ha, ya)
+        tb, hb = e.evolve_apply(tb, 1.5, hb, yb)
+        assert abs(ta - tb) <= 1e-12 * abs(ta)
+        assert abs(ha - hb) <= 1e-9 * abs(ha)
+        assert rel_l2(yb, ya) < 1e-12
+
+
+def _eta_u(y, nx):
+    eh = y[:nx] + 1j * y[nx:2 * nx]
+    uh = y[2 * nx:3 * nx] + 1j * y[3 * nx:]
+    return np.fft.ifft(eh).real, np.fft.ifft(uh).real
+
+
+@pytest.mark.parametrize("nx,model,varying,cluster", [(1024, "HS2", False, 1), (2048, "HS3", True, 2),
+                                                      (4096, "HS2", False, 2)])
+def test_run_parity(tmp_path, nx, model, varying, cluster):
+    deck = small_deck(tmp_path, f"run_{nx}_{model}", nx=nx, model=model, varying=varying, T_end=6.0)
+    o = ol.Oracle(deck, eps_abs=1e-8, eps_rel=1e-6)
+    tim, _, _ = o.run()
+    y_ref = np.zeros(4 * nx)
+    # the oracle's run owns its state; re-run by stepping to read the final state
+    o2 = ol.Oracle(deck, eps_abs=1e-8, eps_rel=1e-6)
+    t, h = float(o2.table("ttrace")[0]), 1e-4
+    y_ref = o2.initial_state()
+    for ti in o2.table("ttrace"):
+        while t < ti:
+            t, h = o2.evolve_apply(t, ti, h, y_ref)
+    e = hw.Engine(deck, cluster=cluster, eps_abs=1e-8, eps_rel=1e-6)
+    e.run()
+    tg, hg, yg = e.state()
+    assert tg == pytest.approx(t, rel=1e-12)
+    er, ur = _eta_u(y_ref, nx)
+    eg, ug = _eta_u(yg, nx)
+    assert rel_l2(eg, er) < 1e-9
+    assert rel_l2(ug, ur) < 1e-9
+    st = e.stats()
+    assert st["status"] == 0 and st["accepted"] > 10
