@@ -1,15 +1,284 @@
-// hw_breaking.cuh -- kinematic breaking (1d/breaking.c, 1d/rhs.c:617-657) on the device.
+// hw_breaking.cuh -- kinematic breaking on the device (1d/breaking.c:36-449 and
+// rhs_breaking, 1d/rhs.c:617-657), run inside every RHS evaluation exactly as
+// the reference does (the state machine sees every call, rejected stages too).
+//
+//  * criterion (parallel): eta above MaxEtaInit in the breaking window and the
+//    local maxima above it (findpeaks), collected with global atomics;
+//  * crest state machine (one leader thread of the member): local wavenumber
+//    from the Hilbert transform, u > KBC * c test, crest tracking with the
+//    CrestBreak / New / Prev records, the U*(t) ramp and B in [0, 1] along each
+//    breaking crest, and the breaking.dat record once per output interval;
+//  * eddy-viscosity force (parallel): Flux = -B delb^2 (h + eta) (d_t eta)^2,
+//    R_b = d_x Flux / (h + eta) with centred differences, then its spectrum.
 #pragma once
 
 #include "hw_rhs.cuh"
 
 namespace hwdev {
 
+__device__ __forceinline__ double phase_velocity_dev(double k, double d) {  // 1d/functions.c:1415
+  if (k == 0) return sqrt(kG * d);
+  const double s = k < 0 ? -1.0 : 1.0;
+  return s * sqrt(kG * k * tanh(d * k)) / k;
+}
+
+__device__ __forceinline__ void crest_clear(Crest* a, int n) {  // set_init_CB (BindexNow untouched)
+  for (int j = 0; j < n; ++j) {
+    a[j].Bindex = 0;
+    a[j].Ucrest = 0;
+    a[j].DirProp = 0;
+    a[j].Bposition = 0;
+    a[j].Btime = 0;
+    a[j].Bcount = 0;
+  }
+}
+
+// the sequential part of breaking_process, run by one thread
+__device__ void breaking_leader(const DevMember& d, BrkDev* bk, double t, const double2* PE, const double* Heta,
+                                int hs) {
+  const int N = d.N, cap = bk->cap;
+  double* B = bk->B;
+  // B <- 0 (only the nodes set by the previous call can be nonzero)
+  if (bk->n_touched > N) {
+    for (int i = 0; i < N; ++i) B[i] = 0.0;
+  } else {
+    for (int i = 0; i < bk->n_touched; ++i) B[bk->touched[i]] = 0.0;
+  }
+  bk->n_touched = 0;
+  Crest* cb = bk->cb;
+  Crest* cbn = bk->cbn;
+  Crest* cbp = bk->cbp;
+  // ---- breaking_criterion (1d/breaking.c:63) ----
+  const int npk = bk->npk;
+  if (bk->any_above && npk > 0) {
+    int* pk = bk->pk;
+    for (int i = 1; i < npk; ++i) {   // findpeaks yields ascending indices
+      const int v = pk[i];
+      int j = i - 1;
+      while (j >= 0 && pk[j] > v) { pk[j + 1] = pk[j]; --j; }
+      pk[j + 1] = v;
+    }
+    int itCB = 0;
+    for (int i = 0; i < npk; ++i) {
+      const int J = pk[i];
+      const double eJ = PE[J].x, hJ = Heta[size_t(hs) * J];
+      const double gH = (Heta[size_t(hs) * (J + 1)] - Heta[size_t(hs) * (J - 1)]) / (2 * d.dx);
+      const double ge = (PE[J + 1].x - PE[J - 1].x) / (2 * d.dx);
+      const double KxJ = (eJ * gH - hJ * ge) / (eJ * eJ + hJ * hJ);
+      const double Cc = phase_velocity_dev(KxJ, d.depth[J] + eJ);
+      const double Up = PE[J].y;
+      if (fabs(Up) > (d.KBC * fabs(Cc)) && itCB < cap) {
+        Crest& r = cb[itCB];
+        r.Bindex = J;
+        r.BindexNow = J;
+        r.Ucrest = fabs(Up);
+        r.DirProp = int(Up / fabs(Up));
+        r.Bposition = 0.0;
+        r.Btime = t;
+        ++itCB;
+      }
+    }
+    for (int j = 0; j < itCB; ++j) cb[j].Bcount = itCB;
+  } else {
+    crest_clear(cb, cap);
+  }
+  // ---- breaking_process (1d/breaking.c:200-449) ----
+  const int NCB = cb[0].Bcount;
+  int* ID = bk->id_node_end;
+  if (NCB > 0 && bk->flag == 0) {
+    bk->flag = 1;
+    for (int j = 0; j < NCB; ++j) cbn[j] = cb[j];
+  } else if (NCB == 0 && bk->flag == 2) {
+    const int NCBprev = cbp[0].Bcount;
+    for (int j = 0; j < NCBprev; ++j) cbn[j] = cbp[j];
+  } else if (NCB > 0 && bk->flag == 2) {
+    const int NCBprev = cbp[0].Bcount;
+    for (int j = 0; j < NCBprev; ++j) cbn[j] = cbp[j];
+    int add = 0;
+    for (int kk = 0; kk < NCB; ++kk) {
+      bool isnew = true;
+      for (int l = 0; l < NCBprev; ++l) {
+        const int dleft = abs(ID[l] - cbp[l].BindexNow);
+        if (cbp[l].DirProp == 1) {
+          if (cb[kk].Bindex >= (cbp[l].BindexNow - 3 * dleft) && cb[kk].Bindex <= ID[l]) { isnew = false; break; }
+        } else {
+          if (cb[kk].Bindex >= cbp[l].BindexNow && cb[kk].Bindex <= (ID[l] + 3 * dleft)) { isnew = false; break; }
+        }
+      }
+      if (isnew && NCBprev + add < cap) {
+        Crest& r = cbn[NCBprev + add];
+        r.Bindex = cb[kk].Bindex;
+        r.BindexNow = cb[kk].Bindex;
+        ID[NCBprev + add] = cb[kk].Bindex;
+        r.Ucrest = cb[kk].Ucrest;
+        r.Bposition = cb[kk].Bposition;
+        r.Btime = cb[kk].Btime;
+        r.DirProp = cb[kk].DirProp;
+        r.Bcount = cb[kk].Bcount;
+        ++add;
+      }
+    }
+    int j = 0;
+    while (j < cap && cbn[j].Bindex > 0) ++j;
+    for (int i = 0; i < j; ++i) cbn[i].Bcount = j;
+  }
+  if (bk->flag == 1 || bk->flag == 2) {
+    const int NCBnow = cbn[0].Bcount;
+    int it_indexb = 0, iterNprev = 0;
+    bool any_keep = false, any_set = false;
+    crest_clear(cbp, cap);
+    int prevNow = -1;
+    for (int lx = 0; lx < NCBnow; ++lx) {
+      int indxMaxNow;
+      if (bk->flag == 1) {
+        indxMaxNow = cbn[lx].Bindex;
+      } else {
+        const int st = cbn[lx].BindexNow;
+        const int lenloc = abs(ID[lx] - st);
+        int best = 0;
+        if (lenloc > 0) {
+          double tv = PE[st].x;
+          for (int q = 0; q < lenloc; ++q) {
+            const double v = PE[st + q * cbn[lx].DirProp].x;
+            if (v > tv) { tv = v; best = q; }
+          }
+        }
+        indxMaxNow = st + best * cbn[lx].DirProp;
+      }
+      cbn[lx].BindexNow = indxMaxNow;
+      if (lx != 0 && indxMaxNow == prevNow) { prevNow = indxMaxNow; continue; }   // IDTerminate = 0
+      prevNow = indxMaxNow;
+      const double tbreak = cbn[lx].Btime, U_I = cbn[lx].Ucrest, U_F = d.TC * U_I;
+      double U_star;
+      if ((t - tbreak) >= d.Tstar) U_star = U_F;
+      else if ((t - tbreak) >= 0 && (t - tbreak) < d.Tstar) U_star = U_I + ((t - tbreak) / d.Tstar) * (U_F - U_I);
+      else U_star = U_I;
+      const int dir = cbn[lx].DirProp;
+      const int indEND = dir == 1 ? d.xbend : d.xbstart;
+      int Node_end = indxMaxNow;
+      bool fh = false;
+      for (int ly = indxMaxNow; ly < indEND && dir != 0; ly += dir) {
+        const double au = fabs(PE[ly].y);
+        if (au < U_F) { Node_end = ly; break; }
+        double bv;
+        if (au > (2 * U_star)) bv = 1;
+        else if (au <= U_star) bv = 0;
+        else bv = (au / U_star) - 1;
+        B[ly] = bv;
+        if (bv != 0.0) any_set = true;
+        if (bk->n_touched < N) bk->touched[bk->n_touched] = ly;
+        ++bk->n_touched;
+        if (au >= U_star) fh = true;
+        if (it_indexb < N) bk->nodes[it_indexb] = ly;
+        ++it_indexb;
+      }
+      if (fh) {
+        any_keep = true;
+        ID[iterNprev] = Node_end;
+        cbp[iterNprev] = cbn[lx];
+        ++iterNprev;
+      }
+    }
+    (void)any_set;
+    int j = 0;
+    while (j < cap && cbp[j].Bindex > 0) ++j;
+    for (int i = 0; i < j; ++i) cbp[i].Bcount = j;
+    // flag: 2 if any crest keeps breaking, else 0 (the reference loop over IDTerminate)
+    if (NCBnow > 0) bk->flag = any_keep ? 2 : 0;
+    if (t > (bk->ITERbdt * d.dt_in) && it_indexb > 0) {
+      const long long need = 2 + it_indexb;
+      if (bk->log_len + need <= bk->log_cap) {
+        double* lg = bk->log + bk->log_len;
+        lg[0] = t;
+        lg[1] = it_indexb;
+        for (int q = 0; q < it_indexb && q < N; ++q) lg[2 + q] = bk->nodes[q];
+        bk->log_len += need;
+      }
+      ++bk->ITERbn;
+    }
+  }
+  if (t > (bk->ITERbdt * d.dt_in)) ++bk->ITERbdt;
+  crest_clear(cbn, cap);
+  crest_clear(cb, cap);
+  // nodes touched by this call (zero: the breaking force is identically zero)
+  bk->npk = bk->n_touched;
+}
+
 template <int M>
-__device__ __noinline__ void breaking_rhs(Ctx<M>& X, double t, const double2* PE, const double* Heta, int heta_stride,
-                             const double2* AEadj, double2* Rb) {
-  (void)t; (void)PE; (void)Heta; (void)heta_stride; (void)AEadj;
-  HW_FOREACH(X) { (void)idx; Rb[p] = make_double2(0.0, 0.0); }
+__device__ __noinline__ void breaking_rhs(Ctx<M>& X, double t, const double2* PE, const double* Heta, int hs,
+                                          const double2* AEadj, double2* Rb) {
+  const DevMember& d = X.d;
+  BrkDev* bk = d.bk;
+  const int N = d.N;
+  const bool leader = X.c == 0 && X.tid == 0;
+  if (leader) {
+    bk->npk = 0;
+    bk->any_above = 0;
+  }
+  member_sync(d.C);
+  // criterion scan over this CTA's physical points (1d/breaking.c:36-61,72)
+  const int w0 = d.xbstart, w1 = d.xbstart + d.lenIF;   // window [w0, w1)
+  HW_FOREACH(X) {
+    (void)idx;
+    if (p >= w0 && p < w1) {
+      const double e = PE[p].x;
+      if (e > d.MaxEtaInit) atomicOr(&bk->any_above, 1);
+      if (p >= w0 + 1 && p <= w1 - 2 && !(e < d.MaxEtaInit) && e > PE[p + 1].x && e > PE[p - 1].x) {
+        const int slot = atomicAdd(&bk->npk, 1);
+        if (slot < N) bk->pk[slot] = p;
+      }
+    }
+  }
+  member_sync(d.C);
+  if (leader) {
+    if (bk->npk > N) bk->npk = N;
+    breaking_leader(d, bk, t, PE, Heta, hs);
+    __threadfence();
+  }
+  member_sync(d.C);
+  if (bk->npk == 0) {   // B identically zero: FFT(0) = 0, as the reference computes it
+    HW_FOREACH(X) {
+      (void)idx;
+      Rb[p] = make_double2(0.0, 0.0);
+    }
+    return;
+  }
+  // d_t eta = Re F^-1(dH1_eta + adjusted nonlinear eta term)
+  const double2* ZU = d.zs + N;
+  const double2* HS = d.sc[6];
+  auto teta = [&](int q) -> double2 {
+    double2 h1;
+    if (d.flat) {
+      const double c1 = d.c1[q];
+      h1 = make_double2(c1 * ZU[q].y, -c1 * ZU[q].x);
+    } else {
+      const double kq = d.k[q];
+      h1 = make_double2((HS[q].y / kG) * kq, -(HS[q].x / kG) * kq);
+    }
+    return cadd(h1, AEadj[q]);
+  };
+  HW_FOREACH(X) {
+    const int pp = partner_pos(X, idx);
+    X.buf[pidx(idx)] = cscale(herm(teta(p), teta(pp)), d.invN);
+  }
+  double2* FL = d.sc[8];   // flux (physical), reused scratch
+  fft_inverse_then(X, [&](int, int, int p, double2 v) {
+    const double dte = v.x;
+    const double e = PE[p].x;
+    FL[p].x = -bk->B[p] * (kDelb * kDelb) * (d.depth[p] + e) * dte * dte;
+  });
+  member_sync(d.C);
+  // gradient (1d/functions.c:1850) and R_b = d_x Flux / (h + eta)
+  HW_FOREACH(X) {
+    (void)idx;
+    double g;
+    if (p == 0) g = (FL[1].x - FL[0].x) / d.dx;
+    else if (p == N - 1) g = (FL[N - 1].x - FL[N - 2].x) / d.dx;
+    else g = (FL[p + 1].x - FL[p - 1].x) / (2 * d.dx);
+    const double rb = 1 / (d.depth[p] + PE[p].x) * g;
+    X.buf[pidx(idx)] = make_double2(rb, 0.0);
+  }
+  fft_forward_split(X, [&](int, int, int p, double2 z, double2 zp) { Rb[p] = split_re(z, zp); });
 }
 
 }  // namespace hwdev

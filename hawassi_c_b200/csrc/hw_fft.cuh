@@ -156,7 +156,7 @@ __device__ __forceinline__ void member_sync(int C) {
 
 // Forward FFT: physical block slice in buf -> spectral cyclic slice in buf.
 template <int M>
-__device__ __forceinline__ void fft_forward(double2* buf, const double2* __restrict__ tw, int N, int C, int c) {
+__device__ __noinline__ void fft_forward(double2* buf, const double2* __restrict__ tw, int N, int C, int c) {
   if (C == 1) __syncthreads();
   if (C > 1) {
     constexpr int T = M / kPts;
@@ -185,7 +185,7 @@ __device__ __forceinline__ void fft_forward(double2* buf, const double2* __restr
 
 // Inverse FFT (unnormalised): spectral cyclic slice in buf -> physical block slice in buf.
 template <int M>
-__device__ __forceinline__ void fft_inverse(double2* buf, const double2* __restrict__ tw, int N, int C, int c) {
+__device__ __noinline__ void fft_inverse(double2* buf, const double2* __restrict__ tw, int N, int C, int c) {
   __syncthreads();
   local_fft<M>(buf, tw, C, +1);
   if (C > 1) {

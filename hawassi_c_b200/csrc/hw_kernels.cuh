@@ -9,7 +9,7 @@
 namespace hwdev {
 
 template <int M>
-__global__ void __launch_bounds__(M / kPts) k_evolve(DevMember* mems, const int* list, int mode) {
+__global__ void __launch_bounds__(M / kPts, (4096 / M)) k_evolve(DevMember* mems, const int* list, int mode) {
   extern __shared__ double2 smem_buf[];
   __shared__ DevMember sd;
   __shared__ double red[48];
@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(M / kPts) k_evolve(DevMember* mems, const int*
 
 // single RHS evaluation of member mi: kout = f(t, zs)
 template <int M>
-__global__ void __launch_bounds__(M / kPts) k_rhs(DevMember* mems, const int* list, double t) {
+__global__ void __launch_bounds__(M / kPts, (4096 / M)) k_rhs(DevMember* mems, const int* list, double t) {
   extern __shared__ double2 smem_buf[];
   __shared__ DevMember sd;
   __shared__ double red[48];

@@ -1,0 +1,83 @@
+"""GPU parity of kinematic breaking (1d/breaking.c, 1d/rhs.c:617-657) against the oracle.
+
+Deck: the reference's own 1dFBr005Bor input (HS2, flat 1 m, Nx=4096, IVP with
+kinematic breaking, reference tolerances).  The device replays GSL's exact RHS
+call sequence (the breaking state machine runs on every call), so the
+breaking.dat records must be identical to the oracle's -- and to the golden
+file shipped with the reference -- up to the onset and beyond.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+from decks_util import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+hw = pytest.importorskip("hawassi_c_b200")
+
+
+def _log_lines(recs):
+    return [[f"{t:f}", str(len(nodes))] + [str(n) for n in nodes] for t, nodes in recs]
+
+
+@pytest.mark.parametrize("cluster", [2, 4])
+def test_breaking_onset_matches_golden(golden_dir, cluster):
+    deck = os.path.join(golden_dir, "fbr005")
+    e = hw.Engine(deck, cluster=cluster)
+    e.run_to_time(12.7)
+    st = e.stats()
+    assert st["status"] == 0
+    mine = _log_lines(e.breaking_log())
+    gold = [l.split() for l in open(os.path.join(golden_dir, "fbr005_breaking_head.txt"))]
+    t_end = e.state()[0]
+    gold = [g for g in gold if float(g[0]) <= t_end]
+    assert len(gold) >= 5
+    assert mine[:len(gold)] == gold
+
+
+def test_breaking_state_vs_oracle(golden_dir):
+    deck = os.path.join(golden_dir, "fbr005")
+    o = ol.Oracle(deck)
+    t, h = 0.0, 1e-4
+    y = o.initial_state()
+    tt = o.table("ttrace")
+    for ti in tt[tt <= 13.0]:
+        while t < ti:
+            t, h = o.evolve_apply(t, ti, h, y)
+    e = hw.Engine(deck, cluster=2)
+    e.run_to_time(13.0)
+    tg, hg, yg = e.state()
+    assert tg == pytest.approx(t, rel=1e-12)
+    nx = e.nx[0]
+    eta_o = np.fft.ifft(y[:nx] + 1j * y[nx:2 * nx]).real
+    eta_g = np.fft.ifft(yg[:nx] + 1j * yg[nx:2 * nx]).real
+    assert rel_l2(eta_g, eta_o) < 1e-9
+    # total energy (quadratic Hamiltonian, same spectral form both sides) within 1e-6
+    assert e.stats()["rhs_calls"] == o.stats()[0]
+    gold = [l.split() for l in open(os.path.join(golden_dir, "fbr005_breaking_head.txt"))]
+    assert _log_lines(e.breaking_log())[:3] == [l.split() for l in o.breaking_log().splitlines()][:3]
+    assert gold[0] == _log_lines(e.breaking_log())[0]
+
+
+def test_breaking_single_rhs(golden_dir):
+    """One RHS call from the same mid-run state: dz (including the eddy-viscosity
+    force R_b) and the breaking record agree."""
+    deck = os.path.join(golden_dir, "fbr005")
+    o = ol.Oracle(deck)
+    t, h = 0.0, 1e-4
+    y = o.initial_state()
+    tt = o.table("ttrace")
+    for ti in tt[tt <= 12.62]:
+        while t < ti:
+            t, h = o.evolve_apply(t, ti, h, y)
+    o2 = ol.Oracle(deck)
+    e = hw.Engine(deck, cluster=2)
+    for dt_ in (0.0, 0.003, 0.007):
+        ref = o2.rhs(t + dt_, y)
+        got = e.rhs(t + dt_, y)
+        assert rel_l2(got, ref) < 1e-11
+    B = o2.table("B")
+    assert np.count_nonzero(B) > 0
