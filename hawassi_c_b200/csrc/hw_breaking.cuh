@@ -34,7 +34,7 @@ __device__ __forceinline__ void crest_clear(Crest* a, int n) {  // set_init_CB (
 }
 
 // the sequential part of breaking_process, run by one thread
-__device__ void breaking_leader(const DevMember& d, BrkDev* bk, double t, const double2* PE, const double* Heta,
+static __device__ __noinline__ void breaking_leader(const DevMember& d, BrkDev* bk, double t, const double2* PE, const double* Heta,
                                 int hs) {
   const int N = d.N, cap = bk->cap;
   double* B = bk->B;
@@ -125,7 +125,7 @@ __device__ void breaking_leader(const DevMember& d, BrkDev* bk, double t, const 
   if (bk->flag == 1 || bk->flag == 2) {
     const int NCBnow = cbn[0].Bcount;
     int it_indexb = 0, iterNprev = 0;
-    bool any_keep = false, any_set = false;
+    bool any_keep = false;
     crest_clear(cbp, cap);
     int prevNow = -1;
     for (int lx = 0; lx < NCBnow; ++lx) {
@@ -165,7 +165,6 @@ __device__ void breaking_leader(const DevMember& d, BrkDev* bk, double t, const 
         else if (au <= U_star) bv = 0;
         else bv = (au / U_star) - 1;
         B[ly] = bv;
-        if (bv != 0.0) any_set = true;
         if (bk->n_touched < N) bk->touched[bk->n_touched] = ly;
         ++bk->n_touched;
         if (au >= U_star) fh = true;
@@ -179,7 +178,6 @@ __device__ void breaking_leader(const DevMember& d, BrkDev* bk, double t, const 
         ++iterNprev;
       }
     }
-    (void)any_set;
     int j = 0;
     while (j < cap && cbp[j].Bindex > 0) ++j;
     for (int i = 0; i < j; ++i) cbp[i].Bcount = j;
