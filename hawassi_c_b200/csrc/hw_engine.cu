@@ -86,6 +86,7 @@ struct Class {
   int* d_list = nullptr;
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
+  cudaEvent_t t_start = nullptr, t_stop = nullptr;   // timing of the last evolve launch
 };
 
 }  // namespace
@@ -334,7 +335,7 @@ bool hw_ctx::init(const std::vector<std::string>& dirs, const hw_opts* o) {
     for (auto& c : classes)
       if (c.M == mem[i].M && c.C == mem[i].C) cls = &c;
     if (!cls) {
-      classes.push_back(Class{mem[i].M, mem[i].C, {}, nullptr, nullptr, nullptr});
+      classes.push_back(Class{mem[i].M, mem[i].C, {}, nullptr, nullptr, nullptr, nullptr, nullptr});
       cls = &classes.back();
     }
     cls->members.push_back(int(i));
@@ -344,6 +345,8 @@ bool hw_ctx::init(const std::vector<std::string>& dirs, const hw_opts* o) {
     HW_CUDA(cudaMemcpy(c.d_list, c.members.data(), sizeof(int) * c.members.size(), cudaMemcpyHostToDevice));
     HW_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     HW_CUDA(cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming));
+    HW_CUDA(cudaEventCreate(&c.t_start));
+    HW_CUDA(cudaEventCreate(&c.t_stop));
   }
   return true;
 }
@@ -371,8 +374,10 @@ bool hw_ctx::run(int i_stop_all, double t_end, bool by_time) {
   HW_CUDA(cudaEventRecord(fork, stream));
   for (auto& c : classes) {
     HW_CUDA(cudaStreamWaitEvent(c.stream, fork, 0));
+    HW_CUDA(cudaEventRecord(c.t_start, c.stream));
     cudaError_t e = launch_any(c.M, 0, d_mems, c.d_list, int(c.members.size()), c.C, 0.0, c.stream);
     if (e != cudaSuccess) { err = std::string("launch: ") + cudaGetErrorString(e); return false; }
+    HW_CUDA(cudaEventRecord(c.t_stop, c.stream));
     HW_CUDA(cudaEventRecord(c.done, c.stream));
     HW_CUDA(cudaStreamWaitEvent(stream, c.done, 0));
   }
@@ -426,6 +431,8 @@ hw_ctx::~hw_ctx() {
     if (c.d_list) cudaFree(c.d_list);
     if (c.stream) cudaStreamDestroy(c.stream);
     if (c.done) cudaEventDestroy(c.done);
+    if (c.t_start) cudaEventDestroy(c.t_start);
+    if (c.t_stop) cudaEventDestroy(c.t_stop);
   }
   if (d_mems) cudaFree(d_mems);
   if (d_single) cudaFree(d_single);
@@ -695,6 +702,65 @@ int hw_deck_table(const char* workdir, const hw_opts* opts, const char* name, do
   const int n = std::min(cap, int(v.size()));
   if (out) std::memcpy(out, v.data(), sizeof(double) * size_t(n));
   return int(v.size());
+}
+
+int hw_get_states(hw_ctx* ctx, double* y_all) {
+  if (!ctx || !y_all) return 1;
+  std::string& err = ctx->err;
+  auto body = [&]() -> bool {
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    size_t off = 0;
+    for (size_t i = 0; i < ctx->mem.size(); ++i) {
+      HostMember& hm = ctx->mem[i];
+      HW_CUDA(cudaMemcpyAsync(&hm.d, ctx->d_mems + i, sizeof(DevMember), cudaMemcpyDeviceToHost, ctx->stream));
+      HW_CUDA(cudaStreamSynchronize(ctx->stream));
+      k_to_reference<<<(hm.N + 255) / 256, 256, 0, ctx->stream>>>(hm.d.y, ctx->d_ref, hm.N, hm.logC, hm.M);
+      HW_CUDA(cudaGetLastError());
+      HW_CUDA(cudaMemcpyAsync(y_all + off, ctx->d_ref, sizeof(double) * 4 * hm.N, cudaMemcpyDeviceToHost,
+                              ctx->stream));
+      HW_CUDA(cudaStreamSynchronize(ctx->stream));
+      off += size_t(4) * hm.N;
+    }
+    return true;
+  };
+  return body() ? 0 : 1;
+}
+
+int hw_set_states(hw_ctx* ctx, const double* y_all) {
+  if (!ctx || !y_all) return 1;
+  std::string& err = ctx->err;
+  auto body = [&]() -> bool {
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    size_t off = 0;
+    for (size_t i = 0; i < ctx->mem.size(); ++i) {
+      HostMember& hm = ctx->mem[i];
+      HW_CUDA(cudaMemcpy(&hm.d, ctx->d_mems + i, sizeof(DevMember), cudaMemcpyDeviceToHost));
+      HW_CUDA(cudaMemcpyAsync(ctx->d_ref, y_all + off, sizeof(double) * 4 * hm.N, cudaMemcpyHostToDevice,
+                              ctx->stream));
+      k_to_internal<<<(hm.N + 255) / 256, 256, 0, ctx->stream>>>(ctx->d_ref, hm.d.y, hm.N, hm.logC, hm.M);
+      HW_CUDA(cudaGetLastError());
+      HW_CUDA(cudaStreamSynchronize(ctx->stream));
+      hm.d.k1_valid = 0;
+      HW_CUDA(cudaMemcpy(&ctx->d_mems[i].k1_valid, &hm.d.k1_valid, sizeof(int), cudaMemcpyHostToDevice));
+      off += size_t(4) * hm.N;
+    }
+    return true;
+  };
+  return body() ? 0 : 1;
+}
+
+int hw_class_timing(hw_ctx* ctx, double* ms, int* members, int* grid_n, int cap) {
+  if (!ctx) return -1;
+  if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return -1;
+  const int n = int(ctx->classes.size());
+  for (int i = 0; i < n && i < cap; ++i) {
+    Class& c = ctx->classes[size_t(i)];
+    float f = 0.f;
+    if (ms) ms[i] = cudaEventElapsedTime(&f, c.t_start, c.t_stop) == cudaSuccess ? double(f) : -1.0;
+    if (members) members[i] = int(c.members.size());
+    if (grid_n) grid_n[i] = c.M * c.C;
+  }
+  return n;
 }
 
 int hw_set_stream(hw_ctx* ctx, void* s) {

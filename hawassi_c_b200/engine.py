@@ -34,7 +34,8 @@ EXPORTS = [
     "hw_create", "hw_ensemble_create", "hw_destroy", "hw_last_error", "hw_members", "hw_nx", "hw_nt",
     "hw_initial_state", "hw_rhs", "hw_gsl_rhs", "hw_evolve_apply", "hw_run", "hw_run_to_time",
     "hw_get_state", "hw_set_state", "hw_reset", "hw_member_stats", "hw_last_dydt", "hw_breaking_log",
-    "hw_set_stream", "hw_synchronize", "hw_deck_table",
+    "hw_set_stream", "hw_synchronize", "hw_deck_table", "hw_get_states", "hw_set_states",
+    "hw_class_timing",
 ]
 
 
@@ -73,6 +74,9 @@ def load_library():
     L.hw_set_stream.argtypes = [vp, vp]
     L.hw_synchronize.argtypes = [vp]
     L.hw_deck_table.argtypes = [ctypes.c_char_p, ctypes.POINTER(HwOpts), ctypes.c_char_p, dp, ip]
+    L.hw_get_states.argtypes = [vp, dp]
+    L.hw_set_states.argtypes = [vp, dp]
+    L.hw_class_timing.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ip]
     _lib = L
     return L
 
@@ -198,6 +202,25 @@ class Engine:
             out.append((t, [int(v) for v in buf[i + 2:i + 2 + cnt]]))
             i += 2 + cnt
         return out
+
+    def get_states(self, out):
+        """All member states into one host buffer (concatenated reference layouts)."""
+        self._check(load_library().hw_get_states(self._h, _dp(out)), "get_states")
+        return out
+
+    def set_states(self, y_all):
+        self._check(load_library().hw_set_states(self._h, _dp(y_all)), "set_states")
+
+    def class_timing(self):
+        """[(ms, members, grid_n), ...] of the last run's evolve launches."""
+        L = load_library()
+        ms = np.zeros(16)
+        mem = (ctypes.c_int * 16)()
+        gn = (ctypes.c_int * 16)()
+        n = L.hw_class_timing(self._h, _dp(ms), mem, gn, 16)
+        if n < 0:
+            raise EngineError("class_timing failed")
+        return [(float(ms[i]), int(mem[i]), int(gn[i])) for i in range(n)]
 
     def set_stream(self, stream_ptr):
         self._check(load_library().hw_set_stream(self._h, ctypes.c_void_p(stream_ptr)), "set_stream")

@@ -83,6 +83,14 @@ int hw_last_dydt(hw_ctx* ctx, int member, double* dydt);
  * written, *len receives the number of doubles. */
 int hw_breaking_log(hw_ctx* ctx, int member, double* out, long long cap, long long* len);
 
+/* All members' states, concatenated in member order (4*Nx doubles each), host buffers. */
+int hw_get_states(hw_ctx* ctx, double* y_all);
+int hw_set_states(hw_ctx* ctx, const double* y_all);
+
+/* Device time (ms) of the last hw_run launch of each grid-size class, with the
+ * class's member count and grid size; returns the number of classes. */
+int hw_class_timing(hw_ctx* ctx, double* ms, int* members, int* grid_n, int cap);
+
 /* Host-only (no GPU needed): build the set-up of <workdir> and copy the named table
  * (x, k, depth, dampchar, dampcoef, aal, ChiAdj, Csqr, L, M0im, gamX, gamX_skew, insig,
  * insig_skew, ttrace, y0, gam_min/plus/mid, Csq_min/plus/mid) or scalar (Nx, n, dx, dt,
