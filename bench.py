@@ -42,6 +42,13 @@ WORKLOAD = ("batched ragged 1D ensemble: 256 members/GPU, Nx in {2048,4096,8192,
             "RKF45 rtol 1e-6 atol 1e-8")
 
 
+T_START = time.time()
+
+
+def log(msg):
+    print(f"[bench +{time.time() - T_START:7.1f}s] {msg}", file=sys.stderr, flush=True)
+
+
 def make_decks(root, rank, members, breaking=True):
     from hawassi_c_b200 import decks
     paths = []
@@ -55,7 +62,7 @@ def make_decks(root, rank, members, breaking=True):
 
 
 # ----------------------------------------------------------------------------
-# CPU side: the oracle port on the host cores (spawned workers)
+# CPU side: the oracle port on the host cores (one thread per core)
 # ----------------------------------------------------------------------------
 def _cpu_worker(args):
     """Advance a fixed set of members through n_steps windows of output samples,
@@ -88,15 +95,19 @@ def _cpu_worker(args):
     return out
 
 
-def cpu_measure(decks, workers, window, n_steps, max_seconds):
-    """Run the oracle port on `workers` spawned processes; returns per-step
-    (RHS grid points, max wall seconds over workers)."""
-    import multiprocessing as mp
-    ctx = mp.get_context("spawn")
+def cpu_measure(decks, workers, window, n_steps, max_seconds, timeout=None):
+    """Run the oracle port on `workers` host threads (ctypes releases the GIL during
+    each C call, so the threads run on separate cores); returns per-step
+    (RHS grid points, max wall seconds over workers) and the simulated seconds."""
+    import concurrent.futures as cf
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as ol
+    ol.lib()
     shards = [decks[w::workers] for w in range(workers)]
     shards = [s for s in shards if s]
-    with ctx.Pool(len(shards)) as pool:
-        res = pool.map(_cpu_worker, [(sh, window, n_steps, max_seconds) for sh in shards])
+    with cf.ThreadPoolExecutor(len(shards)) as ex:
+        futs = [ex.submit(_cpu_worker, (sh, window, n_steps, max_seconds)) for sh in shards]
+        res = [f.result(timeout=timeout) for f in futs]
     steps = min(len(r) for r in res)
     return [(sum(r[k][0] for r in res), max(r[k][1] for r in res)) for k in range(steps)], \
         sum(r[steps - 1][2] for r in res)
@@ -110,7 +121,7 @@ def run_reference(args, rank, world):
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib as ol
     ol.lib()
-    cores = os.cpu_count() or 1
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
     root = os.path.join(tempfile.gettempdir(), "hw_bench_decks_r0")
     decks = make_decks(root, 0, min(MEMBERS, cores))
     steps, _ = cpu_measure(decks, cores, args.window, args.warmup + args.steps, 1e9)
@@ -199,17 +210,20 @@ def main():
 
     root = os.path.join(tempfile.gettempdir(), f"hw_bench_decks_r{rank}")
     decks = make_decks(root, rank, args.members)
+    log(f"{len(decks)} decks ready")
 
     # CPU baseline on the host cores (spawned before any CUDA work), rank 0 at N=1 only
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cores = min(os.cpu_count() or 1, 64)
+        cores = min(len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count() or 1, 64)
         sample = decks[:cores]
-        steps, sims = cpu_measure(sample, cores, args.window, 10 ** 6, 15.0)
+        log(f"cpu baseline on {cores} threads")
+        steps, sims = cpu_measure(sample, cores, args.window, 10 ** 6, 15.0, timeout=240)
         cpu = {"value": sum(p for p, _ in steps) / sum(t for _, t in steps), "unit": "RHS grid-point evaluations/s",
                "cores": cores, "kind": "port",
-               "sample": f"{len(sample)} ensemble members on {cores} worker processes, {len(steps)} windows of "
+               "sample": f"{len(sample)} ensemble members on {cores} threads, {len(steps)} windows of "
                          f"{args.window} output samples from t0 (~15 s of CPU time, {sims:.1f} simulated s)"}
+        log(f"cpu baseline {cpu['value']:.3e} pts/s")
 
     import torch
     import torch.distributed as dist
@@ -219,7 +233,9 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     import hawassi_c_b200 as hw
     eng = hw.Engine(decks, eps_abs=EPS_ABS, eps_rel=EPS_REL, device=local)
-    stream = torch.cuda.current_stream()
+    log("engine created")
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     eng.set_stream(stream.cuda_stream)
     nx = eng.nx
 
@@ -237,6 +253,7 @@ def main():
     for _ in range(args.warmup):
         i_stop += args.window
         eng.run(i_stop, sync=True)
+        log(f"warmup step to sample {i_stop}")
     torch.cuda.synchronize()
     pts0, sim0 = rhs_pts(), sim_time()
     barrier()
@@ -252,6 +269,7 @@ def main():
     barrier()
     clocks = clk.stop()
     ms = ev0.elapsed_time(ev1)
+    log(f"timed {args.steps} steps: {ms:.1f} ms")
     pts1, sim1 = rhs_pts(), sim_time()
     launches = args.steps * len(eng.class_timing())
     if world > 1:
@@ -321,6 +339,7 @@ def main():
         dist.all_reduce(t[:1], op=dist.ReduceOp.MAX)
         dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
         ems, e_pts = float(t[0].item()), float(t[1].item())
+    log(f"e2e {args.steps} steps: {ems:.1f} ms")
     e2e = {"value": e_pts / (ems / 1e3), "unit": "RHS grid-point evaluations/s",
            "h2d_bytes_per_step": tot_doubles * 8, "d2h_bytes_per_step": tot_doubles * 8}
     statuses = [eng.stats(i)["status"] for i in range(eng.members)]

@@ -79,8 +79,10 @@ static __device__ __noinline__ void breaking_leader(const DevMember& d, BrkDev* 
       }
     }
     for (int j = 0; j < itCB; ++j) cb[j].Bcount = itCB;
+    if (itCB > bk->dirty_cb) bk->dirty_cb = itCB;
   } else {
-    crest_clear(cb, cap);
+    crest_clear(cb, bk->dirty_cb);
+    bk->dirty_cb = 0;
   }
   // ---- breaking_process (1d/breaking.c:200-449) ----
   const int NCB = cb[0].Bcount;
@@ -88,12 +90,15 @@ static __device__ __noinline__ void breaking_leader(const DevMember& d, BrkDev* 
   if (NCB > 0 && bk->flag == 0) {
     bk->flag = 1;
     for (int j = 0; j < NCB; ++j) cbn[j] = cb[j];
+    if (NCB > bk->dirty_cbn) bk->dirty_cbn = NCB;
   } else if (NCB == 0 && bk->flag == 2) {
     const int NCBprev = cbp[0].Bcount;
     for (int j = 0; j < NCBprev; ++j) cbn[j] = cbp[j];
+    if (NCBprev > bk->dirty_cbn) bk->dirty_cbn = NCBprev;
   } else if (NCB > 0 && bk->flag == 2) {
     const int NCBprev = cbp[0].Bcount;
     for (int j = 0; j < NCBprev; ++j) cbn[j] = cbp[j];
+    if (NCBprev > bk->dirty_cbn) bk->dirty_cbn = NCBprev;
     int add = 0;
     for (int kk = 0; kk < NCB; ++kk) {
       bool isnew = true;
@@ -116,17 +121,19 @@ static __device__ __noinline__ void breaking_leader(const DevMember& d, BrkDev* 
         r.DirProp = cb[kk].DirProp;
         r.Bcount = cb[kk].Bcount;
         ++add;
+        if (NCBprev + add > bk->dirty_cbn) bk->dirty_cbn = NCBprev + add;
       }
     }
     int j = 0;
-    while (j < cap && cbn[j].Bindex > 0) ++j;
+    while (j < bk->dirty_cbn && cbn[j].Bindex > 0) ++j;
     for (int i = 0; i < j; ++i) cbn[i].Bcount = j;
   }
   if (bk->flag == 1 || bk->flag == 2) {
     const int NCBnow = cbn[0].Bcount;
     int it_indexb = 0, iterNprev = 0;
     bool any_keep = false;
-    crest_clear(cbp, cap);
+    crest_clear(cbp, bk->dirty_cbp);
+    bk->dirty_cbp = 0;
     int prevNow = -1;
     for (int lx = 0; lx < NCBnow; ++lx) {
       int indxMaxNow;
@@ -176,10 +183,11 @@ static __device__ __noinline__ void breaking_leader(const DevMember& d, BrkDev* 
         ID[iterNprev] = Node_end;
         cbp[iterNprev] = cbn[lx];
         ++iterNprev;
+        if (iterNprev > bk->dirty_cbp) bk->dirty_cbp = iterNprev;
       }
     }
     int j = 0;
-    while (j < cap && cbp[j].Bindex > 0) ++j;
+    while (j < bk->dirty_cbp && cbp[j].Bindex > 0) ++j;
     for (int i = 0; i < j; ++i) cbp[i].Bcount = j;
     // flag: 2 if any crest keeps breaking, else 0 (the reference loop over IDTerminate)
     if (NCBnow > 0) bk->flag = any_keep ? 2 : 0;
@@ -196,8 +204,10 @@ static __device__ __noinline__ void breaking_leader(const DevMember& d, BrkDev* 
     }
   }
   if (t > (bk->ITERbdt * d.dt_in)) ++bk->ITERbdt;
-  crest_clear(cbn, cap);
-  crest_clear(cb, cap);
+  crest_clear(cbn, bk->dirty_cbn);
+  crest_clear(cb, bk->dirty_cb);
+  bk->dirty_cbn = 0;
+  bk->dirty_cb = 0;
   // nodes touched by this call (zero: the breaking force is identically zero)
   bk->npk = bk->n_touched;
 }

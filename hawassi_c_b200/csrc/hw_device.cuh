@@ -28,6 +28,7 @@ struct BrkDev {
   int npk;            // candidate crests found by the parallel criterion
   int any_above;      // eta above MaxEtaInit somewhere in the breaking window
   int cap;            // Nx / 4
+  int dirty_cb, dirty_cbn, dirty_cbp;   // records [0, dirty) may be nonzero
   Crest* cb;          // CrestBreak (from the criterion)
   Crest* cbn;         // CrestBreakNew
   Crest* cbp;         // CrestBreakPrev

@@ -26,6 +26,12 @@ namespace {
 // ---------------------------------------------------------------------------
 // kernels
 // ---------------------------------------------------------------------------
+// clear the budget status so that a bounded launch can continue where it stopped
+__global__ void k_resume(DevMember* mems, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && mems[i].status == kBudget) mems[i].status = kOk;
+}
+
 // reference layout (4N doubles) -> internal (2N double2, spectral permuted)
 __global__ void k_to_internal(const double* __restrict__ ref, double2* __restrict__ dst, int N, int logC, int M) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -262,6 +268,7 @@ bool hw_ctx::upload_member(HostMember& h) {
   d.i_stop = 0;
   d.status = kOk;
   d.exact = m.breaking ? 1 : 0;
+  d.rhs_budget = 400000;   // RHS evaluations per member and launch
   double* tmp = nullptr;
   HW_CUDA(cudaMalloc(&tmp, sizeof(double) * 4 * N));
   HW_CUDA(cudaMemcpy(tmp, m.y0.data(), sizeof(double) * 4 * N, cudaMemcpyHostToDevice));
@@ -305,7 +312,8 @@ bool hw_ctx::init(const std::vector<std::string>& dirs, const hw_opts* o) {
       return false;
     }
     h.N = N;
-    int C = opt.cluster > 0 ? opt.cluster : std::max(1, N / 2048);
+    const int slice = opt.slice > 0 ? opt.slice : 2048;
+    int C = opt.cluster > 0 ? opt.cluster : std::max(1, N / slice);
     if ((C & (C - 1)) != 0 || N / C < 256 || N / C > 2048 || C > 16) {
       err = "invalid cluster size " + std::to_string(C) + " for Nx=" + std::to_string(N);
       return false;
@@ -371,6 +379,9 @@ bool hw_ctx::run(int i_stop_all, double t_end, bool by_time) {
     }
     HW_CUDA(cudaMemcpyAsync(&d_mems[i].i_stop, &stop, sizeof(int), cudaMemcpyHostToDevice, stream));
   }
+  // a member stopped by the per-launch RHS budget resumes here
+  k_resume<<<(unsigned(mem.size()) + 127) / 128, 128, 0, stream>>>(d_mems, int(mem.size()));
+  HW_CUDA(cudaGetLastError());
   HW_CUDA(cudaEventRecord(fork, stream));
   for (auto& c : classes) {
     HW_CUDA(cudaStreamWaitEvent(c.stream, fork, 0));
@@ -409,6 +420,7 @@ bool hw_ctx::reset() {
     BrkDev bk;
     HW_CUDA(cudaMemcpy(&bk, h.d.bk, sizeof bk, cudaMemcpyDeviceToHost));
     bk.flag = bk.ITERbdt = bk.ITERbn = bk.n_touched = bk.npk = bk.any_above = 0;
+    bk.dirty_cb = bk.dirty_cbn = bk.dirty_cbp = 0;
     bk.log_len = 0;
     HW_CUDA(cudaMemset(bk.cb, 0, sizeof(Crest) * bk.cap));
     HW_CUDA(cudaMemset(bk.cbn, 0, sizeof(Crest) * bk.cap));

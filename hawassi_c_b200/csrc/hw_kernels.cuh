@@ -32,7 +32,10 @@ __global__ void __launch_bounds__(M / kPts, (4096 / M)) k_evolve(DevMember* mems
     } else {
       while (iout < sd.i_stop && S.status == kOk) {
         const double ti = sd.tt[iout];
-        while (S.t < ti && S.status == kOk) evolve_apply<M>(X, B, S, ti);
+        while (S.t < ti && S.status == kOk) {
+          evolve_apply<M>(X, B, S, ti);
+          if (S.rhs >= sd.rhs_budget && S.status == kOk) S.status = kBudget;   // bounded launch
+        }
         if (S.status == kOk) ++iout;
       }
     }

@@ -23,6 +23,7 @@ class HwOpts(ctypes.Structure):
         ("exact_sequence", ctypes.c_int),
         ("cluster", ctypes.c_int),
         ("device", ctypes.c_int),
+        ("slice", ctypes.c_int),
     ]
 
 
@@ -90,12 +91,12 @@ class Engine:
     (``Engine(["deck0", "deck1", ...])``) on one GPU."""
 
     def __init__(self, decks, eps_abs=0.0, eps_rel=0.0, h0=0.0, seed=0, nref=0, exact_sequence=False,
-                 cluster=0, device=0):
+                 cluster=0, device=0, slice=0):
         L = load_library()
         if isinstance(decks, (str, os.PathLike)):
             decks = [decks]
         self.decks = [os.fspath(d) for d in decks]
-        opts = HwOpts(eps_abs, eps_rel, h0, seed, nref, int(bool(exact_sequence)), cluster, device)
+        opts = HwOpts(eps_abs, eps_rel, h0, seed, nref, int(bool(exact_sequence)), cluster, device, slice)
         arr = (ctypes.c_char_p * len(self.decks))(*[d.encode() for d in self.decks])
         self._h = L.hw_ensemble_create(arr, len(self.decks), ctypes.byref(opts))
         if not self._h:
@@ -232,7 +233,7 @@ class Engine:
 def deck_table(deck, name, seed=0, nref=0):
     """Host-side set-up table of a deck (no GPU involved)."""
     L = load_library()
-    opts = HwOpts(0.0, 0.0, 0.0, seed, nref, 0, 0, 0)
+    opts = HwOpts(0.0, 0.0, 0.0, seed, nref, 0, 0, 0, 0)
     n = L.hw_deck_table(os.fspath(deck).encode(), ctypes.byref(opts), name.encode(), None, 0)
     if n < 0:
         raise EngineError(L.hw_last_error(None).decode())

@@ -28,6 +28,7 @@ typedef struct hw_opts {
     int exact_sequence;      /* 1: evaluate the RHS exactly where GSL does even when it is stateless */
     int cluster;             /* CTAs per member, power of two (0 = automatic) */
     int device;              /* CUDA device ordinal */
+    int slice;               /* grid points per CTA when cluster == 0 (0 = 2048) */
 } hw_opts;
 
 /* Replaces the reference's set-up (1d/main.cc:42-226): parse <workdir>/input.txt and
@@ -64,6 +65,8 @@ int hw_evolve_apply(hw_ctx* ctx, int member, double* t, double t1, double* h, do
  * each sample time like the reference. i_stop < 0 means all samples. Asynchronous on
  * the context's stream. */
 int hw_run(hw_ctx* ctx, int i_stop);
+/* A launch stops a member after 400000 RHS evaluations (status 3, resumed by the next
+ * hw_run), so no launch runs unbounded. */
 /* Same, stopping at the last output sample whose time is <= t_end. */
 int hw_run_to_time(hw_ctx* ctx, double t_end);
 
@@ -98,7 +101,8 @@ int hw_class_timing(hw_ctx* ctx, double* ms, int* members, int* grid_n, int cap)
  * Tp_peak) into out.  Returns the full length, -1 on error. */
 int hw_deck_table(const char* workdir, const hw_opts* opts, const char* name, double* out, int cap);
 
-/* Run on a caller-provided cudaStream_t (NULL: the context's own stream). */
+/* Run on a caller-provided cudaStream_t (NULL: the context's own stream; pass
+ * cudaStreamLegacy explicitly for the legacy default stream). */
 int hw_set_stream(hw_ctx* ctx, void* cuda_stream);
 int hw_synchronize(hw_ctx* ctx);
 
