@@ -93,6 +93,24 @@ __device__ __forceinline__ void dft_small<8>(double2* v, int sign) {
   }
 }
 
+
+// w^1..w^(R-1) from w^1: one table load per butterfly, powers by short products
+// (w^2 = w w, w^3 = w^2 w, w^4 = w^2 w^2, w^5 = w^4 w, w^6 = w^4 w^2, w^7 = w^4 w^3)
+template <int R>
+__device__ __forceinline__ void twiddle_powers(double2 w1, double2* w) {
+  w[1] = w1;
+  if constexpr (R > 2) {
+    w[2] = cmul(w1, w1);
+    w[3] = cmul(w[2], w1);
+  }
+  if constexpr (R > 4) {
+    w[4] = cmul(w[2], w[2]);
+    w[5] = cmul(w[4], w1);
+    w[6] = cmul(w[4], w[2]);
+    w[7] = cmul(w[4], w[3]);
+  }
+}
+
 // One in-place Stockham radix-R pass over the M-point slice in shared memory.
 // tw_stride converts an index in units of 1/M of a turn to the N-point table.
 template <int M, int R>
@@ -116,8 +134,10 @@ __device__ __forceinline__ void stockham_pass(double2* buf, int Ns, const double
     const int jm = j & (Ns - 1);
     if (Ns > 1) {
       const int qb = jm * (M / (Ns * R));
+      double2 w[R];
+      twiddle_powers<R>(twd(tw, qb * tw_stride, sign), w);
 #pragma unroll
-      for (int r = 1; r < R; ++r) v[u][r] = cmul(v[u][r], twd(tw, qb * r * tw_stride, sign));
+      for (int r = 1; r < R; ++r) v[u][r] = cmul(v[u][r], w[r]);
     }
     dft_small<R>(v[u], sign);
     const int idxD = (j - jm) * R + jm;
@@ -210,6 +230,138 @@ __device__ __noinline__ void fft_inverse(double2* buf, const double2* __restrict
     for (int u = 0; u < kPts; ++u) buf[pidx(threadIdx.x + u * T)] = acc[u];
     __syncthreads();
   }
+}
+
+}  // namespace hwdev
+
+namespace hwdev {
+
+// ---------------------------------------------------------------------------
+// Dual transforms: two M-point slices (A and B) in one sweep -- twice the
+// independent work per thread, one set of twiddle loads and barriers for both.
+// ---------------------------------------------------------------------------
+template <int M, int R>
+__device__ __forceinline__ void stockham_pass2(double2* A, double2* B, int Ns, const double2* __restrict__ tw,
+                                               int tw_stride, int sign) {
+  constexpr int T = M / kPts;
+  constexpr int NB = M / R;
+  constexpr int BPT = kPts / R;
+  double2 va[BPT][R], vb[BPT][R];
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int u = 0; u < BPT; ++u) {
+    const int j = tid + u * T;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      va[u][r] = A[pidx(j + r * NB)];
+      vb[u][r] = B[pidx(j + r * NB)];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < BPT; ++u) {
+    const int j = tid + u * T;
+    const int jm = j & (Ns - 1);
+    if (Ns > 1) {
+      const int qb = jm * (M / (Ns * R));
+      double2 w[R];
+      twiddle_powers<R>(twd(tw, qb * tw_stride, sign), w);
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        va[u][r] = cmul(va[u][r], w[r]);
+        vb[u][r] = cmul(vb[u][r], w[r]);
+      }
+    }
+    dft_small<R>(va[u], sign);
+    dft_small<R>(vb[u], sign);
+    const int idxD = (j - jm) * R + jm;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      A[pidx(idxD + r * Ns)] = va[u][r];
+      B[pidx(idxD + r * Ns)] = vb[u][r];
+    }
+  }
+  __syncthreads();
+}
+
+template <int M>
+__device__ __forceinline__ void local_fft2(double2* A, double2* B, const double2* __restrict__ tw, int tw_stride,
+                                           int sign) {
+  int Ns = 1;
+  constexpr int L8 = (M >= 512) ? 3 : (M >= 64 ? 2 : 1);
+  constexpr int rem = M / (1 << (3 * L8));
+#pragma unroll
+  for (int p = 0; p < L8; ++p) {
+    stockham_pass2<M, 8>(A, B, Ns, tw, tw_stride, sign);
+    Ns *= 8;
+  }
+  if constexpr (rem == 8) {
+    stockham_pass2<M, 8>(A, B, Ns, tw, tw_stride, sign);
+  } else if constexpr (rem == 4) {
+    stockham_pass2<M, 4>(A, B, Ns, tw, tw_stride, sign);
+  } else if constexpr (rem == 2) {
+    stockham_pass2<M, 2>(A, B, Ns, tw, tw_stride, sign);
+  }
+}
+
+// cross-CTA step of the distributed transform for both slices (see fft_forward /
+// fft_inverse): forward = C-point DFT then twiddle, inverse = twiddle then DFT.
+template <int M>
+__device__ __forceinline__ void cross_step2(double2* A, double2* B, const double2* __restrict__ tw, int N, int C,
+                                            int c, int sign) {
+  constexpr int T = M / kPts;
+  cg::cluster_group cl = cg::this_cluster();
+  cl.sync();
+  double2 sa[kPts], sb[kPts];
+  const int NC = N / C;
+#pragma unroll
+  for (int u = 0; u < kPts; ++u) {
+    const int i = threadIdx.x + u * T;
+    double2 a = make_double2(0.0, 0.0), b = make_double2(0.0, 0.0);
+    for (int r = 0; r < C; ++r) {
+      const double2* pa = cl.map_shared_rank(A, r);
+      const double2* pb = cl.map_shared_rank(B, r);
+      double2 xa = pa[pidx(i)], xb = pb[pidx(i)];
+      if (sign > 0) {   // inverse: peer r is the spectral class k1 = r
+        const double2 w = twd(tw, i * r, +1);
+        xa = cmul(xa, w);
+        xb = cmul(xb, w);
+      }
+      const double2 wc = twd(tw, ((r * c) % C) * NC, sign);
+      a = cadd(a, cmul(xa, wc));
+      b = cadd(b, cmul(xb, wc));
+    }
+    if (sign < 0) {
+      const double2 w = twd(tw, i * c, -1);
+      a = cmul(a, w);
+      b = cmul(b, w);
+    }
+    sa[u] = a;
+    sb[u] = b;
+  }
+  cl.sync();
+#pragma unroll
+  for (int u = 0; u < kPts; ++u) {
+    A[pidx(threadIdx.x + u * T)] = sa[u];
+    B[pidx(threadIdx.x + u * T)] = sb[u];
+  }
+  __syncthreads();
+}
+
+template <int M>
+__device__ __noinline__ void fft_forward2(double2* A, double2* B, const double2* __restrict__ tw, int N, int C,
+                                          int c) {
+  __syncthreads();
+  if (C > 1) cross_step2<M>(A, B, tw, N, C, c, -1);
+  local_fft2<M>(A, B, tw, C, -1);
+}
+
+template <int M>
+__device__ __noinline__ void fft_inverse2(double2* A, double2* B, const double2* __restrict__ tw, int N, int C,
+                                          int c) {
+  __syncthreads();
+  local_fft2<M>(A, B, tw, C, +1);
+  if (C > 1) cross_step2<M>(A, B, tw, N, C, c, +1);
 }
 
 }  // namespace hwdev

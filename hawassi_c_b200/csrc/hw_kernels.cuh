@@ -3,6 +3,7 @@
 #pragma once
 
 #include "hw_breaking.cuh"
+#include "hw_rhs_fast.cuh"
 #include "hw_kernels.h"
 #include "hw_stepper.cuh"
 
@@ -19,7 +20,7 @@ __global__ void __launch_bounds__(M / kPts, (4096 / M)) k_evolve(DevMember* mems
   const int mi = list[blockIdx.x / C];
   if (threadIdx.x == 0) sd = mems[mi];
   __syncthreads();
-  Ctx<M> X{sd, smem_buf, red, rank, int(threadIdx.x)};
+  Ctx<M> X{sd, smem_buf, smem_buf + padded(M), red, rank, int(threadIdx.x)};
   Bufs B;
   B.y = sd.y;
   B.yn = sd.ynew;
@@ -69,7 +70,7 @@ __global__ void __launch_bounds__(M / kPts, (4096 / M)) k_rhs(DevMember* mems, c
   const int mi = list[blockIdx.x / C];
   if (threadIdx.x == 0) sd = mems[mi];
   __syncthreads();
-  Ctx<M> X{sd, smem_buf, red, rank, int(threadIdx.x)};
+  Ctx<M> X{sd, smem_buf, smem_buf + padded(M), red, rank, int(threadIdx.x)};
   rhs_eval<M>(X, t, sd.kb[6]);
   member_sync(C);
   if (rank == 0 && threadIdx.x == 0) mems[mi].rhs_calls += 1;
@@ -78,7 +79,7 @@ __global__ void __launch_bounds__(M / kPts, (4096 / M)) k_rhs(DevMember* mems, c
 
 template <int M>
 cudaError_t set_attrs() {
-  const int bytes = padded(M) * int(sizeof(double2));
+  const int bytes = 2 * padded(M) * int(sizeof(double2));
   cudaError_t e;
   if ((e = cudaFuncSetAttribute(k_evolve<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
   if ((e = cudaFuncSetAttribute(k_rhs<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
@@ -91,7 +92,7 @@ cudaError_t launch(int mode, DevMember* mems, const int* list, int nmem, int C, 
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(unsigned(nmem * C));
   cfg.blockDim = dim3(M / kPts);
-  cfg.dynamicSmemBytes = size_t(padded(M)) * sizeof(double2);
+  cfg.dynamicSmemBytes = 2 * size_t(padded(M)) * sizeof(double2);
   cfg.stream = s;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;

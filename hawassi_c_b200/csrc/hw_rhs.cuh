@@ -16,6 +16,7 @@ struct Ctx {
   static constexpr int T = M / kPts;
   const DevMember& d;
   double2* buf;   // M-point FFT slice (padded) in shared memory
+  double2* buf2;  // second slice for the dual transforms
   double* red;    // reduction scratch in shared memory
   int c;          // rank of this CTA in the member's cluster
   int tid;
@@ -144,6 +145,9 @@ __device__ __noinline__ void hss(Ctx<M>& X, const double2* __restrict__ A, const
 template <int M>
 __device__ __noinline__ void breaking_rhs(Ctx<M>& X, double t, const double2* PE, const double* Heta, int heta_stride,
                              const double2* AEadj, double2* Rb);
+// HS2 flat-bottom fast path (hw_rhs_fast.cuh)
+template <int M>
+__device__ __noinline__ void rhs_hs2_flat(Ctx<M>& X, double t, double2* __restrict__ dz);
 
 // One RHS evaluation dz = f(t, zs), zs = [eta^ | u^] (permuted spectral, 2N).
 template <int M>
@@ -166,6 +170,10 @@ __device__ __noinline__ void rhs_eval(Ctx<M>& X, double t, double2* __restrict__
   double2* S10 = d.sc[10]; // spectral scratch
   double2* RB = d.sc[11];  // FFT(breaking force)
   const bool hs2 = d.model >= 2, hs3 = d.model == 3, brk = d.brk != 0, flat = d.flat != 0;
+  if (d.model == 2 && flat) {
+    rhs_hs2_flat<M>(X, t, dz);
+    return;
+  }
 
   member_sync(d.C);   // zs written by all CTAs of the member
 
