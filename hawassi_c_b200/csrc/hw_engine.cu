@@ -123,6 +123,11 @@ struct hw_ctx {
 
 static std::string g_create_err;
 
+// no-allocation RHS (hw_noalloc.cu)
+int hw_noalloc_max_nx();
+bool hw_noalloc_rhs_launch(const DevMember* mems, int mi, int N, int M, int C, double t, const double* y,
+                           double* dy, cudaStream_t s, std::string& err);
+
 namespace {
 
 std::vector<double> permute(const std::vector<double>& v, int N, int C, int M) {
@@ -529,6 +534,23 @@ int hw_rhs(hw_ctx* ctx, int m, double t, const double* y, double* dydt) {
     return true;
   };
   return body() ? 0 : 1;
+}
+
+int hw_rhs_noalloc(hw_ctx* ctx, int m, double t, const double* y_dev, double* dydt_dev, void* cuda_stream) {
+  if (!valid_member(ctx, m) || !y_dev || !dydt_dev) return 1;
+  int cur = -1;
+  if (cudaGetDevice(&cur) != cudaSuccess || cur != ctx->device) {
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) {
+      ctx->err = std::string("hw_rhs_noalloc: cudaSetDevice: ") + cudaGetErrorString(e);
+      return 1;
+    }
+  }
+  const HostMember& h = ctx->mem[size_t(m)];
+  return hw_noalloc_rhs_launch(ctx->d_mems, m, h.N, h.M, h.C, t, y_dev, dydt_dev,
+                               static_cast<cudaStream_t>(cuda_stream), ctx->err)
+             ? 0
+             : 1;
 }
 
 int hw_gsl_rhs(double t, const double* y, double* dydt, void* params) {

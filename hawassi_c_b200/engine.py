@@ -36,7 +36,7 @@ EXPORTS = [
     "hw_initial_state", "hw_rhs", "hw_gsl_rhs", "hw_evolve_apply", "hw_run", "hw_run_to_time",
     "hw_get_state", "hw_set_state", "hw_reset", "hw_member_stats", "hw_last_dydt", "hw_breaking_log",
     "hw_set_stream", "hw_synchronize", "hw_deck_table", "hw_get_states", "hw_set_states",
-    "hw_class_timing",
+    "hw_class_timing", "hw_rhs_noalloc",
 ]
 
 
@@ -75,6 +75,7 @@ def load_library():
     L.hw_set_stream.argtypes = [vp, vp]
     L.hw_synchronize.argtypes = [vp]
     L.hw_deck_table.argtypes = [ctypes.c_char_p, ctypes.POINTER(HwOpts), ctypes.c_char_p, dp, ip]
+    L.hw_rhs_noalloc.argtypes = [vp, ip, dd, vp, vp, vp]
     L.hw_get_states.argtypes = [vp, dp]
     L.hw_set_states.argtypes = [vp, dp]
     L.hw_class_timing.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ip]
@@ -142,6 +143,13 @@ class Engine:
         dz = np.empty_like(y)
         self._check(load_library().hw_rhs(self._h, member, float(t), _dp(y), _dp(dz)), "rhs")
         return dz
+
+    def rhs_noalloc(self, t, y_dev_ptr, dydt_dev_ptr, stream=0, member=0):
+        """RHS on caller-owned device buffers (reference layout) with no device
+        allocation at call time; asynchronous on `stream` (a cudaStream_t value)."""
+        rc = load_library().hw_rhs_noalloc(self._h, member, float(t), ctypes.c_void_p(y_dev_ptr),
+                                           ctypes.c_void_p(dydt_dev_ptr), ctypes.c_void_p(stream))
+        self._check(rc, "rhs_noalloc")
 
     def evolve_apply(self, t, t1, h, y, member=0):
         """In place on y; returns (t, h) like gsl_odeiv_evolve_apply's outputs."""

@@ -56,6 +56,19 @@ int hw_rhs(hw_ctx* ctx, int member, double t, const double* y, double* dydt);
  *   gsl_odeiv_system sys = {hw_gsl_rhs, NULL, 4 * Nx, ctx};   (1d/functions.c:71-89) */
 int hw_gsl_rhs(double t, const double* y, double* dydt, void* params);
 
+/* No counterpart in the reference.  One RHS evaluation like hw_rhs, for callers
+ * that cannot allocate device memory at call time (for instance code that runs
+ * under a device-memory budget managed by another framework's pool, or that must
+ * not trigger allocations between set-up and tear-down).  y_dev and dydt_dev are
+ * DEVICE pointers (4*Nx doubles, reference layout) owned by the caller; the call
+ * allocates nothing: its scratch is a 1 MiB static device array held by every GPU
+ * that loads the library, so Nx is limited to 4096 (larger grids are rejected with
+ * an error).  The first call on a device looks up the array's device address;
+ * make that call before any stream capture.  All calls share the one array:
+ * calls that overlap on the GPU (different streams, contexts or threads) race.
+ * No scratch field needs to start at zero.  cuda_stream NULL: the default stream. */
+int hw_rhs_noalloc(hw_ctx* ctx, int member, double t, const double* y_dev, double* dydt_dev, void* cuda_stream);
+
 /* Replaces gsl_odeiv_evolve_apply(e, c, s, &sys, &t, t1, &h, y) with rkf45 and
  * control_y (1d/functions.c:550): one accepted step, whole step on the device. */
 int hw_evolve_apply(hw_ctx* ctx, int member, double* t, double t1, double* h, double* y);
