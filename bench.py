@@ -85,7 +85,7 @@ def _cpu_worker(args):
             c0 = o.stats()[0]
             stop = min(i + window, len(tt))
             for ti in tt[i:stop]:
-                while t < ti:
+                while t < ti and time.perf_counter() - t_start <= max_seconds:
                     t, h = o.evolve_apply(t, ti, h, y)
             mb[2], mb[3], mb[5] = t, h, stop
             pts += (o.stats()[0] - c0) * o.nx

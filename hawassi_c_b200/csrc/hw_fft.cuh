@@ -23,9 +23,10 @@ namespace cg = cooperative_groups;
 
 constexpr int kPts = 8;  // points per thread
 
-// bank skew: keeps radix-8 Stockham strides (1, 8, 64, 512) conflict-free
-__device__ __forceinline__ int pidx(int i) { return i + (i >> 3) + (i >> 6) + (i >> 9); }
-__host__ __device__ constexpr int padded(int m) { return m + (m >> 3) + (m >> 6) + (m >> 9) + 1; }
+// bank skew: one pad slot per 8 double2 keeps the stride-8 stores of the first
+// Stockham pass conflict-free (all other accesses are unit-stride)
+__device__ __forceinline__ int pidx(int i) { return i + (i >> 3); }
+__host__ __device__ constexpr int padded(int m) { return m + (m >> 3) + 1; }
 
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
@@ -168,6 +169,70 @@ __device__ __forceinline__ void local_fft(double2* buf, const double2* __restric
   }
 }
 
+
+// Cross-CTA step of the distributed transform, as gather / C-point DFT / scatter:
+// the M positions of the slice are shared out over the C*T threads of the cluster;
+// the thread owning position i gathers the C values at i from every CTA's slice,
+// applies the C-point DFT (forward: then the twiddles W_N^(i k1); inverse: the
+// twiddles W_N^-(i k1) first) and stores output j into CTA j's slice at i.
+template <int M, int C, int NBUF>
+__device__ __forceinline__ void cross_gs(double2* A, double2* B, const double2* __restrict__ tw, int c, int sign) {
+  constexpr int T = M / kPts;
+  constexpr int PER = kPts / C;   // positions per thread
+  cg::cluster_group cl = cg::this_cluster();
+  double2 va[PER][C], vb[PER][C];
+  cl.sync();
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int i = c * T + threadIdx.x + q * (C * T);
+#pragma unroll
+    for (int r = 0; r < C; ++r) {
+      va[q][r] = cl.map_shared_rank(A, r)[pidx(i)];
+      if constexpr (NBUF == 2) vb[q][r] = cl.map_shared_rank(B, r)[pidx(i)];
+    }
+  }
+  cl.sync();
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int i = c * T + threadIdx.x + q * (C * T);
+    double2 w[C > 1 ? C : 2];
+    if (sign > 0) {   // inverse: twiddle by W_N^(+i k1) before the DFT over k1
+      twiddle_powers<C>(twd(tw, i, +1), w);
+#pragma unroll
+      for (int r = 1; r < C; ++r) {
+        va[q][r] = cmul(va[q][r], w[r]);
+        if constexpr (NBUF == 2) vb[q][r] = cmul(vb[q][r], w[r]);
+      }
+    }
+    dft_small<C>(va[q], sign);
+    if constexpr (NBUF == 2) dft_small<C>(vb[q], sign);
+    if (sign < 0) {   // forward: output k1 gets W_N^(-i k1)
+      twiddle_powers<C>(twd(tw, i, -1), w);
+#pragma unroll
+      for (int r = 1; r < C; ++r) {
+        va[q][r] = cmul(va[q][r], w[r]);
+        if constexpr (NBUF == 2) vb[q][r] = cmul(vb[q][r], w[r]);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < C; ++r) {
+      cl.map_shared_rank(A, r)[pidx(i)] = va[q][r];
+      if constexpr (NBUF == 2) cl.map_shared_rank(B, r)[pidx(i)] = vb[q][r];
+    }
+  }
+  cl.sync();
+}
+
+// dispatch on the cluster size (2, 4, 8); returns false for other sizes
+template <int M, int NBUF>
+__device__ __forceinline__ bool cross_fast(double2* A, double2* B, const double2* __restrict__ tw, int C, int c,
+                                           int sign) {
+  if (C == 2) { cross_gs<M, 2, NBUF>(A, B, tw, c, sign); return true; }
+  if (C == 4) { cross_gs<M, 4, NBUF>(A, B, tw, c, sign); return true; }
+  if (C == 8) { cross_gs<M, 8, NBUF>(A, B, tw, c, sign); return true; }
+  return false;
+}
+
 // cluster-wide barrier (block barrier when the member is a single CTA)
 __device__ __forceinline__ void member_sync(int C) {
   if (C > 1) cg::this_cluster().sync();
@@ -178,6 +243,10 @@ __device__ __forceinline__ void member_sync(int C) {
 template <int M>
 __device__ __noinline__ void fft_forward(double2* buf, const double2* __restrict__ tw, int N, int C, int c) {
   if (C == 1) __syncthreads();
+  if (C > 1 && cross_fast<M, 1>(buf, buf, tw, C, c, -1)) {
+    local_fft<M>(buf, tw, C, -1);
+    return;
+  }
   if (C > 1) {
     constexpr int T = M / kPts;
     cg::cluster_group cl = cg::this_cluster();
@@ -208,6 +277,10 @@ template <int M>
 __device__ __noinline__ void fft_inverse(double2* buf, const double2* __restrict__ tw, int N, int C, int c) {
   __syncthreads();
   local_fft<M>(buf, tw, C, +1);
+  if (C > 1 && cross_fast<M, 1>(buf, buf, tw, C, c, +1)) {
+    __syncthreads();
+    return;
+  }
   if (C > 1) {
     constexpr int T = M / kPts;
     cg::cluster_group cl = cg::this_cluster();
@@ -352,7 +425,7 @@ template <int M>
 __device__ __noinline__ void fft_forward2(double2* A, double2* B, const double2* __restrict__ tw, int N, int C,
                                           int c) {
   __syncthreads();
-  if (C > 1) cross_step2<M>(A, B, tw, N, C, c, -1);
+  if (C > 1 && !cross_fast<M, 2>(A, B, tw, C, c, -1)) cross_step2<M>(A, B, tw, N, C, c, -1);
   local_fft2<M>(A, B, tw, C, -1);
 }
 
@@ -361,7 +434,10 @@ __device__ __noinline__ void fft_inverse2(double2* A, double2* B, const double2*
                                           int c) {
   __syncthreads();
   local_fft2<M>(A, B, tw, C, +1);
-  if (C > 1) cross_step2<M>(A, B, tw, N, C, c, +1);
+  if (C > 1) {
+    if (!cross_fast<M, 2>(A, B, tw, C, c, +1)) cross_step2<M>(A, B, tw, N, C, c, +1);
+    __syncthreads();
+  }
 }
 
 }  // namespace hwdev
