@@ -719,6 +719,9 @@ int hw_deck_table(const char* workdir, const hw_opts* opts, const char* name, do
   else if (nm == "insig_skew") v = m.insig_skew; else if (nm == "ttrace") v = m.ttrace; else if (nm == "y0") v = m.y0;
   else if (nm == "gamX") { v = m.gamX_re; v.insert(v.end(), m.gamX_im.begin(), m.gamX_im.end()); }
   else if (nm == "gamX_skew") { v = m.gamXs_re; v.insert(v.end(), m.gamXs_im.begin(), m.gamXs_im.end()); }
+  else if (nm == "CsqK" || nm == "gamK") {
+    for (const auto& r : (nm == "CsqK" ? m.Csq_ref : m.gam_ref)) v.insert(v.end(), r.begin(), r.end());
+  }
   else if (nm.rfind("gam_", 0) == 0 || nm.rfind("Csq_", 0) == 0) {
     // gam_min / gam_plus / gam_mid and Csq_* in the reference's naming (ref order min, plus, mid)
     const int j = nm.find("min") != std::string::npos ? 0 : nm.find("plus") != std::string::npos ? 1 : 2;
@@ -795,6 +798,28 @@ int hw_class_timing(hw_ctx* ctx, double* ms, int* members, int* grid_n, int cap)
     if (grid_n) grid_n[i] = c.M * c.C;
   }
   return n;
+}
+
+int hw_energy(hw_ctx* ctx, int m, const double* y, double* energy) {
+  if (!valid_member(ctx, m) || !energy) return 1;
+  const hw::Member& mb = ctx->mem[size_t(m)].m;
+  const int N = mb.Nx;
+  std::vector<double> own;
+  if (!y) {
+    own.resize(size_t(4) * N);
+    if (hw_get_state(ctx, m, nullptr, nullptr, own.data()) != 0) return 1;
+    y = own.data();
+  }
+  // quadratic Hamiltonian 1/2 int (g eta^2 + u (C^2/g) u) dx in spectral form (Parseval),
+  // C^2 at the depth of the influx point
+  double s = 0.0;
+  for (int k = 0; k < N; ++k) {
+    const double e2 = y[k] * y[k] + y[N + k] * y[N + k];
+    const double u2 = y[2 * N + k] * y[2 * N + k] + y[3 * N + k] * y[3 * N + k];
+    s += hwdev::kG * e2 + mb.Csqr[size_t(k)] / hwdev::kG * u2;
+  }
+  *energy = 0.5 * s * mb.dx / N;
+  return 0;
 }
 
 int hw_set_stream(hw_ctx* ctx, void* s) {

@@ -450,6 +450,33 @@ void interp_two_three(Member& m, double nu, int three, double D_min, double D_mi
   }
 }
 
+// K reference depths (K > 3, no counterpart in the reference): log-spaced between
+// the shallowest and the deepest point; each point uses the two-reference system of
+// Up2IP (1d/functions.c:2195-2245) on its bracketing pair, solved at its own depth.
+void interp_k(Member& m, double nu, int K, double Dmin, double Dmax) {
+  const int Nx = m.Nx;
+  std::vector<double> D(K);
+  for (int j = 0; j < K; ++j) D[j] = Dmin * std::pow(Dmax / Dmin, double(j) / double(K - 1));
+  D[0] = Dmin;
+  D[K - 1] = Dmax;
+  m.Csq_ref.assign(K, std::vector<double>(Nx));
+  m.gam_ref.assign(K, std::vector<double>(Nx, 0.0));
+  for (int j = 0; j < K; ++j)
+    for (int i = 0; i < Nx; ++i) m.Csq_ref[j][i] = std::pow(phase_velocity_i(m.k[i], D[j]), 2);
+  for (int i = 0; i < Nx; ++i) {
+    const double h = m.depth[i];
+    int j = 0;
+    while (j < K - 2 && h > D[j + 1]) ++j;
+    const double kap = invers_omega(nu, h);
+    const double Cp_a = std::pow(phase_velocity_i(kap, D[j]), 2), Cp_b = std::pow(phase_velocity_i(kap, D[j + 1]), 2);
+    const double Cp_h = std::pow(phase_velocity_i(kap, h), 2);
+    const double Om_a = omega_i(kap, D[j]), Om_b = omega_i(kap, D[j + 1]), Om_h = omega_i(kap, h);
+    const double det = Cp_a * Om_b - Cp_b * Om_a;
+    m.gam_ref[j][i] = (Om_b * Cp_h - Cp_b * Om_h) / det;
+    m.gam_ref[j + 1][i] = (-Om_a * Cp_h + Cp_a * Om_h) / det;
+  }
+}
+
 }  // namespace
 
 void host_dft(std::vector<double>& re, std::vector<double>& im, int sign) {
@@ -792,8 +819,10 @@ bool build_member(const std::string& dir, const SetupOptions& opt, Member& m, st
       double Dmid = (Dmax + Dmin) / 2;
       if (!d.mid_temp.empty() && d.mid_temp != "default") Dmid = mid1;
       interp_two_three(m, m.nu_peak, m.nref == 3, Dmin, Dmid, Dmax);
+    } else if (m.nref <= 16) {
+      interp_k(m, m.nu_peak, m.nref, Dmin, Dmax);
     } else {
-      err = "more than 3 reference depths needs the K-reference operator";
+      err = "at most 16 reference depths";
       return false;
     }
   }

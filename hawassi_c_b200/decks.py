@@ -210,3 +210,23 @@ def ensemble_member_deck(path, seed, T_end=100.0, breaking=True):
     return write_deck(path, nx=nx, length=length, xinflux=0.1 * length, depth=depth, model="HS2",
                       breaking=breaking, T_end=T_end, n_samples=2048, n_lines=1024, Hs=Hs, Tp=Tp, gamma=gamma,
                       seed=seed, damp=(0.05 * length, 0.05 * length), adjcoef=0.5)
+
+
+def config2_deck(path, seed=0, T_end=200.0, nx=16384, length=400.0):
+    """1D varying bathymetry with breaking: L=400 m, Nx=16384, 1.0 m flat up to x=150 m,
+    then a 1:30 slope to 0.05 m; HS3; breaking KBC 0.8, TC 0.2, Tchar 0.5; JONSWAP
+    Hs 0.15 m, Tp 2.5 s, gamma 3.3 with seeded phases; influx at x=20 m."""
+    bath = slope_bathymetry(nx, length, h0=1.0, x_toe=150.0, slope=1.0 / 30.0, h_min=0.05)
+    return write_deck(path, nx=nx, length=length, xinflux=20.0, depth=1.0, bath=bath, model="HS3", breaking=True,
+                      T_end=T_end, n_samples=2048, n_lines=1024, Hs=0.15, Tp=2.5, gamma=3.3, seed=seed,
+                      damp=(10.0, 10.0), adjcoef=0.5, kbc=0.8, tc=0.2, tchar=0.5)
+
+
+def config4_deck(path, seed=0, T_end=100.0, nx=16384, length=400.0):
+    """Random bathymetry for the learned depth operator: L=400 m, Nx=16384, depth in
+    [0.05, 2.0] m from 8 seeded Gaussian bumps/troughs, HS2, JONSWAP influx."""
+    bath = bump_bathymetry(nx, length, seed, n_bumps=8, h_min=0.05, h_max=2.0)
+    u = splitmix64_uniform(31 * seed + 5, 3)
+    return write_deck(path, nx=nx, length=length, xinflux=20.0, depth=float(bath.max()), bath=bath, model="HS2",
+                      breaking=False, T_end=T_end, n_samples=2048, n_lines=1024, Hs=0.05 + 0.1 * u[0],
+                      Tp=1.5 + 1.5 * u[1], gamma=1.0 + 4.0 * u[2], seed=seed, damp=(10.0, 10.0), adjcoef=0.5)

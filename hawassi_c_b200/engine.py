@@ -36,7 +36,7 @@ EXPORTS = [
     "hw_initial_state", "hw_rhs", "hw_gsl_rhs", "hw_evolve_apply", "hw_run", "hw_run_to_time",
     "hw_get_state", "hw_set_state", "hw_reset", "hw_member_stats", "hw_last_dydt", "hw_breaking_log",
     "hw_set_stream", "hw_synchronize", "hw_deck_table", "hw_get_states", "hw_set_states",
-    "hw_class_timing", "hw_rhs_noalloc",
+    "hw_class_timing", "hw_rhs_noalloc", "hw_energy",
 ]
 
 
@@ -76,6 +76,7 @@ def load_library():
     L.hw_synchronize.argtypes = [vp]
     L.hw_deck_table.argtypes = [ctypes.c_char_p, ctypes.POINTER(HwOpts), ctypes.c_char_p, dp, ip]
     L.hw_rhs_noalloc.argtypes = [vp, ip, dd, vp, vp, vp]
+    L.hw_energy.argtypes = [vp, ip, dp, dp]
     L.hw_get_states.argtypes = [vp, dp]
     L.hw_set_states.argtypes = [vp, dp]
     L.hw_class_timing.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ip]
@@ -191,6 +192,14 @@ class Engine:
         self._check(load_library().hw_member_stats(self._h, member, ctypes.byref(a), ctypes.byref(b),
                                                    ctypes.byref(c), ctypes.byref(s)), "stats")
         return {"rhs_calls": a.value, "accepted": b.value, "rejected": c.value, "status": s.value}
+
+    def energy(self, y=None, member=0):
+        """Quadratic Hamiltonian of y (host state) or of the member's current state."""
+        e = np.zeros(1)
+        yy = None if y is None else np.ascontiguousarray(y, dtype=np.float64)
+        self._check(load_library().hw_energy(self._h, member, _dp(yy) if yy is not None else None, _dp(e)),
+                    "energy")
+        return float(e[0])
 
     def last_dydt(self, member=0):
         y = np.zeros(4 * self.nx[member])

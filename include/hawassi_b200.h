@@ -24,7 +24,9 @@ typedef struct hw_opts {
     double eps_rel;          /* <= 0: the reference's 1e-4 (1d/functions.c:530) */
     double h0;               /* <= 0: the reference's first step 1e-4 (1d/functions.c:541) */
     unsigned long long seed; /* phase seed for wavename = jonswap (reference: srand(time(0))) */
-    int nref;                /* varying depth: 0 or 3 = three reference depths (Up3IP), 2 = Up2IP */
+    int nref;                /* varying depth: 0 or 3 = three reference depths (Up3IP), 2 = Up2IP,
+                                4..16 = that many log-spaced reference depths, each point on its
+                                bracketing pair (no counterpart in the reference) */
     int exact_sequence;      /* 1: evaluate the RHS exactly where GSL does even when it is stateless */
     int cluster;             /* CTAs per member, power of two (0 = automatic) */
     int device;              /* CUDA device ordinal */
@@ -106,6 +108,12 @@ int hw_set_states(hw_ctx* ctx, const double* y_all);
 /* Device time (ms) of the last hw_run launch of each grid-size class, with the
  * class's member count and grid size; returns the number of classes. */
 int hw_class_timing(hw_ctx* ctx, double* ms, int* members, int* grid_n, int cap);
+
+/* Energy diagnostic (no counterpart in the reference): the quadratic Hamiltonian
+ * 1/2 int (g eta^2 + u (C^2/g) u) dx of a state in spectral form (Parseval), with C^2
+ * at the influx depth.  y: a host state in the reference layout, or NULL for the
+ * member's current state. */
+int hw_energy(hw_ctx* ctx, int member, const double* y, double* energy);
 
 /* Host-only (no GPU needed): build the set-up of <workdir> and copy the named table
  * (x, k, depth, dampchar, dampcoef, aal, ChiAdj, Csqr, L, M0im, gamX, gamX_skew, insig,

@@ -370,6 +370,7 @@ struct or_ctx {
     /* operators */
     double *Csqr, *L, *M0im;
     double *Csq_min, *Csq_mid, *Csq_plus, *gam_min, *gam_mid, *gam_plus;
+    double *CsqK, *gamK;   /* K > 3 reference depths: [K][Nx] */
 
     /* breaking (1d/header.h:79-83,106-109) */
     int brk;
@@ -888,6 +889,36 @@ static void up_ip(or_ctx* c, double nu, int three) {
     free(Dd); free(gm); free(gc); free(gp);
 }
 
+/* K-reference operator (no counterpart in the reference, which stops at 3): K
+ * log-spaced reference depths D_0 < ... < D_{K-1} spanning [min h, max h]; each point
+ * takes the two-reference system of Up2IP (1d/functions.c:2195-2245) on its
+ * bracketing pair, solved at its own depth (no 101-sample spline), so at most two of
+ * the K weights are nonzero at any point. */
+static void up_k(or_ctx* c, double nu, int K) {
+    int Nx = c->Nx;
+    double D_min = search_min_val(c->depth, Nx), D_plus = search_max_val(c->depth, Nx);
+    double* D = (double*)malloc(sizeof(double) * (size_t)K);
+    for (int j = 0; j < K; j++) D[j] = D_min * pow(D_plus / D_min, (double)j / (double)(K - 1));
+    D[0] = D_min; D[K - 1] = D_plus;
+    c->CsqK = (double*)calloc((size_t)K * Nx, sizeof(double));
+    c->gamK = (double*)calloc((size_t)K * Nx, sizeof(double));
+    for (int j = 0; j < K; j++)
+        for (int i = 0; i < Nx; i++) c->CsqK[(size_t)j * Nx + i] = pow(phase_velocity_i(c->k[i], D[j]), 2);
+    for (int i = 0; i < Nx; i++) {
+        double h = c->depth[i];
+        int j = 0;
+        while (j < K - 2 && h > D[j + 1]) j++;
+        double kap = invers_omega(nu, h);
+        double Cp_a = pow(phase_velocity_i(kap, D[j]), 2), Cp_b = pow(phase_velocity_i(kap, D[j + 1]), 2);
+        double Cp_h = pow(phase_velocity_i(kap, h), 2);
+        double Om_a = omega_i(kap, D[j]), Om_b = omega_i(kap, D[j + 1]), Om_h = omega_i(kap, h);
+        double det = Cp_a * Om_b - Cp_b * Om_a;
+        c->gamK[(size_t)j * Nx + i] = (Om_b * Cp_h - Cp_b * Om_h) / det;
+        c->gamK[(size_t)(j + 1) * Nx + i] = (-Om_a * Cp_h + Cp_a * Om_h) / det;
+    }
+    free(D);
+}
+
 /* define_operator (1d/functions.c:2828) + alias (1d/functions.c:1774) */
 static void define_operator(or_ctx* c, double nu) {
     int Nx = c->Nx;
@@ -897,6 +928,8 @@ static void define_operator(or_ctx* c, double nu) {
             c->L[i] = pow(c->k[i], 2) * pow(phase_velocity_i(c->k[i], c->depthinf), 2) / G;
             c->M0im[i] = -c->k[i] * c->Csqr[i] / G;
         }
+    } else if (c->nref > 3) {
+        up_k(c, nu, c->nref);
     } else {
         up_ip(c, nu, c->nref != 2);
     }
@@ -914,7 +947,8 @@ static void ctx_free(or_ctx* c) {
                   c->x, c->k, c->depth, c->dampchar, c->dampcoef, c->spatgamX, c->Ug, c->aal, c->ChiAdj, c->gauge, c->gamX, c->gamX_skew,
                   c->temp_wave, c->temp_u, c->Csqr, c->L, c->M0im, c->Csq_min, c->Csq_mid, c->Csq_plus, c->gam_min, c->gam_mid, c->gam_plus,
                   c->CrestBreak, c->CrestBreakNew, c->CrestBreakPrev, c->ID_Node_end, c->Break_nodes, c->B, c->blog, c->dy, c->Rb_hat,
-                  c->y0, c->yerr, c->dydt_in, c->dydt_out, c->k1, c->k2, c->k3, c->k4, c->k5, c->k6, c->ytmp};
+                  c->y0, c->yerr, c->dydt_in, c->dydt_out, c->k1, c->k2, c->k3, c->k4, c->k5, c->k6, c->ytmp,
+                  c->CsqK, c->gamK};
     for (size_t i = 0; i < sizeof ps / sizeof ps[0]; i++) free(ps[i]);
     cspline_free(&c->sp_in); cspline_free(&c->sp_skew);
     plan_free(&c->plan);
@@ -1091,9 +1125,32 @@ static void fft_rc_nx(or_ctx* c, const double* in, cpx* out) {
 static double p1ik_re(double a, double br, double bi) { (void)br; return (0.0 * br) - (a * bi); }
 static double p1ik_im(double a, double br, double bi) { (void)bi; return (0.0 * bi) + (a * br); }
 
+/* HSS over K > 3 references: 1/2 sum_j [F(gam_j Re F^-1(Csq_j u^)) + Csq_j F(gam_j Re F^-1(u^))] */
+static void HSS_K(or_ctx* c, const cpx* uh, cpx* out) {
+    int Nx = c->Nx, K = c->nref;
+    double *iu = dnew(Nx), *is = dnew(Nx), *a = dnew(Nx), *b = dnew(Nx);
+    cpx *Cu = cnew(Nx), *F1 = cnew(Nx), *F2 = cnew(Nx);
+    ifft_cr_nx(c, uh, iu);
+    for (int i = 0; i < Nx; i++) { out[i].re = 0; out[i].im = 0; }
+    for (int j = 0; j < K; j++) {
+        const double* Cs = c->CsqK + (size_t)j * Nx;
+        const double* gm = c->gamK + (size_t)j * Nx;
+        for (int i = 0; i < Nx; i++) { Cu[i].re = Cs[i] * uh[i].re; Cu[i].im = Cs[i] * uh[i].im; }
+        ifft_cr_nx(c, Cu, is);
+        for (int i = 0; i < Nx; i++) { a[i] = gm[i] * is[i]; b[i] = gm[i] * iu[i]; }
+        fft_rc_nx(c, a, F1); fft_rc_nx(c, b, F2);
+        for (int i = 0; i < Nx; i++) {
+            out[i].re += (F1[i].re + Cs[i] * F2[i].re) / 2;
+            out[i].im += (F1[i].im + Cs[i] * F2[i].im) / 2;
+        }
+    }
+    free(iu); free(is); free(a); free(b); free(Cu); free(F1); free(F2);
+}
+
 /* HSS (1d/functions.c:2861-2977): varying-depth operator with 2 or 3 refs */
 static void HSS(or_ctx* c, const cpx* uh, cpx* out) {
     int Nx = c->Nx;
+    if (c->nref > 3) { HSS_K(c, uh, out); return; }
     cpx *Cm = cnew(Nx), *Cp = cnew(Nx);
     for (int i = 0; i < Nx; i++) {
         Cm[i].re = c->Csq_min[i] * uh[i].re; Cm[i].im = c->Csq_min[i] * uh[i].im;
@@ -1735,6 +1792,7 @@ int or_table(const or_ctx* c, const char* nm, double* out, int cap) {
     R("insig", c->insig, c->n) R("insig_skew", c->insig_skew, c->n) R("ttrace", c->ttrace, c->n) R("dy", c->dy, 4 * Nx)
     R("spatgamX", c->spatgamX, Nx) R("B", c->B, Nx) R("gauge", c->gauge, c->ngauge)
     C("gamX", c->gamX) C("gamX_skew", c->gamX_skew) C("Rb_hat", c->Rb_hat)
+    R("CsqK", c->CsqK, (c->CsqK ? c->nref * Nx : 0)) R("gamK", c->gamK, (c->gamK ? c->nref * Nx : 0))
 #undef R
 #undef C
     return -1;

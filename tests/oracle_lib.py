@@ -93,7 +93,7 @@ class Oracle:
         return lib().or_scalar(self.h, name.encode())
 
     def table(self, name):
-        cap = 4 * max(self.nx, self.n) + 16
+        cap = 16 * max(self.nx, self.n) + 16
         out = np.zeros(cap)
         m = lib().or_table(self.h, name.encode(), _p(out), cap)
         if m < 0:

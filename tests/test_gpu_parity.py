@@ -30,6 +30,21 @@ CASES = [
     ("hs2_flat_256", 256, "HS2", False, 1),
 ]
 
+KREF_CASES = [(1024, "HS2", 4, 1), (1024, "HS3", 16, 1), (2048, "HS3", 16, 2), (4096, "HS2", 16, 2)]
+
+
+@pytest.mark.parametrize("nx,model,nref,cluster", KREF_CASES)
+def test_rhs_parity_kref(tmp_path, nx, model, nref, cluster):
+    """The K-reference varying-depth operator (no counterpart in the reference:
+    K log-spaced reference depths, two-reference system per bracketing pair)."""
+    deck = small_deck(tmp_path, f"k{nref}_{nx}_{model}", nx=nx, model=model, varying=True)
+    o = ol.Oracle(deck, nref=nref)
+    e = hw.Engine(deck, cluster=cluster, nref=nref)
+    for i, t in enumerate([0.0, 3.3]):
+        y = random_state(nx, 70 + i)
+        assert rel_l2(e.rhs(t, y), o.rhs(t, y)) < 1e-12
+    e.close()
+
 
 @pytest.mark.parametrize("name,nx,model,varying,cluster", CASES)
 def test_rhs_parity(tmp_path, name, nx, model, varying, cluster):
@@ -70,21 +85,21 @@ def _eta_u(y, nx):
     return np.fft.ifft(eh).real, np.fft.ifft(uh).real
 
 
-@pytest.mark.parametrize("nx,model,varying,cluster", [(1024, "HS2", False, 1), (2048, "HS3", True, 2),
-                                                      (4096, "HS2", False, 2)])
-def test_run_parity(tmp_path, nx, model, varying, cluster):
+@pytest.mark.parametrize("nx,model,varying,cluster,nref", [(1024, "HS2", False, 1, 0), (2048, "HS3", True, 2, 0),
+                                                           (4096, "HS2", False, 2, 0), (2048, "HS3", True, 1, 16)])
+def test_run_parity(tmp_path, nx, model, varying, cluster, nref):
     deck = small_deck(tmp_path, f"run_{nx}_{model}", nx=nx, model=model, varying=varying, T_end=6.0)
-    o = ol.Oracle(deck, eps_abs=1e-8, eps_rel=1e-6)
+    o = ol.Oracle(deck, eps_abs=1e-8, eps_rel=1e-6, nref=nref)
     tim, _, _ = o.run()
     y_ref = np.zeros(4 * nx)
     # the oracle's run owns its state; re-run by stepping to read the final state
-    o2 = ol.Oracle(deck, eps_abs=1e-8, eps_rel=1e-6)
+    o2 = ol.Oracle(deck, eps_abs=1e-8, eps_rel=1e-6, nref=nref)
     t, h = float(o2.table("ttrace")[0]), 1e-4
     y_ref = o2.initial_state()
     for ti in o2.table("ttrace"):
         while t < ti:
             t, h = o2.evolve_apply(t, ti, h, y_ref)
-    e = hw.Engine(deck, cluster=cluster, eps_abs=1e-8, eps_rel=1e-6)
+    e = hw.Engine(deck, cluster=cluster, eps_abs=1e-8, eps_rel=1e-6, nref=nref)
     e.run()
     tg, hg, yg = e.state()
     assert tg == pytest.approx(t, rel=1e-12)
@@ -94,3 +109,5 @@ def test_run_parity(tmp_path, nx, model, varying, cluster):
     assert rel_l2(ug, ur) < 1e-9
     st = e.stats()
     assert st["status"] == 0 and st["accepted"] > 10
+    # energy diagnostic: same spectral form on both sides
+    assert e.energy() == pytest.approx(e.energy(y_ref), rel=1e-6)

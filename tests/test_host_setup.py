@@ -1,0 +1,82 @@
+"""CPU tests of the product's host side (no GPU): the C++ deck parser and table
+set-up against the oracle, the deck writer, and the C ABI's exported symbols."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+from decks_util import small_deck
+from hawassi_c_b200 import decks, engine
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+TABLES = ["x", "k", "depth", "dampchar", "dampcoef", "aal", "ChiAdj", "Csqr", "gamX", "gamX_skew", "insig",
+          "insig_skew", "ttrace"]
+SCALARS = ["Nx", "n", "dx", "nu_peak", "kp", "lambda_p", "Hs_in", "MaxEtaInit"]
+
+
+def _compare(deck, nref=0):
+    o = ol.Oracle(deck, nref=nref)
+    for nm in TABLES:
+        a, b = o.table(nm), engine.deck_table(deck, nm, nref=nref)
+        assert a.size == b.size, nm
+        np.testing.assert_allclose(b, a, rtol=0, atol=1e-13 * max(1.0, np.abs(a).max()), err_msg=nm)
+    for nm in SCALARS:
+        assert engine.deck_table(deck, nm, nref=nref)[0] == pytest.approx(o.scalar(nm), rel=1e-14), nm
+    np.testing.assert_allclose(engine.deck_table(deck, "y0", nref=nref), o.initial_state(), rtol=0, atol=1e-12)
+    return o
+
+
+def test_golden_deck_setup(golden_dir):
+    o = _compare(os.path.join(golden_dir, "fbr005"))
+    assert o.scalar("breaking") == 1
+
+
+@pytest.mark.parametrize("model,varying,nref", [("HS2", False, 0), ("HS3", True, 0), ("HS3", True, 2),
+                                                ("HS2", True, 16), ("HS1", False, 0)])
+def test_synthetic_deck_setup(tmp_path, model, varying, nref):
+    deck = small_deck(tmp_path, f"d_{model}_{nref}", nx=1024, model=model, varying=varying)
+    o = _compare(deck, nref)
+    if varying:
+        if nref > 3:
+            np.testing.assert_array_equal(engine.deck_table(deck, "gamK", nref=nref), o.table("gamK"))
+        else:
+            for nm in ("gam_min", "gam_plus", "Csq_min", "Csq_plus"):
+                np.testing.assert_array_equal(engine.deck_table(deck, nm, nref=nref), o.table(nm))
+
+
+def test_config_decks_parse(tmp_path):
+    d1 = decks.config1_deck(str(tmp_path / "c1"), seed=2)
+    assert engine.deck_table(d1, "Nx")[0] == 4096
+    assert engine.deck_table(d1, "n")[0] == 2048
+    d2 = decks.config2_deck(str(tmp_path / "c2"), seed=2)
+    assert engine.deck_table(d2, "Nx")[0] == 16384
+    assert engine.deck_table(d2, "depth").min() == pytest.approx(0.05)
+
+
+def test_bad_deck_reports_error(tmp_path):
+    p = tmp_path / "bad"
+    p.mkdir()
+    (p / "input.txt").write_text("&INFLUX_SIGNAL\nwavename = zero\n")
+    with pytest.raises(engine.EngineError):
+        engine.deck_table(str(p), "Nx")
+
+
+def test_seeded_influx_reproducible(tmp_path):
+    t1, e1 = decks.jonswap_signal(100.0, 2048, 1024, 0.1, 2.0, 3.3, seed=5)
+    t2, e2 = decks.jonswap_signal(100.0, 2048, 1024, 0.1, 2.0, 3.3, seed=5)
+    _, e3 = decks.jonswap_signal(100.0, 2048, 1024, 0.1, 2.0, 3.3, seed=6)
+    assert np.array_equal(e1, e2) and not np.array_equal(e1, e3)
+    assert 4 * e1.std() == pytest.approx(0.1, rel=1e-12)
+
+
+def test_library_exports_every_declared_symbol():
+    header = open(os.path.join(ROOT, "include", "hawassi_b200.h")).read()
+    declared = set(re.findall(r"\b(hw_[a-z_]+)\s*\(", header))
+    lib = ctypes.CDLL(engine.library_path())
+    missing = [s for s in sorted(declared) if not hasattr(lib, s)]
+    assert not missing, missing
+    assert set(engine.EXPORTS) <= declared
