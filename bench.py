@@ -283,20 +283,20 @@ def main():
         tot_pts, tot_sim = float(pts1 - pts0), sim1 - sim0
     value = tot_pts / (ms / 1e3)
 
-    # roofline of the dominant kernel: the evolve launches of one more step, timed per class
-    roof = None
-    pts_a = [eng.stats(i)["rhs_calls"] * nx[i] for i in range(eng.members)]
+    # roofline of the dominant kernel: k_evolve (99% of device time).  One step is one
+    # launch of it per grid-size class, all classes running concurrently on forked
+    # streams, so the launch group of one more step is timed as a unit with events
+    # on the launching stream and credited with every RHS point it evaluated.
+    pts_a = rhs_pts()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
     i_stop += args.window
-    eng.run(i_stop, sync=True)
-    pts_b = [eng.stats(i)["rhs_calls"] * nx[i] for i in range(eng.members)]
-    ct = eng.class_timing()
-    per_class = {}
-    for i in range(eng.members):
-        per_class.setdefault(nx[i], 0)
-        per_class[nx[i]] += pts_b[i] - pts_a[i]
-    dom = max(ct, key=lambda c: c[0])
-    cls_pts = per_class.get(dom[2], 0)
-    achieved = cls_pts * BYTES_PER_RHS_PT / (dom[0] / 1e3) / 1e9
+    eng.run(i_stop, sync=False)
+    g1.record(stream)
+    torch.cuda.synchronize()
+    gms = g0.elapsed_time(g1)
+    grp_pts = rhs_pts() - pts_a
+    achieved = grp_pts * BYTES_PER_RHS_PT / (gms / 1e3) / 1e9
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -307,12 +307,16 @@ def main():
     try:
         for line in open(os.path.join(ROOT, "profiles", "k_evolve_ensemble.md")):
             if line.startswith("dram_bytes_per_rhs_pt:"):
-                traffic = float(line.split(":")[1]) * cls_pts
+                traffic = float(line.split(":")[1]) * grp_pts / len(eng.class_timing())
     except OSError:
         pass
+    classes = eng.class_timing()
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": traffic, "kernel": f"k_evolve<{min(dom[2], 2048)}> (Nx={dom[2]} class, {dom[1]} members)",
-            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+            "traffic": traffic, "kernel": "k_evolve<2048>",
+            "launch": f"one step = {len(classes)} concurrent launches (one per grid-size class), "
+                      f"{gms:.2f} ms, {grp_pts:.3e} RHS grid points, {BYTES_PER_RHS_PT:.1f} algorithmic B/point",
+            "class_ms": [round(c[0], 3) for c in classes],
+            "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback"}
 
     # end to end through the C ABI with host buffers: H2D of every member's state, the
     # step, D2H of every state
