@@ -115,7 +115,7 @@ struct hw_ctx {
   bool upload_member(HostMember& h);
   bool launch_class(const Class& c, const int* list, int nblocks_members, int mode, cudaStream_t s);
   bool launch_member(int mi, int mode, double t_rhs);
-  bool run(int i_stop_all, double t_end, bool by_time);
+  bool run(int i_stop_all, double t_end, bool by_time, const int* per_member = nullptr);
   bool sync_desc();
   bool reset();
   ~hw_ctx();
@@ -371,12 +371,14 @@ bool hw_ctx::launch_member(int mi, int mode, double t_rhs) {
   return true;
 }
 
-bool hw_ctx::run(int i_stop_all, double t_end, bool by_time) {
+bool hw_ctx::run(int i_stop_all, double t_end, bool by_time, const int* per_member) {
   // set stop indices on the device descriptors
   for (size_t i = 0; i < mem.size(); ++i) {
     const hw::Member& m = mem[i].m;
     int stop = m.n;
-    if (by_time) {
+    if (per_member) {
+      stop = per_member[i] < 0 ? 0 : std::min(per_member[i], m.n);
+    } else if (by_time) {
       stop = 0;
       while (stop < m.n && m.ttrace[size_t(stop)] <= t_end) ++stop;
     } else if (i_stop_all >= 0) {
@@ -623,6 +625,11 @@ int hw_run(hw_ctx* ctx, int i_stop) {
   return ctx->run(i_stop, 0.0, false) ? 0 : 1;
 }
 
+int hw_run_members(hw_ctx* ctx, const int* i_stop) {
+  if (!ctx || !i_stop) return 1;
+  return ctx->run(-1, 0.0, false, i_stop) ? 0 : 1;
+}
+
 int hw_run_to_time(hw_ctx* ctx, double t_end) {
   if (!ctx) return 1;
   return ctx->run(-1, t_end, true) ? 0 : 1;
@@ -798,6 +805,31 @@ int hw_class_timing(hw_ctx* ctx, double* ms, int* members, int* grid_n, int cap)
     if (grid_n) grid_n[i] = c.M * c.C;
   }
   return n;
+}
+
+int hw_set_operator_weights(hw_ctx* ctx, int m, int K, const double* depths, const double* gam) {
+  if (!valid_member(ctx, m) || !depths || !gam) return 1;
+  HostMember& h = ctx->mem[size_t(m)];
+  if (h.m.flat || K != h.d.nref) {
+    ctx->err = "operator weights need a varying-depth member created with nref = " + std::to_string(K);
+    return 1;
+  }
+  std::string& err = ctx->err;
+  auto body = [&]() -> bool {
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    const int N = h.N;
+    for (int j = 0; j < K; ++j) {
+      std::vector<double> row = permute(hw::csq_row(h.m.k, depths[j]), N, h.C, h.M);
+      HW_CUDA(cudaMemcpy(const_cast<double*>(h.d.Csq) + size_t(j) * N, row.data(), sizeof(double) * N,
+                         cudaMemcpyHostToDevice));
+      HW_CUDA(cudaMemcpy(const_cast<double*>(h.d.gam) + size_t(j) * N, gam + size_t(j) * N, sizeof(double) * N,
+                         cudaMemcpyHostToDevice));
+      h.m.Csq_ref[size_t(j)] = hw::csq_row(h.m.k, depths[j]);
+      h.m.gam_ref[size_t(j)].assign(gam + size_t(j) * N, gam + size_t(j + 1) * N);
+    }
+    return true;
+  };
+  return body() ? 0 : 1;
 }
 
 int hw_energy(hw_ctx* ctx, int m, const double* y, double* energy) {

@@ -479,6 +479,12 @@ void interp_k(Member& m, double nu, int K, double Dmin, double Dmax) {
 
 }  // namespace
 
+std::vector<double> csq_row(const std::vector<double>& k, double D) {
+  std::vector<double> r(k.size());
+  for (size_t i = 0; i < k.size(); ++i) r[i] = std::pow(phase_velocity_i(k[i], D), 2);
+  return r;
+}
+
 void host_dft(std::vector<double>& re, std::vector<double>& im, int sign) {
   std::vector<cplx> a(re.size());
   for (size_t i = 0; i < re.size(); ++i) a[i] = cplx(re[i], im[i]);

@@ -63,6 +63,9 @@ struct Member {
 // false with a message in err on malformed or unsupported input.
 bool build_member(const std::string& dir, const SetupOptions& opt, Member& m, std::string& err);
 
+// C^2(k, D) for every wavenumber of k (exact dispersion, 1d/functions.c:1415)
+std::vector<double> csq_row(const std::vector<double>& k, double D);
+
 // Host FFT used by the set-up (any length; FFTW sign convention, unnormalised).
 void host_dft(std::vector<double>& re, std::vector<double>& im, int sign);
 

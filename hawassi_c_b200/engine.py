@@ -36,7 +36,9 @@ EXPORTS = [
     "hw_initial_state", "hw_rhs", "hw_gsl_rhs", "hw_evolve_apply", "hw_run", "hw_run_to_time",
     "hw_get_state", "hw_set_state", "hw_reset", "hw_member_stats", "hw_last_dydt", "hw_breaking_log",
     "hw_set_stream", "hw_synchronize", "hw_deck_table", "hw_get_states", "hw_set_states",
-    "hw_class_timing", "hw_rhs_noalloc", "hw_energy",
+    "hw_class_timing", "hw_rhs_noalloc", "hw_energy", "hw_run_members", "hw_set_operator_weights",
+    "hw_mlp_sizes", "hw_mlp_create", "hw_mlp_destroy", "hw_mlp_last_error", "hw_mlp_get_params",
+    "hw_mlp_set_params", "hw_mlp_grad", "hw_mlp_grad_device", "hw_mlp_train", "hw_mlp_infer",
 ]
 
 
@@ -77,6 +79,22 @@ def load_library():
     L.hw_deck_table.argtypes = [ctypes.c_char_p, ctypes.POINTER(HwOpts), ctypes.c_char_p, dp, ip]
     L.hw_rhs_noalloc.argtypes = [vp, ip, dd, vp, vp, vp]
     L.hw_energy.argtypes = [vp, ip, dp, dp]
+    L.hw_run_members.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+    L.hw_set_operator_weights.argtypes = [vp, ip, ip, dp, dp]
+    fp = ctypes.POINTER(ctypes.c_float)
+    ipp = ctypes.POINTER(ctypes.c_int)
+    L.hw_mlp_sizes.argtypes = [ipp, ipp, ipp, ipp, ipp]
+    L.hw_mlp_create.restype = vp
+    L.hw_mlp_create.argtypes = [ctypes.c_ulonglong, ip]
+    L.hw_mlp_destroy.argtypes = [vp]
+    L.hw_mlp_last_error.restype = ctypes.c_char_p
+    L.hw_mlp_last_error.argtypes = [vp]
+    L.hw_mlp_get_params.argtypes = [vp, fp]
+    L.hw_mlp_set_params.argtypes = [vp, fp]
+    L.hw_mlp_grad.argtypes = [vp, fp, ip, fp, fp]
+    L.hw_mlp_grad_device.argtypes = [vp, vp, ip, fp, fp]
+    L.hw_mlp_train.argtypes = [vp, fp, ip, ip, ip, ctypes.c_float, fp]
+    L.hw_mlp_infer.argtypes = [vp, fp, ip, dp]
     L.hw_get_states.argtypes = [vp, dp]
     L.hw_set_states.argtypes = [vp, dp]
     L.hw_class_timing.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ip]
@@ -164,6 +182,21 @@ class Engine:
         self._check(load_library().hw_run(self._h, int(i_stop)), "run")
         if sync:
             self.synchronize()
+
+    def run_members(self, i_stop, sync=True):
+        """Advance each member m through output sample i_stop[m] (exclusive); members
+        whose stop is not past their current index hold."""
+        arr = (ctypes.c_int * self.members)(*[int(v) for v in i_stop])
+        self._check(load_library().hw_run_members(self._h, arr), "run_members")
+        if sync:
+            self.synchronize()
+
+    def set_operator_weights(self, member, depths, gam):
+        """Install K reference depths and per-point weights gam[K][Nx] (varying-depth member)."""
+        d = np.ascontiguousarray(depths, dtype=np.float64)
+        g = np.ascontiguousarray(gam, dtype=np.float64)
+        self._check(load_library().hw_set_operator_weights(self._h, member, d.size, _dp(d), _dp(g)),
+                    "set_operator_weights")
 
     def run_to_time(self, t_end, sync=True):
         self._check(load_library().hw_run_to_time(self._h, float(t_end)), "run_to_time")

@@ -1,0 +1,260 @@
+"""Learned depth operator (no counterpart in the reference).
+
+The plain varying-depth operator HSS interpolates the exact dispersion over 16
+reference depths (each grid point on its bracketing pair).  The learned operator
+keeps K = 4 reference depths and lets a small per-point network pick the blend
+weights (softmax over the 4), so HSS needs ceil(4/2) + 4 = 6 transforms instead of
+8 + 16 = 24.  The network sees 5 features per point -- the depth, the depth
+smoothed at three scales (2, 8, 32 m) and the log of the local dominant
+wavenumber -- and is trained so that the blended phase speed sum_j w_j C^2(kappa, D_j)
+matches the 16-reference operator's at 8 wavenumbers spanning the point's
+dominant band [kappa_d/2, 2.5 kappa_d].  The dominant band comes from fields the
+plain 16-reference method produced (local wavenumber of eta by the Hilbert
+transform, linear dispersion where no wave has arrived yet).
+
+Training (forward, backward, Adam) and inference run on the GPU through the C ABI
+(hw_mlp_*); the plain 16-reference run is the fallback (a periodic shadow step
+measures the eta error of each member and switches it when above a threshold) and
+the judge of the error.
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from . import engine as _eng
+
+G = 9.80665
+BAND = np.array([0.5, 0.63, 0.79, 1.0, 1.26, 1.59, 2.0, 2.5])
+K_LEARN = 4
+K_PLAIN = 16
+SCALES_M = (2.0, 8.0, 32.0)
+
+
+def csq(kappa, depth):
+    """C^2(kappa, d) = g tanh(kappa d) / kappa (exact dispersion, kappa > 0)."""
+    kappa = np.asarray(kappa, dtype=np.float64)
+    return G * np.tanh(kappa * depth) / kappa
+
+
+def reference_depths(depth, K):
+    """K log-spaced reference depths over [min h, max h] (the K-reference operator's)."""
+    dmin, dmax = float(np.min(depth)), float(np.max(depth))
+    D = dmin * (dmax / dmin) ** (np.arange(K) / (K - 1))
+    D[0], D[-1] = dmin, dmax
+    return D
+
+
+def kappa_linear(omega, depth):
+    """Wavenumber of frequency omega at depth d (Newton on omega^2 = g k tanh(k d))."""
+    d = np.asarray(depth, dtype=np.float64)
+    k = omega / np.sqrt(G * d)
+    for _ in range(50):
+        t = np.tanh(k * d)
+        f = G * k * t - omega ** 2
+        df = G * t + G * k * d * (1 - t * t)
+        k = k - f / df
+    return k
+
+
+def smooth(a, dx, sigma):
+    """Gaussian smoothing (periodic, by FFT) with standard deviation sigma (m)."""
+    n = a.size
+    kk = 2 * np.pi * np.fft.fftfreq(n, d=dx)
+    return np.fft.ifft(np.fft.fft(a) * np.exp(-0.5 * (kk * sigma) ** 2)).real
+
+
+def local_wavenumber(eta, dx, fallback, rel_amp=0.2):
+    """Local wavenumber of eta from its Hilbert transform (smoothed); where the local
+    amplitude is below rel_amp of the largest, the fallback field is used."""
+    n = eta.size
+    e = eta - eta.mean()
+    H = np.fft.ifft(-1j * np.sign(np.fft.fftfreq(n)) * np.fft.fft(e)).real
+    ge, gH = np.gradient(e, dx), np.gradient(H, dx)
+    amp2 = e * e + H * H
+    num = smooth(e * gH - H * ge, dx, 4.0)
+    den = smooth(amp2, dx, 4.0)
+    k = np.where(den > 0, num / np.maximum(den, 1e-300), 0.0)
+    amp = np.sqrt(np.maximum(smooth(amp2, dx, 4.0), 0))
+    ok = (amp > rel_amp * amp.max()) & (k > 0.2 * fallback) & (k < 5 * fallback)
+    return np.where(ok, k, fallback)
+
+
+def features(depth, dx, kdom):
+    """(Nx, 5) float32 features: h, h smoothed at 2/8/32 m, log kappa_dom (normalised)."""
+    f = [depth] + [smooth(depth, dx, s) for s in SCALES_M] + [np.log(kdom)]
+    F = np.stack(f, axis=1)
+    F[:, :4] = F[:, :4] / 2.0 - 0.5
+    F[:, 4] = F[:, 4] / 2.0
+    return F.astype(np.float32)
+
+
+def records(depth, dx, kdom, D16, gam16, D4):
+    """(Nx, 45) float32 training records: features, G[m][j] = C^2(kappa_m, D4_j),
+    T[m] = sum_j gam16_j C^2(kappa_m, D16_j) (the 16-reference operator's)."""
+    Nx = depth.size
+    kap = kdom[:, None] * BAND[None, :]                        # (Nx, 8)
+    Gm = np.stack([csq(kap, d) for d in D4], axis=2)            # (Nx, 8, 4)
+    T = np.zeros((Nx, BAND.size))
+    for j, d in enumerate(D16):
+        T += gam16[j][:, None] * csq(kap, d)
+    R = np.concatenate([features(depth, dx, kdom), Gm.reshape(Nx, -1), T], axis=1)
+    return R.astype(np.float32)
+
+
+class MLP:
+    """The per-point network on the GPU (hw_mlp_*)."""
+
+    def __init__(self, seed=0, device=0):
+        L = _eng.load_library()
+        self._h = L.hw_mlp_create(seed, device)
+        if not self._h:
+            raise _eng.EngineError(L.hw_mlp_last_error(None).decode())
+        n = [ctypes.c_int() for _ in range(5)]
+        self.rec = L.hw_mlp_sizes(*[ctypes.byref(v) for v in n])
+        self.n_in, self.n_hidden, self.n_out, self.n_band, self.n_params = [v.value for v in n]
+
+    def close(self):
+        if self._h:
+            _eng.load_library().hw_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise _eng.EngineError(f"{what}: " + _eng.load_library().hw_mlp_last_error(self._h).decode())
+
+    @staticmethod
+    def _fp(a):
+        return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+    def params(self):
+        p = np.zeros(self.n_params, dtype=np.float32)
+        self._check(_eng.load_library().hw_mlp_get_params(self._h, self._fp(p)), "get_params")
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        self._check(_eng.load_library().hw_mlp_set_params(self._h, self._fp(p)), "set_params")
+
+    def grad(self, recs):
+        r = np.ascontiguousarray(recs, dtype=np.float32)
+        g = np.zeros(self.n_params, dtype=np.float32)
+        loss = np.zeros(1, dtype=np.float32)
+        self._check(_eng.load_library().hw_mlp_grad(self._h, self._fp(r), r.shape[0], self._fp(g), self._fp(loss)),
+                    "grad")
+        return float(loss[0]), g
+
+    def train(self, recs, epochs=20, batch=4096, lr=3e-3):
+        r = np.ascontiguousarray(recs, dtype=np.float32)
+        losses = np.zeros(epochs, dtype=np.float32)
+        self._check(_eng.load_library().hw_mlp_train(self._h, self._fp(r), r.shape[0], epochs, batch, lr,
+                                                      self._fp(losses)), "train")
+        return losses
+
+    def infer(self, feats):
+        f = np.ascontiguousarray(feats, dtype=np.float32)
+        w = np.zeros((self.n_out, f.shape[0]))
+        self._check(_eng.load_library().hw_mlp_infer(self._h, self._fp(f), f.shape[0],
+                                                      w.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "infer")
+        return w
+
+
+def eta_of(y, nx):
+    return np.fft.ifft(y[:nx] + 1j * y[nx:2 * nx]).real
+
+
+def member_fields(deck, y, omega_p):
+    """depth, dx, dominant wavenumber field of one member from a plain-run state y."""
+    depth = _eng.deck_table(deck, "depth")
+    dx = float(_eng.deck_table(deck, "dx")[0])
+    kfall = kappa_linear(omega_p, depth)
+    kdom = local_wavenumber(eta_of(y, depth.size), dx, kfall)
+    return depth, dx, kdom
+
+
+def training_records(decks, t_run, stride=1, device=0):
+    """Run the plain 16-reference method on the decks (one batched launch) for t_run
+    seconds and build the training records from the fields it produced."""
+    plain = _eng.Engine(decks, eps_abs=1e-8, eps_rel=1e-6, nref=K_PLAIN, device=device)
+    plain.run_to_time(t_run)
+    out = []
+    for m, d in enumerate(decks):
+        _, _, y = plain.state(m)
+        omega_p = float(_eng.deck_table(d, "nu_peak")[0])
+        depth, dx, kdom = member_fields(d, y, omega_p)
+        gam16 = _eng.deck_table(d, "gamK", nref=K_PLAIN).reshape(K_PLAIN, -1)
+        R = records(depth, dx, kdom, reference_depths(depth, K_PLAIN), gam16, reference_depths(depth, K_LEARN))
+        out.append(R[::stride])
+    plain.close()
+    return np.concatenate(out, axis=0)
+
+
+def learned_weights(mlp, deck, kdom=None):
+    """Per-point weights [4][Nx] and the 4 reference depths for a deck."""
+    depth = _eng.deck_table(deck, "depth")
+    dx = float(_eng.deck_table(deck, "dx")[0])
+    if kdom is None:
+        kdom = kappa_linear(float(_eng.deck_table(deck, "nu_peak")[0]), depth)
+    return mlp.infer(features(depth, dx, kdom)), reference_depths(depth, K_LEARN)
+
+
+def install(eng, decks, weights):
+    """Install per-member (weights, depths) into an engine created with nref = 4."""
+    for m, (w, D) in enumerate(weights):
+        eng.set_operator_weights(m, D, w)
+
+
+class ShadowedEnsemble:
+    """Learned-operator ensemble with the plain 16-reference method as fallback: every
+    `period` output samples each active member is copied into the plain engine, both
+    advance one sample, and a member whose eta differs by more than `threshold`
+    (relative L2) continues on the plain operator from then on."""
+
+    def __init__(self, decks, weights, period=20, threshold=1e-3, device=0, **kw):
+        self.decks = list(decks)
+        self.learned = _eng.Engine(self.decks, nref=K_LEARN, device=device, **kw)
+        install(self.learned, self.decks, weights)
+        self.plain = _eng.Engine(self.decks, nref=K_PLAIN, device=device, **kw)
+        self.period, self.threshold = period, threshold
+        self.fallback = np.zeros(len(self.decks), dtype=bool)
+        self.i = 0
+        self.checks = []
+
+    def advance(self, n_samples):
+        target = self.i + n_samples
+        while self.i < target:
+            nxt = min(target, (self.i // self.period + 1) * self.period)
+            stops = [nxt if not f else -1 for f in self.fallback]
+            self.learned.run_members(stops)
+            fb = [nxt if f else -1 for f in self.fallback]
+            if self.fallback.any():
+                self.plain.run_members(fb)
+            self.i = nxt
+            if self.i % self.period == 0:
+                self._shadow_check()
+
+    def _shadow_check(self):
+        active = [m for m in range(len(self.decks)) if not self.fallback[m]]
+        for m in active:
+            t, h, y = self.learned.state(m)
+            self.plain.set_state(t, h, y, member=m, i_out=self.i)
+        stops = [self.i + 1 if m in active else -1 for m in range(len(self.decks))]
+        self.plain.run_members(stops)
+        self.learned.run_members(stops)
+        self.i += 1
+        for m in active:
+            nx = self.learned.nx[m]
+            el = eta_of(self.learned.state(m)[2], nx)
+            ep = eta_of(self.plain.state(m)[2], nx)
+            err = float(np.linalg.norm(el - ep) / max(np.linalg.norm(ep), 1e-300))
+            self.checks.append((self.i, m, err))
+            if err > self.threshold:
+                self.fallback[m] = True
+                t, h, y = self.plain.state(m)
+                self.plain.set_state(t, h, y, member=m, i_out=self.i)

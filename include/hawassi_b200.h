@@ -82,6 +82,8 @@ int hw_evolve_apply(hw_ctx* ctx, int member, double* t, double t1, double* h, do
 int hw_run(hw_ctx* ctx, int i_stop);
 /* A launch stops a member after 400000 RHS evaluations (status 3, resumed by the next
  * hw_run), so no launch runs unbounded. */
+/* Same with a stop index per member (i_stop[m] <= current index: the member holds). */
+int hw_run_members(hw_ctx* ctx, const int* i_stop);
 /* Same, stopping at the last output sample whose time is <= t_end. */
 int hw_run_to_time(hw_ctx* ctx, double t_end);
 
@@ -108,6 +110,30 @@ int hw_set_states(hw_ctx* ctx, const double* y_all);
 /* Device time (ms) of the last hw_run launch of each grid-size class, with the
  * class's member count and grid size; returns the number of classes. */
 int hw_class_timing(hw_ctx* ctx, double* ms, int* members, int* grid_n, int cap);
+
+/* Replace the K reference depths and the per-point weights gam[K][Nx] of a
+ * varying-depth member created with nref = K (no counterpart in the reference: used to
+ * install the learned operator's weights). */
+int hw_set_operator_weights(hw_ctx* ctx, int member, int K, const double* depths, const double* gam);
+
+/* The learned operator's per-point network (no counterpart in the reference):
+ * 5 features -> 32 -> 32 (tanh) -> 4 softmax weights, FP32, trained on the GPU.
+ * A training record is 45 floats: 5 features, the 8x4 band matrix
+ * G[m][j] = C^2(kappa_m, D_j) and 8 targets T[m]; loss = mean_m ((G w - T)_m / T_m)^2. */
+typedef struct hw_mlp hw_mlp;
+int         hw_mlp_sizes(int* n_in, int* n_hidden, int* n_out, int* n_band, int* n_params);
+hw_mlp*     hw_mlp_create(unsigned long long seed, int device);
+void        hw_mlp_destroy(hw_mlp* mlp);
+const char* hw_mlp_last_error(const hw_mlp* mlp);
+int         hw_mlp_get_params(hw_mlp* mlp, float* params);
+int         hw_mlp_set_params(hw_mlp* mlp, const float* params);
+/* summed loss and parameter gradients over n host records */
+int         hw_mlp_grad(hw_mlp* mlp, const float* records, int n, float* grad, float* loss);
+int         hw_mlp_grad_device(hw_mlp* mlp, const float* records_dev, int n, float* grad, float* loss);
+/* Adam over minibatches of `batch` records for `epochs` passes; losses[e] = mean loss */
+int         hw_mlp_train(hw_mlp* mlp, const float* records, int n, int epochs, int batch, float lr, float* losses);
+/* per-point weights w[4][n] (double) from n feature rows of 5 floats */
+int         hw_mlp_infer(hw_mlp* mlp, const float* features, int n, double* w);
 
 /* Energy diagnostic (no counterpart in the reference): the quadratic Hamiltonian
  * 1/2 int (g eta^2 + u (C^2/g) u) dx of a state in spectral form (Parseval), with C^2

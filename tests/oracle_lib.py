@@ -58,6 +58,9 @@ def lib():
         L.or_breaking_log.argtypes = [vp]
         L.or_reset.argtypes = [vp]
         L.or_fft.argtypes = [ip, dp, dp, dp, dp, ip]
+        L.or_mlp_nparams.restype = ip
+        L.or_mlp_loss_grad.restype = ctypes.c_double
+        L.or_mlp_loss_grad.argtypes = [dp, ctypes.POINTER(ctypes.c_float), ip, dp]
         _lib = L
     return _lib
 
@@ -149,3 +152,13 @@ def fft(x, sign=-1):
     io = np.zeros(n)
     lib().or_fft(n, _p(re), _p(im), _p(ro), _p(io), sign)
     return ro + 1j * io
+
+
+def mlp_loss_grad(params, records):
+    """FP64 summed loss and parameter gradient of the learned operator's network."""
+    P = np.ascontiguousarray(params, dtype=np.float64)
+    R = np.ascontiguousarray(records, dtype=np.float32)
+    g = np.zeros(lib().or_mlp_nparams())
+    n = R.shape[0]
+    L = lib().or_mlp_loss_grad(_p(P), R.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n, _p(g))
+    return L, g
