@@ -8,7 +8,7 @@ weights (softmax over the 4), so HSS needs ceil(4/2) + 4 = 6 transforms instead 
 smoothed at three scales (2, 8, 32 m) and the log of the local dominant
 wavenumber -- and is trained so that the blended phase speed sum_j w_j C^2(kappa, D_j)
 matches the 16-reference operator's at 8 wavenumbers spanning the point's
-dominant band [kappa_d/2, 2.5 kappa_d].  The dominant band comes from fields the
+dominant band [0.6 kappa_d, 2 kappa_d].  The dominant band comes from fields the
 plain 16-reference method produced (local wavenumber of eta by the Hilbert
 transform, linear dispersion where no wave has arrived yet).
 
@@ -25,7 +25,7 @@ import numpy as np
 from . import engine as _eng
 
 G = 9.80665
-BAND = np.array([0.5, 0.63, 0.79, 1.0, 1.26, 1.59, 2.0, 2.5])
+BAND = np.array([0.6, 0.75, 0.9, 1.0, 1.1, 1.3, 1.6, 2.0])
 K_LEARN = 4
 K_PLAIN = 16
 SCALES_M = (2.0, 8.0, 32.0)
