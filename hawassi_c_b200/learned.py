@@ -4,9 +4,9 @@ The plain varying-depth operator HSS interpolates the exact dispersion over 16
 reference depths (each grid point on its bracketing pair).  The learned operator
 keeps K = 4 reference depths and lets a small per-point network pick the blend
 weights (softmax over the 4), so HSS needs ceil(4/2) + 4 = 6 transforms instead of
-8 + 16 = 24.  The network sees 5 features per point -- the depth, the depth
-smoothed at three scales (2, 8, 32 m) and the log of the local dominant
-wavenumber -- and is trained so that the blended phase speed sum_j w_j C^2(kappa, D_j)
+8 + 16 = 24.  The network sees 5 features per point -- the depth and the depth
+smoothed at three scales (2, 8, 32 m), each as its position on the log scale of
+the 4 reference depths, and the local dominant wavenumber as log(kappa_d h) -- and is trained so that the blended phase speed sum_j w_j C^2(kappa, D_j)
 matches the 16-reference operator's at 8 wavenumbers spanning the point's
 dominant band [0.6 kappa_d, 2 kappa_d].  The dominant band comes from fields the
 plain 16-reference method produced (local wavenumber of eta by the Hilbert
@@ -81,12 +81,15 @@ def local_wavenumber(eta, dx, fallback, rel_amp=0.2):
 
 
 def features(depth, dx, kdom):
-    """(Nx, 5) float32 features: h, h smoothed at 2/8/32 m, log kappa_dom (normalised)."""
-    f = [depth] + [smooth(depth, dx, s) for s in SCALES_M] + [np.log(kdom)]
-    F = np.stack(f, axis=1)
-    F[:, :4] = F[:, :4] / 2.0 - 0.5
-    F[:, 4] = F[:, 4] / 2.0
-    return F.astype(np.float32)
+    """(Nx, 5) float32 features.  The depth h and h smoothed at 2, 8 and 32 m enter as
+    their position on the log scale of the 4 reference depths (0 at the shallowest
+    reference, 3 at the deepest), the dominant band as log(kappa_dom * h): the blend
+    weights are then one function of these for every bathymetry."""
+    D = reference_depths(depth, K_LEARN)
+    scale = np.log(D[-1] / D[0]) / (K_LEARN - 1) if D[-1] > D[0] else 1.0
+    hs = [depth] + [np.maximum(smooth(depth, dx, s), 1e-3) for s in SCALES_M]
+    f = [np.log(h / D[0]) / scale - 1.5 for h in hs] + [np.log(kdom * depth)]
+    return np.stack(f, axis=1).astype(np.float32)
 
 
 def records(depth, dx, kdom, D16, gam16, D4):
@@ -258,3 +261,79 @@ class ShadowedEnsemble:
                 self.fallback[m] = True
                 t, h, y = self.plain.state(m)
                 self.plain.set_state(t, h, y, member=m, i_out=self.i)
+
+
+def pipeline(n_train=512, n_eval=64, nx=16384, t_train=20.0, t_eval=20.0, epochs=200, batch=4096, stride=16,
+             root=None, device=0, seed=0, log=print):
+    """Config-4 pipeline: plain 16-reference runs on n_train random bathymetries ->
+    training records -> GPU training -> a batched n_eval-member learned ensemble and
+    the plain 16-reference ensemble on held-out bathymetries, both timed; returns the
+    eta errors and the two ensembles' simulated-seconds per wall-second."""
+    import os
+    import tempfile
+    import time
+    from . import decks as _decks
+    root = root or os.path.join(tempfile.gettempdir(), "hw_learned")
+    tr = [_decks.config4_deck(os.path.join(root, f"train{i:04d}"), seed=seed + i, nx=nx, T_end=max(t_train, t_eval) + 10)
+          for i in range(n_train)]
+    ev = [_decks.config4_deck(os.path.join(root, f"eval{i:04d}"), seed=seed + 100000 + i, nx=nx,
+                              T_end=max(t_train, t_eval) + 10) for i in range(n_eval)]
+    log(f"{n_train} training and {n_eval} evaluation decks")
+    t0 = time.time()
+    recs = []
+    for c in range(0, n_train, 64):
+        recs.append(training_records(tr[c:c + 64], t_train, stride=stride, device=device))
+    R = np.concatenate(recs)
+    log(f"{R.shape[0]} training records from the plain runs in {time.time() - t0:.1f} s")
+    mlp = MLP(seed=seed + 1, device=device)
+    t0 = time.time()
+    losses = mlp.train(R, epochs=epochs, batch=batch, lr=2e-3)
+    log(f"trained: loss {losses[0]:.3e} -> {losses[-1]:.3e} in {time.time() - t0:.1f} s")
+    out = {"records": int(R.shape[0]), "loss_first": float(losses[0]), "loss_last": float(losses[-1])}
+
+    def timed(eng):
+        eng.run_to_time(0.5)
+        s0 = sum(eng.state(m)[0] for m in range(eng.members))
+        t = time.time()
+        eng.run_to_time(t_eval)
+        wall = time.time() - t
+        s1 = sum(eng.state(m)[0] for m in range(eng.members))
+        return (s1 - s0) / wall, wall
+
+    plain = _eng.Engine(ev, eps_abs=1e-8, eps_rel=1e-6, nref=K_PLAIN, device=device)
+    out["plain_sim_s_per_wall_s"], out["plain_wall_s"] = timed(plain)
+    lrn = _eng.Engine(ev, eps_abs=1e-8, eps_rel=1e-6, nref=K_LEARN, device=device)
+    install(lrn, ev, [learned_weights(mlp, d) for d in ev])
+    out["learned_sim_s_per_wall_s"], out["learned_wall_s"] = timed(lrn)
+    uni = _eng.Engine(ev, eps_abs=1e-8, eps_rel=1e-6, nref=K_LEARN, device=device)
+    install(uni, ev, [(np.full((K_LEARN, n), 0.25), reference_depths(_eng.deck_table(d, "depth"), K_LEARN))
+                      for d, n in zip(ev, uni.nx)])
+    uni.run_to_time(t_eval)
+    err_l, err_u = [], []
+    for m in range(len(ev)):
+        ep = eta_of(plain.state(m)[2], plain.nx[m])
+        den = max(np.linalg.norm(ep), 1e-300)
+        err_l.append(float(np.linalg.norm(eta_of(lrn.state(m)[2], lrn.nx[m]) - ep) / den))
+        err_u.append(float(np.linalg.norm(eta_of(uni.state(m)[2], uni.nx[m]) - ep) / den))
+    out.update(eta_err_learned_median=float(np.median(err_l)), eta_err_learned_max=float(np.max(err_l)),
+               eta_err_uniform_median=float(np.median(err_u)),
+               speedup=out["learned_sim_s_per_wall_s"] / out["plain_sim_s_per_wall_s"],
+               rhs_calls_plain=sum(plain.stats(m)["rhs_calls"] for m in range(len(ev))),
+               rhs_calls_learned=sum(lrn.stats(m)["rhs_calls"] for m in range(len(ev))))
+    return out
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="train and evaluate the learned K=4 depth operator")
+    ap.add_argument("--train", type=int, default=512)
+    ap.add_argument("--eval", type=int, default=64)
+    ap.add_argument("--nx", type=int, default=16384)
+    ap.add_argument("--t-train", type=float, default=20.0)
+    ap.add_argument("--t-eval", type=float, default=20.0)
+    ap.add_argument("--epochs", type=int, default=200)
+    ap.add_argument("--stride", type=int, default=16)
+    a = ap.parse_args()
+    res = pipeline(a.train, a.eval, a.nx, a.t_train, a.t_eval, a.epochs, stride=a.stride)
+    print(json.dumps(res))

@@ -58,7 +58,7 @@ def test_training_gain_and_fallback(tmp_path):
     test = [_bump_deck(tmp_path, f"e{i}", seed=900 + i) for i in range(2)]
     R = learned.training_records(train, t_run=15.0, stride=2)
     mlp = learned.MLP(seed=7)
-    losses = mlp.train(R, epochs=60, batch=2048, lr=3e-3)
+    losses = mlp.train(R, epochs=300, batch=512, lr=2e-3)
     print("training loss first/last epoch:", losses[0], losses[-1])
     assert losses[-1] < 0.2 * losses[0]
     # held-out members: plain 16-reference run is the judge
@@ -78,7 +78,10 @@ def test_training_gain_and_fallback(tmp_path):
         assert all(eng.stats(m)["status"] == 0 for m in range(len(test)))
         eng.close()
     print("eta rel L2 vs plain 16-ref:", errs)
-    assert errs["trained"] < 0.5 * errs["uniform"]
+    assert errs["trained"] < 0.1 * errs["uniform"]
+    # the best convex blend of 4 references over the band (per-point simplex least
+    # squares) bounds what any network can reach: report the trained loss beside it
+    print("trained loss", float(losses[-1]))
     # fallback: a zero threshold sends every member back to the plain operator
     weights = [learned.learned_weights(mlp, d) for d in test]
     sh = learned.ShadowedEnsemble(test, weights, period=10, threshold=0.0, eps_abs=1e-8, eps_rel=1e-6)
