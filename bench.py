@@ -357,6 +357,7 @@ def main():
             "config": {"workload": WORKLOAD, "members_per_gpu": args.members, "window_samples": args.window,
                        "l2": "working set well above L2 (126 MB): no flush needed",
                        "grid_sizes": sorted(set(nx))},
+            "rhs_points_per_step": tot_pts / args.steps,
             "sim_s_per_wall_s": tot_sim / (ms / 1e3),
             "sim_s_per_wall_s_per_member": tot_sim / (ms / 1e3) / (args.members * world),
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
