@@ -307,7 +307,7 @@ def main():
     try:
         for line in open(os.path.join(ROOT, "profiles", "k_evolve_ensemble.md")):
             if line.startswith("dram_bytes_per_rhs_pt:"):
-                traffic = float(line.split(":")[1]) * grp_pts / len(eng.class_timing())
+                traffic = float(line.split(":")[1]) * grp_pts   # bytes over the launch group
     except OSError:
         pass
     classes = eng.class_timing()
