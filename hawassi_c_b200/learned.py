@@ -177,7 +177,12 @@ def member_fields(deck, y, omega_p):
     depth = _eng.deck_table(deck, "depth")
     dx = float(_eng.deck_table(deck, "dx")[0])
     kfall = kappa_linear(omega_p, depth)
-    kdom = local_wavenumber(eta_of(y, depth.size), dx, kfall)
+    eta = eta_of(y, depth.size)
+    if not np.all(np.isfinite(eta)):
+        # the plain run diverged (waves steepening over the shallowest bumps with no
+        # breaking): its fields carry no band information, use linear dispersion
+        return depth, dx, kfall
+    kdom = local_wavenumber(eta, dx, kfall)
     return depth, dx, kdom
 
 
