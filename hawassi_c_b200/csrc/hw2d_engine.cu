@@ -1,0 +1,476 @@
+// hw2d_engine.cu -- C ABI of the 2D flat-bottom engine: tables upload, the
+// RHS entry points and the device-resident rkf45 loop.
+//
+// One step attempt is a fixed launch sequence captured once as a CUDA graph:
+//   [RHS k1, if needed] [RHS stages 2..6] combine control [RHS k_out, if accepted] finalize
+// Every kernel reads the device control block (t, h, h0, done, buffer indices)
+// and does nothing once the target time is reached, so the host replays the
+// graph in batches and reads the control block back between batches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/hawassi_b200.h"
+#include "hw2d.cuh"
+#include "hw_setup.hpp"
+
+using hw2d::Ctl2;
+using hw2d::RK2;
+using hw2d::Tab2;
+using hw2d::Work2;
+
+namespace {
+
+std::string g_err2d;
+
+constexpr int kMinM = 64, kMaxM = 1024;
+constexpr long long kMaxAttemptsPerRun = 2000000;
+
+template <int M>
+size_t smem_bytes(int slices) { return (size_t)slices * hwdev::padded(M) * sizeof(double2); }
+
+template <int M>
+void set_attrs() {
+  cudaFuncSetAttribute(hw2d::k2_rowA<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(6));
+  cudaFuncSetAttribute(hw2d::k2_colB<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(8));
+  cudaFuncSetAttribute(hw2d::k2_rowC<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(8));
+  cudaFuncSetAttribute(hw2d::k2_colD<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(10));
+  cudaFuncSetAttribute(hw2d::k2_rowE<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(8));
+}
+
+// the five kernels of one RHS for a row length Mx and a column length My
+template <int M>
+void launch_row(int which, int nblocks, cudaStream_t s, const Tab2& tb, const Work2& w, const RK2& rk,
+                const Ctl2* ctl, Ctl2* ctlw, int mode, int cond, double2* out) {
+  const dim3 blk(hw2d::kGroups * (M / 8));
+  if (which == 0) hw2d::k2_rowA<M><<<nblocks, blk, smem_bytes<M>(6), s>>>(tb, w, rk, ctl, ctlw, mode, cond);
+  else if (which == 2) hw2d::k2_rowC<M><<<nblocks, blk, smem_bytes<M>(8), s>>>(tb, w, ctl, cond);
+  else hw2d::k2_rowE<M><<<nblocks, blk, smem_bytes<M>(8), s>>>(tb, w, rk, ctl, mode, cond, out);
+}
+template <int M>
+void launch_col(int which, int nblocks, cudaStream_t s, const Tab2& tb, const Work2& w, const Ctl2* ctl, int cond) {
+  const dim3 blk(hw2d::kGroups * (M / 8));
+  if (which == 1) hw2d::k2_colB<M><<<nblocks, blk, smem_bytes<M>(8), s>>>(tb, w, ctl, cond);
+  else hw2d::k2_colD<M><<<nblocks, blk, smem_bytes<M>(10), s>>>(tb, w, ctl, cond);
+}
+
+void row_dispatch(int M, int which, int nb, cudaStream_t s, const Tab2& tb, const Work2& w, const RK2& rk,
+                  const Ctl2* ctl, Ctl2* ctlw, int mode, int cond, double2* out) {
+  switch (M) {
+    case 64: launch_row<64>(which, nb, s, tb, w, rk, ctl, ctlw, mode, cond, out); break;
+    case 128: launch_row<128>(which, nb, s, tb, w, rk, ctl, ctlw, mode, cond, out); break;
+    case 256: launch_row<256>(which, nb, s, tb, w, rk, ctl, ctlw, mode, cond, out); break;
+    case 512: launch_row<512>(which, nb, s, tb, w, rk, ctl, ctlw, mode, cond, out); break;
+    default: launch_row<1024>(which, nb, s, tb, w, rk, ctl, ctlw, mode, cond, out); break;
+  }
+}
+void col_dispatch(int M, int which, int nb, cudaStream_t s, const Tab2& tb, const Work2& w, const Ctl2* ctl,
+                  int cond) {
+  switch (M) {
+    case 64: launch_col<64>(which, nb, s, tb, w, ctl, cond); break;
+    case 128: launch_col<128>(which, nb, s, tb, w, ctl, cond); break;
+    case 256: launch_col<256>(which, nb, s, tb, w, ctl, cond); break;
+    case 512: launch_col<512>(which, nb, s, tb, w, ctl, cond); break;
+    default: launch_col<1024>(which, nb, s, tb, w, ctl, cond); break;
+  }
+}
+
+void set_all_attrs() {
+  static bool done[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64 || done[dev]) return;
+  set_attrs<64>(); set_attrs<128>(); set_attrs<256>(); set_attrs<512>(); set_attrs<1024>();
+  done[dev] = true;
+}
+
+std::vector<double2> twiddles(int n) {
+  std::vector<double2> t(n);
+  for (int q = 0; q < n; ++q) {
+    const double a = 2.0 * M_PI * double(q) / double(n);
+    t[q] = make_double2(std::cos(a), -std::sin(a));
+  }
+  return t;
+}
+
+bool pow2_in_range(int v) { return v >= kMinM && v <= kMaxM && (v & (v - 1)) == 0; }
+
+}  // namespace
+
+struct hw2d_ctx {
+  int device = 0;
+  int nx = 0, ny = 0;
+  size_t n = 0;
+  cudaStream_t own_stream = nullptr, stream = nullptr;
+  Tab2 tb{};
+  Work2 w{};
+  RK2 rk{};
+  Ctl2* ctl = nullptr;     // device
+  Ctl2* hctl = nullptr;    // pinned host copy
+  double* dref = nullptr;  // 6n staging for reference-layout transfers
+  double2* dout = nullptr; // 3n direct RHS output
+  std::vector<void*> allocs;
+  cudaGraphExec_t attempt = nullptr;
+  cudaStream_t graph_stream = nullptr;
+  double h_first = 0.0;
+  std::string err;
+
+  template <class T>
+  T* dalloc(size_t count) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) return nullptr;
+    allocs.push_back(p);
+    return static_cast<T*>(p);
+  }
+  template <class T>
+  T* upload(const std::vector<T>& v) {
+    T* p = dalloc<T>(v.size());
+    if (p && cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) return nullptr;
+    return p;
+  }
+  bool check(const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      err = std::string(what) + ": " + cudaGetErrorString(e);
+      return false;
+    }
+    return true;
+  }
+  void rhs_launch(int mode, int cond, cudaStream_t s, double2* out) {
+    const int rows = ny / 2, cols = nx / 2;
+    row_dispatch(nx, 0, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
+    col_dispatch(ny, 1, cols, s, tb, w, ctl, cond);
+    row_dispatch(nx, 2, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
+    if (!tb.chi_one || tb.has_src) col_dispatch(ny, 3, cols, s, tb, w, ctl, cond);
+    row_dispatch(nx, 4, rows, s, tb, w, rk, ctl, ctl, mode, cond, out);
+  }
+  void attempt_launch(cudaStream_t s) {
+    rhs_launch(1, hw2d::kIfK1, s, nullptr);
+    for (int st = 2; st <= 6; ++st) rhs_launch(st, hw2d::kIfStage, s, nullptr);
+    hw2d::k2_combine<<<hw2d::kCombBlocks, hw2d::kCombThreads, 0, s>>>(rk, w, ctl, 3 * n);
+    hw2d::k2_control<<<1, 256, 0, s>>>(ctl, w, hw2d::kCombBlocks);
+    rhs_launch(7, hw2d::kIfKout, s, nullptr);
+    hw2d::k2_finalize<<<1, 1, 0, s>>>(ctl);
+  }
+  bool build_graph() {
+    if (attempt) return true;
+    if (cudaStreamCreateWithFlags(&graph_stream, cudaStreamNonBlocking) != cudaSuccess) {
+      err = "stream create failed";
+      return false;
+    }
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(graph_stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      err = "graph capture failed to start";
+      return false;
+    }
+    attempt_launch(graph_stream);
+    if (cudaStreamEndCapture(graph_stream, &g) != cudaSuccess || !g) {
+      err = "graph capture failed";
+      cudaGetLastError();
+      return false;
+    }
+    const cudaError_t e = cudaGraphInstantiate(&attempt, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      err = std::string("graph instantiate: ") + cudaGetErrorString(e);
+      return false;
+    }
+    return true;
+  }
+  bool read_ctl() {
+    if (cudaMemcpyAsync(hctl, ctl, sizeof(Ctl2), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess)
+      return check("control read-back");
+    return true;
+  }
+  // evolve on the device until t1 (or one accepted step when one_step)
+  int run(double t1, bool one_step) {
+    if (!build_graph()) return 1;
+    hw2d::k2_begin<<<1, 1, 0, stream>>>(ctl, t1);
+    if (!check("begin")) return 1;
+    if (!read_ctl()) return 1;
+    const long long acc0 = hctl->acc;
+    int batch = one_step ? 1 : 2;
+    long long launched = 0;
+    for (;;) {
+      if (hctl->done) break;
+      if (launched > kMaxAttemptsPerRun) {
+        err = "time integration stopped: attempt budget of one run exceeded (step size collapsed)";
+        return 1;
+      }
+      launched += batch;
+      for (int b = 0; b < batch; ++b)
+        if (cudaGraphLaunch(attempt, stream) != cudaSuccess) return check("graph launch") ? 1 : 1;
+      if (!read_ctl()) return 1;
+      if (hctl->status != hw2d::kOk) break;
+      if (one_step && hctl->acc > acc0) {
+        // stop here: the next call recomputes its dydt_in like GSL's evolve_apply
+        break;
+      }
+      if (!one_step && batch < 16) batch *= 2;
+    }
+    if (hctl->status == hw2d::kNonFinite) { err = "non-finite state (the step size collapsed)"; return 1; }
+    if (hctl->status == hw2d::kStepFailed) { err = "time integration failed (too many rejected steps)"; return 1; }
+    return 0;
+  }
+  ~hw2d_ctx() {
+    if (attempt) cudaGraphExecDestroy(attempt);
+    if (graph_stream) cudaStreamDestroy(graph_stream);
+    for (void* p : allocs) cudaFree(p);
+    if (hctl) cudaFreeHost(hctl);
+    if (own_stream) cudaStreamDestroy(own_stream);
+  }
+};
+
+extern "C" {
+
+hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
+  if (!t || !t->kx || !t->ky || !t->c2d || !t->l2d || !t->aal || !t->charac || !t->chiadj) {
+    g_err2d = "hw2d_create: missing table";
+    return nullptr;
+  }
+  if (!pow2_in_range(t->nx) || !pow2_in_range(t->ny)) {
+    g_err2d = "hw2d_create: nx and ny must be powers of two in [64, 1024]";
+    return nullptr;
+  }
+  if (t->model != 2) {
+    g_err2d = "hw2d_create: only the HS2 model is built on the device";
+    return nullptr;
+  }
+  if (t->propagation < 0 || t->propagation > 2) {
+    g_err2d = "hw2d_create: propagation must be 0 (Uni+), 1 (Uni-) or 2 (Bi)";
+    return nullptr;
+  }
+  auto* c = new hw2d_ctx();
+  c->device = o ? o->device : 0;
+  if (cudaSetDevice(c->device) != cudaSuccess) {
+    g_err2d = "hw2d_create: cannot select the CUDA device";
+    delete c;
+    return nullptr;
+  }
+  set_all_attrs();
+  const int nx = t->nx, ny = t->ny;
+  const size_t n = (size_t)nx * ny;
+  c->nx = nx; c->ny = ny; c->n = n;
+  const bool has_src = t->nt >= 2 && t->sig && t->tsig && t->newgam;
+
+  // host tables (reference formulas: C2d^2/grav as pow(C2d, 2)/grav, 7*Cpeak*charac)
+  std::vector<double> c2g(n), damp(n);
+  bool chi_one = true;
+  for (size_t q = 0; q < n; ++q) {
+    c2g[q] = std::pow(t->c2d[q], 2) / hw2d::kGrav;
+    damp[q] = 7 * t->cpeak * t->charac[q];
+    if (t->chiadj[q] != 1.0) chi_one = false;
+  }
+  Tab2& tb = c->tb;
+  tb.nx = nx; tb.ny = ny; tb.n = (int)n; tb.model = t->model; tb.chi_one = chi_one ? 1 : 0;
+  tb.has_src = has_src ? 1 : 0;
+  tb.fac_src = t->propagation == 2 ? 2.0 : 1.0;
+  tb.kx = c->upload(std::vector<double>(t->kx, t->kx + nx));
+  tb.ky = c->upload(std::vector<double>(t->ky, t->ky + ny));
+  tb.c2g = c->upload(c2g);
+  tb.l2d = c->upload(std::vector<double>(t->l2d, t->l2d + n));
+  tb.aal = c->upload(std::vector<double>(t->aal, t->aal + n));
+  tb.damp = c->upload(damp);
+  tb.chi = c->upload(std::vector<double>(t->chiadj, t->chiadj + n));
+  tb.twx = c->upload(twiddles(nx));
+  tb.twy = c->upload(twiddles(ny));
+  if (has_src) {
+    // row transforms of the area kernels (the source's row pass is done once here)
+    const double sk = t->propagation == 0 ? -1.0 : (t->propagation == 1 ? 1.0 : 0.0);
+    std::vector<double2> gx(n), sx(n);
+    std::vector<double> re(nx), im(nx);
+    for (int i = 0; i < ny; ++i) {
+      for (int j = 0; j < nx; ++j) { re[j] = t->newgam[(size_t)i * nx + j]; im[j] = 0.0; }
+      hw::host_dft(re, im, -1);
+      for (int j = 0; j < nx; ++j) gx[(size_t)i * nx + j] = make_double2(re[j], im[j]);
+      for (int j = 0; j < nx; ++j) {
+        re[j] = t->skewgam ? sk * t->skewgam[(size_t)i * nx + j] : 0.0;
+        im[j] = 0.0;
+      }
+      hw::host_dft(re, im, -1);
+      for (int j = 0; j < nx; ++j) sx[(size_t)i * nx + j] = make_double2(re[j], im[j]);
+    }
+    tb.gx = c->upload(gx);
+    tb.sx = c->upload(sx);
+    const int nt = t->nt;
+    tb.nt = nt;
+    std::vector<double> ts(t->tsig, t->tsig + nt);
+    std::vector<double> sig((size_t)ny * nt), sigc((size_t)ny * nt), sigs((size_t)ny * nt, 0.0),
+        sigsc((size_t)ny * nt, 0.0);
+    for (int i = 0; i < ny; ++i) {
+      std::vector<double> a(t->sig + (size_t)i * nt, t->sig + (size_t)(i + 1) * nt);
+      std::vector<double> ca = hw::natural_spline_c(ts, a);
+      std::copy(a.begin(), a.end(), sig.begin() + (size_t)i * nt);
+      std::copy(ca.begin(), ca.end(), sigc.begin() + (size_t)i * nt);
+      if (t->sigskew) {
+        std::vector<double> b(t->sigskew + (size_t)i * nt, t->sigskew + (size_t)(i + 1) * nt);
+        std::vector<double> cb = hw::natural_spline_c(ts, b);
+        std::copy(b.begin(), b.end(), sigs.begin() + (size_t)i * nt);
+        std::copy(cb.begin(), cb.end(), sigsc.begin() + (size_t)i * nt);
+      }
+    }
+    tb.tsig = c->upload(ts);
+    tb.sig = c->upload(sig);
+    tb.sigc = c->upload(sigc);
+    tb.sigs = c->upload(sigs);
+    tb.sigsc = c->upload(sigsc);
+    c->h_first = (ts[nt - 1] - ts[0]) / (nt - 1) / 5.0;   // h = dt/5 (2d/fun_odesolver.c:2580)
+  } else {
+    c->h_first = 1e-3;
+  }
+  if (o && o->h0 > 0) c->h_first = o->h0;
+
+  Work2& w = c->w;
+  w.z = c->dalloc<double2>(3 * n);
+  w.R = c->dalloc<double2>(3 * n);
+  w.Q = c->dalloc<double2>(4 * n);
+  w.D = c->dalloc<double2>(3 * n);
+  w.W = chi_one ? nullptr : c->dalloc<double2>(4 * n);
+  w.V = c->dalloc<double2>(4 * n);
+  w.src = has_src ? c->dalloc<double2>(n) : nullptr;
+  w.insig = c->dalloc<double>(ny);
+  w.insigs = c->dalloc<double>(ny);
+  w.part = c->dalloc<double>(hw2d::kCombBlocks);
+  RK2& rk = c->rk;
+  for (int i = 0; i < 2; ++i) rk.y[i] = c->dalloc<double2>(3 * n);
+  for (int i = 0; i < 2; ++i) rk.kk[i] = c->dalloc<double2>(3 * n);
+  for (int i = 0; i < 5; ++i) rk.ks[i] = c->dalloc<double2>(3 * n);
+  c->dref = c->dalloc<double>(6 * n);
+  c->dout = c->dalloc<double2>(3 * n);
+  c->ctl = c->dalloc<Ctl2>(1);
+  bool ok = tb.kx && tb.ky && tb.c2g && tb.l2d && tb.aal && tb.damp && tb.chi && tb.twx && tb.twy && w.z && w.R &&
+            w.Q && w.D && w.V && w.insig && w.insigs && w.part && c->dref && c->dout && c->ctl &&
+            (chi_one || w.W) && (!has_src || (tb.gx && tb.sx && tb.sig && w.src));
+  for (int i = 0; i < 2; ++i) ok = ok && rk.y[i] && rk.kk[i];
+  for (int i = 0; i < 5; ++i) ok = ok && rk.ks[i];
+  if (!ok || cudaMallocHost(&c->hctl, sizeof(Ctl2)) != cudaSuccess) {
+    g_err2d = "hw2d_create: device allocation failed";
+    delete c;
+    return nullptr;
+  }
+  cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+  c->stream = c->own_stream;
+  Ctl2 h{};
+  h.eps_abs = (o && o->eps_abs > 0) ? o->eps_abs : 1e-3;
+  h.eps_rel = (o && o->eps_rel > 0) ? o->eps_rel : 1e-2;
+  h.h = c->h_first;
+  h.need_k1 = 1;
+  h.done = 1;
+  cudaMemcpy(c->ctl, &h, sizeof h, cudaMemcpyHostToDevice);
+  cudaMemset(rk.y[0], 0, 3 * n * sizeof(double2));
+  if (!c->check("hw2d_create")) {
+    g_err2d = c->err;
+    delete c;
+    return nullptr;
+  }
+  return c;
+}
+
+void hw2d_destroy(hw2d_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  delete c;
+}
+
+const char* hw2d_last_error(const hw2d_ctx* c) { return c ? c->err.c_str() : g_err2d.c_str(); }
+int hw2d_nx(const hw2d_ctx* c) { return c ? c->nx : 0; }
+int hw2d_ny(const hw2d_ctx* c) { return c ? c->ny : 0; }
+
+int hw2d_rhs(hw2d_ctx* c, double t, const double* y, double* dydt) {
+  if (!c || !y || !dydt) return 1;
+  cudaSetDevice(c->device);
+  const size_t n = c->n;
+  cudaMemcpyAsync(c->dref, y, 6 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+  hw2d::k2_to_internal<<<592, 256, 0, c->stream>>>(c->dref, c->w.z, n);
+  cudaMemcpyAsync(&c->ctl->t_direct, &t, sizeof(double), cudaMemcpyHostToDevice, c->stream);
+  c->rhs_launch(0, hw2d::kAlways, c->stream, c->dout);
+  hw2d::k2_to_reference<<<592, 256, 0, c->stream>>>(c->dout, c->dref, n);
+  cudaMemcpyAsync(dydt, c->dref, 6 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return c->check("hw2d_rhs") ? 1 : 1;
+  return c->check("hw2d_rhs") ? 0 : 1;
+}
+
+int hw2d_gsl_rhs(double t, const double* y, double* dydt, void* params) {
+  return hw2d_rhs(static_cast<hw2d_ctx*>(params), t, y, dydt);
+}
+
+int hw2d_set_state(hw2d_ctx* c, double t, double h, const double* y) {
+  if (!c || !y) return 1;
+  cudaSetDevice(c->device);
+  if (!c->read_ctl()) return 1;
+  Ctl2 s = *c->hctl;
+  s.t = t;
+  s.h = h > 0 ? h : c->h_first;
+  s.cur = 0;
+  s.need_k1 = 1;
+  s.need_kout = 0;
+  s.done = 1;
+  s.status = hw2d::kOk;
+  *c->hctl = s;
+  cudaMemcpyAsync(c->dref, y, 6 * c->n * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+  hw2d::k2_to_internal<<<592, 256, 0, c->stream>>>(c->dref, c->rk.y[0], c->n);
+  cudaMemcpyAsync(c->ctl, c->hctl, sizeof(Ctl2), cudaMemcpyHostToDevice, c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return c->check("hw2d_set_state") ? 1 : 1;
+  return c->check("hw2d_set_state") ? 0 : 1;
+}
+
+int hw2d_get_state(hw2d_ctx* c, double* t, double* h, double* y) {
+  if (!c) return 1;
+  cudaSetDevice(c->device);
+  if (!c->read_ctl()) return 1;
+  if (t) *t = c->hctl->t;
+  if (h) *h = c->hctl->h;
+  if (y) {
+    hw2d::k2_to_reference<<<592, 256, 0, c->stream>>>(c->rk.y[c->hctl->cur], c->dref, c->n);
+    cudaMemcpyAsync(y, c->dref, 6 * c->n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return c->check("hw2d_get_state") ? 1 : 1;
+  }
+  return c->check("hw2d_get_state") ? 0 : 1;
+}
+
+int hw2d_run_to_time(hw2d_ctx* c, double t1) {
+  if (!c) return 1;
+  cudaSetDevice(c->device);
+  return c->run(t1, false);
+}
+
+int hw2d_evolve_apply(hw2d_ctx* c, double* t, double t1, double* h, double* y) {
+  if (!c || !t || !h || !y) return 1;
+  if (hw2d_set_state(c, *t, *h, y)) return 1;
+  // gsl_odeiv2_evolve_apply rejects a step whose direction disagrees with t1 - t
+  const double dt = t1 - *t;
+  if ((dt < 0.0 && *h > 0.0) || (dt > 0.0 && *h < 0.0)) {
+    c->err = "step direction does not match t1 - t";
+    return 1;
+  }
+  if (c->run(t1, true)) return 1;
+  return hw2d_get_state(c, t, h, y);
+}
+
+int hw2d_stats(const hw2d_ctx* cc, long long* r, long long* a, long long* j) {
+  auto* c = const_cast<hw2d_ctx*>(cc);
+  if (!c || !c->read_ctl()) return 1;
+  if (r) *r = c->hctl->rhs;
+  if (a) *a = c->hctl->acc;
+  if (j) *j = c->hctl->rej;
+  return 0;
+}
+
+int hw2d_set_stream(hw2d_ctx* c, void* s) {
+  if (!c) return 1;
+  c->stream = s ? static_cast<cudaStream_t>(s) : c->own_stream;
+  return 0;
+}
+
+int hw2d_synchronize(hw2d_ctx* c) {
+  if (!c) return 1;
+  return cudaStreamSynchronize(c->stream) == cudaSuccess ? 0 : 1;
+}
+
+}  // extern "C"

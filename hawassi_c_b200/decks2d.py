@@ -1,0 +1,281 @@
+"""Operator tables of the HAWASSI 2D flat-bottom RHS for seeded synthetic decks.
+
+The 2D RHS (2d/fun_odesolver.c:4404-4540) reads tables that the reference's
+set-up builds: the wavenumber grids (freqspace, 2d/functions.c:1810-1832), the
+exact-dispersion operators C2d and L2d (fun_operator_setup, :1514-1523), the
+aliasing mask (fun_aal2D, :1834-1880), the damping characteristic (fun_fbdy2D /
+fun_cfSA2D, :1958-2132), the nonlinear adjustment ChiAdj (fun_calcseacharacteristic
+with cfv, :787-793, :905-921), the area-source kernels newGam / SkewGam
+(fun_area_generation, vertical influx line, :2991-3085) and one influx signal
+per row (Spline_Signal / Spline_SkewSignal, :3241-3250).  This module restates
+those constructions in numpy for a flat bottom, no wall, no coupling and a
+vertical influx line spanning the domain, and synthesises the line signals from
+a seeded directional JONSWAP spectrum (cos^2s spreading) on the (ky, omega) grid.
+
+`tables()` returns a dict with the arrays the engine's `hw2d_tables` takes.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+GRAV = 9.80665   # 2d/var_initialization.h:246
+
+
+def freqspace(length: float, n: int) -> np.ndarray:
+    """2d/functions.c:1810-1832 (its quirks included: spacing 2 pi (N-2)/(len (N-1))
+    for even N, and k[0] = 1e-10)."""
+    dk = 2 * math.pi / length
+    fmin = -0.5 * 2 * math.pi / (length / (n - 1))
+    fmax = -fmin - dk if n % 2 == 0 else -fmin
+    d = (fmax - fmin) / (n - 1)
+    out = np.empty(n)
+    for i in range(n // 2):
+        out[i] = fmin + (n // 2 + i) * d
+    for ni, i in enumerate(range(n // 2, n)):
+        out[i] = fmin + ni * d
+    out[0] = 1e-10
+    return out
+
+
+def aal2d(kx: np.ndarray, ky: np.ndarray, cutfrac: int) -> np.ndarray:
+    """fun_aal2D (2d/functions.c:1834-1880)."""
+    nx, ny = kx.size, ky.size
+    idx = max(int(math.floor(nx / cutfrac)) - 1, 0)
+    idy = max(int(math.floor(ny / cutfrac)) - 1, 0)
+    kxmax, kymax = abs(kx[idx]), abs(ky[idy])
+    KK = np.sqrt(kx[None, :] ** 2 + ky[:, None] ** 2)
+    if idx > 0 and idy > 0:
+        kmax = math.sqrt(kxmax ** 2 + kymax ** 2)
+        return np.where(np.abs(KK) > kmax, 0.0, 1.0)
+    alx = np.where(np.abs(kx) > kxmax, 0.0, 1.0)
+    aly = np.where(np.abs(ky) > kymax, 0.0, 1.0)
+    return aly[:, None] * alx[None, :]
+
+
+def _closest(a: np.ndarray, ref: float) -> int:
+    """fun_closest (2d/functions1.c:786-799): first index of the minimum distance."""
+    return int(np.argmin(np.abs(ref - a)))
+
+
+def _sign(v):
+    return np.where(np.asarray(v) < 0, -1.0, 1.0)
+
+
+def cfsa2d(x, y, Lleft, Lright, Lbottom, Ltop) -> np.ndarray:
+    """fun_cfSA2D (2d/functions.c:2084-2132)."""
+    nx, ny = x.size, y.size
+    ixl = _closest(x, x[0] + Lleft)
+    ixr = _closest(x, x[nx - 1] - Lright)
+    iyb = _closest(y, y[0] + Lbottom)
+    iyt = _closest(y, y[ny - 1] - Ltop)
+    hxl = (x - x[0] >= 0).astype(float)
+    hxr = (x - x[ixr] >= 0).astype(float)
+    hyb = (y - y[0] >= 0).astype(float)
+    hyt = (y - y[iyt] >= 0).astype(float)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        A = _sign(x - x[ixl])
+        B = (1 - np.cos((x - x[0]) * math.pi / Lleft)) / 2 if Lleft else np.zeros(nx)
+        cfxl = hxl * np.maximum(A, B)
+        C = _sign(x - x[nx - 1])
+        D = (1 - np.cos((x - x[ixr]) * math.pi / Lright)) / 2 if Lright else np.zeros(nx)
+        cfxr = hxr * np.maximum(C, D)
+        if Lleft == 0:
+            cfxl = np.ones(nx)
+        if Lright == 0:
+            cfxr = np.zeros(nx)
+        E = _sign(y - y[iyb])
+        F = (1 - np.cos((y - y[0]) * math.pi / Lbottom)) / 2 if Lbottom else np.zeros(ny)
+        cfyb = hyb * np.maximum(E, F)
+        G = _sign(y - y[ny - 1])
+        H = (1 - np.cos((y - y[iyt]) * math.pi / Ltop)) / 2 if Ltop else np.zeros(ny)
+        cfyt = hyt * np.maximum(G, H)
+        if Lbottom == 0:
+            cfyb = np.ones(ny)
+        if Ltop == 0:
+            cfyt = np.zeros(ny)
+    return (cfyb - cfyt)[:, None] * (cfxl - cfxr)[None, :]
+
+
+def fbdy2d(x, y, Lleft, Lright, Lbottom, Ltop) -> np.ndarray:
+    """fun_fbdy2D (2d/functions.c:1958-2082), no wall and no coupling: the zone
+    length L of the last matching side (7 where it is 0) scales (1 - cfSA)/(0.9 L)."""
+    nx, ny = x.size, y.size
+    cf = cfsa2d(x, y, Lleft, Lright, Lbottom, Ltop)
+    ixl = _closest(x, x[0] + Lleft)
+    ixr = _closest(x, x[nx - 1] - Lright)
+    iyb = _closest(y, y[0] + Lbottom)
+    iyt = _closest(y, y[ny - 1] - Ltop)
+    out = np.empty((ny, nx))
+    L = 7.0
+    for i in range(ny):
+        for j in range(nx):
+            if j <= ixl:
+                L = Lleft
+            if j >= ixr:
+                L = Lright
+            if i < iyb and ixl < j < ixr:
+                L = Lbottom
+            if i > iyt and ixl < j < ixr:
+                L = Ltop
+            if L == 0:
+                L = 7.0
+            out[i, j] = (1 - cf[i, j]) / (0.9 * L)
+    return out
+
+
+def exact_cp(kx, ky, depth, ux=0.0, uy=0.0):
+    """fun_exact_Cp_val (2d/functions.c:101-112)."""
+    K = np.sqrt(kx ** 2 + ky ** 2)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        c = np.sqrt(GRAV * np.tanh(K * depth) / K) + (kx * ux + ky * uy) / K
+    return np.where(K == 0, math.sqrt(GRAV * depth), c)
+
+
+def exact_disp(kx, ky, depth, mdir=0.0, ux=0.0, uy=0.0):
+    """fun_exact_disp_val (2d/functions.c:114-120)."""
+    s = _sign(kx * math.cos(mdir) + ky * math.sin(mdir))
+    K = np.sqrt(kx ** 2 + ky ** 2)
+    return s * np.sqrt(GRAV * K * np.tanh(K * depth)) + kx * ux + ky * uy
+
+
+def exact_ug(k, d, U=0.0):
+    """fun_exact_Ug_val (2d/functions.c:82-92)."""
+    k = np.asarray(k, dtype=float)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        th = np.tanh(d * k)
+        ug = _sign(k) * math.sqrt(GRAV) / 2 / np.sqrt(k * th) * (th + k * (1 - th ** 2) * d) + U
+    return np.where(k == 0, math.sqrt(GRAV * d) + U, ug)
+
+
+def invers_omega(w: float, depth: float) -> float:
+    """Root k of w^2 = g k tanh(k depth) (Newton, as invers_omega, 2d/functions1.c:997)."""
+    k = w * w / GRAV
+    for _ in range(200):
+        f = GRAV * k * math.tanh(k * depth) - w * w
+        df = GRAV * math.tanh(k * depth) + GRAV * k * depth / math.cosh(k * depth) ** 2
+        dk = f / df
+        k -= dk
+        if abs(dk) < 1e-14 * k:
+            break
+    return k
+
+
+def _cf(x, Xi, dl):
+    """cfv/cfh profile (2d/functions.c:787-799)."""
+    h = (x - Xi >= 0).astype(float)
+    return h * np.maximum(_sign(x - (Xi + dl)), (1 - np.cos((x - Xi) * math.pi / dl)) / 2)
+
+
+def chiadj_vertical(x, ny, x_line, nadj, lam):
+    """ChiAdj of a vertical influx line spanning every row (2d/functions.c:905-921):
+    1 - cf(x, X - Nadj lam, Nadj lam) + cf(x, X, Nadj lam) on each row."""
+    if nadj == 0:
+        return np.ones((ny, x.size))
+    dl = nadj * lam
+    row = 1 - _cf(x, x_line - dl, dl) + _cf(x, x_line, dl)
+    return np.tile(row, (ny, 1))
+
+
+def area_kernels_vertical(x, y, kx, depth, x_line, Lbottom, Ltop):
+    """newGam and SkewGam of a vertical line spanning every row (fun_area_generation,
+    2d/functions.c:2991-3085): the group-velocity kernel of the x wavenumbers
+    (make_1d_sym + real inverse transform), shifted to the line, its x derivative, a
+    heaviside in y that leaves out the bottom/top damping zones, scaled by
+    (2 pi)^2 / (dx dy).  Returned in [row y][column x] layout."""
+    nx, ny = x.size, y.size
+    dx, dy = x[1] - x[0], y[1] - y[0]
+    ug_hat = exact_ug(kx, depth).astype(float)
+    for idd, j in enumerate(range(nx - 1, nx // 2, -1), start=1):   # make_1d_sym
+        ug_hat[j] = ug_hat[idd]
+    ugx = np.fft.ifft(ug_hat).real
+    ugx = np.roll(ugx, int(round((x_line - x[0]) / dx)))
+    dug = np.fft.fft(ugx)
+    d_hat = 1j * kx * dug
+    for idd, j in enumerate(range(nx - 1, nx // 2, -1), start=1):   # make_1dcom_sym
+        d_hat[j] = np.conj(d_hat[idd])
+    dxg = np.fft.ifft(d_hat).real
+    hb = np.ones(ny) if Lbottom == 0 else (y - (y[0] + Lbottom) >= 0).astype(float)
+    ht = np.zeros(ny) if Ltop == 0 else (y - (y[ny - 1] - Ltop) >= 0).astype(float)
+    heav = hb * (1 - ht)
+    fact = (2 * math.pi) ** 2 / (dx * dy)
+    return fact * heav[:, None] * ugx[None, :], fact * heav[:, None] * dxg[None, :]
+
+
+def directional_signals(y, t, Hs, Tp, gamma, s_spread, depth, n_freq, n_dir, seed, ramp=2.0, mdir=0.0):
+    """Seeded directional JONSWAP line signals on the influx line: n_freq x n_dir
+    components, frequencies on the time grid's Fourier lines and cross-line
+    wavenumbers k(omega) sin(theta) on the y grid's, cos^2s spreading about mdir,
+    uniform random phases.  Returns (signal, skew signal) [ny][nt]: the elevation
+    along the line and its quadrature, both with a cosine ramp of `ramp` s."""
+    rng = np.random.default_rng(seed)
+    ny, nt = y.size, t.size
+    dt = t[1] - t[0]
+    Ly = ny * (y[1] - y[0])
+    wp = 2 * math.pi / Tp
+    w = np.linspace(0.5 * wp, 3.0 * wp, n_freq)
+    sig = np.where(w <= wp, 0.07, 0.09)
+    S = (GRAV ** 2 / w ** 5) * np.exp(-1.25 * (wp / w) ** 4) * gamma ** np.exp(-((w - wp) ** 2) / (2 * sig ** 2 * wp ** 2))
+    dw = w[1] - w[0]
+    m0 = np.sum(S) * dw
+    S *= (Hs / 4.0) ** 2 / m0
+    th = np.linspace(-math.pi / 2, math.pi / 2, n_dir)
+    D = np.cos((th - mdir) / 2) ** (2 * s_spread)
+    dth = th[1] - th[0]
+    D /= np.sum(D) * dth
+    spec = np.zeros((ny, nt), dtype=complex)
+    for m in range(n_freq):
+        k = invers_omega(w[m], depth)
+        n_w = int(round(w[m] * nt * dt / (2 * math.pi)))
+        for d in range(n_dir):
+            a = math.sqrt(2 * S[m] * D[d] * dw * dth)
+            n_k = int(round(k * math.sin(th[d]) * Ly / (2 * math.pi))) % ny
+            spec[n_k, (-n_w) % nt] += a * np.exp(1j * rng.uniform(0, 2 * math.pi))
+    z = np.fft.ifft2(spec) * (ny * nt)   # sum_a a exp(i (ky y - w t + phi))
+    r = np.clip(t / ramp, 0, 1) if ramp > 0 else np.ones(nt)
+    r = 0.5 * (1 - np.cos(math.pi * r))
+    return z.real * r[None, :], z.imag * r[None, :]
+
+
+def tables(nx=1024, ny=1024, Lx=300.0, Ly=300.0, depth=3.0, Hs=0.5, Tp=6.0, gamma=3.3, s_spread=10,
+           n_freq=256, n_dir=64, t_end=300.0, dt=0.1, damp=30.0, x_line=45.0, nadj=1.0, model=2,
+           propagation=0, seed=0) -> dict:
+    """All tables of a flat-bottom 2D deck (vertical influx line at x_line)."""
+    x = np.linspace(0.0, Lx, nx)          # fun_intervaltovector (2d/functions1.c:204)
+    y = np.linspace(0.0, Ly, ny)
+    kx = freqspace(x[-1] - x[0], nx)
+    ky = freqspace(y[-1] - y[0], ny)
+    KX, KY = np.meshgrid(kx, ky)
+    c2d = exact_cp(KX, KY, depth)
+    om = exact_disp(KX, KY, depth)
+    l2d = om * om / GRAV
+    cutfrac = {1: 2, 2: 4}[model]
+    aal = aal2d(kx, ky, cutfrac)
+    charac = fbdy2d(x, y, damp, damp, damp, damp)
+    wp = 2 * math.pi / Tp
+    kp = invers_omega(wp, depth)
+    cpeak = wp / kp                        # fun_exact_Cp1d_val(kp, depth, 0)
+    chi = chiadj_vertical(x, ny, x_line, nadj, 2 * math.pi / kp)
+    newgam, skewgam = area_kernels_vertical(x, y, kx, depth, x_line, damp, damp)
+    nt = int(round(t_end / dt)) + 1
+    tsig = np.arange(nt) * dt
+    sig, sigs = directional_signals(y, tsig, Hs, Tp, gamma, s_spread, depth, n_freq, n_dir, seed)
+    # The area kernel carries (2 pi)^2 / (dx dy) and integrates to that times dx along
+    # x; scaling the elevation by dy / (2 pi)^2 makes the line generate the target
+    # elevation (the reference reaches the same end by dividing the influx spectrum by
+    # the transform of the area function, 2d/functions.c:3196-3214).
+    scale = (y[1] - y[0]) / (2 * math.pi) ** 2
+    sig, sigs = sig * scale, sigs * scale
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    return dict(nx=nx, ny=ny, model=model, propagation=propagation, cpeak=float(cpeak), kx=f64(kx), ky=f64(ky),
+                c2d=f64(c2d), l2d=f64(l2d), aal=f64(aal), charac=f64(charac), chiadj=f64(chi),
+                newgam=f64(newgam), skewgam=f64(skewgam), nt=nt, tsig=f64(tsig), sig=f64(sig), sigskew=f64(sigs),
+                dt_out=dt, x=x, y=y)
+
+
+def config5(seed=0, **kw) -> dict:
+    """The 2D workload: 1024 x 1024 on 300 m x 300 m, flat 3 m depth, directional
+    JONSWAP Hs 0.5 m Tp 6 s gamma 3.3, cos^2s spreading s = 10, 256 x 64 seeded
+    components, HS2, 30 m damping zones, influx line at x = 45 m."""
+    return tables(seed=seed, **kw)

@@ -1,0 +1,136 @@
+"""ctypes binding of the 2D entry points (hw2d_*) of include/hawassi_b200.h.
+
+:class:`Engine2D` takes the operator tables of a 2D flat-bottom deck (the dict
+built by :mod:`hawassi_c_b200.decks2d`, or the reference's own set-up globals)
+and exposes ``rhs`` (rhs_AB2_2DF_uv, 2d/fun_odesolver.c:4458), ``evolve_apply``
+(gsl_odeiv2_evolve_apply, :2643) and ``run_to_time`` (the inner loop of
+ode_solver_uv, :2641-2647) with the state resident on the device.
+"""
+import ctypes
+
+import numpy as np
+
+from .engine import EngineError, HwOpts, load_library
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class Hw2dTables(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("model", ctypes.c_int), ("propagation", ctypes.c_int),
+        ("cpeak", ctypes.c_double),
+        ("kx", _dp), ("ky", _dp), ("c2d", _dp), ("l2d", _dp), ("aal", _dp), ("charac", _dp), ("chiadj", _dp),
+        ("newgam", _dp), ("skewgam", _dp),
+        ("nt", ctypes.c_int), ("tsig", _dp), ("sig", _dp), ("sigskew", _dp),
+    ]
+
+
+_bound = False
+
+
+def _lib():
+    global _bound
+    L = load_library()
+    if not _bound:
+        vp, dp, dd = ctypes.c_void_p, _dp, ctypes.c_double
+        llp = ctypes.POINTER(ctypes.c_longlong)
+        L.hw2d_create.restype = vp
+        L.hw2d_create.argtypes = [ctypes.POINTER(Hw2dTables), ctypes.POINTER(HwOpts)]
+        L.hw2d_destroy.argtypes = [vp]
+        L.hw2d_last_error.restype = ctypes.c_char_p
+        L.hw2d_last_error.argtypes = [vp]
+        L.hw2d_nx.argtypes = [vp]
+        L.hw2d_ny.argtypes = [vp]
+        L.hw2d_rhs.argtypes = [vp, dd, dp, dp]
+        L.hw2d_gsl_rhs.argtypes = [dd, dp, dp, vp]
+        L.hw2d_evolve_apply.argtypes = [vp, dp, dd, dp, dp]
+        L.hw2d_set_state.argtypes = [vp, dd, dd, dp]
+        L.hw2d_get_state.argtypes = [vp, dp, dp, dp]
+        L.hw2d_run_to_time.argtypes = [vp, dd]
+        L.hw2d_stats.argtypes = [vp, llp, llp, llp]
+        L.hw2d_set_stream.argtypes = [vp, vp]
+        L.hw2d_synchronize.argtypes = [vp]
+        _bound = True
+    return L
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+class Engine2D:
+    def __init__(self, tables, eps_abs=0.0, eps_rel=0.0, h0=0.0, device=0):
+        self._L = _lib()
+        keep = {}
+        for k in ("kx", "ky", "c2d", "l2d", "aal", "charac", "chiadj", "newgam", "skewgam", "tsig", "sig", "sigskew"):
+            v = tables.get(k)
+            keep[k] = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
+        self._keep = keep
+        tb = Hw2dTables(nx=int(tables["nx"]), ny=int(tables["ny"]), model=int(tables.get("model", 2)),
+                        propagation=int(tables.get("propagation", 0)), cpeak=float(tables["cpeak"]),
+                        nt=int(tables.get("nt", 0) if keep["sig"] is not None else 0),
+                        **{k: _ptr(v) for k, v in keep.items()})
+        o = HwOpts(eps_abs=eps_abs, eps_rel=eps_rel, h0=h0, device=device)
+        self._h = self._L.hw2d_create(ctypes.byref(tb), ctypes.byref(o))
+        if not self._h:
+            raise EngineError(self._L.hw2d_last_error(None).decode())
+        self.nx, self.ny = int(tables["nx"]), int(tables["ny"])
+        self.n = self.nx * self.ny
+
+    def _err(self):
+        return EngineError(self._L.hw2d_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.hw2d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def rhs(self, t, y):
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        out = np.empty(6 * self.n)
+        if self._L.hw2d_rhs(self._h, float(t), _ptr(y), _ptr(out)):
+            raise self._err()
+        return out
+
+    def evolve_apply(self, t, t1, h, y):
+        """One gsl_odeiv2_evolve_apply call; y (float64, 6*nx*ny) is updated in place."""
+        tt, hh = ctypes.c_double(t), ctypes.c_double(h)
+        if self._L.hw2d_evolve_apply(self._h, ctypes.byref(tt), float(t1), ctypes.byref(hh), _ptr(y)):
+            raise self._err()
+        return tt.value, hh.value
+
+    def set_state(self, t, h, y):
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        if self._L.hw2d_set_state(self._h, float(t), float(h), _ptr(y)):
+            raise self._err()
+
+    def state(self, with_y=True):
+        t, h = ctypes.c_double(), ctypes.c_double()
+        y = np.empty(6 * self.n) if with_y else None
+        if self._L.hw2d_get_state(self._h, ctypes.byref(t), ctypes.byref(h), _ptr(y)):
+            raise self._err()
+        return t.value, h.value, y
+
+    def run_to_time(self, t1):
+        if self._L.hw2d_run_to_time(self._h, float(t1)):
+            raise self._err()
+
+    def stats(self):
+        r, a, j = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        if self._L.hw2d_stats(self._h, ctypes.byref(r), ctypes.byref(a), ctypes.byref(j)):
+            raise self._err()
+        return {"rhs_calls": r.value, "accepted": a.value, "rejected": j.value}
+
+    def set_stream(self, stream_handle):
+        if self._L.hw2d_set_stream(self._h, ctypes.c_void_p(stream_handle)):
+            raise self._err()
+
+    def synchronize(self):
+        if self._L.hw2d_synchronize(self._h):
+            raise self._err()

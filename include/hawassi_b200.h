@@ -153,6 +153,61 @@ int hw_deck_table(const char* workdir, const hw_opts* opts, const char* name, do
 int hw_set_stream(hw_ctx* ctx, void* cuda_stream);
 int hw_synchronize(hw_ctx* ctx);
 
+/* ------------------------------------------------------------------------ */
+/* 2D flat-bottom twin (HS2, no wall, no breaking): rhs_AB2_2DF_uv and the    */
+/* gsl_odeiv2 rkf45 loop of ode_solver_uv (2d/fun_odesolver.c:2565-2647,     */
+/* 4458-4540).  State: 6*nx*ny doubles [Re eta^|Im eta^|Re u^|Im u^|Re v^|    */
+/* Im v^], row-major i*nx + j (2d/main.c:198-201).  The operator tables are   */
+/* the ones the reference's 2D set-up leaves in its globals (dominfo, Oprt,   */
+/* ChiAdj, newGam, SkewGam, Spline_Signal); the caller passes them here.      */
+/* ------------------------------------------------------------------------ */
+typedef struct hw2d_ctx hw2d_ctx;
+
+typedef struct hw2d_tables {
+    int nx, ny;                 /* powers of two, 64..1024                      */
+    int model;                  /* 2 = HS2 (evolinfo.model)                     */
+    int propagation;            /* 0 = Uni+, 1 = Uni-, 2 = Bi (vertical line)   */
+    double cpeak;               /* Oprt.Cpeak                                   */
+    const double* kx;           /* [nx] dominfo.kx                              */
+    const double* ky;           /* [ny] dominfo.ky                              */
+    const double* c2d;          /* [ny*nx] Oprt.C2d                             */
+    const double* l2d;          /* [ny*nx] Oprt.L2d                             */
+    const double* aal;          /* [ny*nx] dominfo.aal                          */
+    const double* charac;       /* [ny*nx] dominfo.fbdy.charac                  */
+    const double* chiadj;       /* [ny*nx] ChiAdj                               */
+    const double* newgam;       /* [ny*nx] newGam[j][i] at i*nx + j             */
+    const double* skewgam;      /* [ny*nx] SkewGam[j][i] at i*nx + j (or NULL)  */
+    int nt;                     /* samples per line signal (0: wavename zero)   */
+    const double* tsig;         /* [nt] dominfo.t                               */
+    const double* sig;          /* [ny*nt] Signal[i] (row i of the line)        */
+    const double* sigskew;      /* [ny*nt] SkewSignal[i] (or NULL)              */
+} hw2d_tables;
+
+/* opts: eps_abs/eps_rel (<= 0: the 2D reference's 1e-3 / 1e-2, 2d/main.c:196-197),
+ * h0 (<= 0: dt/5 of the signal grid, 2d/fun_odesolver.c:2580), device. */
+hw2d_ctx*   hw2d_create(const hw2d_tables* tables, const hw_opts* opts);
+void        hw2d_destroy(hw2d_ctx* ctx);
+const char* hw2d_last_error(const hw2d_ctx* ctx);   /* ctx may be NULL */
+int         hw2d_nx(const hw2d_ctx* ctx);
+int         hw2d_ny(const hw2d_ctx* ctx);
+
+/* One RHS evaluation (replaces rhs_AB2_2DF_uv). */
+int hw2d_rhs(hw2d_ctx* ctx, double t, const double* y, double* dydt);
+/* gsl_odeiv2_system.function-compatible (params = hw2d_ctx*):
+ *   gsl_odeiv2_system sys = {hw2d_gsl_rhs, NULL, 6 * nx * ny, ctx};  (2d/main.c:205) */
+int hw2d_gsl_rhs(double t, const double* y, double* dydt, void* params);
+/* gsl_odeiv2_evolve_apply(e, c, s, &sys, &t, t1, &h, y) with rkf45 + control_y. */
+int hw2d_evolve_apply(hw2d_ctx* ctx, double* t, double t1, double* h, double* y);
+
+/* Device-resident state: set it, run the evolve loop to t1 (the inner loop of
+ * ode_solver_uv) without returning to the host, read it back. */
+int hw2d_set_state(hw2d_ctx* ctx, double t, double h, const double* y);
+int hw2d_get_state(hw2d_ctx* ctx, double* t, double* h, double* y);   /* y may be NULL */
+int hw2d_run_to_time(hw2d_ctx* ctx, double t1);
+int hw2d_stats(const hw2d_ctx* ctx, long long* rhs_calls, long long* accepted, long long* rejected);
+int hw2d_set_stream(hw2d_ctx* ctx, void* cuda_stream);
+int hw2d_synchronize(hw2d_ctx* ctx);
+
 #ifdef __cplusplus
 }
 #endif

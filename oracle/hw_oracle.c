@@ -294,6 +294,18 @@ static double cspline_eval(const cspline* s, double x) {
     return y_lo + delx * (b_i + delx * (c_i + delx * d_i));
 }
 
+/* exported for the 2D restatement (hw_oracle2d.c), which evaluates the same
+ * GSL natural spline on each influx-line signal */
+void or_cspline_coeffs(int n, const double* x, const double* y, double* c_out) {
+    cspline s; cspline_init(&s, x, y, n);
+    memcpy(c_out, s.c, sizeof(double) * (size_t)n);
+    cspline_free(&s);
+}
+double or_cspline_eval(int n, const double* x, const double* y, const double* c, double t) {
+    cspline s; s.n = n; s.x = (double*)x; s.y = (double*)y; s.c = (double*)c;
+    return cspline_eval(&s, t);
+}
+
 /* ------------------------------------------------------------------------ */
 /* Exact dispersion (dispersion = "exact", 1d/main.cc:31)                   */
 /* ------------------------------------------------------------------------ */

@@ -1,0 +1,465 @@
+/*
+ * hw_oracle2d.c -- CPU restatement of the HAWASSI 2D flat-bottom RHS and its
+ * gsl_odeiv2 rkf45 stepping (TEST INFRASTRUCTURE ONLY, see hw_oracle2d.h).
+ *
+ * Every transform is the full complex 2D DFT the reference runs through FFTW
+ * (fftw_plan_dft_2d, unnormalised); the symmetrisation before each inverse
+ * transform, the real parts taken after it, the complex intermediate of
+ * fun_adjust and the order of the pointwise products follow the reference's
+ * statements one by one.
+ */
+#include "hw_oracle2d.h"
+
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+static const double GRAV = 9.80665;   /* 2d/var_initialization.h:246 */
+
+void or_fft(int n, const double* re_in, const double* im_in, double* re_out, double* im_out, int sign);
+void or_cspline_coeffs(int n, const double* x, const double* y, double* c_out);
+double or_cspline_eval(int n, const double* x, const double* y, const double* c, double t);
+
+static char g_err2[512];
+const char* or2d_last_error(void) { return g_err2; }
+static void set_err2(const char* fmt, ...) {
+    va_list ap; va_start(ap, fmt); vsnprintf(g_err2, sizeof g_err2, fmt, ap); va_end(ap);
+}
+
+typedef struct { double re, im; } cx;
+
+struct or2d_ctx {
+    int nx, ny, n, model, prop, nt;
+    double cpeak, eps_abs, eps_rel;
+    double *kx, *ky, *c2d, *l2d, *aal, *charac, *chiadj, *newgam, *skewgam;
+    double *tsig, *sig, *sigskew, *csig, *csigskew;   /* spline second-derivative coefficients */
+    long long rhs_calls, acc, rej;
+    /* rkf45 work vectors */
+    double *k1, *k2, *k3, *k4, *k5, *k6, *ytmp, *y0, *yerr, *dydt_in, *dydt_out;
+};
+
+static double* dup(const double* a, size_t n) {
+    double* p = (double*)malloc(sizeof(double) * n);
+    memcpy(p, a, sizeof(double) * n);
+    return p;
+}
+
+/* ------------------------------------------------------------------------ */
+/* 2D DFT = 1D transforms over rows, then over columns (FFTW's 2D result).   */
+/* ------------------------------------------------------------------------ */
+static void fft2(int nx, int ny, cx* a, int sign) {
+    int m = nx > ny ? nx : ny;
+    double *ri = malloc(sizeof(double) * m), *ii = malloc(sizeof(double) * m);
+    double *ro = malloc(sizeof(double) * m), *io = malloc(sizeof(double) * m);
+    for (int i = 0; i < ny; i++) {
+        for (int j = 0; j < nx; j++) { ri[j] = a[i * nx + j].re; ii[j] = a[i * nx + j].im; }
+        or_fft(nx, ri, ii, ro, io, sign);
+        for (int j = 0; j < nx; j++) { a[i * nx + j].re = ro[j]; a[i * nx + j].im = io[j]; }
+    }
+    for (int j = 0; j < nx; j++) {
+        for (int i = 0; i < ny; i++) { ri[i] = a[i * nx + j].re; ii[i] = a[i * nx + j].im; }
+        or_fft(ny, ri, ii, ro, io, sign);
+        for (int i = 0; i < ny; i++) { a[i * nx + j].re = ro[i]; a[i * nx + j].im = io[i]; }
+    }
+    free(ri); free(ii); free(ro); free(io);
+}
+
+void or2d_fft(int nx, int ny, const double* re_in, const double* im_in, double* re_out, double* im_out, int sign) {
+    int n = nx * ny;
+    cx* a = malloc(sizeof(cx) * n);
+    for (int q = 0; q < n; q++) { a[q].re = re_in[q]; a[q].im = im_in ? im_in[q] : 0.0; }
+    fft2(nx, ny, a, sign);
+    for (int q = 0; q < n; q++) { re_out[q] = a[q].re; im_out[q] = a[q].im; }
+    free(a);
+}
+
+/* fftwcomplex_2d_sym (2d/functions1.c:492-521), called there with (Nxy, Nt) =
+ * (Nx, Ny): the right half of every row is overwritten by the conjugate mirror
+ * of the left half, column 0 below row Ny/2 by the mirror of its upper half, and
+ * the four self-conjugate points lose their imaginary parts.  Column Nx/2 is left
+ * as it is (rows other than 0 and Ny/2). */
+static void sym2(cx* a, int Nxy, int Nt) {
+    a[0].im = 0;
+    a[0 * Nxy + (Nxy / 2)].im = 0;
+    a[Nt / 2 * Nxy].im = 0;
+    a[Nt / 2 * Nxy + (Nxy / 2)].im = 0;
+    for (int j = 1; j < Nxy / 2; j++) {
+        a[Nxy - j].re = a[j].re;
+        a[Nxy - j].im = -a[j].im;
+        a[Nt / 2 * Nxy + Nxy - j].re = a[Nt / 2 * Nxy + j].re;
+        a[Nt / 2 * Nxy + Nxy - j].im = -a[Nt / 2 * Nxy + j].im;
+    }
+    for (int i = 1; i < Nt / 2; i++) {
+        a[(Nt - i) * Nxy].re = a[i * Nxy].re;
+        a[(Nt - i) * Nxy].im = -a[i * Nxy].im;
+    }
+    int it = 1;
+    for (int i = 1; i < Nt; i++) {
+        int iy = 1;
+        for (int j = Nxy / 2 + 1; j < Nxy; j++) {
+            a[i * Nxy + j].re = a[(Nt - it) * Nxy + Nxy / 2 - iy].re;
+            a[i * Nxy + j].im = -a[(Nt - it) * Nxy + Nxy / 2 - iy].im;
+            iy++;
+        }
+        it++;
+    }
+}
+
+void or2d_sym(int nx, int ny, double* re, double* im) {
+    int n = nx * ny;
+    cx* a = malloc(sizeof(cx) * n);
+    for (int q = 0; q < n; q++) { a[q].re = re[q]; a[q].im = im[q]; }
+    sym2(a, nx, ny);
+    for (int q = 0; q < n; q++) { re[q] = a[q].re; im[q] = a[q].im; }
+    free(a);
+}
+
+/* ------------------------------------------------------------------------ */
+or2d_ctx* or2d_create(const or2d_tables* tb, double eps_abs, double eps_rel) {
+    if (!tb || tb->nx < 4 || tb->ny < 4 || (tb->nx & 1) || (tb->ny & 1)) {
+        set_err2("or2d_create: grid must be even and at least 4x4");
+        return NULL;
+    }
+    if (tb->model != 1 && tb->model != 2) { set_err2("or2d_create: model must be 1 (HS1) or 2 (HS2)"); return NULL; }
+    or2d_ctx* c = calloc(1, sizeof(or2d_ctx));
+    c->nx = tb->nx; c->ny = tb->ny; c->n = tb->nx * tb->ny;
+    c->model = tb->model; c->prop = tb->propagation; c->cpeak = tb->cpeak;
+    c->eps_abs = eps_abs > 0 ? eps_abs : 1e-3;
+    c->eps_rel = eps_rel > 0 ? eps_rel : 1e-2;
+    size_t n = (size_t)c->n;
+    c->kx = dup(tb->kx, c->nx); c->ky = dup(tb->ky, c->ny);
+    c->c2d = dup(tb->c2d, n); c->l2d = dup(tb->l2d, n); c->aal = dup(tb->aal, n);
+    c->charac = dup(tb->charac, n); c->chiadj = dup(tb->chiadj, n);
+    c->nt = (tb->sig && tb->newgam && tb->tsig) ? tb->nt : 0;
+    if (c->nt > 0) {
+        c->newgam = dup(tb->newgam, n);
+        c->skewgam = tb->skewgam ? dup(tb->skewgam, n) : calloc(n, sizeof(double));
+        c->tsig = dup(tb->tsig, c->nt);
+        c->sig = dup(tb->sig, n / c->nx * c->nt);
+        c->sigskew = tb->sigskew ? dup(tb->sigskew, (size_t)c->ny * c->nt) : calloc((size_t)c->ny * c->nt, sizeof(double));
+        c->csig = malloc(sizeof(double) * (size_t)c->ny * c->nt);
+        c->csigskew = malloc(sizeof(double) * (size_t)c->ny * c->nt);
+        for (int i = 0; i < c->ny; i++) {
+            or_cspline_coeffs(c->nt, c->tsig, c->sig + (size_t)i * c->nt, c->csig + (size_t)i * c->nt);
+            or_cspline_coeffs(c->nt, c->tsig, c->sigskew + (size_t)i * c->nt, c->csigskew + (size_t)i * c->nt);
+        }
+    }
+    size_t d = 6 * n;
+    double** w[] = {&c->k1, &c->k2, &c->k3, &c->k4, &c->k5, &c->k6, &c->ytmp, &c->y0, &c->yerr, &c->dydt_in, &c->dydt_out};
+    for (size_t q = 0; q < sizeof w / sizeof w[0]; q++) *w[q] = calloc(d, sizeof(double));
+    return c;
+}
+
+void or2d_destroy(or2d_ctx* c) {
+    if (!c) return;
+    double* f[] = {c->kx, c->ky, c->c2d, c->l2d, c->aal, c->charac, c->chiadj, c->newgam, c->skewgam, c->tsig,
+                   c->sig, c->sigskew, c->csig, c->csigskew, c->k1, c->k2, c->k3, c->k4, c->k5, c->k6, c->ytmp,
+                   c->y0, c->yerr, c->dydt_in, c->dydt_out};
+    for (size_t q = 0; q < sizeof f / sizeof f[0]; q++) free(f[q]);
+    free(c);
+}
+
+void or2d_stats(const or2d_ctx* c, long long* r, long long* a, long long* j) {
+    if (r) *r = c->rhs_calls;
+    if (a) *a = c->acc;
+    if (j) *j = c->rej;
+}
+
+/* ------------------------------------------------------------------------ */
+/* fun_adjust (2d/fun_odesolver.c:810-833): symmetrise Ahat in place, complex
+ * inverse transform, multiply both parts by ChiAdj/(Nx*Ny), forward transform. */
+static void fun_adjust(const or2d_ctx* c, cx* AChi_hat, cx* Ahat) {
+    int Nx = c->nx, Ny = c->ny, n = c->n;
+    cx* A = malloc(sizeof(cx) * n);
+    sym2(Ahat, Nx, Ny);
+    memcpy(A, Ahat, sizeof(cx) * n);
+    fft2(Nx, Ny, A, +1);
+    for (int i = 0; i < Ny; i++)
+        for (int j = 0; j < Nx; j++) {
+            AChi_hat[i * Nx + j].re = (A[i * Nx + j].re * c->chiadj[i * Nx + j] / (Nx * Ny));
+            AChi_hat[i * Nx + j].im = (A[i * Nx + j].im * c->chiadj[i * Nx + j] / (Nx * Ny));
+        }
+    fft2(Nx, Ny, AChi_hat, -1);
+    free(A);
+}
+
+/* fun_source (2d/fun_odesolver.c:886-983), vertical influx line: one signal per
+ * row, Source[i][j] = INsig_t[i] newGam[j][i] (twice that for Bi), SkewSource =
+ * -/+ INsig_skew_t[i] SkewGam[j][i] for Uni+/Uni- (0 for Bi); Source_hat is the
+ * sum of the two forward transforms. */
+static void fun_source(const or2d_ctx* c, double t, cx* Source_hat) {
+    int Nx = c->nx, Ny = c->ny, n = c->n;
+    if (c->nt <= 0) { memset(Source_hat, 0, sizeof(cx) * n); return; }
+    double* ins = malloc(sizeof(double) * Ny);
+    double* inss = malloc(sizeof(double) * Ny);
+    for (int j = 0; j < Ny; j++) {
+        ins[j] = or_cspline_eval(c->nt, c->tsig, c->sig + (size_t)j * c->nt, c->csig + (size_t)j * c->nt, t);
+        inss[j] = or_cspline_eval(c->nt, c->tsig, c->sigskew + (size_t)j * c->nt, c->csigskew + (size_t)j * c->nt, t);
+    }
+    cx* S0 = malloc(sizeof(cx) * n);
+    cx* SS = malloc(sizeof(cx) * n);
+    for (int i = 0; i < Ny; i++)
+        for (int j = 0; j < Nx; j++) {
+            double src, skew;
+            if (c->prop == 0) { src = ins[i] * c->newgam[i * Nx + j]; skew = -1 * inss[i] * c->skewgam[i * Nx + j]; }
+            else if (c->prop == 1) { src = ins[i] * c->newgam[i * Nx + j]; skew = 1 * inss[i] * c->skewgam[i * Nx + j]; }
+            else { src = 2 * ins[i] * c->newgam[i * Nx + j]; skew = 0; }
+            S0[i * Nx + j].re = src; S0[i * Nx + j].im = 0;
+            SS[i * Nx + j].re = skew; SS[i * Nx + j].im = 0;
+        }
+    fft2(Nx, Ny, S0, -1);
+    fft2(Nx, Ny, SS, -1);
+    for (int q = 0; q < n; q++) {
+        Source_hat[q].re = S0[q].re + SS[q].re;
+        Source_hat[q].im = S0[q].im + SS[q].im;
+    }
+    free(ins); free(inss); free(S0); free(SS);
+}
+
+/* rhs_AB1_2DF_uv / rhs_AB2_2DF_uv (2d/fun_odesolver.c:4404-4540) with the term
+ * functions fun_delphiH1hat (no wall, :2270-2283), fun_termshat_AB1_2DF_uv
+ * (:2962-3027) and fun_termshat_AB2_2DF_uv (:3136-3325); no friction, coupling,
+ * breaking or wall. */
+int or2d_rhs(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
+    const int Nx = c->nx, Ny = c->ny, n = c->n;
+    const double factIFFT = (double)Nx * Ny;
+    const double* kx = c->kx;
+    const double* ky = c->ky;
+    c->rhs_calls++;
+    cx* delphiH1hat = malloc(sizeof(cx) * n);
+    for (int i = 0; i < Ny; i++)
+        for (int j = 0; j < Nx; j++) {
+            const int q = i * Nx + j;
+            const double c2 = pow(c->c2d[q], 2);
+            cx du = {c2 / GRAV * Zhat[2 * n + q], c2 / GRAV * Zhat[3 * n + q]};
+            cx dv = {c2 / GRAV * Zhat[4 * n + q], c2 / GRAV * Zhat[5 * n + q]};
+            delphiH1hat[q].re = kx[j] * du.im + ky[i] * dv.im;
+            delphiH1hat[q].im = -kx[j] * du.re - ky[i] * dv.re;
+        }
+
+    /* spectra of the state, copies symmetrised before the inverse transforms */
+    cx *eta = malloc(sizeof(cx) * n), *u = malloc(sizeof(cx) * n), *v = malloc(sizeof(cx) * n);
+    cx *Lphi = NULL, *M0u = NULL, *M0v = NULL;
+    for (int q = 0; q < n; q++) {
+        eta[q].re = Zhat[q]; eta[q].im = Zhat[n + q];
+        u[q].re = Zhat[2 * n + q]; u[q].im = Zhat[3 * n + q];
+        v[q].re = Zhat[4 * n + q]; v[q].im = Zhat[5 * n + q];
+    }
+    if (c->model == 2) {
+        Lphi = malloc(sizeof(cx) * n); M0u = malloc(sizeof(cx) * n); M0v = malloc(sizeof(cx) * n);
+        for (int i = 0; i < Ny; i++)
+            for (int j = 0; j < Nx; j++) {
+                const int q = i * Nx + j;
+                const double c2 = pow(c->c2d[q], 2);
+                M0u[q].re = c2 / GRAV * kx[j] * Zhat[3 * n + q];
+                M0u[q].im = -c2 / GRAV * kx[j] * Zhat[2 * n + q];
+                M0v[q].re = c2 / GRAV * ky[i] * Zhat[5 * n + q];
+                M0v[q].im = -c2 / GRAV * ky[i] * Zhat[4 * n + q];
+                Lphi[q].re = M0u[q].re + M0v[q].re;
+                Lphi[q].im = M0u[q].im + M0v[q].im;
+            }
+    }
+    sym2(eta, Nx, Ny); sym2(u, Nx, Ny); sym2(v, Nx, Ny);
+    fft2(Nx, Ny, eta, +1); fft2(Nx, Ny, u, +1); fft2(Nx, Ny, v, +1);
+    if (c->model == 2) {
+        sym2(Lphi, Nx, Ny); sym2(M0u, Nx, Ny); sym2(M0v, Nx, Ny);
+        fft2(Nx, Ny, Lphi, +1); fft2(Nx, Ny, M0u, +1); fft2(Nx, Ny, M0v, +1);
+    }
+
+    /* physical products */
+    const double sevenC = 7 * c->cpeak;
+    cx *dampeta = malloc(sizeof(cx) * n), *dampu = malloc(sizeof(cx) * n), *dampv = malloc(sizeof(cx) * n);
+    cx *etaM0u = NULL, *eta_u = NULL, *etaM0v = NULL, *eta_v = NULL, *deletaH2 = NULL;
+    if (c->model == 2) {
+        etaM0u = malloc(sizeof(cx) * n); eta_u = malloc(sizeof(cx) * n);
+        etaM0v = malloc(sizeof(cx) * n); eta_v = malloc(sizeof(cx) * n); deletaH2 = malloc(sizeof(cx) * n);
+    }
+    const double f2 = pow(factIFFT, 2);
+    for (int q = 0; q < n; q++) {
+        const double ch = c->charac[q];
+        dampeta[q].re = sevenC * ch * eta[q].re / factIFFT; dampeta[q].im = 0;
+        dampu[q].re = sevenC * ch * u[q].re / factIFFT; dampu[q].im = 0;
+        dampv[q].re = sevenC * ch * v[q].re / factIFFT; dampv[q].im = 0;
+        if (c->model == 2) {
+            const double wallchar = 1.0;
+            etaM0u[q].re = eta[q].re * M0u[q].re / f2 * wallchar; etaM0u[q].im = 0;
+            eta_u[q].re = eta[q].re * u[q].re / f2 * wallchar; eta_u[q].im = 0;
+            etaM0v[q].re = eta[q].re * M0v[q].re / f2 * wallchar; etaM0v[q].im = 0;
+            eta_v[q].re = eta[q].re * v[q].re / f2 * wallchar; eta_v[q].im = 0;
+            deletaH2[q].re = 0.5 * ((pow(u[q].re, 2) + pow(v[q].re, 2)) - pow(Lphi[q].re, 2)) / f2 * wallchar;
+            deletaH2[q].im = 0;
+        }
+    }
+    fft2(Nx, Ny, dampeta, -1); fft2(Nx, Ny, dampu, -1); fft2(Nx, Ny, dampv, -1);
+
+    cx *ikxH2adj = NULL, *ikyH2adj = NULL, *deluH2adj = NULL, *delvH2adj = NULL;
+    if (c->model == 2) {
+        fft2(Nx, Ny, etaM0u, -1); fft2(Nx, Ny, eta_u, -1); fft2(Nx, Ny, etaM0v, -1);
+        fft2(Nx, Ny, eta_v, -1); fft2(Nx, Ny, deletaH2, -1);
+        cx *ikx = malloc(sizeof(cx) * n), *iky = malloc(sizeof(cx) * n);
+        cx *delu = malloc(sizeof(cx) * n), *delv = malloc(sizeof(cx) * n);
+        for (int i = 0; i < Ny; i++)
+            for (int j = 0; j < Nx; j++) {
+                const int q = i * Nx + j;
+                ikx[q].re = -kx[j] * deletaH2[q].im;
+                ikx[q].im = kx[j] * deletaH2[q].re;
+                iky[q].re = -ky[i] * deletaH2[q].im;
+                iky[q].im = ky[i] * deletaH2[q].re;
+                cx Lu = {c->l2d[q] * etaM0u[q].re, c->l2d[q] * etaM0u[q].im};
+                cx Lv = {c->l2d[q] * etaM0v[q].re, c->l2d[q] * etaM0v[q].im};
+                delu[q].re = -Lu.re + kx[j] * eta_u[q].im;
+                delu[q].im = -Lu.im - kx[j] * eta_u[q].re;
+                delv[q].re = -Lv.re + ky[i] * eta_v[q].im;
+                delv[q].im = -Lv.im - ky[i] * eta_v[q].re;
+            }
+        deluH2adj = malloc(sizeof(cx) * n); delvH2adj = malloc(sizeof(cx) * n);
+        ikxH2adj = malloc(sizeof(cx) * n); ikyH2adj = malloc(sizeof(cx) * n);
+        fun_adjust(c, deluH2adj, delu);
+        fun_adjust(c, delvH2adj, delv);
+        fun_adjust(c, ikxH2adj, ikx);
+        fun_adjust(c, ikyH2adj, iky);
+        free(ikx); free(iky); free(delu); free(delv);
+    }
+
+    cx* Source_hat = malloc(sizeof(cx) * n);
+    fun_source(c, t, Source_hat);
+
+    for (int i = 0; i < Ny; i++)
+        for (int j = 0; j < Nx; j++) {
+            const int q = i * Nx + j;
+            const double a = c->aal[q];
+            cx dphi = delphiH1hat[q];
+            cx ix = {0, 0}, iy = {0, 0};
+            if (c->model == 2) {
+                dphi.re = delphiH1hat[q].re + deluH2adj[q].re + delvH2adj[q].re;
+                dphi.im = delphiH1hat[q].im + deluH2adj[q].im + delvH2adj[q].im;
+                ix = ikxH2adj[q];
+                iy = ikyH2adj[q];
+            }
+            dt_Zhat[q] = (Source_hat[q].re + dphi.re - dampeta[q].re) * a;
+            dt_Zhat[n + q] = (Source_hat[q].im + dphi.im - dampeta[q].im) * a;
+            dt_Zhat[2 * n + q] = (GRAV * kx[j] * Zhat[n + q] - ix.re - dampu[q].re) * a;
+            dt_Zhat[3 * n + q] = (-GRAV * kx[j] * Zhat[q] - ix.im - dampu[q].im) * a;
+            dt_Zhat[4 * n + q] = (GRAV * ky[i] * Zhat[n + q] - iy.re - dampv[q].re) * a;
+            dt_Zhat[5 * n + q] = (-GRAV * ky[i] * Zhat[q] - iy.im - dampv[q].im) * a;
+        }
+
+    free(delphiH1hat); free(eta); free(u); free(v); free(Lphi); free(M0u); free(M0v);
+    free(dampeta); free(dampu); free(dampv); free(etaM0u); free(eta_u); free(etaM0v); free(eta_v);
+    free(deletaH2); free(ikxH2adj); free(ikyH2adj); free(deluH2adj); free(delvH2adj); free(Source_hat);
+    for (int q = 0; q < 6 * n; q++)
+        if (!isfinite(dt_Zhat[q])) return 1;
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* gsl_odeiv2 rkf45 (Fehlberg tableau, 5th-order solution propagated),
+ * control_y (a_y = 1, a_dydt = 0, safety 0.9) and evolve_apply (dydt_in at
+ * every call, final-step clipping, retry on an effective decrease), as called
+ * at 2d/fun_odesolver.c:2567-2647.                                          */
+/* ------------------------------------------------------------------------ */
+static const double ah[] = {1.0 / 4.0, 3.0 / 8.0, 12.0 / 13.0, 1.0, 1.0 / 2.0};
+static const double b3[] = {3.0 / 32.0, 9.0 / 32.0};
+static const double b4[] = {1932.0 / 2197.0, -7200.0 / 2197.0, 7296.0 / 2197.0};
+static const double b5[] = {8341.0 / 4104.0, -32832.0 / 4104.0, 29440.0 / 4104.0, -845.0 / 4104.0};
+static const double b6[] = {-6080.0 / 20520.0, 41040.0 / 20520.0, -28352.0 / 20520.0, 9295.0 / 20520.0, -5643.0 / 20520.0};
+static const double c1 = 902880.0 / 7618050.0, c3 = 3953664.0 / 7618050.0, c4 = 3855735.0 / 7618050.0,
+                    c5 = -1371249.0 / 7618050.0, c6 = 277020.0 / 7618050.0;
+static const double ec[] = {0.0, 1.0 / 360.0, 0.0, -128.0 / 4275.0, -2197.0 / 75240.0, 1.0 / 50.0, 2.0 / 55.0};
+
+static int rkf45_apply(or2d_ctx* c, double t, double h, double* y, double* yerr, const double* dydt_in, double* dydt_out) {
+    const int dim = 6 * c->n;
+    double *k1 = c->k1, *k2 = c->k2, *k3 = c->k3, *k4 = c->k4, *k5 = c->k5, *k6 = c->k6, *ytmp = c->ytmp;
+    memcpy(k1, dydt_in, sizeof(double) * dim);
+    for (int i = 0; i < dim; i++) ytmp[i] = y[i] + ah[0] * h * k1[i];
+    if (or2d_rhs(c, t + ah[0] * h, ytmp, k2)) return 1;
+    for (int i = 0; i < dim; i++) ytmp[i] = y[i] + h * (b3[0] * k1[i] + b3[1] * k2[i]);
+    if (or2d_rhs(c, t + ah[1] * h, ytmp, k3)) return 1;
+    for (int i = 0; i < dim; i++) ytmp[i] = y[i] + h * (b4[0] * k1[i] + b4[1] * k2[i] + b4[2] * k3[i]);
+    if (or2d_rhs(c, t + ah[2] * h, ytmp, k4)) return 1;
+    for (int i = 0; i < dim; i++) ytmp[i] = y[i] + h * (b5[0] * k1[i] + b5[1] * k2[i] + b5[2] * k3[i] + b5[3] * k4[i]);
+    if (or2d_rhs(c, t + ah[3] * h, ytmp, k5)) return 1;
+    for (int i = 0; i < dim; i++)
+        ytmp[i] = y[i] + h * (b6[0] * k1[i] + b6[1] * k2[i] + b6[2] * k3[i] + b6[3] * k4[i] + b6[4] * k5[i]);
+    if (or2d_rhs(c, t + ah[4] * h, ytmp, k6)) return 1;
+    for (int i = 0; i < dim; i++) {
+        const double di = c1 * k1[i] + c3 * k3[i] + c4 * k4[i] + c5 * k5[i] + c6 * k6[i];
+        y[i] += h * di;
+    }
+    if (or2d_rhs(c, t + h, y, dydt_out)) return 1;
+    for (int i = 0; i < dim; i++)
+        yerr[i] = h * (ec[1] * k1[i] + ec[3] * k3[i] + ec[4] * k4[i] + ec[5] * k5[i] + ec[6] * k6[i]);
+    return 0;
+}
+
+/* std_control_hadjust: -1 decrease, +1 increase, 0 keep */
+static int hadjust(const or2d_ctx* c, const double* y, const double* yerr, double* h) {
+    const int dim = 6 * c->n;
+    const double S = 0.9, ord = 5.0;
+    const double h_old = *h;
+    double rmax = 2.2250738585072014e-308;
+    for (int i = 0; i < dim; i++) {
+        const double D0 = c->eps_rel * (1.0 * fabs(y[i])) + c->eps_abs;
+        const double r = fabs(yerr[i]) / fabs(D0);
+        rmax = r > rmax ? r : rmax;
+    }
+    if (rmax > 1.1) {
+        double r = S / pow(rmax, 1.0 / ord);
+        if (r < 0.2) r = 0.2;
+        *h = r * h_old;
+        return -1;
+    } else if (rmax < 0.5) {
+        double r = S / pow(rmax, 1.0 / (ord + 1.0));
+        if (r > 5.0) r = 5.0;
+        if (r < 1.0) r = 1.0;
+        *h = r * h_old;
+        return 1;
+    }
+    return 0;
+}
+
+int or2d_evolve_apply(or2d_ctx* c, double* t, double t1, double* h, double* y) {
+    const int dim = 6 * c->n;
+    const double t0 = *t;
+    double h0 = *h;
+    const double dt = t1 - t0;
+    if ((dt < 0.0 && h0 > 0.0) || (dt > 0.0 && h0 < 0.0)) { set_err2("step direction"); return 1; }
+    memcpy(c->y0, y, sizeof(double) * dim);
+    if (or2d_rhs(c, t0, y, c->dydt_in)) { set_err2("non-finite RHS"); return 1; }
+    for (int attempt = 0; attempt < 1000; attempt++) {
+        int final_step = 0;
+        if ((dt >= 0.0 && h0 > dt) || (dt < 0.0 && h0 < dt)) { h0 = dt; final_step = 1; }
+        if (rkf45_apply(c, t0, h0, y, c->yerr, c->dydt_in, c->dydt_out)) {
+            memcpy(y, c->y0, sizeof(double) * dim);
+            set_err2("non-finite RHS");
+            return 1;
+        }
+        *t = final_step ? t1 : t0 + h0;
+        const double h_old = h0;
+        const int adj = hadjust(c, y, c->yerr, &h0);
+        if (adj == -1) {
+            const double t_curr = *t, t_next = (*t) + h0;
+            if (fabs(h0) < fabs(h_old) && t_next != t_curr) {
+                memcpy(y, c->y0, sizeof(double) * dim);
+                c->rej++;
+                continue;
+            }
+            h0 = h_old;
+        }
+        c->acc++;
+        *h = h0;
+        return 0;
+    }
+    set_err2("too many rejected steps");
+    return 1;
+}
+
+int or2d_run_to(or2d_ctx* c, double* t, double t1, double* h, double* y) {
+    while (*t < t1) {
+        int s = or2d_evolve_apply(c, t, t1, h, y);
+        if (s) return s;
+    }
+    return 0;
+}

@@ -1,0 +1,68 @@
+/*
+ * hw_oracle2d.h -- CPU oracle for the HAWASSI 2D flat-bottom pseudo-spectral RHS
+ * (rhs_AB1_2DF_uv / rhs_AB2_2DF_uv) and its gsl_odeiv2 rkf45 time stepping.
+ *
+ * TEST INFRASTRUCTURE ONLY: linked by the test-suite, __graft_entry__.smoke() and
+ * bench.py's CPU legs, never by the product library.  It restates
+ * 2d/fun_odesolver.c (RHS, term functions, symmetrisation, fun_adjust,
+ * fun_source, ode_solver_uv) on the operator tables the reference's set-up
+ * builds (kx, ky, C2d, L2d, aal, fbdy.charac, ChiAdj, newGam, SkewGam, the
+ * influx-line signals): the tables are inputs here, exactly as they are globals
+ * there.
+ *
+ * Parity unpinned: the reference ships no outputs for its 2D decks, so this
+ * restatement is checked only by its own consistency tests (linear dispersion of
+ * a free wave, Hermitian symmetry, the adjust identity at ChiAdj = 1).
+ */
+#ifndef HW_ORACLE2D_H
+#define HW_ORACLE2D_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct or2d_ctx or2d_ctx;
+
+typedef struct or2d_tables {
+    int nx, ny;                 /* grid, x fastest: index i*nx + j, i = y row  */
+    int model;                  /* 1 = HS1, 2 = HS2                            */
+    int propagation;            /* 0 = Uni+, 1 = Uni-, 2 = Bi (vertical line)  */
+    double cpeak;               /* Oprt.Cpeak                                  */
+    const double* kx;           /* [nx]  dominfo.kx (freqspace)                */
+    const double* ky;           /* [ny]  dominfo.ky                            */
+    const double* c2d;          /* [ny*nx] Oprt.C2d                            */
+    const double* l2d;          /* [ny*nx] Oprt.L2d                            */
+    const double* aal;          /* [ny*nx] dominfo.aal                         */
+    const double* charac;       /* [ny*nx] dominfo.fbdy.charac                 */
+    const double* chiadj;       /* [ny*nx] ChiAdj                              */
+    const double* newgam;       /* [ny*nx] newGam[j][i] stored at i*nx + j     */
+    const double* skewgam;      /* [ny*nx] SkewGam, same layout; NULL: none    */
+    int nt;                     /* samples of each line signal (0: no source)  */
+    const double* tsig;         /* [nt]                                        */
+    const double* sig;          /* [ny*nt] INsig of row i at sig[i*nt + n]     */
+    const double* sigskew;      /* [ny*nt] skew signal, same layout            */
+} or2d_tables;
+
+/* Copies every table.  eps <= 0 selects the reference's 2D values (abs 1e-3,
+ * rel 1e-2, 2d/main.c:196-197).  Returns NULL on error (or2d_last_error). */
+or2d_ctx* or2d_create(const or2d_tables* tb, double eps_abs, double eps_rel);
+void or2d_destroy(or2d_ctx* c);
+const char* or2d_last_error(void);
+
+/* One RHS evaluation; y, dydt in the reference layout 6*nx*ny
+ * [Re eta^ | Im eta^ | Re u^ | Im u^ | Re v^ | Im v^]. */
+int or2d_rhs(or2d_ctx* c, double t, const double* y, double* dydt);
+/* gsl_odeiv2_evolve_apply restated (rkf45 + control_y).  Returns 0 on success. */
+int or2d_evolve_apply(or2d_ctx* c, double* t, double t1, double* h, double* y);
+/* evolve_apply until t == t1 (the inner loop of ode_solver_uv) */
+int or2d_run_to(or2d_ctx* c, double* t, double t1, double* h, double* y);
+void or2d_stats(const or2d_ctx* c, long long* rhs_calls, long long* accepted, long long* rejected);
+/* 2D complex DFT (FFTW sign convention, unnormalised), for tests. */
+void or2d_fft(int nx, int ny, const double* re_in, const double* im_in, double* re_out, double* im_out, int sign);
+/* the reference's fftwcomplex_2d_sym applied in place to a complex [ny*nx] array */
+void or2d_sym(int nx, int ny, double* re, double* im);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

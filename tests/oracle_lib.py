@@ -29,6 +29,19 @@ class OrOpts(ctypes.Structure):
     ]
 
 
+_dpt = ctypes.POINTER(ctypes.c_double)
+
+
+class Or2dTables(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("model", ctypes.c_int), ("propagation", ctypes.c_int),
+        ("cpeak", ctypes.c_double),
+        ("kx", _dpt), ("ky", _dpt), ("c2d", _dpt), ("l2d", _dpt), ("aal", _dpt), ("charac", _dpt),
+        ("chiadj", _dpt), ("newgam", _dpt), ("skewgam", _dpt),
+        ("nt", ctypes.c_int), ("tsig", _dpt), ("sig", _dpt), ("sigskew", _dpt),
+    ]
+
+
 def build():
     subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
 
@@ -36,8 +49,7 @@ def build():
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            build()
+        build()   # make: rebuilds only what changed
         L = ctypes.CDLL(LIB_PATH)
         vp, dp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int
         L.or_create.restype = vp
@@ -61,6 +73,16 @@ def lib():
         L.or_mlp_nparams.restype = ip
         L.or_mlp_loss_grad.restype = ctypes.c_double
         L.or_mlp_loss_grad.argtypes = [dp, ctypes.POINTER(ctypes.c_float), ip, dp]
+        L.or2d_create.restype = vp
+        L.or2d_create.argtypes = [ctypes.POINTER(Or2dTables), ctypes.c_double, ctypes.c_double]
+        L.or2d_destroy.argtypes = [vp]
+        L.or2d_last_error.restype = ctypes.c_char_p
+        L.or2d_rhs.argtypes = [vp, ctypes.c_double, dp, dp]
+        L.or2d_evolve_apply.argtypes = [vp, dp, ctypes.c_double, dp, dp]
+        L.or2d_run_to.argtypes = [vp, dp, ctypes.c_double, dp, dp]
+        L.or2d_stats.argtypes = [vp] + [ctypes.POINTER(ctypes.c_longlong)] * 3
+        L.or2d_fft.argtypes = [ip, ip, dp, dp, dp, dp, ip]
+        L.or2d_sym.argtypes = [ip, ip, dp, dp]
         _lib = L
     return _lib
 
@@ -162,3 +184,78 @@ def mlp_loss_grad(params, records):
     n = R.shape[0]
     L = lib().or_mlp_loss_grad(_p(P), R.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n, _p(g))
     return L, g
+
+
+class Oracle2D:
+    """The 2D flat-bottom restatement (oracle/hw_oracle2d.c) on a table dict."""
+
+    def __init__(self, tables, eps_abs=0.0, eps_rel=0.0):
+        L = lib()
+        keep = {}
+        for k in ("kx", "ky", "c2d", "l2d", "aal", "charac", "chiadj", "newgam", "skewgam", "tsig", "sig", "sigskew"):
+            v = tables.get(k)
+            keep[k] = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
+        self._keep = keep
+        tb = Or2dTables(nx=int(tables["nx"]), ny=int(tables["ny"]), model=int(tables.get("model", 2)),
+                        propagation=int(tables.get("propagation", 0)), cpeak=float(tables["cpeak"]),
+                        nt=int(tables.get("nt", 0) if keep["sig"] is not None else 0),
+                        **{k: (None if v is None else _p(v)) for k, v in keep.items()})
+        self.h = L.or2d_create(ctypes.byref(tb), eps_abs, eps_rel)
+        if not self.h:
+            raise RuntimeError("oracle2d: " + L.or2d_last_error().decode())
+        self.nx, self.ny = int(tables["nx"]), int(tables["ny"])
+        self.n = self.nx * self.ny
+
+    def close(self):
+        if self.h:
+            lib().or2d_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def rhs(self, t, y):
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        out = np.zeros(6 * self.n)
+        if lib().or2d_rhs(self.h, float(t), _p(y), _p(out)):
+            raise RuntimeError("oracle2d: non-finite RHS")
+        return out
+
+    def evolve_apply(self, t, t1, h, y):
+        tt, hh = ctypes.c_double(t), ctypes.c_double(h)
+        if lib().or2d_evolve_apply(self.h, ctypes.byref(tt), float(t1), ctypes.byref(hh), _p(y)):
+            raise RuntimeError("oracle2d: " + lib().or2d_last_error().decode())
+        return tt.value, hh.value
+
+    def run_to(self, t, t1, h, y):
+        tt, hh = ctypes.c_double(t), ctypes.c_double(h)
+        if lib().or2d_run_to(self.h, ctypes.byref(tt), float(t1), ctypes.byref(hh), _p(y)):
+            raise RuntimeError("oracle2d: " + lib().or2d_last_error().decode())
+        return tt.value, hh.value
+
+    def stats(self):
+        a, b, c = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        lib().or2d_stats(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+        return {"rhs_calls": a.value, "accepted": b.value, "rejected": c.value}
+
+
+def fft2(x, sign=-1):
+    x = np.asarray(x, dtype=np.complex128)
+    ny, nx = x.shape
+    re = np.ascontiguousarray(x.real).ravel()
+    im = np.ascontiguousarray(x.imag).ravel()
+    ro, io = np.zeros(nx * ny), np.zeros(nx * ny)
+    lib().or2d_fft(nx, ny, _p(re), _p(im), _p(ro), _p(io), sign)
+    return (ro + 1j * io).reshape(ny, nx)
+
+
+def sym2(x):
+    x = np.asarray(x, dtype=np.complex128)
+    ny, nx = x.shape
+    re = np.ascontiguousarray(x.real).ravel().copy()
+    im = np.ascontiguousarray(x.imag).ravel().copy()
+    lib().or2d_sym(nx, ny, _p(re), _p(im))
+    return (re + 1j * im).reshape(ny, nx)

@@ -1,0 +1,110 @@
+"""2D flat-bottom engine (hw2d_*) against the 2D oracle restatement."""
+import numpy as np
+import pytest
+
+from hawassi_c_b200 import decks2d
+from hawassi_c_b200.engine2d import Engine2D
+from oracle_lib import Oracle2D
+
+pytestmark = pytest.mark.gpu
+
+
+def tables(nx, ny, nadj=1.0, propagation=0, seed=1, source=True):
+    tb = decks2d.tables(nx=nx, ny=ny, Lx=0.9 * nx, Ly=0.9 * ny, depth=2.0, Hs=0.1, Tp=3.0, n_freq=24, n_dir=6,
+                        t_end=6.0, dt=0.1, damp=6.0, x_line=10.0, nadj=nadj, propagation=propagation, seed=seed)
+    if not source:
+        for k in ("newgam", "skewgam", "tsig", "sig", "sigskew"):
+            tb[k] = None
+        tb["nt"] = 0
+    return tb
+
+
+def band_limited_state(tb, amp, seed):
+    """Random spectral state inside the aliasing mask (what the stepper keeps)."""
+    rng = np.random.default_rng(seed)
+    n = tb["nx"] * tb["ny"]
+    a = np.tile(tb["aal"].ravel(), 6)
+    return amp * rng.standard_normal(6 * n) * a * np.sqrt(n)
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+@pytest.mark.parametrize("nx,ny,nadj,prop", [
+    (64, 64, 1.0, 0), (128, 64, 1.0, 1), (64, 128, 0.0, 2), (256, 256, 1.0, 0), (1024, 64, 1.0, 0),
+    (64, 1024, 1.0, 0),
+])
+def test_rhs_parity(nx, ny, nadj, prop):
+    tb = tables(nx, ny, nadj=nadj, propagation=prop)
+    eng, ora = Engine2D(tb, 1e-8, 1e-6), Oracle2D(tb, 1e-8, 1e-6)
+    for seed, t in ((1, 0.7), (2, 3.3)):
+        y = band_limited_state(tb, 0.02, seed)
+        assert rel(eng.rhs(t, y), ora.rhs(t, y)) < 1e-11
+
+
+def test_rhs_parity_unfiltered_state():
+    """Every wavenumber excited (the Nyquist lines and the symmetrisation edges too)."""
+    tb = tables(128, 64)
+    eng, ora = Engine2D(tb), Oracle2D(tb)
+    rng = np.random.default_rng(9)
+    y = 0.01 * rng.standard_normal(6 * tb["nx"] * tb["ny"]) * 90
+    assert rel(eng.rhs(1.0, y), ora.rhs(1.0, y)) < 1e-11
+
+
+def test_rhs_without_source():
+    tb = tables(128, 128, source=False)
+    eng, ora = Engine2D(tb), Oracle2D(tb)
+    y = band_limited_state(tb, 0.02, 4)
+    assert rel(eng.rhs(0.0, y), ora.rhs(0.0, y)) < 1e-11
+
+
+def test_evolve_apply_replay():
+    """One gsl_odeiv2_evolve_apply call from the same state, on both sides."""
+    tb = tables(64, 64)
+    eng, ora = Engine2D(tb, 1e-8, 1e-6), Oracle2D(tb, 1e-8, 1e-6)
+    y0 = band_limited_state(tb, 0.01, 5)
+    for t0, h0 in ((0.5, 0.01), (1.0, 0.2), (2.0, 1e-3)):
+        yg, yo = y0.copy(), y0.copy()
+        tg, hg = eng.evolve_apply(t0, t0 + 0.5, h0, yg)
+        to, ho = ora.evolve_apply(t0, t0 + 0.5, h0, yo)
+        assert abs(tg - to) <= 1e-13 * max(1.0, abs(to))
+        assert abs(hg - ho) <= 1e-6 * abs(ho)
+        assert rel(yg, yo) < 1e-12
+
+
+def test_run_to_time_parity():
+    tb = tables(64, 64)
+    eng, ora = Engine2D(tb, 1e-8, 1e-6), Oracle2D(tb, 1e-8, 1e-6)
+    n6 = 6 * tb["nx"] * tb["ny"]
+    y = np.zeros(n6)
+    eng.set_state(0.0, 0.02, y)
+    to, ho = 0.0, 0.02
+    for T in (1.0, 2.5, 4.0):
+        eng.run_to_time(T)
+        to, ho = ora.run_to(to, T, ho, y)
+        tg, hg, yg = eng.state()
+        assert tg == T
+        assert rel(yg, y) < 1e-9
+    sg, so = eng.stats(), ora.stats()
+    assert sg["accepted"] == so["accepted"] and sg["rejected"] == so["rejected"]
+
+
+def test_gsl_rhs_entry_matches_rhs():
+    import ctypes
+    tb = tables(64, 64)
+    eng = Engine2D(tb)
+    y = band_limited_state(tb, 0.02, 7)
+    a = eng.rhs(1.5, y)
+    out = np.empty_like(y)
+    dp = ctypes.POINTER(ctypes.c_double)
+    rc = eng._L.hw2d_gsl_rhs(1.5, y.ctypes.data_as(dp), out.ctypes.data_as(dp), ctypes.c_void_p(eng._h))
+    assert rc == 0
+    assert np.array_equal(a, out)
+
+
+def test_bad_tables_rejected():
+    tb = tables(64, 64)
+    tb["nx"] = 96
+    with pytest.raises(Exception):
+        Engine2D(tb)

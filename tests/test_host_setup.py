@@ -75,7 +75,7 @@ def test_seeded_influx_reproducible(tmp_path):
 
 def test_library_exports_every_declared_symbol():
     header = open(os.path.join(ROOT, "include", "hawassi_b200.h")).read()
-    declared = set(re.findall(r"\b(hw_[a-z_]+)\s*\(", header))
+    declared = set(re.findall(r"\b(hw2?d?_[a-z_0-9]+)\s*\(", header))
     lib = ctypes.CDLL(engine.library_path())
     missing = [s for s in sorted(declared) if not hasattr(lib, s)]
     assert not missing, missing

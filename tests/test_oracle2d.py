@@ -1,0 +1,119 @@
+"""CPU checks of the 2D flat-bottom oracle and of the Hermitian bookkeeping the
+device's row passes use (no GPU needed)."""
+import numpy as np
+import pytest
+
+from hawassi_c_b200 import decks2d
+from oracle_lib import Oracle2D, fft2, sym2
+
+GRAV = 9.80665
+
+
+def small_tables(nx=64, ny=32, nadj=1.0, propagation=0, seed=1, with_source=True):
+    tb = decks2d.tables(nx=nx, ny=ny, Lx=0.9 * nx, Ly=0.9 * ny, depth=2.0, Hs=0.1, Tp=3.0, n_freq=24, n_dir=6,
+                        t_end=6.0, dt=0.1, damp=6.0, x_line=10.0, nadj=nadj, propagation=propagation, seed=seed)
+    if not with_source:
+        for k in ("newgam", "skewgam", "tsig", "sig", "sigskew"):
+            tb[k] = None
+        tb["nt"] = 0
+    return tb
+
+
+def sym_at_grid(A, herm):
+    """The device's per-point formula (hw2d.cuh sym_at) evaluated on the whole grid."""
+    ny, nx = A.shape
+    out = np.empty_like(A)
+    for r in range(ny):
+        mr = (ny - r) % ny
+        for c in range(nx):
+            cm = (nx - c) % nx
+            a, m = A[r, c], A[mr, cm]
+            if 1 <= c < nx // 2:
+                v = a
+            elif c > nx // 2:
+                v = np.conj(m)
+            elif r == 0 or r == ny // 2:
+                v = complex(a.real, 0.0)
+            elif c == 0:
+                v = a if r < ny // 2 else np.conj(m)
+            else:
+                v = 0.5 * (a + np.conj(m)) if herm else a
+            out[r, c] = v
+    return out
+
+
+@pytest.mark.parametrize("shape", [(8, 16), (16, 8), (32, 32)])
+def test_symmetrisation_matches_reference_operator(shape):
+    rng = np.random.default_rng(3)
+    A = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    S = sym2(A)                                   # the reference's fftwcomplex_2d_sym
+    assert np.array_equal(sym_at_grid(A, herm=False), S)
+    # E = Hermitian part of S: what the real part of the inverse transform sees
+    ny, nx = shape
+    mirror = np.conj(S[(-np.arange(ny)) % ny][:, (-np.arange(nx)) % nx])
+    E = 0.5 * (S + mirror)
+    assert np.allclose(sym_at_grid(A, herm=True), E, rtol=0, atol=1e-15)
+    # the real part of iFFT(S) equals iFFT(E), which is real
+    assert np.allclose(np.fft.ifft2(S).real, np.fft.ifft2(E).real, atol=1e-15)
+    assert np.abs(np.fft.ifft2(E).imag).max() < 1e-15
+
+
+def test_packed_split_recovers_two_real_transforms():
+    rng = np.random.default_rng(4)
+    a, b = rng.standard_normal((16, 32)), rng.standard_normal((16, 32))
+    Z = fft2(a + 1j * b)
+    ny, nx = Z.shape
+    Zm = Z[(-np.arange(ny)) % ny][:, (-np.arange(nx)) % nx]
+    A = 0.5 * (Z + np.conj(Zm))
+    B = (Z - np.conj(Zm)) / 2j
+    assert np.allclose(A, np.fft.fft2(a), atol=1e-12)
+    assert np.allclose(B, np.fft.fft2(b), atol=1e-12)
+
+
+def test_oracle_fft2_matches_numpy():
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal((32, 64)) + 1j * rng.standard_normal((32, 64))
+    assert np.allclose(fft2(x, -1), np.fft.fft2(x), atol=1e-11)
+    assert np.allclose(fft2(x, +1), np.fft.ifft2(x) * x.size, atol=1e-11)
+
+
+def test_linear_limit_is_exact_dispersion():
+    """A small free wave, no source, no damping, no aliasing: the RHS is the linear
+    operator d eta^ = -i (kx u^ + ky v^) C^2/g, d u^ = -i g kx eta^."""
+    tb = small_tables(with_source=False, nadj=0.0)
+    tb["charac"] = np.zeros_like(tb["charac"])
+    tb["aal"] = np.ones_like(tb["aal"])
+    nx, ny, n = tb["nx"], tb["ny"], tb["nx"] * tb["ny"]
+    o = Oracle2D(tb, 1e-8, 1e-6)
+    rng = np.random.default_rng(6)
+    eta = 1e-9 * (rng.standard_normal((ny, nx)) + 1j * rng.standard_normal((ny, nx)))
+    u = 1e-9 * (rng.standard_normal((ny, nx)) + 1j * rng.standard_normal((ny, nx)))
+    v = 1e-9 * (rng.standard_normal((ny, nx)) + 1j * rng.standard_normal((ny, nx)))
+    y = np.concatenate([eta.real.ravel(), eta.imag.ravel(), u.real.ravel(), u.imag.ravel(),
+                        v.real.ravel(), v.imag.ravel()])
+    d = o.rhs(0.0, y)
+    kx, ky = np.meshgrid(tb["kx"], tb["ky"])
+    c2 = tb["c2d"].reshape(ny, nx) ** 2 / GRAV
+    deta = -1j * (kx * c2 * u + ky * c2 * v)
+    du = -1j * GRAV * kx * eta
+    dv = -1j * GRAV * ky * eta
+    got_eta = (d[:n] + 1j * d[n:2 * n]).reshape(ny, nx)
+    got_u = (d[2 * n:3 * n] + 1j * d[3 * n:4 * n]).reshape(ny, nx)
+    got_v = (d[4 * n:5 * n] + 1j * d[5 * n:] ).reshape(ny, nx)
+    scale = np.abs(deta).max()
+    assert np.abs(got_eta - deta).max() < 1e-6 * scale   # HS2 terms are O(amplitude^2)
+    assert np.allclose(got_u, du, rtol=0, atol=1e-6 * np.abs(du).max())
+    assert np.allclose(got_v, dv, rtol=0, atol=1e-6 * np.abs(dv).max())
+
+
+def test_source_generates_the_target_elevation():
+    tb = small_tables()
+    n = tb["nx"] * tb["ny"]
+    o = Oracle2D(tb, 1e-8, 1e-6)
+    y = np.zeros(6 * n)
+    t, h = o.run_to(0.0, 4.0, 0.02, y)
+    assert t == 4.0
+    eta = np.fft.ifft2((y[:n] + 1j * y[n:2 * n]).reshape(tb["ny"], tb["nx"])).real
+    assert 0.01 < np.abs(eta).max() < 0.2
+    st = o.stats()
+    assert st["accepted"] > 10 and st["rhs_calls"] >= 7 * st["accepted"]
