@@ -117,6 +117,8 @@ struct hw2d_ctx {
   cudaGraphExec_t attempt = nullptr;
   cudaStream_t graph_stream = nullptr;
   double h_first = 0.0;
+  long long launches = 0;   // kernels issued (graph nodes counted one by one)
+  int per_rhs = 5;
   std::string err;
 
   template <class T>
@@ -147,7 +149,9 @@ struct hw2d_ctx {
     row_dispatch(nx, 2, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
     if (!tb.chi_one || tb.has_src) col_dispatch(ny, 3, cols, s, tb, w, ctl, cond);
     row_dispatch(nx, 4, rows, s, tb, w, rk, ctl, ctl, mode, cond, out);
+    per_rhs = (!tb.chi_one || tb.has_src) ? 5 : 4;
   }
+  long long kernels_per_attempt() const { return 7LL * per_rhs + 3; }
   void attempt_launch(cudaStream_t s) {
     rhs_launch(1, hw2d::kIfK1, s, nullptr);
     for (int st = 2; st <= 6; ++st) rhs_launch(st, hw2d::kIfStage, s, nullptr);
@@ -191,6 +195,7 @@ struct hw2d_ctx {
   int run(double t1, bool one_step) {
     if (!build_graph()) return 1;
     hw2d::k2_begin<<<1, 1, 0, stream>>>(ctl, t1);
+    launches += 1;
     if (!check("begin")) return 1;
     if (!read_ctl()) return 1;
     const long long acc0 = hctl->acc;
@@ -205,6 +210,7 @@ struct hw2d_ctx {
       launched += batch;
       for (int b = 0; b < batch; ++b)
         if (cudaGraphLaunch(attempt, stream) != cudaSuccess) return check("graph launch") ? 1 : 1;
+      launches += batch * kernels_per_attempt();
       if (!read_ctl()) return 1;
       if (hctl->status != hw2d::kOk) break;
       if (one_step && hctl->acc > acc0) {
@@ -391,6 +397,7 @@ int hw2d_rhs(hw2d_ctx* c, double t, const double* y, double* dydt) {
   cudaMemcpyAsync(&c->ctl->t_direct, &t, sizeof(double), cudaMemcpyHostToDevice, c->stream);
   c->rhs_launch(0, hw2d::kAlways, c->stream, c->dout);
   hw2d::k2_to_reference<<<592, 256, 0, c->stream>>>(c->dout, c->dref, n);
+  c->launches += c->per_rhs + 2;
   cudaMemcpyAsync(dydt, c->dref, 6 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) return c->check("hw2d_rhs") ? 1 : 1;
   return c->check("hw2d_rhs") ? 0 : 1;
@@ -415,6 +422,7 @@ int hw2d_set_state(hw2d_ctx* c, double t, double h, const double* y) {
   *c->hctl = s;
   cudaMemcpyAsync(c->dref, y, 6 * c->n * sizeof(double), cudaMemcpyHostToDevice, c->stream);
   hw2d::k2_to_internal<<<592, 256, 0, c->stream>>>(c->dref, c->rk.y[0], c->n);
+  c->launches += 1;
   cudaMemcpyAsync(c->ctl, c->hctl, sizeof(Ctl2), cudaMemcpyHostToDevice, c->stream);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) return c->check("hw2d_set_state") ? 1 : 1;
   return c->check("hw2d_set_state") ? 0 : 1;
@@ -428,6 +436,7 @@ int hw2d_get_state(hw2d_ctx* c, double* t, double* h, double* y) {
   if (h) *h = c->hctl->h;
   if (y) {
     hw2d::k2_to_reference<<<592, 256, 0, c->stream>>>(c->rk.y[c->hctl->cur], c->dref, c->n);
+    c->launches += 1;
     cudaMemcpyAsync(y, c->dref, 6 * c->n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return c->check("hw2d_get_state") ? 1 : 1;
   }
@@ -461,6 +470,8 @@ int hw2d_stats(const hw2d_ctx* cc, long long* r, long long* a, long long* j) {
   if (j) *j = c->hctl->rej;
   return 0;
 }
+
+long long hw2d_launches(const hw2d_ctx* c) { return c ? c->launches : 0; }
 
 int hw2d_set_stream(hw2d_ctx* c, void* s) {
   if (!c) return 1;

@@ -41,7 +41,7 @@ EXPORTS = [
     "hw_mlp_set_params", "hw_mlp_grad", "hw_mlp_grad_device", "hw_mlp_train", "hw_mlp_infer",
     "hw2d_create", "hw2d_destroy", "hw2d_last_error", "hw2d_nx", "hw2d_ny", "hw2d_rhs", "hw2d_gsl_rhs",
     "hw2d_evolve_apply", "hw2d_set_state", "hw2d_get_state", "hw2d_run_to_time", "hw2d_stats",
-    "hw2d_set_stream", "hw2d_synchronize",
+    "hw2d_set_stream", "hw2d_synchronize", "hw2d_launches",
 ]
 
 

@@ -50,6 +50,8 @@ def _lib():
         L.hw2d_stats.argtypes = [vp, llp, llp, llp]
         L.hw2d_set_stream.argtypes = [vp, vp]
         L.hw2d_synchronize.argtypes = [vp]
+        L.hw2d_launches.restype = ctypes.c_longlong
+        L.hw2d_launches.argtypes = [vp]
         _bound = True
     return L
 
@@ -117,6 +119,14 @@ class Engine2D:
             raise self._err()
         return t.value, h.value, y
 
+    def state_into(self, y):
+        """Read the state into the caller's float64 array (pinned memory makes the copy
+        a direct DMA); returns (t, h)."""
+        t, h = ctypes.c_double(), ctypes.c_double()
+        if self._L.hw2d_get_state(self._h, ctypes.byref(t), ctypes.byref(h), _ptr(y)):
+            raise self._err()
+        return t.value, h.value
+
     def run_to_time(self, t1):
         if self._L.hw2d_run_to_time(self._h, float(t1)):
             raise self._err()
@@ -130,6 +140,9 @@ class Engine2D:
     def set_stream(self, stream_handle):
         if self._L.hw2d_set_stream(self._h, ctypes.c_void_p(stream_handle)):
             raise self._err()
+
+    def launches(self):
+        return int(self._L.hw2d_launches(self._h))
 
     def synchronize(self):
         if self._L.hw2d_synchronize(self._h):

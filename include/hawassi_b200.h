@@ -205,6 +205,8 @@ int hw2d_set_state(hw2d_ctx* ctx, double t, double h, const double* y);
 int hw2d_get_state(hw2d_ctx* ctx, double* t, double* h, double* y);   /* y may be NULL */
 int hw2d_run_to_time(hw2d_ctx* ctx, double t1);
 int hw2d_stats(const hw2d_ctx* ctx, long long* rhs_calls, long long* accepted, long long* rejected);
+/* kernels this context has launched so far (each node of a replayed graph counted) */
+long long hw2d_launches(const hw2d_ctx* ctx);
 int hw2d_set_stream(hw2d_ctx* ctx, void* cuda_stream);
 int hw2d_synchronize(hw2d_ctx* ctx);
 
