@@ -62,6 +62,14 @@ struct Tab2 {
   const double* sigsc;
   const double2* twx;           // exp(-2 pi i q / nx)
   const double2* twy;           // exp(-2 pi i q / ny)
+  // varying bottom, two reference depths (rhs_AB2_2DB_uv); var = 0 on a flat bottom
+  int var;
+  const double* gmin;           // Gam_min, Gam_plus (physical)
+  const double* gplus;
+  const double* cmin;           // Csqr2d_min, Csqr2d_plus (spectral)
+  const double* cplus;
+  const double* omin;           // Om2dSq_min, Om2dSq_plus (spectral)
+  const double* oplus;
 };
 
 struct Work2 {
@@ -75,6 +83,11 @@ struct Work2 {
   double* insig;                // [ny] line signal at the stage time
   double* insigs;
   double* part;                 // per-block maxima of the error ratio
+  // varying bottom only
+  double* phys;                 // eta, u, v in physical space (3 real fields)
+  double* pe;                   // eta M0u, eta M0v in physical space (2 real fields)
+  double2* H1;                  // delu H1^, delv H1^ (2 fields)
+  double2* EU;                  // (eta u)^, (eta v)^, deletaH2^ (3 fields)
 };
 
 // device control block of the stepper (one per engine)
@@ -606,11 +619,18 @@ k2_rowE(Tab2 tb, Work2 w, RK2 rk, const Ctl2* __restrict__ ctl, int mode, int co
     for (int j = threadIdx.x; j < Nx; j += blockDim.x) {
       const size_t q = (size_t)r * Nx + j;
       const double kxv = tb.kx[j];
-      const double a = tb.aal[q], cg = tb.c2g[q];
+      const double a = tb.aal[q], cg = tb.var ? 0.0 : tb.c2g[q];
       const double2 ze = w.z[q], zu = w.z[n + q], zv = w.z[2 * n + q];
-      // delphiH1^ = -i (kx C^2/g u^ + ky C^2/g v^)
-      const double2 du1 = make_double2(cg * zu.x, cg * zu.y), dv1 = make_double2(cg * zv.x, cg * zv.y);
-      double2 dphi = make_double2(kxv * du1.y + kyv * dv1.y, -kxv * du1.x - kyv * dv1.x);
+      double2 dphi;
+      if (tb.var) {
+        // delu H1^ + delv H1^ from the two-depth operator (2d/fun_odesolver.c:4560-4563)
+        const double2 h1u = w.H1[q], h1v = w.H1[n + q];
+        dphi = make_double2(h1u.x + h1v.x, h1u.y + h1v.y);
+      } else {
+        // delphiH1^ = -i (kx C^2/g u^ + ky C^2/g v^)
+        const double2 du1 = make_double2(cg * zu.x, cg * zu.y), dv1 = make_double2(cg * zv.x, cg * zv.y);
+        dphi = make_double2(kxv * du1.y + kyv * dv1.y, -kxv * du1.x - kyv * dv1.x);
+      }
       const double2 ix = slot(sm, M, 0 + k, j), iy = slot(sm, M, 2 + k, j);
       const double2 au = slot(sm, M, 4 + k, j), av = slot(sm, M, 6 + k, j);
       dphi = make_double2(dphi.x + au.x + av.x, dphi.y + au.y + av.y);

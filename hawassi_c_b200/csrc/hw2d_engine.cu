@@ -16,6 +16,7 @@
 
 #include "../../include/hawassi_b200.h"
 #include "hw2d.cuh"
+#include "hw2d_var.cuh"
 #include "hw_setup.hpp"
 
 using hw2d::Ctl2;
@@ -40,6 +41,13 @@ void set_attrs() {
   cudaFuncSetAttribute(hw2d::k2_rowC<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(8));
   cudaFuncSetAttribute(hw2d::k2_colD<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(10));
   cudaFuncSetAttribute(hw2d::k2_rowE<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(8));
+  cudaFuncSetAttribute(hw2d::k2v_rowA<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(8));
+  cudaFuncSetAttribute(hw2d::k2v_colB<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(12));
+  cudaFuncSetAttribute(hw2d::k2v_rowC<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(12));
+  cudaFuncSetAttribute(hw2d::k2v_colD<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(6));
+  cudaFuncSetAttribute(hw2d::k2v_rowE<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(6));
+  cudaFuncSetAttribute(hw2d::k2v_colF<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(8));
+  cudaFuncSetAttribute(hw2d::k2v_rowG<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(8));
 }
 
 // the five kernels of one RHS for a row length Mx and a column length My
@@ -49,12 +57,19 @@ void launch_row(int which, int nblocks, cudaStream_t s, const Tab2& tb, const Wo
   const dim3 blk(hw2d::kGroups * (M / 8));
   if (which == 0) hw2d::k2_rowA<M><<<nblocks, blk, smem_bytes<M>(6), s>>>(tb, w, rk, ctl, ctlw, mode, cond);
   else if (which == 2) hw2d::k2_rowC<M><<<nblocks, blk, smem_bytes<M>(8), s>>>(tb, w, ctl, cond);
+  else if (which == 10) hw2d::k2v_rowA<M><<<nblocks, blk, smem_bytes<M>(8), s>>>(tb, w, rk, ctl, ctlw, mode, cond);
+  else if (which == 12) hw2d::k2v_rowC<M><<<nblocks, blk, smem_bytes<M>(12), s>>>(tb, w, ctl, cond);
+  else if (which == 14) hw2d::k2v_rowE<M><<<nblocks, blk, smem_bytes<M>(6), s>>>(tb, w, ctl, cond);
+  else if (which == 16) hw2d::k2v_rowG<M><<<nblocks, blk, smem_bytes<M>(8), s>>>(tb, w, ctl, cond);
   else hw2d::k2_rowE<M><<<nblocks, blk, smem_bytes<M>(8), s>>>(tb, w, rk, ctl, mode, cond, out);
 }
 template <int M>
 void launch_col(int which, int nblocks, cudaStream_t s, const Tab2& tb, const Work2& w, const Ctl2* ctl, int cond) {
   const dim3 blk(hw2d::kGroups * (M / 8));
   if (which == 1) hw2d::k2_colB<M><<<nblocks, blk, smem_bytes<M>(8), s>>>(tb, w, ctl, cond);
+  else if (which == 11) hw2d::k2v_colB<M><<<nblocks, blk, smem_bytes<M>(12), s>>>(tb, w, ctl, cond);
+  else if (which == 13) hw2d::k2v_colD<M><<<nblocks, blk, smem_bytes<M>(6), s>>>(tb, w, ctl, cond);
+  else if (which == 15) hw2d::k2v_colF<M><<<nblocks, blk, smem_bytes<M>(8), s>>>(tb, w, ctl, cond);
   else hw2d::k2_colD<M><<<nblocks, blk, smem_bytes<M>(10), s>>>(tb, w, ctl, cond);
 }
 
@@ -144,6 +159,19 @@ struct hw2d_ctx {
   }
   void rhs_launch(int mode, int cond, cudaStream_t s, double2* out) {
     const int rows = ny / 2, cols = nx / 2;
+    if (tb.var) {
+      row_dispatch(nx, 10, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
+      col_dispatch(ny, 11, cols, s, tb, w, ctl, cond);
+      row_dispatch(nx, 12, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
+      col_dispatch(ny, 13, cols, s, tb, w, ctl, cond);
+      row_dispatch(nx, 14, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
+      col_dispatch(ny, 15, cols, s, tb, w, ctl, cond);
+      row_dispatch(nx, 16, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
+      if (!tb.chi_one || tb.has_src) col_dispatch(ny, 3, cols, s, tb, w, ctl, cond);
+      row_dispatch(nx, 4, rows, s, tb, w, rk, ctl, ctl, mode, cond, out);
+      per_rhs = (!tb.chi_one || tb.has_src) ? 9 : 8;
+      return;
+    }
     row_dispatch(nx, 0, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
     col_dispatch(ny, 1, cols, s, tb, w, ctl, cond);
     row_dispatch(nx, 2, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
@@ -330,11 +358,27 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
     c->h_first = 1e-3;
   }
   if (o && o->h0 > 0) c->h_first = o->h0;
+  const bool var = t->gam_min && t->gam_plus && t->csq_min && t->csq_plus && t->om2_min && t->om2_plus;
+  tb.var = var ? 1 : 0;
+  if (var) {
+    tb.gmin = c->upload(std::vector<double>(t->gam_min, t->gam_min + n));
+    tb.gplus = c->upload(std::vector<double>(t->gam_plus, t->gam_plus + n));
+    tb.cmin = c->upload(std::vector<double>(t->csq_min, t->csq_min + n));
+    tb.cplus = c->upload(std::vector<double>(t->csq_plus, t->csq_plus + n));
+    tb.omin = c->upload(std::vector<double>(t->om2_min, t->om2_min + n));
+    tb.oplus = c->upload(std::vector<double>(t->om2_plus, t->om2_plus + n));
+  }
 
   Work2& w = c->w;
   w.z = c->dalloc<double2>(3 * n);
-  w.R = c->dalloc<double2>(3 * n);
-  w.Q = c->dalloc<double2>(4 * n);
+  w.R = c->dalloc<double2>(4 * n);
+  w.Q = c->dalloc<double2>((var ? 6 : 4) * n);
+  if (var) {
+    w.phys = c->dalloc<double>(3 * n);
+    w.pe = c->dalloc<double>(2 * n);
+    w.H1 = c->dalloc<double2>(2 * n);
+    w.EU = c->dalloc<double2>(3 * n);
+  }
   w.D = c->dalloc<double2>(3 * n);
   w.W = chi_one ? nullptr : c->dalloc<double2>(4 * n);
   w.V = c->dalloc<double2>(4 * n);
@@ -351,7 +395,9 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
   c->ctl = c->dalloc<Ctl2>(1);
   bool ok = tb.kx && tb.ky && tb.c2g && tb.l2d && tb.aal && tb.damp && tb.chi && tb.twx && tb.twy && w.z && w.R &&
             w.Q && w.D && w.V && w.insig && w.insigs && w.part && c->dref && c->dout && c->ctl &&
-            (chi_one || w.W) && (!has_src || (tb.gx && tb.sx && tb.sig && w.src));
+            (chi_one || w.W) && (!has_src || (tb.gx && tb.sx && tb.sig && w.src)) &&
+            (!var || (tb.gmin && tb.gplus && tb.cmin && tb.cplus && tb.omin && tb.oplus && w.phys && w.pe && w.H1 &&
+                      w.EU));
   for (int i = 0; i < 2; ++i) ok = ok && rk.y[i] && rk.kk[i];
   for (int i = 0; i < 5; ++i) ok = ok && rk.ks[i];
   if (!ok || cudaMallocHost(&c->hctl, sizeof(Ctl2)) != cudaSuccess) {

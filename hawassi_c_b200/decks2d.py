@@ -238,10 +238,62 @@ def directional_signals(y, t, Hs, Tp, gamma, s_spread, depth, n_freq, n_dir, see
     return z.real * r[None, :], z.imag * r[None, :]
 
 
+def two_depth_operator(depth, kx, ky, omega_p, U=0.0, mdir=0.0):
+    """Tables of the two-reference-depth operator (funOprt_DispInterpolation_2p,
+    2d/functions.c:1534-1626): on 101 depths between the shallowest and deepest
+    point, the weights (gam_min, gam_plus) that make the blend of the two reference
+    phase speeds and squared frequencies exact at the local wavenumber of the peak
+    frequency; a natural cubic spline in depth gives them per point.  The spectral
+    tables are C^2 and Om^2 of the two reference depths."""
+    from scipy.interpolate import CubicSpline
+    d_min, d_max = float(depth.min()), float(depth.max())
+    N = 101
+    dD = (d_max - d_min) / (N - 1)
+    DD = d_min + dD * np.arange(N)
+    DD[-1] += 0.1 * dD
+
+    def cp1(k, D):
+        return math.sqrt(GRAV * D) + U if k == 0 else (math.copysign(1.0, k) * math.sqrt(GRAV * k * math.tanh(k * D)) + k * U) / k
+
+    def om2(k, D):
+        return (math.copysign(1.0, k) * math.sqrt(GRAV * k * math.tanh(k * D)) + k * U) ** 2
+
+    gmin, gplus = np.empty(N), np.empty(N)
+    for i in range(N):
+        kap = invers_omega(omega_p, DD[i])
+        cD, cm, cp = cp1(kap, DD[i]), cp1(kap, d_min), cp1(kap, d_max)
+        oD, om_, op_ = om2(kap, DD[i]), om2(kap, d_min), om2(kap, d_max)
+        det = cm * op_ - cp * om_
+        gmin[i] = (op_ * cD - cp * oD) / det
+        gplus[i] = (-om_ * cD + cm * oD) / det
+    sm_, sp_ = CubicSpline(DD, gmin, bc_type="natural"), CubicSpline(DD, gplus, bc_type="natural")
+    KX, KY = np.meshgrid(kx, ky)
+    out = {"gam_min": sm_(depth), "gam_plus": sp_(depth)}
+    for name, D in (("min", d_min), ("plus", d_max)):
+        out[f"om2_{name}"] = exact_disp(KX, KY, D, mdir, 0.0, 0.0) ** 2
+        out[f"csq_{name}"] = exact_cp(KX, KY, D) ** 2
+    return out
+
+
+def shoal_bathymetry(x, y, deep=5.0, shallow=0.5, x1=100.0, x2=285.0, seed=0):
+    """Depth 0.5-5 m: deep up to x1, a linear slope to `shallow` at x2, and a seeded
+    Gaussian shoal on the slope; clipped to [shallow, deep]."""
+    rng = np.random.default_rng(seed + 7919)
+    X, Y = np.meshgrid(x, y)
+    d = deep + (shallow - deep) * np.clip((X - x1) / (x2 - x1), 0.0, 1.0)
+    xc = x1 + (x2 - x1) * rng.uniform(0.3, 0.6)
+    yc = y[0] + (y[-1] - y[0]) * rng.uniform(0.3, 0.7)
+    sig = 0.08 * (x[-1] - x[0])
+    d -= 1.5 * np.exp(-((X - xc) ** 2 + (Y - yc) ** 2) / (2 * sig ** 2))
+    return np.clip(d, shallow, deep)
+
+
 def tables(nx=1024, ny=1024, Lx=300.0, Ly=300.0, depth=3.0, Hs=0.5, Tp=6.0, gamma=3.3, s_spread=10,
            n_freq=256, n_dir=64, t_end=300.0, dt=0.1, damp=30.0, x_line=45.0, nadj=1.0, model=2,
-           propagation=0, seed=0) -> dict:
-    """All tables of a flat-bottom 2D deck (vertical influx line at x_line)."""
+           propagation=0, seed=0, bathymetry="flat", shallow=0.5) -> dict:
+    """All tables of a 2D deck (vertical influx line at x_line).  bathymetry "flat":
+    depth everywhere (rhs_AB2_2DF_uv); "shoal": `depth` offshore sloping to
+    `shallow` with a seeded shoal, two reference depths (rhs_AB2_2DB_uv)."""
     x = np.linspace(0.0, Lx, nx)          # fun_intervaltovector (2d/functions1.c:204)
     y = np.linspace(0.0, Ly, ny)
     kx = freqspace(x[-1] - x[0], nx)
@@ -254,8 +306,14 @@ def tables(nx=1024, ny=1024, Lx=300.0, Ly=300.0, depth=3.0, Hs=0.5, Tp=6.0, gamm
     aal = aal2d(kx, ky, cutfrac)
     charac = fbdy2d(x, y, damp, damp, damp, damp)
     wp = 2 * math.pi / Tp
+    var = None
+    depth_field = None
+    if bathymetry != "flat":
+        depth_field = shoal_bathymetry(x, y, deep=depth, shallow=shallow,
+                                       x1=x[0] + 0.33 * (x[-1] - x[0]), x2=x[0] + 0.95 * (x[-1] - x[0]), seed=seed)
+        var = two_depth_operator(depth_field, kx, ky, wp)
     kp = invers_omega(wp, depth)
-    cpeak = wp / kp                        # fun_exact_Cp1d_val(kp, depth, 0)
+    cpeak = wp / kp                        # fun_exact_Cp1d_val(kp, depth at the influx line, 0)
     chi = chiadj_vertical(x, ny, x_line, nadj, 2 * math.pi / kp)
     newgam, skewgam = area_kernels_vertical(x, y, kx, depth, x_line, damp, damp)
     nt = int(round(t_end / dt)) + 1
@@ -268,14 +326,22 @@ def tables(nx=1024, ny=1024, Lx=300.0, Ly=300.0, depth=3.0, Hs=0.5, Tp=6.0, gamm
     scale = (y[1] - y[0]) / (2 * math.pi) ** 2
     sig, sigs = sig * scale, sigs * scale
     f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
-    return dict(nx=nx, ny=ny, model=model, propagation=propagation, cpeak=float(cpeak), kx=f64(kx), ky=f64(ky),
+    extra = {k: f64(v) for k, v in var.items()} if var else {}
+    if depth_field is not None:
+        extra["depth"] = f64(depth_field)
+    return dict(**extra, nx=nx, ny=ny, model=model, propagation=propagation, cpeak=float(cpeak), kx=f64(kx), ky=f64(ky),
                 c2d=f64(c2d), l2d=f64(l2d), aal=f64(aal), charac=f64(charac), chiadj=f64(chi),
                 newgam=f64(newgam), skewgam=f64(skewgam), nt=nt, tsig=f64(tsig), sig=f64(sig), sigskew=f64(sigs),
                 dt_out=dt, x=x, y=y)
 
 
-def config5(seed=0, **kw) -> dict:
-    """The 2D workload: 1024 x 1024 on 300 m x 300 m, flat 3 m depth, directional
-    JONSWAP Hs 0.5 m Tp 6 s gamma 3.3, cos^2s spreading s = 10, 256 x 64 seeded
-    components, HS2, 30 m damping zones, influx line at x = 45 m."""
-    return tables(seed=seed, **kw)
+def config5(seed=0, bathymetry="shoal", **kw) -> dict:
+    """The 2D workload: 1024 x 1024 on 300 m x 300 m, depth 5 m offshore sloping to
+    0.5 m with a seeded shoal (two reference depths; bathymetry="flat" gives a flat
+    3 m bottom), directional JONSWAP Hs 0.5 m Tp 6 s gamma 3.3, cos^2s spreading
+    s = 10, 256 x 64 seeded components, HS2, 30 m damping zones, influx line at
+    x = 45 m."""
+    if bathymetry == "flat":
+        return tables(seed=seed, **kw)
+    kw.setdefault("depth", 5.0)
+    return tables(seed=seed, bathymetry=bathymetry, **kw)

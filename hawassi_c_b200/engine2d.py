@@ -22,6 +22,8 @@ class Hw2dTables(ctypes.Structure):
         ("kx", _dp), ("ky", _dp), ("c2d", _dp), ("l2d", _dp), ("aal", _dp), ("charac", _dp), ("chiadj", _dp),
         ("newgam", _dp), ("skewgam", _dp),
         ("nt", ctypes.c_int), ("tsig", _dp), ("sig", _dp), ("sigskew", _dp),
+        ("gam_min", _dp), ("gam_plus", _dp), ("csq_min", _dp), ("csq_plus", _dp), ("om2_min", _dp),
+        ("om2_plus", _dp),
     ]
 
 
@@ -64,7 +66,8 @@ class Engine2D:
     def __init__(self, tables, eps_abs=0.0, eps_rel=0.0, h0=0.0, device=0):
         self._L = _lib()
         keep = {}
-        for k in ("kx", "ky", "c2d", "l2d", "aal", "charac", "chiadj", "newgam", "skewgam", "tsig", "sig", "sigskew"):
+        for k in ("kx", "ky", "c2d", "l2d", "aal", "charac", "chiadj", "newgam", "skewgam", "tsig", "sig", "sigskew",
+                  "gam_min", "gam_plus", "csq_min", "csq_plus", "om2_min", "om2_plus"):
             v = tables.get(k)
             keep[k] = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
         self._keep = keep

@@ -154,7 +154,7 @@ int hw_set_stream(hw_ctx* ctx, void* cuda_stream);
 int hw_synchronize(hw_ctx* ctx);
 
 /* ------------------------------------------------------------------------ */
-/* 2D flat-bottom twin (HS2, no wall, no breaking): rhs_AB2_2DF_uv and the    */
+/* 2D twin (HS2, no wall, no breaking): rhs_AB2_2DF_uv / rhs_AB2_2DB_uv and the*/
 /* gsl_odeiv2 rkf45 loop of ode_solver_uv (2d/fun_odesolver.c:2565-2647,     */
 /* 4458-4540).  State: 6*nx*ny doubles [Re eta^|Im eta^|Re u^|Im u^|Re v^|    */
 /* Im v^], row-major i*nx + j (2d/main.c:198-201).  The operator tables are   */
@@ -181,6 +181,14 @@ typedef struct hw2d_tables {
     const double* tsig;         /* [nt] dominfo.t                               */
     const double* sig;          /* [ny*nt] Signal[i] (row i of the line)        */
     const double* sigskew;      /* [ny*nt] SkewSignal[i] (or NULL)              */
+    /* varying bottom, two reference depths (rhs_AB2_2DB_uv, ninterp = 2); all NULL
+     * for a flat bottom (rhs_AB2_2DF_uv, which reads c2d and l2d instead) */
+    const double* gam_min;      /* [ny*nx] Oprt.InterpD.Gam_min                 */
+    const double* gam_plus;     /* [ny*nx] Oprt.InterpD.Gam_plus                */
+    const double* csq_min;      /* [ny*nx] Oprt.InterpD.Csqr2d_min              */
+    const double* csq_plus;     /* [ny*nx] Oprt.InterpD.Csqr2d_plus             */
+    const double* om2_min;      /* [ny*nx] Oprt.InterpD.Om2dSq_min              */
+    const double* om2_plus;     /* [ny*nx] Oprt.InterpD.Om2dSq_plus             */
 } hw2d_tables;
 
 /* opts: eps_abs/eps_rel (<= 0: the 2D reference's 1e-3 / 1e-2, 2d/main.c:196-197),

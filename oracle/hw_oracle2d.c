@@ -35,6 +35,8 @@ struct or2d_ctx {
     double cpeak, eps_abs, eps_rel;
     double *kx, *ky, *c2d, *l2d, *aal, *charac, *chiadj, *newgam, *skewgam;
     double *tsig, *sig, *sigskew, *csig, *csigskew;   /* spline second-derivative coefficients */
+    int var;                                           /* varying bottom (two reference depths) */
+    double *gmin, *gplus, *cmin, *cplus, *omin, *oplus;
     long long rhs_calls, acc, rej;
     /* rkf45 work vectors */
     double *k1, *k2, *k3, *k4, *k5, *k6, *ytmp, *y0, *yerr, *dydt_in, *dydt_out;
@@ -146,6 +148,13 @@ or2d_ctx* or2d_create(const or2d_tables* tb, double eps_abs, double eps_rel) {
             or_cspline_coeffs(c->nt, c->tsig, c->sigskew + (size_t)i * c->nt, c->csigskew + (size_t)i * c->nt);
         }
     }
+    if (tb->gam_min && tb->gam_plus && tb->csq_min && tb->csq_plus && tb->om2_min && tb->om2_plus) {
+        if (c->model != 2) { set_err2("or2d_create: the varying-bottom RHS is restated for HS2 only"); free(c); return NULL; }
+        c->var = 1;
+        c->gmin = dup(tb->gam_min, n); c->gplus = dup(tb->gam_plus, n);
+        c->cmin = dup(tb->csq_min, n); c->cplus = dup(tb->csq_plus, n);
+        c->omin = dup(tb->om2_min, n); c->oplus = dup(tb->om2_plus, n);
+    }
     size_t d = 6 * n;
     double** w[] = {&c->k1, &c->k2, &c->k3, &c->k4, &c->k5, &c->k6, &c->ytmp, &c->y0, &c->yerr, &c->dydt_in, &c->dydt_out};
     for (size_t q = 0; q < sizeof w / sizeof w[0]; q++) *w[q] = calloc(d, sizeof(double));
@@ -156,7 +165,8 @@ void or2d_destroy(or2d_ctx* c) {
     if (!c) return;
     double* f[] = {c->kx, c->ky, c->c2d, c->l2d, c->aal, c->charac, c->chiadj, c->newgam, c->skewgam, c->tsig,
                    c->sig, c->sigskew, c->csig, c->csigskew, c->k1, c->k2, c->k3, c->k4, c->k5, c->k6, c->ytmp,
-                   c->y0, c->yerr, c->dydt_in, c->dydt_out};
+                   c->y0, c->yerr, c->dydt_in, c->dydt_out, c->gmin, c->gplus, c->cmin, c->cplus, c->omin,
+                   c->oplus};
     for (size_t q = 0; q < sizeof f / sizeof f[0]; q++) free(f[q]);
     free(c);
 }
@@ -218,11 +228,160 @@ static void fun_source(const or2d_ctx* c, double t, cx* Source_hat) {
     free(ins); free(inss); free(S0); free(SS);
 }
 
+
+/* HSSgen_2depth (2d/fun_odesolver.c:500-586): with phi the unnormalised physical
+ * field (its real part used) and phihat its spectrum,
+ * result = [F(gam_min Re F^-1 S(Op_min phihat)) + Op_min F(gam_min phi)
+ *           + F(gam_plus Re F^-1 S(Op_plus phihat)) + Op_plus F(gam_plus phi)] / 2 */
+static void hssgen_2depth(const or2d_ctx* c, const cx* phi, const cx* phihat, const double* Om, const double* Op,
+                          cx* result) {
+    const int Nx = c->nx, Ny = c->ny, n = c->n;
+    const double factIFFT = (double)Nx * Ny;
+    cx *L0m = malloc(sizeof(cx) * n), *L0p = malloc(sizeof(cx) * n);
+    for (int q = 0; q < n; q++) {
+        L0m[q].re = Om[q] * phihat[q].re; L0m[q].im = Om[q] * phihat[q].im;
+        L0p[q].re = Op[q] * phihat[q].re; L0p[q].im = Op[q] * phihat[q].im;
+    }
+    sym2(L0m, Nx, Ny); sym2(L0p, Nx, Ny);
+    fft2(Nx, Ny, L0m, +1); fft2(Nx, Ny, L0p, +1);
+    cx *gm = malloc(sizeof(cx) * n), *gp = malloc(sizeof(cx) * n);
+    cx *gmL = malloc(sizeof(cx) * n), *gpL = malloc(sizeof(cx) * n);
+    for (int q = 0; q < n; q++) {
+        gm[q].re = c->gmin[q] * phi[q].re / factIFFT; gm[q].im = 0;
+        gp[q].re = c->gplus[q] * phi[q].re / factIFFT; gp[q].im = 0;
+        gmL[q].re = c->gmin[q] * L0m[q].re / (Nx * Ny); gmL[q].im = 0;
+        gpL[q].re = c->gplus[q] * L0p[q].re / (Nx * Ny); gpL[q].im = 0;
+    }
+    fft2(Nx, Ny, gm, -1); fft2(Nx, Ny, gp, -1); fft2(Nx, Ny, gmL, -1); fft2(Nx, Ny, gpL, -1);
+    for (int q = 0; q < n; q++) {
+        result[q].re = (gmL[q].re + Om[q] * gm[q].re + gpL[q].re + Op[q] * gp[q].re) / 2;
+        result[q].im = (gmL[q].im + Om[q] * gm[q].im + gpL[q].im + Op[q] * gp[q].im) / 2;
+    }
+    free(L0m); free(L0p); free(gm); free(gp); free(gmL); free(gpL);
+}
+
+/* rhs_AB2_2DB_uv (2d/fun_odesolver.c:4542-4626) with fun_termshat_AB1_2DB_uv
+ * (:2874-2960) and fun_termshat_AB2_2DB_uv (:3327-3510), ninterp = 2, no wall,
+ * friction, coupling or breaking. */
+static int rhs_2db(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
+    const int Nx = c->nx, Ny = c->ny, n = c->n;
+    const double factIFFT = (double)Nx * Ny;
+    const double* kx = c->kx;
+    const double* ky = c->ky;
+    c->rhs_calls++;
+    /* AB1: symmetrised copies, inverse transforms, HSS of u^ and v^ with Csqr */
+    cx *eta_hat = malloc(sizeof(cx) * n), *u_hat = malloc(sizeof(cx) * n), *v_hat = malloc(sizeof(cx) * n);
+    for (int q = 0; q < n; q++) {
+        eta_hat[q].re = Zhat[q]; eta_hat[q].im = Zhat[n + q];
+        u_hat[q].re = Zhat[2 * n + q]; u_hat[q].im = Zhat[3 * n + q];
+        v_hat[q].re = Zhat[4 * n + q]; v_hat[q].im = Zhat[5 * n + q];
+    }
+    sym2(eta_hat, Nx, Ny); sym2(u_hat, Nx, Ny); sym2(v_hat, Nx, Ny);
+    cx *eta = malloc(sizeof(cx) * n), *u = malloc(sizeof(cx) * n), *v = malloc(sizeof(cx) * n);
+    memcpy(eta, eta_hat, sizeof(cx) * n); memcpy(u, u_hat, sizeof(cx) * n); memcpy(v, v_hat, sizeof(cx) * n);
+    fft2(Nx, Ny, eta, +1); fft2(Nx, Ny, u, +1); fft2(Nx, Ny, v, +1);
+    cx *Csqr_uhat = malloc(sizeof(cx) * n), *Csqr_vhat = malloc(sizeof(cx) * n);
+    hssgen_2depth(c, u, u_hat, c->cmin, c->cplus, Csqr_uhat);
+    hssgen_2depth(c, v, v_hat, c->cmin, c->cplus, Csqr_vhat);
+    const double sevenC = 7 * c->cpeak;
+    cx *dampeta = malloc(sizeof(cx) * n), *dampu = malloc(sizeof(cx) * n), *dampv = malloc(sizeof(cx) * n);
+    cx *deluH1 = malloc(sizeof(cx) * n), *delvH1 = malloc(sizeof(cx) * n);
+    for (int i = 0; i < Ny; i++)
+        for (int j = 0; j < Nx; j++) {
+            const int q = i * Nx + j;
+            const double ch = c->charac[q];
+            dampeta[q].re = sevenC * ch * eta[q].re / factIFFT; dampeta[q].im = 0;
+            dampu[q].re = sevenC * ch * u[q].re / factIFFT; dampu[q].im = 0;
+            dampv[q].re = sevenC * ch * v[q].re / factIFFT; dampv[q].im = 0;
+            deluH1[q].re = Csqr_uhat[q].im / GRAV * kx[j];
+            deluH1[q].im = -Csqr_uhat[q].re / GRAV * kx[j];
+            delvH1[q].re = Csqr_vhat[q].im / GRAV * ky[i];
+            delvH1[q].im = -Csqr_vhat[q].re / GRAV * ky[i];
+        }
+    fft2(Nx, Ny, dampeta, -1); fft2(Nx, Ny, dampu, -1); fft2(Nx, Ny, dampv, -1);
+    free(eta_hat); free(u_hat); free(v_hat); free(Csqr_uhat); free(Csqr_vhat);
+
+    /* AB2: the physical fields again (same transforms as AB1), M0 u = delu H1 */
+    cx *M0u = malloc(sizeof(cx) * n), *M0v = malloc(sizeof(cx) * n), *Lphi = malloc(sizeof(cx) * n);
+    for (int q = 0; q < n; q++) {
+        M0u[q] = deluH1[q];
+        M0v[q] = delvH1[q];
+        Lphi[q].re = deluH1[q].re + delvH1[q].re;
+        Lphi[q].im = deluH1[q].im + delvH1[q].im;
+    }
+    sym2(M0u, Nx, Ny); sym2(M0v, Nx, Ny); sym2(Lphi, Nx, Ny);
+    fft2(Nx, Ny, M0u, +1); fft2(Nx, Ny, M0v, +1); fft2(Nx, Ny, Lphi, +1);
+    const double f2 = pow(factIFFT, 2);
+    cx *etaM0u = malloc(sizeof(cx) * n), *eta_u = malloc(sizeof(cx) * n), *etaM0v = malloc(sizeof(cx) * n);
+    cx *eta_v = malloc(sizeof(cx) * n), *deletaH2 = malloc(sizeof(cx) * n);
+    for (int q = 0; q < n; q++) {
+        const double wallchar = 1.0;
+        etaM0u[q].re = eta[q].re * M0u[q].re / f2 * wallchar; etaM0u[q].im = 0;
+        eta_u[q].re = eta[q].re * u[q].re / f2 * wallchar; eta_u[q].im = 0;
+        etaM0v[q].re = eta[q].re * M0v[q].re / f2 * wallchar; etaM0v[q].im = 0;
+        eta_v[q].re = eta[q].re * v[q].re / f2 * wallchar; eta_v[q].im = 0;
+        deletaH2[q].re = 0.5 * ((pow(u[q].re, 2) + pow(v[q].re, 2)) - pow(Lphi[q].re, 2)) / f2 * wallchar;
+        deletaH2[q].im = 0;
+    }
+    cx *etaM0uhat = malloc(sizeof(cx) * n), *etaM0vhat = malloc(sizeof(cx) * n);
+    memcpy(etaM0uhat, etaM0u, sizeof(cx) * n); memcpy(etaM0vhat, etaM0v, sizeof(cx) * n);
+    fft2(Nx, Ny, etaM0uhat, -1); fft2(Nx, Ny, eta_u, -1); fft2(Nx, Ny, etaM0vhat, -1);
+    fft2(Nx, Ny, eta_v, -1); fft2(Nx, Ny, deletaH2, -1);
+    for (int q = 0; q < n; q++) {   /* "for operator": back to the unnormalised scale HSSgen divides out */
+        etaM0u[q].re = etaM0u[q].re * factIFFT;
+        etaM0v[q].re = etaM0v[q].re * factIFFT;
+    }
+    cx *LetaM0u = malloc(sizeof(cx) * n), *LetaM0v = malloc(sizeof(cx) * n);
+    hssgen_2depth(c, etaM0u, etaM0uhat, c->omin, c->oplus, LetaM0u);
+    hssgen_2depth(c, etaM0v, etaM0vhat, c->omin, c->oplus, LetaM0v);
+    cx *ikx = malloc(sizeof(cx) * n), *iky = malloc(sizeof(cx) * n);
+    cx *delu = malloc(sizeof(cx) * n), *delv = malloc(sizeof(cx) * n);
+    for (int i = 0; i < Ny; i++)
+        for (int j = 0; j < Nx; j++) {
+            const int q = i * Nx + j;
+            ikx[q].re = -kx[j] * deletaH2[q].im; ikx[q].im = kx[j] * deletaH2[q].re;
+            iky[q].re = -ky[i] * deletaH2[q].im; iky[q].im = ky[i] * deletaH2[q].re;
+            delu[q].re = kx[j] * eta_u[q].im - LetaM0u[q].re / GRAV;
+            delu[q].im = -kx[j] * eta_u[q].re - LetaM0u[q].im / GRAV;
+            delv[q].re = ky[i] * eta_v[q].im - LetaM0v[q].re / GRAV;
+            delv[q].im = -ky[i] * eta_v[q].re - LetaM0v[q].im / GRAV;
+        }
+    cx *deluH2adj = malloc(sizeof(cx) * n), *delvH2adj = malloc(sizeof(cx) * n);
+    cx *ikxH2adj = malloc(sizeof(cx) * n), *ikyH2adj = malloc(sizeof(cx) * n);
+    fun_adjust(c, deluH2adj, delu);
+    fun_adjust(c, delvH2adj, delv);
+    fun_adjust(c, ikxH2adj, ikx);
+    fun_adjust(c, ikyH2adj, iky);
+    cx* Source_hat = malloc(sizeof(cx) * n);
+    fun_source(c, t, Source_hat);
+    for (int i = 0; i < Ny; i++)
+        for (int j = 0; j < Nx; j++) {
+            const int q = i * Nx + j;
+            const double a = c->aal[q];
+            const double dre = deluH1[q].re + delvH1[q].re + deluH2adj[q].re + delvH2adj[q].re;
+            const double dim = deluH1[q].im + delvH1[q].im + deluH2adj[q].im + delvH2adj[q].im;
+            dt_Zhat[q] = (Source_hat[q].re + dre - dampeta[q].re) * a;
+            dt_Zhat[n + q] = (Source_hat[q].im + dim - dampeta[q].im) * a;
+            dt_Zhat[2 * n + q] = (GRAV * kx[j] * Zhat[n + q] - ikxH2adj[q].re - dampu[q].re) * a;
+            dt_Zhat[3 * n + q] = (-GRAV * kx[j] * Zhat[q] - ikxH2adj[q].im - dampu[q].im) * a;
+            dt_Zhat[4 * n + q] = (GRAV * ky[i] * Zhat[n + q] - ikyH2adj[q].re - dampv[q].re) * a;
+            dt_Zhat[5 * n + q] = (-GRAV * ky[i] * Zhat[q] - ikyH2adj[q].im - dampv[q].im) * a;
+        }
+    cx* fr[] = {eta, u, v, dampeta, dampu, dampv, deluH1, delvH1, M0u, M0v, Lphi, etaM0u, eta_u, etaM0v, eta_v,
+                deletaH2, etaM0uhat, etaM0vhat, LetaM0u, LetaM0v, ikx, iky, delu, delv, deluH2adj, delvH2adj,
+                ikxH2adj, ikyH2adj, Source_hat};
+    for (size_t q = 0; q < sizeof fr / sizeof fr[0]; q++) free(fr[q]);
+    for (int q = 0; q < 6 * n; q++)
+        if (!isfinite(dt_Zhat[q])) return 1;
+    return 0;
+}
+
 /* rhs_AB1_2DF_uv / rhs_AB2_2DF_uv (2d/fun_odesolver.c:4404-4540) with the term
  * functions fun_delphiH1hat (no wall, :2270-2283), fun_termshat_AB1_2DF_uv
  * (:2962-3027) and fun_termshat_AB2_2DF_uv (:3136-3325); no friction, coupling,
  * breaking or wall. */
 int or2d_rhs(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
+    if (c->var) return rhs_2db(c, t, Zhat, dt_Zhat);
     const int Nx = c->nx, Ny = c->ny, n = c->n;
     const double factIFFT = (double)Nx * Ny;
     const double* kx = c->kx;

@@ -1,6 +1,7 @@
 /*
- * hw_oracle2d.h -- CPU oracle for the HAWASSI 2D flat-bottom pseudo-spectral RHS
- * (rhs_AB1_2DF_uv / rhs_AB2_2DF_uv) and its gsl_odeiv2 rkf45 time stepping.
+ * hw_oracle2d.h -- CPU oracle for the HAWASSI 2D pseudo-spectral RHS (flat
+ * bottom: rhs_AB1_2DF_uv / rhs_AB2_2DF_uv; varying bottom with two reference
+ * depths: rhs_AB2_2DB_uv) and its gsl_odeiv2 rkf45 time stepping.
  *
  * TEST INFRASTRUCTURE ONLY: linked by the test-suite, __graft_entry__.smoke() and
  * bench.py's CPU legs, never by the product library.  It restates
@@ -41,6 +42,13 @@ typedef struct or2d_tables {
     const double* tsig;         /* [nt]                                        */
     const double* sig;          /* [ny*nt] INsig of row i at sig[i*nt + n]     */
     const double* sigskew;      /* [ny*nt] skew signal, same layout            */
+    /* varying bottom, two reference depths (ninterp = 2): NULL for a flat bottom */
+    const double* gam_min;      /* [ny*nx] Oprt.InterpD.Gam_min                */
+    const double* gam_plus;     /* [ny*nx] Oprt.InterpD.Gam_plus               */
+    const double* csq_min;      /* [ny*nx] Oprt.InterpD.Csqr2d_min             */
+    const double* csq_plus;     /* [ny*nx] Oprt.InterpD.Csqr2d_plus            */
+    const double* om2_min;      /* [ny*nx] Oprt.InterpD.Om2dSq_min             */
+    const double* om2_plus;     /* [ny*nx] Oprt.InterpD.Om2dSq_plus            */
 } or2d_tables;
 
 /* Copies every table.  eps <= 0 selects the reference's 2D values (abs 1e-3,

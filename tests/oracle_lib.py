@@ -39,6 +39,8 @@ class Or2dTables(ctypes.Structure):
         ("kx", _dpt), ("ky", _dpt), ("c2d", _dpt), ("l2d", _dpt), ("aal", _dpt), ("charac", _dpt),
         ("chiadj", _dpt), ("newgam", _dpt), ("skewgam", _dpt),
         ("nt", ctypes.c_int), ("tsig", _dpt), ("sig", _dpt), ("sigskew", _dpt),
+        ("gam_min", _dpt), ("gam_plus", _dpt), ("csq_min", _dpt), ("csq_plus", _dpt), ("om2_min", _dpt),
+        ("om2_plus", _dpt),
     ]
 
 
@@ -192,7 +194,8 @@ class Oracle2D:
     def __init__(self, tables, eps_abs=0.0, eps_rel=0.0):
         L = lib()
         keep = {}
-        for k in ("kx", "ky", "c2d", "l2d", "aal", "charac", "chiadj", "newgam", "skewgam", "tsig", "sig", "sigskew"):
+        for k in ("kx", "ky", "c2d", "l2d", "aal", "charac", "chiadj", "newgam", "skewgam", "tsig", "sig", "sigskew",
+                  "gam_min", "gam_plus", "csq_min", "csq_plus", "om2_min", "om2_plus"):
             v = tables.get(k)
             keep[k] = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
         self._keep = keep

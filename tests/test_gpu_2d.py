@@ -9,9 +9,10 @@ from oracle_lib import Oracle2D
 pytestmark = pytest.mark.gpu
 
 
-def tables(nx, ny, nadj=1.0, propagation=0, seed=1, source=True):
-    tb = decks2d.tables(nx=nx, ny=ny, Lx=0.9 * nx, Ly=0.9 * ny, depth=2.0, Hs=0.1, Tp=3.0, n_freq=24, n_dir=6,
-                        t_end=6.0, dt=0.1, damp=6.0, x_line=10.0, nadj=nadj, propagation=propagation, seed=seed)
+def tables(nx, ny, nadj=1.0, propagation=0, seed=1, source=True, bathymetry="flat"):
+    tb = decks2d.tables(nx=nx, ny=ny, Lx=0.9 * nx, Ly=0.9 * ny, depth=2.0, shallow=0.6, Hs=0.1, Tp=3.0, n_freq=24,
+                        n_dir=6, t_end=6.0, dt=0.1, damp=6.0, x_line=10.0, nadj=nadj, propagation=propagation,
+                        seed=seed, bathymetry=bathymetry)
     if not source:
         for k in ("newgam", "skewgam", "tsig", "sig", "sigskew"):
             tb[k] = None
@@ -108,3 +109,37 @@ def test_bad_tables_rejected():
     tb["nx"] = 96
     with pytest.raises(Exception):
         Engine2D(tb)
+
+
+# --- varying bottom, two reference depths (rhs_AB2_2DB_uv) -------------------
+@pytest.mark.parametrize("nx,ny,nadj", [(64, 64, 1.0), (128, 64, 0.0), (64, 128, 1.0), (256, 256, 1.0)])
+def test_rhs_parity_varying_depth(nx, ny, nadj):
+    tb = tables(nx, ny, nadj=nadj, bathymetry="shoal")
+    eng, ora = Engine2D(tb, 1e-8, 1e-6), Oracle2D(tb, 1e-8, 1e-6)
+    for seed, t in ((1, 0.7), (2, 3.3)):
+        y = band_limited_state(tb, 0.02, seed)
+        assert rel(eng.rhs(t, y), ora.rhs(t, y)) < 1e-11
+
+
+def test_rhs_parity_varying_depth_unfiltered():
+    tb = tables(128, 64, bathymetry="shoal")
+    eng, ora = Engine2D(tb), Oracle2D(tb)
+    rng = np.random.default_rng(11)
+    y = 0.01 * rng.standard_normal(6 * tb["nx"] * tb["ny"]) * 90
+    assert rel(eng.rhs(1.0, y), ora.rhs(1.0, y)) < 1e-11
+
+
+def test_run_to_time_parity_varying_depth():
+    tb = tables(64, 64, bathymetry="shoal")
+    eng, ora = Engine2D(tb, 1e-8, 1e-6), Oracle2D(tb, 1e-8, 1e-6)
+    y = np.zeros(6 * tb["nx"] * tb["ny"])
+    eng.set_state(0.0, 0.02, y)
+    to, ho = 0.0, 0.02
+    for T in (1.0, 2.5):
+        eng.run_to_time(T)
+        to, ho = ora.run_to(to, T, ho, y)
+        tg, hg, yg = eng.state()
+        assert tg == T
+        assert rel(yg, y) < 1e-9
+    sg, so = eng.stats(), ora.stats()
+    assert sg["accepted"] == so["accepted"] and sg["rejected"] == so["rejected"]
