@@ -126,11 +126,20 @@ __device__ __forceinline__ bool rhs_active(const Ctl2* c, int cond) {
 }
 
 // ---------------------------------------------------------------------------
-// one M-point slice in shared memory, transformed by one group of M/8 threads
+// one M-point slice in shared memory, transformed by one group of M/8 threads.
+// Groups of at least a warp synchronise on their own named barrier (id 1 + g), so
+// the groups of a CTA run their transforms independently; smaller groups fall
+// back to the CTA barrier and keep step with each other.
 // ---------------------------------------------------------------------------
+template <int T>
+__device__ __forceinline__ void group_sync(int g) {
+  if constexpr (T >= 32) asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(T) : "memory");
+  else __syncthreads();
+}
+
 template <int M, int R>
 __device__ __forceinline__ void gpass(double2* buf, int Ns, const double2* __restrict__ tw, int sign, int tid,
-                                      bool act) {
+                                      int g, bool act) {
   constexpr int T = M / 8;
   constexpr int NB = M / R;
   constexpr int BPT = 8 / R;
@@ -143,7 +152,7 @@ __device__ __forceinline__ void gpass(double2* buf, int Ns, const double2* __res
       for (int r = 0; r < R; ++r) v[u][r] = buf[pidx(j + r * NB)];
     }
   }
-  __syncthreads();
+  group_sync<T>(g);
   if (act) {
 #pragma unroll
     for (int u = 0; u < BPT; ++u) {
@@ -162,33 +171,41 @@ __device__ __forceinline__ void gpass(double2* buf, int Ns, const double2* __res
       for (int r = 0; r < R; ++r) buf[pidx(idxD + r * Ns)] = v[u][r];
     }
   }
-  __syncthreads();
+  group_sync<T>(g);
 }
 
 template <int M>
-__device__ __forceinline__ void gfft(double2* buf, const double2* __restrict__ tw, int sign, int tid, bool act) {
+__device__ __forceinline__ void gfft(double2* buf, const double2* __restrict__ tw, int sign, int tid, int g,
+                                     bool act) {
   constexpr int L8 = (M >= 512) ? 3 : (M >= 64 ? 2 : 1);
   constexpr int rem = M / (1 << (3 * L8));
   int Ns = 1;
 #pragma unroll
   for (int p = 0; p < L8; ++p) {
-    gpass<M, 8>(buf, Ns, tw, sign, tid, act);
+    gpass<M, 8>(buf, Ns, tw, sign, tid, g, act);
     Ns *= 8;
   }
-  if constexpr (rem == 8) gpass<M, 8>(buf, Ns, tw, sign, tid, act);
-  else if constexpr (rem == 4) gpass<M, 4>(buf, Ns, tw, sign, tid, act);
-  else if constexpr (rem == 2) gpass<M, 2>(buf, Ns, tw, sign, tid, act);
+  if constexpr (rem == 8) gpass<M, 8>(buf, Ns, tw, sign, tid, g, act);
+  else if constexpr (rem == 4) gpass<M, 4>(buf, Ns, tw, sign, tid, g, act);
+  else if constexpr (rem == 2) gpass<M, 2>(buf, Ns, tw, sign, tid, g, act);
 }
 
-// transform slices [0, ns) of the CTA's smem, kGroups at a time
+// transform slices [0, ns) of the CTA's smem, kGroups at a time; CTA-wide barriers
+// on entry and exit (the phases around read and write every slice)
 template <int M>
 __device__ __forceinline__ void fft_slices(double2* sm, int ns, const double2* __restrict__ tw, int sign) {
   constexpr int T = M / 8;
   const int g = threadIdx.x / T, tid = threadIdx.x % T;
+  __syncthreads();
   for (int base = 0; base < ns; base += kGroups) {
     const int s = base + g;
-    gfft<M>(sm + (size_t)s * padded(M), tw, sign, tid, s < ns);
+    if constexpr (T >= 32) {
+      if (s < ns) gfft<M>(sm + (size_t)s * padded(M), tw, sign, tid, g, true);
+    } else {
+      gfft<M>(sm + (size_t)s * padded(M), tw, sign, tid, g, s < ns);
+    }
   }
+  __syncthreads();
 }
 
 __device__ __forceinline__ double2 slot(double2* sm, int M, int s, int i) { return sm[(size_t)s * padded(M) + pidx(i)]; }
@@ -286,6 +303,17 @@ __device__ __forceinline__ double2 stage_value(const RK2& B, const Ctl2* c, int 
 }
 
 // ---------------------------------------------------------------------------
+// stage input z = y + h sum_j b_sj k_j of every point, a streaming pass ahead of the
+// first row pass (mode 1 and 7: z = y)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+k2_stage(RK2 rk, Work2 w, const Ctl2* __restrict__ ctl, int mode, int cond, size_t n3) {
+  if (!rhs_active(ctl, cond)) return;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n3; q += (size_t)gridDim.x * blockDim.x)
+    w.z[q] = stage_value(rk, ctl, mode, q);
+}
+
+// ---------------------------------------------------------------------------
 // A: row pass, stage input -> symmetrised spectra -> inverse row FFT
 // smem slices: 2f + k = field f (0: eta|Lphi, 1: u|M0u, 2: v|M0v), row r[k]
 // ---------------------------------------------------------------------------
@@ -316,14 +344,7 @@ k2_rowA(Tab2 tb, Work2 w, RK2 rk, const Ctl2* __restrict__ ctl, Ctl2* ctlw, int 
 #pragma unroll
       for (int s = 0; s < 2; ++s) {
         const size_t q = (size_t)r * Nx + cc[s];
-        double2 ze, zu, zv;
-        if (mode == 0) { ze = w.z[q]; zu = w.z[n + q]; zv = w.z[2 * n + q]; }
-        else {
-          ze = stage_value(rk, ctl, mode, q);
-          zu = stage_value(rk, ctl, mode, n + q);
-          zv = stage_value(rk, ctl, mode, 2 * n + q);
-          if (s == 0 || cm != j) { w.z[q] = ze; w.z[n + q] = zu; w.z[2 * n + q] = zv; }
-        }
+        const double2 ze = w.z[q], zu = w.z[n + q], zv = w.z[2 * n + q];
         e[k][s] = ze; u[k][s] = zu; v[k][s] = zv;
         // M0 u^ = -i (C^2/g) kx u^ ; M0 v^ = -i (C^2/g) ky v^
         const double cg = tb.c2g[q];
@@ -359,7 +380,6 @@ k2_rowA(Tab2 tb, Work2 w, RK2 rk, const Ctl2* __restrict__ ctl, Ctl2* ctlw, int 
         put(sm, M, 0 + k, c, make_double2(E1.x - E2.y, E1.y + E2.x));
       }
   }
-  __syncthreads();
   fft_slices<M>(sm, 6, tb.twx, +1);
   for (int s = 0; s < 6; ++s) {
     const int f = s >> 1, k = s & 1;
@@ -398,7 +418,6 @@ k2_colB(Tab2 tb, Work2 w, const Ctl2* __restrict__ ctl, int cond) {
   const size_t n = (size_t)tb.n;
   const int c = blockIdx.x;
   for (int f = 0; f < 3; ++f) col_load<M>(sm, 2 * f, w.R + f * n, Nx, c);
-  __syncthreads();
   fft_slices<M>(sm, 6, tb.twy, +1);
   const double invN = 1.0 / ((double)tb.n);
   for (int y = threadIdx.x; y < M; y += blockDim.x) {
@@ -417,7 +436,6 @@ k2_colB(Tab2 tb, Work2 w, const Ctl2* __restrict__ ctl, int cond) {
       put(sm, M, 6 + k, y, make_double2(eta * m0v, eta * v));
     }
   }
-  __syncthreads();
   fft_slices<M>(sm, 8, tb.twy, -1);
   for (int f = 0; f < 4; ++f) col_store<M>(sm, 2 * f, w.Q + f * n, Nx, c);
 }
@@ -439,7 +457,6 @@ k2_rowC(Tab2 tb, Work2 w, const Ctl2* __restrict__ ctl, int cond) {
     const double2* src = w.Q + f * n + (size_t)P.r[k] * Nx;
     for (int j = threadIdx.x; j < Nx; j += blockDim.x) put(sm, M, s, j, src[j]);
   }
-  __syncthreads();
   fft_slices<M>(sm, 8, tb.twx, -1);
   // Each quad (columns j and Nx - j of both rows) is read and rewritten by one
   // thread at its own positions only, so no barrier separates the reads from the

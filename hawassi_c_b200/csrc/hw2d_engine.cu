@@ -159,6 +159,7 @@ struct hw2d_ctx {
   }
   void rhs_launch(int mode, int cond, cudaStream_t s, double2* out) {
     const int rows = ny / 2, cols = nx / 2;
+    if (mode != 0) hw2d::k2_stage<<<hw2d::kCombBlocks, 256, 0, s>>>(rk, w, ctl, mode, cond, 3 * n);
     if (tb.var) {
       row_dispatch(nx, 10, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
       col_dispatch(ny, 11, cols, s, tb, w, ctl, cond);
@@ -169,7 +170,7 @@ struct hw2d_ctx {
       row_dispatch(nx, 16, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
       if (!tb.chi_one || tb.has_src) col_dispatch(ny, 3, cols, s, tb, w, ctl, cond);
       row_dispatch(nx, 4, rows, s, tb, w, rk, ctl, ctl, mode, cond, out);
-      per_rhs = (!tb.chi_one || tb.has_src) ? 9 : 8;
+      per_rhs = ((!tb.chi_one || tb.has_src) ? 9 : 8) + 1;
       return;
     }
     row_dispatch(nx, 0, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
@@ -177,7 +178,7 @@ struct hw2d_ctx {
     row_dispatch(nx, 2, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
     if (!tb.chi_one || tb.has_src) col_dispatch(ny, 3, cols, s, tb, w, ctl, cond);
     row_dispatch(nx, 4, rows, s, tb, w, rk, ctl, ctl, mode, cond, out);
-    per_rhs = (!tb.chi_one || tb.has_src) ? 5 : 4;
+    per_rhs = ((!tb.chi_one || tb.has_src) ? 5 : 4) + 1;
   }
   long long kernels_per_attempt() const { return 7LL * per_rhs + 3; }
   void attempt_launch(cudaStream_t s) {

@@ -69,41 +69,58 @@ k2v_rowA(Tab2 tb, Work2 w, RK2 rk, const Ctl2* __restrict__ ctl, Ctl2* ctlw, int
   for (int j = threadIdx.x; j <= Nx / 2; j += blockDim.x) {
     const int cm = (Nx - j) % Nx;
     const int cc[2] = {j, cm};
-    double2 e[2][2], u[2][2], v[2][2];
+    // one pair of output slices at a time keeps the quad's live values few
+    double2 a[2][2], b[2][2];
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < 2; ++k)
 #pragma unroll
       for (int s = 0; s < 2; ++s) {
         const size_t q = (size_t)P.r[k] * Nx + cc[s];
-        double2 ze, zu, zv;
-        if (mode == 0) { ze = w.z[q]; zu = w.z[n + q]; zv = w.z[2 * n + q]; }
-        else {
-          ze = stage_value(rk, ctl, mode, q);
-          zu = stage_value(rk, ctl, mode, n + q);
-          zv = stage_value(rk, ctl, mode, 2 * n + q);
-          if (s == 0 || cm != j) { w.z[q] = ze; w.z[n + q] = zu; w.z[2 * n + q] = zv; }
-        }
-        e[k][s] = ze; u[k][s] = zu; v[k][s] = zv;
+        a[k][s] = w.z[q];
+        b[k][s] = w.z[n + q];
       }
-    }
-    double2 cmu[2][2], cpu_[2][2], cmv[2][2], cpv[2][2];
-    op_sym(u, P, cc, r0, r1, Nx, Ny, tb.cmin, cmu);
-    op_sym(u, P, cc, r0, r1, Nx, Ny, tb.cplus, cpu_);
-    op_sym(v, P, cc, r0, r1, Nx, Ny, tb.cmin, cmv);
-    op_sym(v, P, cc, r0, r1, Nx, Ny, tb.cplus, cpv);
 #pragma unroll
     for (int k = 0; k < 2; ++k)
 #pragma unroll
       for (int s = 0; s < 2; ++s) {
         if (s == 1 && cm == j) continue;
         const int c = cc[s];
-        put(sm, M, 0 + k, c, packc(sym_at(e, P, k, s, c, Nx, Ny, true), sym_at(u, P, k, s, c, Nx, Ny, true)));
-        put(sm, M, 2 + k, c, packc(sym_at(v, P, k, s, c, Nx, Ny, true), sym_at(cmu, P, k, s, c, Nx, Ny, true)));
-        put(sm, M, 4 + k, c, packc(sym_at(cpu_, P, k, s, c, Nx, Ny, true), sym_at(cmv, P, k, s, c, Nx, Ny, true)));
-        put(sm, M, 6 + k, c, packc(sym_at(cpv, P, k, s, c, Nx, Ny, true), make_double2(0.0, 0.0)));
+        put(sm, M, 0 + k, c, packc(sym_at(a, P, k, s, c, Nx, Ny, true), sym_at(b, P, k, s, c, Nx, Ny, true)));
+      }
+    double2 t[2][2];
+    op_sym(b, P, cc, r0, r1, Nx, Ny, tb.cmin, t);        // Cm S(u^)
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+#pragma unroll
+      for (int s = 0; s < 2; ++s) a[k][s] = w.z[2 * n + (size_t)P.r[k] * Nx + cc[s]];   // v^
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        if (s == 1 && cm == j) continue;
+        const int c = cc[s];
+        put(sm, M, 2 + k, c, packc(sym_at(a, P, k, s, c, Nx, Ny, true), sym_at(t, P, k, s, c, Nx, Ny, true)));
+      }
+    op_sym(b, P, cc, r0, r1, Nx, Ny, tb.cplus, t);       // Cp S(u^)
+    op_sym(a, P, cc, r0, r1, Nx, Ny, tb.cmin, b);        // Cm S(v^)
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        if (s == 1 && cm == j) continue;
+        const int c = cc[s];
+        put(sm, M, 4 + k, c, packc(sym_at(t, P, k, s, c, Nx, Ny, true), sym_at(b, P, k, s, c, Nx, Ny, true)));
+      }
+    op_sym(a, P, cc, r0, r1, Nx, Ny, tb.cplus, t);       // Cp S(v^)
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        if (s == 1 && cm == j) continue;
+        const int c = cc[s];
+        put(sm, M, 6 + k, c, packc(sym_at(t, P, k, s, c, Nx, Ny, true), make_double2(0.0, 0.0)));
       }
   }
-  __syncthreads();
   fft_slices<M>(sm, 8, tb.twx, +1);
   for (int s = 0; s < 8; ++s) {
     const int f = s >> 1, k = s & 1;
@@ -122,7 +139,6 @@ k2v_colB(Tab2 tb, Work2 w, const Ctl2* __restrict__ ctl, int cond) {
   const size_t n = (size_t)tb.n;
   const int c = blockIdx.x;
   for (int f = 0; f < 4; ++f) col_load<M>(sm, 2 * f, w.R + f * n, Nx, c);
-  __syncthreads();
   fft_slices<M>(sm, 8, tb.twy, +1);
   const double invN = 1.0 / ((double)tb.n);
   for (int y = threadIdx.x; y < M; y += blockDim.x) {
@@ -145,7 +161,6 @@ k2v_colB(Tab2 tb, Work2 w, const Ctl2* __restrict__ ctl, int cond) {
       put(sm, M, 10 + k, y, make_double2(gp * lpv, 0.0));
     }
   }
-  __syncthreads();
   fft_slices<M>(sm, 12, tb.twy, -1);
   for (int f = 0; f < 6; ++f) col_store<M>(sm, 2 * f, w.Q + f * n, Nx, c);
 }
@@ -164,7 +179,6 @@ k2v_rowC(Tab2 tb, Work2 w, const Ctl2* __restrict__ ctl, int cond) {
     const double2* src = w.Q + f * n + (size_t)P.r[k] * Nx;
     for (int j = threadIdx.x; j < Nx; j += blockDim.x) put(sm, M, s, j, src[j]);
   }
-  __syncthreads();
   fft_slices<M>(sm, 12, tb.twx, -1);
   for (int j = threadIdx.x; j <= Nx / 2; j += blockDim.x) {
     const int cm = (Nx - j) % Nx;
@@ -266,7 +280,6 @@ k2v_rowC(Tab2 tb, Work2 w, const Ctl2* __restrict__ ctl, int cond) {
         put(sm, M, 2 + k, c, packc(sym_at(tu, P, k, s, c, Nx, Ny, true), make_double2(0.0, 0.0)));
       }
   }
-  __syncthreads();
   fft_slices<M>(sm, 4, tb.twx, +1);
   for (int s = 0; s < 4; ++s) {
     const int f = s >> 1, k = s & 1;
@@ -285,7 +298,6 @@ k2v_colD(Tab2 tb, Work2 w, const Ctl2* __restrict__ ctl, int cond) {
   const size_t n = (size_t)tb.n;
   const int c = blockIdx.x;
   for (int f = 0; f < 2; ++f) col_load<M>(sm, 2 * f, w.R + f * n, Nx, c);
-  __syncthreads();
   fft_slices<M>(sm, 4, tb.twy, +1);
   const double invN = 1.0 / ((double)tb.n);
   for (int y = threadIdx.x; y < M; y += blockDim.x) {
@@ -303,7 +315,6 @@ k2v_colD(Tab2 tb, Work2 w, const Ctl2* __restrict__ ctl, int cond) {
       put(sm, M, 4 + k, y, make_double2(0.5 * ((u * u + v * v) - lphi * lphi), 0.0));
     }
   }
-  __syncthreads();
   fft_slices<M>(sm, 6, tb.twy, -1);
   for (int f = 0; f < 3; ++f) col_store<M>(sm, 2 * f, w.Q + f * n, Nx, c);
 }
@@ -323,7 +334,6 @@ k2v_rowE(Tab2 tb, Work2 w, const Ctl2* __restrict__ ctl, int cond) {
     const double2* src = w.Q + f * n + (size_t)P.r[k] * Nx;
     for (int j = threadIdx.x; j < Nx; j += blockDim.x) put(sm, M, s, j, src[j]);
   }
-  __syncthreads();
   fft_slices<M>(sm, 6, tb.twx, -1);
   for (int j = threadIdx.x; j <= Nx / 2; j += blockDim.x) {
     const int cm = (Nx - j) % Nx;
@@ -383,7 +393,6 @@ k2v_rowE(Tab2 tb, Work2 w, const Ctl2* __restrict__ ctl, int cond) {
         put(sm, M, 2 + k, cc[s], packc(sym_at(xm, P, k, s, cc[s], Nx, Ny, true), sym_at(xp, P, k, s, cc[s], Nx, Ny, true)));
       }
   }
-  __syncthreads();
   fft_slices<M>(sm, 4, tb.twx, +1);
   for (int s = 0; s < 4; ++s) {
     const int f = s >> 1, k = s & 1;
@@ -402,7 +411,6 @@ k2v_colF(Tab2 tb, Work2 w, const Ctl2* __restrict__ ctl, int cond) {
   const size_t n = (size_t)tb.n;
   const int c = blockIdx.x;
   for (int f = 0; f < 2; ++f) col_load<M>(sm, 2 * f, w.R + f * n, Nx, c);
-  __syncthreads();
   fft_slices<M>(sm, 4, tb.twy, +1);
   const double invN = 1.0 / ((double)tb.n);
   for (int y = threadIdx.x; y < M; y += blockDim.x) {
@@ -419,7 +427,6 @@ k2v_colF(Tab2 tb, Work2 w, const Ctl2* __restrict__ ctl, int cond) {
       put(sm, M, 6 + k, y, make_double2(gm * lmv, gp * lpv));
     }
   }
-  __syncthreads();
   fft_slices<M>(sm, 8, tb.twy, -1);
   for (int f = 0; f < 4; ++f) col_store<M>(sm, 2 * f, w.Q + f * n, Nx, c);
 }
@@ -438,7 +445,6 @@ k2v_rowG(Tab2 tb, Work2 w, const Ctl2* __restrict__ ctl, int cond) {
     const double2* src = w.Q + f * n + (size_t)P.r[k] * Nx;
     for (int j = threadIdx.x; j < Nx; j += blockDim.x) put(sm, M, s, j, src[j]);
   }
-  __syncthreads();
   fft_slices<M>(sm, 8, tb.twx, -1);
   for (int j = threadIdx.x; j <= Nx / 2; j += blockDim.x) {
     const int cm = (Nx - j) % Nx;
