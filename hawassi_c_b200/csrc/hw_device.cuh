@@ -79,6 +79,13 @@ struct DevMember {
   double2* zs;          // stage input
   double2* sc[kScratch];
   BrkDev* bk;
+  // output stage: gauge series on the device (1d/functions.c:700-760)
+  int ngauge;
+  const double* xg;     // grid x (natural order)
+  const double* gpos;   // gauge positions
+  const int* gidx;      // spline interval of each gauge (-1: outside the grid)
+  double* gout;         // [n][2 ngauge]: eta, d eta / dt at the gauges per output sample
+  double* gtim;         // [n]: time of each output sample
   // control state
   double t, h, t1;      // current time, step, target of a single evolve_apply
   int i_out, i_stop;    // next output index, stop index (exclusive)

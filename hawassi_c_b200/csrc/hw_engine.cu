@@ -167,6 +167,12 @@ bool hw_ctx::upload_member(HostMember& h) {
   add(sizeof(double) * N);
   const long long log_cap = m.breaking ? (1LL << 22) : 16;
   add(sizeof(double) * log_cap);
+  const int ng = int(m.gauge.size());
+  add(sizeof(double) * N);                                                   // grid x
+  add(sizeof(double) * std::max(ng, 1));                                     // gauge positions
+  add(sizeof(int) * std::max(ng, 1));                                        // gauge intervals
+  add(sizeof(double) * size_t(std::max(n, 1)) * 2 * std::max(ng, 1));        // gauge series
+  add(sizeof(double) * size_t(std::max(n, 1)));                              // sample times
   bytes += 4096;
   HW_CUDA(cudaMalloc(&h.dev, bytes));
   HW_CUDA(cudaMemset(h.dev, 0, bytes));
@@ -242,6 +248,28 @@ bool hw_ctx::upload_member(HostMember& h) {
   d.KBC = m.KBC; d.TC = m.TC; d.Tstar = m.Tstar; d.MaxEtaInit = m.MaxEtaInit; d.dt_in = m.dt;
   d.xbstart = m.xbstart; d.xbend = m.xbend; d.xbendL = m.xbendL; d.xbstartR = m.xbstartR;
   d.lenIF = m.lenIF; d.ILL = m.ILL; d.IFF = m.IFF;
+  // output stage: gauges (interval index by GSL's bsearch rule)
+  d.ngauge = ng;
+  d.xg = up(m.x, N);
+  d.gpos = up(m.gauge, size_t(std::max(ng, 1)));
+  {
+    std::vector<int> gi(size_t(std::max(ng, 1)), -1);
+    for (int g = 0; g < ng; ++g) {
+      const double xq = m.gauge[g];
+      if (!(xq >= m.x[0] && xq <= m.x[N - 1])) continue;
+      int lo = 0, hi = N - 1;
+      while (hi > lo + 1) {
+        const int i = (hi + lo) / 2;
+        if (m.x[i] > xq) hi = i; else lo = i;
+      }
+      gi[g] = lo;
+    }
+    int* p = a.take<int>(gi.size());
+    cudaMemcpy(p, gi.data(), sizeof(int) * gi.size(), cudaMemcpyHostToDevice);
+    d.gidx = p;
+  }
+  d.gout = a.take<double>(size_t(std::max(n, 1)) * 2 * std::max(ng, 1));
+  d.gtim = a.take<double>(size_t(std::max(n, 1)));
   d.y = a.take<double2>(2 * N);
   d.ynew = a.take<double2>(2 * N);
   for (int i = 0; i < 7; ++i) d.kb[i] = a.take<double2>(2 * N);
@@ -852,6 +880,37 @@ int hw_energy(hw_ctx* ctx, int m, const double* y, double* energy) {
   }
   *energy = 0.5 * s * mb.dx / N;
   return 0;
+}
+
+int hw_gauges(hw_ctx* ctx, int member, double* eta, double* dteta, double* tim, int cap) {
+  if (!ctx || member < 0 || member >= int(ctx->mem.size())) return -1;
+  if (!ctx->sync_desc()) return -1;
+  const HostMember& h = ctx->mem[size_t(member)];
+  const int ng = h.d.ngauge;
+  const int rows = std::min(h.d.i_out, cap);
+  if (rows <= 0) return 0;
+  if (ng > 0 && (eta || dteta)) {
+    std::vector<double> buf(size_t(rows) * 2 * ng);
+    if (cudaMemcpy(buf.data(), h.d.gout, sizeof(double) * buf.size(), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      ctx->err = "gauge read-back failed";
+      return -1;
+    }
+    for (int r = 0; r < rows; ++r)
+      for (int g = 0; g < ng; ++g) {
+        if (eta) eta[size_t(r) * ng + g] = buf[size_t(r) * 2 * ng + g];
+        if (dteta) dteta[size_t(r) * ng + g] = buf[size_t(r) * 2 * ng + ng + g];
+      }
+  }
+  if (tim && cudaMemcpy(tim, h.d.gtim, sizeof(double) * rows, cudaMemcpyDeviceToHost) != cudaSuccess) {
+    ctx->err = "gauge read-back failed";
+    return -1;
+  }
+  return rows;
+}
+
+int hw_ngauge(const hw_ctx* ctx, int member) {
+  if (!ctx || member < 0 || member >= int(ctx->mem.size())) return -1;
+  return int(ctx->mem[size_t(member)].m.gauge.size());
 }
 
 int hw_set_stream(hw_ctx* ctx, void* s) {

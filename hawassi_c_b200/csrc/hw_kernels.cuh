@@ -6,6 +6,7 @@
 #include "hw_rhs_fast.cuh"
 #include "hw_kernels.h"
 #include "hw_stepper.cuh"
+#include "hw_output.cuh"
 
 namespace hwdev {
 
@@ -37,7 +38,10 @@ __global__ void __launch_bounds__(M / kPts, (4096 / M)) k_evolve(DevMember* mems
           evolve_apply<M>(X, B, S, ti);
           if (S.rhs >= sd.rhs_budget && S.status == kOk) S.status = kBudget;   // bounded launch
         }
-        if (S.status == kOk) ++iout;
+        if (S.status == kOk) {
+          if (sd.ngauge > 0) gauge_stage<M>(X, B, S, iout);
+          ++iout;
+        }
       }
     }
   }

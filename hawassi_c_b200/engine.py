@@ -41,7 +41,7 @@ EXPORTS = [
     "hw_mlp_set_params", "hw_mlp_grad", "hw_mlp_grad_device", "hw_mlp_train", "hw_mlp_infer",
     "hw2d_create", "hw2d_destroy", "hw2d_last_error", "hw2d_nx", "hw2d_ny", "hw2d_rhs", "hw2d_gsl_rhs",
     "hw2d_evolve_apply", "hw2d_set_state", "hw2d_get_state", "hw2d_run_to_time", "hw2d_stats",
-    "hw2d_set_stream", "hw2d_synchronize", "hw2d_launches",
+    "hw2d_set_stream", "hw2d_synchronize", "hw2d_launches", "hw_gauges", "hw_ngauge",
 ]
 
 
@@ -81,6 +81,8 @@ def load_library():
     L.hw_synchronize.argtypes = [vp]
     L.hw_deck_table.argtypes = [ctypes.c_char_p, ctypes.POINTER(HwOpts), ctypes.c_char_p, dp, ip]
     L.hw_rhs_noalloc.argtypes = [vp, ip, dd, vp, vp, vp]
+    L.hw_gauges.argtypes = [vp, ip, dp, dp, dp, ip]
+    L.hw_ngauge.argtypes = [vp, ip]
     L.hw_energy.argtypes = [vp, ip, dp, dp]
     L.hw_run_members.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     L.hw_set_operator_weights.argtypes = [vp, ip, ip, dp, dp]
@@ -241,6 +243,21 @@ class Engine:
         y = np.zeros(4 * self.nx[member])
         self._check(load_library().hw_last_dydt(self._h, member, _dp(y)), "last_dydt")
         return y
+
+    def gauges(self, member=0):
+        """Gauge series the device computed at every output sample reached so far:
+        (tim [rows], eta [rows, ngauge], deta/dt [rows, ngauge])."""
+        L = load_library()
+        ng = L.hw_ngauge(self._h, member)
+        cap = max(self.nt[member] if hasattr(self, "nt") else 0, 1)
+        cap = max(cap, L.hw_nt(self._h, member))
+        eta = np.zeros((cap, max(ng, 1)))
+        dt = np.zeros((cap, max(ng, 1)))
+        tim = np.zeros(cap)
+        rows = L.hw_gauges(self._h, member, _dp(eta), _dp(dt), _dp(tim), cap)
+        if rows < 0:
+            raise EngineError(L.hw_last_error(self._h).decode())
+        return tim[:rows], eta[:rows, :ng], dt[:rows, :ng]
 
     def breaking_log(self, member=0):
         """breaking.dat records [(t, [nodes...]), ...] of the member."""

@@ -150,6 +150,14 @@ int hw_deck_table(const char* workdir, const hw_opts* opts, const char* name, do
 
 /* Run on a caller-provided cudaStream_t (NULL: the context's own stream; pass
  * cudaStreamLegacy explicitly for the legacy default stream). */
+/* Output stage (1d/functions.c:700-760) computed on the device at every output
+ * sample of hw_run: elevation and d eta / dt at the gauges of gauges.dat (GSL
+ * natural cubic spline of the physical fields, print_data_gauge), rows of ngauge
+ * values per sample, and the sample times.  Returns the rows copied (samples
+ * reached so far, at most cap) or -1. */
+int hw_gauges(hw_ctx* ctx, int member, double* eta, double* dteta, double* tim, int cap);
+int hw_ngauge(const hw_ctx* ctx, int member);
+
 int hw_set_stream(hw_ctx* ctx, void* cuda_stream);
 int hw_synchronize(hw_ctx* ctx);
 
