@@ -56,6 +56,19 @@ def log(msg):
     print(f"[bench +{time.time() - T_START:7.1f}s] {msg}", file=sys.stderr, flush=True)
 
 
+def reduce_ranks(max_vals, sum_vals, device):
+    """Whole-job figures across ranks: the max of the time-like values and the sum of
+    the counts, as one MAX and one SUM all-reduce taken in the same order on every
+    rank (NCCL on the GPUs, gloo in the CPU tests)."""
+    import torch
+    import torch.distributed as dist
+    tm = torch.tensor([float(v) for v in max_vals], device=device, dtype=torch.float64)
+    ts = torch.tensor([float(v) for v in sum_vals], device=device, dtype=torch.float64)
+    dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+    dist.all_reduce(ts, op=dist.ReduceOp.SUM)
+    return [float(v) for v in tm.tolist()], [float(v) for v in ts.tolist()]
+
+
 def make_decks(root, rank, members, breaking=True):
     from hawassi_c_b200 import decks
     paths = []
@@ -318,10 +331,7 @@ def main_2d(args, rank, world, local):
     s1, l1 = eng.stats(), eng.launches()
     pts = float((s1["rhs_calls"] - s0["rhs_calls"]) * n)
     if world > 1:
-        t = torch.tensor([ms, pts], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-        ms, pts = float(t[0].item()), float(t[1].item())
+        (ms,), (pts,) = reduce_ranks([ms], [pts], "cuda")
     value = pts / (ms / 1e3)
     achieved = value * BYTES_PER_RHS_PT_2D / 1e9
     peaks = {}
@@ -469,12 +479,7 @@ def main():
     pts1, sim1 = rhs_pts(), sim_time()
     launches = args.steps * len(eng.class_timing())
     if world > 1:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        p = torch.tensor([float(pts1 - pts0), sim1 - sim0], device="cuda", dtype=torch.float64)
-        dist.all_reduce(p, op=dist.ReduceOp.SUM)
-        tot_pts, tot_sim = float(p[0].item()), float(p[1].item())
+        (ms,), (tot_pts, tot_sim) = reduce_ranks([ms], [float(pts1 - pts0), sim1 - sim0], "cuda")
     else:
         tot_pts, tot_sim = float(pts1 - pts0), sim1 - sim0
     value = tot_pts / (ms / 1e3)
@@ -535,10 +540,7 @@ def main():
     ems = e0.elapsed_time(e1)
     e_pts = float(rhs_pts() - pe0)
     if world > 1:
-        t = torch.tensor([ems, e_pts], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-        ems, e_pts = float(t[0].item()), float(t[1].item())
+        (ems,), (e_pts,) = reduce_ranks([ems], [e_pts], "cuda")
     log(f"e2e {args.steps} steps: {ems:.1f} ms")
     e2e = {"value": e_pts / (ems / 1e3), "unit": "RHS grid-point evaluations/s",
            "h2d_bytes_per_step": tot_doubles * 8, "d2h_bytes_per_step": tot_doubles * 8}

@@ -8,10 +8,15 @@
 #include "hw_stepper.cuh"
 #include "hw_output.cuh"
 
+// resident CTAs per SM the register allocation is sized for (slice M, M / 8 threads)
+#ifndef HW_EVOLVE_MIN_BLOCKS
+#define HW_EVOLVE_MIN_BLOCKS(M) (4096 / (M))
+#endif
+
 namespace hwdev {
 
 template <int M>
-__global__ void __launch_bounds__(M / kPts, (4096 / M)) k_evolve(DevMember* mems, const int* list, int mode) {
+__global__ void __launch_bounds__(M / kPts, HW_EVOLVE_MIN_BLOCKS(M)) k_evolve(DevMember* mems, const int* list, int mode) {
   extern __shared__ double2 smem_buf[];
   __shared__ DevMember sd;
   __shared__ double red[48];
