@@ -220,7 +220,7 @@ STEP_2D = 0.5
 # damping, ChiAdj, two complex source kernels): 35/6 * 6 * 8 + 13 * 8
 BYTES_PER_RHS_PT_2D = 35.0 / 6.0 * 6 * 8 + 13 * 8
 WORKLOAD_2D = ("2D twin: 1024x1024 on 300 m x 300 m, depth 5 m offshore sloping to 0.5 m with a seeded shoal "
-               "(two reference depths), HS2, vertical line source of a directional JONSWAP (Hs 0.5 m, Tp 6 s, "
+               "(two reference depths), harbour breakwater of reflection 0.5, HS2, vertical line source of a directional JONSWAP (Hs 0.5 m, Tp 6 s, "
                "gamma 3.3, cos^2s s=10, 256x64 seeded components), 30 m damping zones, RKF45 rtol 1e-6 atol 1e-8")
 
 

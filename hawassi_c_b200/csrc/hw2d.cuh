@@ -70,6 +70,7 @@ struct Tab2 {
   const double* cplus;
   const double* omin;           // Om2dSq_min, Om2dSq_plus (spectral)
   const double* oplus;
+  const double* wallchar;       // dominfo.wallchar (harbour walls), nullptr: none
 };
 
 struct Work2 {

@@ -369,6 +369,14 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
     tb.omin = c->upload(std::vector<double>(t->om2_min, t->om2_min + n));
     tb.oplus = c->upload(std::vector<double>(t->om2_plus, t->om2_plus + n));
   }
+  if (t->wallchar) {
+    if (!var) {
+      g_err2d = "hw2d_create: walls are built for the two-depth (varying-bottom) RHS only";
+      delete c;
+      return nullptr;
+    }
+    tb.wallchar = c->upload(std::vector<double>(t->wallchar, t->wallchar + n));
+  }
 
   Work2& w = c->w;
   w.z = c->dalloc<double2>(3 * n);
@@ -398,7 +406,7 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
             w.Q && w.D && w.V && w.insig && w.insigs && w.part && c->dref && c->dout && c->ctl &&
             (chi_one || w.W) && (!has_src || (tb.gx && tb.sx && tb.sig && w.src)) &&
             (!var || (tb.gmin && tb.gplus && tb.cmin && tb.cplus && tb.omin && tb.oplus && w.phys && w.pe && w.H1 &&
-                      w.EU));
+                      w.EU)) && (!t->wallchar || tb.wallchar);
   for (int i = 0; i < 2; ++i) ok = ok && rk.y[i] && rk.kk[i];
   for (int i = 0; i < 5; ++i) ok = ok && rk.ks[i];
   if (!ok || cudaMallocHost(&c->hctl, sizeof(Ctl2)) != cudaSuccess) {

@@ -307,12 +307,13 @@ k2v_colD(Tab2 tb, Work2 w, const Ctl2* __restrict__ ctl, int cond) {
       const double2 P1 = slot(sm, M, 0 + k, y), P2 = slot(sm, M, 2 + k, y);
       const double m0u = P1.x * invN, m0v = P1.y * invN, lphi = P2.x * invN;
       const double eta = w.phys[q], u = w.phys[n + q], v = w.phys[2 * n + q];
-      const double em = eta * m0u, evm = eta * m0v;
+      const double wc = tb.wallchar ? tb.wallchar[q] : 1.0;   // H2 products x wallchar (:3416-3430)
+      const double em = eta * m0u * wc, evm = eta * m0v * wc;
       w.pe[q] = em;
       w.pe[n + q] = evm;
-      put(sm, M, 0 + k, y, make_double2(em, eta * u));
-      put(sm, M, 2 + k, y, make_double2(evm, eta * v));
-      put(sm, M, 4 + k, y, make_double2(0.5 * ((u * u + v * v) - lphi * lphi), 0.0));
+      put(sm, M, 0 + k, y, make_double2(em, eta * u * wc));
+      put(sm, M, 2 + k, y, make_double2(evm, eta * v * wc));
+      put(sm, M, 4 + k, y, make_double2(0.5 * ((u * u + v * v) - lphi * lphi) * wc, 0.0));
     }
   }
   fft_slices<M>(sm, 6, tb.twy, -1);

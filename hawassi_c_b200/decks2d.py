@@ -98,11 +98,50 @@ def cfsa2d(x, y, Lleft, Lright, Lbottom, Ltop) -> np.ndarray:
     return (cfyb - cfyt)[:, None] * (cfxl - cfxr)[None, :]
 
 
-def fbdy2d(x, y, Lleft, Lright, Lbottom, Ltop) -> np.ndarray:
-    """fun_fbdy2D (2d/functions.c:1958-2082), no wall and no coupling: the zone
-    length L of the last matching side (7 where it is 0) scales (1 - cfSA)/(0.9 L)."""
+def cutoff(refl, model=2):
+    """fun_cutoff (2d/functions.c:225-258), with the reference's operator precedence."""
+    a, b, c = (0.8086, 0.2413, 0.0044) if model == 1 else (0.7289, 0.3229, -0.00058)
+    if refl == 1:
+        return 1.0
+    if refl == 0:
+        return 0.0
+    return -b + math.sqrt(b ** 2 - 4 * a * (c - refl)) / (2 * a)
+
+
+def _heav_band(v, lo, hi):
+    """fun_Heav2d along one axis: 1 for lo <= v < hi (the side clearances 0 keep
+    that side open)."""
+    hb = np.ones(v.size) if lo - v[0] == 0 else (v - lo >= 0).astype(float)
+    ht = np.zeros(v.size) if v[-1] - hi == 0 else (v - hi >= 0).astype(float)
+    return hb * (1 - ht)
+
+
+def wallchar2d(x, y, walls, refl, model=2):
+    """fun_wallchar (2d/functions.c:260-390) for rectangular walls (x0, y0, x1, y1):
+    wallchar = 1 - cutoff(refl) inside any wall, 1 elsewhere; cfSAwall = 0 inside the
+    first wall (direct damping), 1 elsewhere."""
+    heav = np.ones((y.size, x.size))
+    for (x0, y0, x1, y1) in walls:
+        heav *= 1 - _heav_band(y, y0, y1)[:, None] * _heav_band(x, x0, x1)[None, :]
+    wc = np.where(heav == 0, 1 - cutoff(refl, model), 1.0)
+    dx, dy = x[1] - x[0], y[1] - y[0]
+    cfw = np.ones((y.size, x.size))
+    if walls:
+        x0, y0, x1, y1 = walls[0]
+        i0, i1 = int(round((y0 - y[0]) / dy)), int(round((y1 - y[0]) / dy))
+        j0, j1 = int(round((x0 - x[0]) / dx)), int(round((x1 - x[0]) / dx))
+        cfw[i0:i1 + 1, j0:j1 + 1] = 0.0
+    return wc, cfw
+
+
+def fbdy2d(x, y, Lleft, Lright, Lbottom, Ltop, cfsa_wall=None, model=2) -> np.ndarray:
+    """fun_fbdy2D (2d/functions.c:1958-2082), no coupling: the zone length L of the
+    last matching side (7 where it is 0) scales (1 - cfSA)/(0.9 L); with walls cfSA
+    is min(cfSA, cfSAwall) and the whole field is ten times stronger (not HS1)."""
     nx, ny = x.size, y.size
     cf = cfsa2d(x, y, Lleft, Lright, Lbottom, Ltop)
+    if cfsa_wall is not None:
+        cf = np.minimum(cf, cfsa_wall)
     ixl = _closest(x, x[0] + Lleft)
     ixr = _closest(x, x[nx - 1] - Lright)
     iyb = _closest(y, y[0] + Lbottom)
@@ -122,6 +161,8 @@ def fbdy2d(x, y, Lleft, Lright, Lbottom, Ltop) -> np.ndarray:
             if L == 0:
                 L = 7.0
             out[i, j] = (1 - cf[i, j]) / (0.9 * L)
+    if cfsa_wall is not None and model != 1:
+        out = 10 * out
     return out
 
 
@@ -290,7 +331,7 @@ def shoal_bathymetry(x, y, deep=5.0, shallow=0.5, x1=100.0, x2=285.0, seed=0):
 
 def tables(nx=1024, ny=1024, Lx=300.0, Ly=300.0, depth=3.0, Hs=0.5, Tp=6.0, gamma=3.3, s_spread=10,
            n_freq=256, n_dir=64, t_end=300.0, dt=0.1, damp=30.0, x_line=45.0, nadj=1.0, model=2,
-           propagation=0, seed=0, bathymetry="flat", shallow=0.5) -> dict:
+           propagation=0, seed=0, bathymetry="flat", shallow=0.5, walls=(), refl=0.5) -> dict:
     """All tables of a 2D deck (vertical influx line at x_line).  bathymetry "flat":
     depth everywhere (rhs_AB2_2DF_uv); "shoal": `depth` offshore sloping to
     `shallow` with a seeded shoal, two reference depths (rhs_AB2_2DB_uv)."""
@@ -304,7 +345,14 @@ def tables(nx=1024, ny=1024, Lx=300.0, Ly=300.0, depth=3.0, Hs=0.5, Tp=6.0, gamm
     l2d = om * om / GRAV
     cutfrac = {1: 2, 2: 4}[model]
     aal = aal2d(kx, ky, cutfrac)
-    charac = fbdy2d(x, y, damp, damp, damp, damp)
+    wall = None
+    if walls:
+        if bathymetry == "flat":
+            raise ValueError("walls need the two-depth (varying-bottom) tables")
+        wall, cfw = wallchar2d(x, y, list(walls), refl, model)
+        charac = fbdy2d(x, y, damp, damp, damp, damp, cfsa_wall=cfw, model=model)
+    else:
+        charac = fbdy2d(x, y, damp, damp, damp, damp)
     wp = 2 * math.pi / Tp
     var = None
     depth_field = None
@@ -329,6 +377,8 @@ def tables(nx=1024, ny=1024, Lx=300.0, Ly=300.0, depth=3.0, Hs=0.5, Tp=6.0, gamm
     extra = {k: f64(v) for k, v in var.items()} if var else {}
     if depth_field is not None:
         extra["depth"] = f64(depth_field)
+    if wall is not None:
+        extra["wallchar"] = f64(wall)
     return dict(**extra, nx=nx, ny=ny, model=model, propagation=propagation, cpeak=float(cpeak), kx=f64(kx), ky=f64(ky),
                 c2d=f64(c2d), l2d=f64(l2d), aal=f64(aal), charac=f64(charac), chiadj=f64(chi),
                 newgam=f64(newgam), skewgam=f64(skewgam), nt=nt, tsig=f64(tsig), sig=f64(sig), sigskew=f64(sigs),
@@ -338,10 +388,13 @@ def tables(nx=1024, ny=1024, Lx=300.0, Ly=300.0, depth=3.0, Hs=0.5, Tp=6.0, gamm
 def config5(seed=0, bathymetry="shoal", **kw) -> dict:
     """The 2D workload: 1024 x 1024 on 300 m x 300 m, depth 5 m offshore sloping to
     0.5 m with a seeded shoal (two reference depths; bathymetry="flat" gives a flat
-    3 m bottom), directional JONSWAP Hs 0.5 m Tp 6 s gamma 3.3, cos^2s spreading
-    s = 10, 256 x 64 seeded components, HS2, 30 m damping zones, influx line at
-    x = 45 m."""
+    3 m bottom and no wall), a harbour breakwater (x 200-206 m, y 90-210 m) of
+    reflection coefficient 0.5, directional JONSWAP Hs 0.5 m Tp 6 s gamma 3.3,
+    cos^2s spreading s = 10, 256 x 64 seeded components, HS2, 30 m damping zones,
+    influx line at x = 45 m."""
     if bathymetry == "flat":
         return tables(seed=seed, **kw)
     kw.setdefault("depth", 5.0)
+    kw.setdefault("walls", ((200.0, 90.0, 206.0, 210.0),))
+    kw.setdefault("refl", 0.5)
     return tables(seed=seed, bathymetry=bathymetry, **kw)

@@ -23,7 +23,7 @@ class Hw2dTables(ctypes.Structure):
         ("newgam", _dp), ("skewgam", _dp),
         ("nt", ctypes.c_int), ("tsig", _dp), ("sig", _dp), ("sigskew", _dp),
         ("gam_min", _dp), ("gam_plus", _dp), ("csq_min", _dp), ("csq_plus", _dp), ("om2_min", _dp),
-        ("om2_plus", _dp),
+        ("om2_plus", _dp), ("wallchar", _dp),
     ]
 
 
@@ -67,7 +67,7 @@ class Engine2D:
         self._L = _lib()
         keep = {}
         for k in ("kx", "ky", "c2d", "l2d", "aal", "charac", "chiadj", "newgam", "skewgam", "tsig", "sig", "sigskew",
-                  "gam_min", "gam_plus", "csq_min", "csq_plus", "om2_min", "om2_plus"):
+                  "gam_min", "gam_plus", "csq_min", "csq_plus", "om2_min", "om2_plus", "wallchar"):
             v = tables.get(k)
             keep[k] = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
         self._keep = keep

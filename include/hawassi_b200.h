@@ -197,6 +197,10 @@ typedef struct hw2d_tables {
     const double* csq_plus;     /* [ny*nx] Oprt.InterpD.Csqr2d_plus             */
     const double* om2_min;      /* [ny*nx] Oprt.InterpD.Om2dSq_min              */
     const double* om2_plus;     /* [ny*nx] Oprt.InterpD.Om2dSq_plus             */
+    /* harbour walls: dominfo.wallchar (1 - cutoff(refl_coef) inside the walls,
+     * 2d/functions.c:260-390); NULL for no wall.  Only with the two-depth tables
+     * (the flat RHS's wall branch of fun_delphiH1hat is not built). */
+    const double* wallchar;     /* [ny*nx]                                      */
 } hw2d_tables;
 
 /* opts: eps_abs/eps_rel (<= 0: the 2D reference's 1e-3 / 1e-2, 2d/main.c:196-197),

@@ -37,6 +37,7 @@ struct or2d_ctx {
     double *tsig, *sig, *sigskew, *csig, *csigskew;   /* spline second-derivative coefficients */
     int var;                                           /* varying bottom (two reference depths) */
     double *gmin, *gplus, *cmin, *cplus, *omin, *oplus;
+    double* wallchar;                                  /* NULL: no wall */
     long long rhs_calls, acc, rej;
     /* rkf45 work vectors */
     double *k1, *k2, *k3, *k4, *k5, *k6, *ytmp, *y0, *yerr, *dydt_in, *dydt_out;
@@ -155,6 +156,10 @@ or2d_ctx* or2d_create(const or2d_tables* tb, double eps_abs, double eps_rel) {
         c->cmin = dup(tb->csq_min, n); c->cplus = dup(tb->csq_plus, n);
         c->omin = dup(tb->om2_min, n); c->oplus = dup(tb->om2_plus, n);
     }
+    if (tb->wallchar) {
+        if (!c->var) { set_err2("or2d_create: walls are restated for the varying-bottom RHS only"); free(c); return NULL; }
+        c->wallchar = dup(tb->wallchar, n);
+    }
     size_t d = 6 * n;
     double** w[] = {&c->k1, &c->k2, &c->k3, &c->k4, &c->k5, &c->k6, &c->ytmp, &c->y0, &c->yerr, &c->dydt_in, &c->dydt_out};
     for (size_t q = 0; q < sizeof w / sizeof w[0]; q++) *w[q] = calloc(d, sizeof(double));
@@ -166,7 +171,7 @@ void or2d_destroy(or2d_ctx* c) {
     double* f[] = {c->kx, c->ky, c->c2d, c->l2d, c->aal, c->charac, c->chiadj, c->newgam, c->skewgam, c->tsig,
                    c->sig, c->sigskew, c->csig, c->csigskew, c->k1, c->k2, c->k3, c->k4, c->k5, c->k6, c->ytmp,
                    c->y0, c->yerr, c->dydt_in, c->dydt_out, c->gmin, c->gplus, c->cmin, c->cplus, c->omin,
-                   c->oplus};
+                   c->oplus, c->wallchar};
     for (size_t q = 0; q < sizeof f / sizeof f[0]; q++) free(f[q]);
     free(c);
 }
@@ -261,8 +266,9 @@ static void hssgen_2depth(const or2d_ctx* c, const cx* phi, const cx* phihat, co
 }
 
 /* rhs_AB2_2DB_uv (2d/fun_odesolver.c:4542-4626) with fun_termshat_AB1_2DB_uv
- * (:2874-2960) and fun_termshat_AB2_2DB_uv (:3327-3510), ninterp = 2, no wall,
- * friction, coupling or breaking. */
+ * (:2874-2960) and fun_termshat_AB2_2DB_uv (:3327-3510), ninterp = 2; walls enter
+ * through dominfo.wallchar in the H2 products (:3416-3430); no friction, coupling
+ * or breaking. */
 static int rhs_2db(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
     const int Nx = c->nx, Ny = c->ny, n = c->n;
     const double factIFFT = (double)Nx * Ny;
@@ -315,7 +321,7 @@ static int rhs_2db(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
     cx *etaM0u = malloc(sizeof(cx) * n), *eta_u = malloc(sizeof(cx) * n), *etaM0v = malloc(sizeof(cx) * n);
     cx *eta_v = malloc(sizeof(cx) * n), *deletaH2 = malloc(sizeof(cx) * n);
     for (int q = 0; q < n; q++) {
-        const double wallchar = 1.0;
+        const double wallchar = c->wallchar ? c->wallchar[q] : 1.0;
         etaM0u[q].re = eta[q].re * M0u[q].re / f2 * wallchar; etaM0u[q].im = 0;
         eta_u[q].re = eta[q].re * u[q].re / f2 * wallchar; eta_u[q].im = 0;
         etaM0v[q].re = eta[q].re * M0v[q].re / f2 * wallchar; etaM0v[q].im = 0;

@@ -49,6 +49,7 @@ typedef struct or2d_tables {
     const double* csq_plus;     /* [ny*nx] Oprt.InterpD.Csqr2d_plus            */
     const double* om2_min;      /* [ny*nx] Oprt.InterpD.Om2dSq_min             */
     const double* om2_plus;     /* [ny*nx] Oprt.InterpD.Om2dSq_plus            */
+    const double* wallchar;     /* [ny*nx] dominfo.wallchar, NULL: no wall (varying bottom only) */
 } or2d_tables;
 
 /* Copies every table.  eps <= 0 selects the reference's 2D values (abs 1e-3,

@@ -40,7 +40,7 @@ class Or2dTables(ctypes.Structure):
         ("chiadj", _dpt), ("newgam", _dpt), ("skewgam", _dpt),
         ("nt", ctypes.c_int), ("tsig", _dpt), ("sig", _dpt), ("sigskew", _dpt),
         ("gam_min", _dpt), ("gam_plus", _dpt), ("csq_min", _dpt), ("csq_plus", _dpt), ("om2_min", _dpt),
-        ("om2_plus", _dpt),
+        ("om2_plus", _dpt), ("wallchar", _dpt),
     ]
 
 
@@ -195,7 +195,7 @@ class Oracle2D:
         L = lib()
         keep = {}
         for k in ("kx", "ky", "c2d", "l2d", "aal", "charac", "chiadj", "newgam", "skewgam", "tsig", "sig", "sigskew",
-                  "gam_min", "gam_plus", "csq_min", "csq_plus", "om2_min", "om2_plus"):
+                  "gam_min", "gam_plus", "csq_min", "csq_plus", "om2_min", "om2_plus", "wallchar"):
             v = tables.get(k)
             keep[k] = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
         self._keep = keep

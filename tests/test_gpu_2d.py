@@ -9,10 +9,10 @@ from oracle_lib import Oracle2D
 pytestmark = pytest.mark.gpu
 
 
-def tables(nx, ny, nadj=1.0, propagation=0, seed=1, source=True, bathymetry="flat"):
+def tables(nx, ny, nadj=1.0, propagation=0, seed=1, source=True, bathymetry="flat", walls=()):
     tb = decks2d.tables(nx=nx, ny=ny, Lx=0.9 * nx, Ly=0.9 * ny, depth=2.0, shallow=0.6, Hs=0.1, Tp=3.0, n_freq=24,
                         n_dir=6, t_end=6.0, dt=0.1, damp=6.0, x_line=10.0, nadj=nadj, propagation=propagation,
-                        seed=seed, bathymetry=bathymetry)
+                        seed=seed, bathymetry=bathymetry, walls=walls)
     if not source:
         for k in ("newgam", "skewgam", "tsig", "sig", "sigskew"):
             tb[k] = None
@@ -143,3 +143,36 @@ def test_run_to_time_parity_varying_depth():
         assert rel(yg, y) < 1e-9
     sg, so = eng.stats(), ora.stats()
     assert sg["accepted"] == so["accepted"] and sg["rejected"] == so["rejected"]
+
+
+# --- harbour wall (dominfo.wallchar in the H2 products, damping inside the wall) --
+def _wall(nx, ny):
+    Lx, Ly = 0.9 * nx, 0.9 * ny
+    return ((0.6 * Lx, 0.3 * Ly, 0.63 * Lx, 0.7 * Ly),)
+
+
+@pytest.mark.parametrize("nx,ny", [(64, 64), (128, 128)])
+def test_rhs_parity_wall(nx, ny):
+    tb = tables(nx, ny, bathymetry="shoal", walls=_wall(nx, ny))
+    assert (tb["wallchar"] < 1).any()
+    eng, ora = Engine2D(tb, 1e-8, 1e-6), Oracle2D(tb, 1e-8, 1e-6)
+    y = band_limited_state(tb, 0.02, 3)
+    assert rel(eng.rhs(1.1, y), ora.rhs(1.1, y)) < 1e-11
+
+
+def test_run_to_time_parity_wall():
+    tb = tables(64, 64, bathymetry="shoal", walls=_wall(64, 64))
+    eng, ora = Engine2D(tb, 1e-8, 1e-6), Oracle2D(tb, 1e-8, 1e-6)
+    y = np.zeros(6 * tb["nx"] * tb["ny"])
+    eng.set_state(0.0, 0.02, y)
+    to, ho = ora.run_to(0.0, 2.0, 0.02, y)
+    eng.run_to_time(2.0)
+    tg, hg, yg = eng.state()
+    assert tg == to and rel(yg, y) < 1e-9
+
+
+def test_wall_on_flat_bottom_rejected():
+    tb = tables(64, 64)
+    tb["wallchar"] = np.ones(64 * 64)
+    with pytest.raises(Exception):
+        Engine2D(tb)
