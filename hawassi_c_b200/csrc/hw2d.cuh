@@ -279,28 +279,44 @@ __device__ __forceinline__ double stage_time(const Ctl2* c, int mode) {
   return c->t + A2_ah[mode - 2] * c->h0;
 }
 
+// IEEE products and sums without fused multiply-add (GSL's rounding)
+__device__ __forceinline__ double rm2(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double ra2(double a, double b) { return __dadd_rn(a, b); }
+
 // stage input at element q (3n double2 per state): GSL rkf45's expression forms
 __device__ __forceinline__ double2 stage_value(const RK2& B, const Ctl2* c, int mode, size_t q) {
   const double2 y = B.y[c->cur][q];
   if (mode <= 1 || mode == 7) return y;
   const double h = c->h0;
   const double2 a = B.kk[c->k1i][q];
-  if (mode == 2) return make_double2(y.x + A2_ah[0] * h * a.x, y.y + A2_ah[0] * h * a.y);
+  if (mode == 2) {
+    const double f = rm2(A2_ah[0], h);
+    return make_double2(ra2(y.x, rm2(f, a.x)), ra2(y.y, rm2(f, a.y)));
+  }
   const double2 b = B.ks[0][q];
   if (mode == 3)
-    return make_double2(y.x + h * (A2_b3[0] * a.x + A2_b3[1] * b.x), y.y + h * (A2_b3[0] * a.y + A2_b3[1] * b.y));
+    return make_double2(ra2(y.x, rm2(h, ra2(rm2(A2_b3[0], a.x), rm2(A2_b3[1], b.x)))),
+                        ra2(y.y, rm2(h, ra2(rm2(A2_b3[0], a.y), rm2(A2_b3[1], b.y)))));
   const double2 c3 = B.ks[1][q];
   if (mode == 4)
-    return make_double2(y.x + h * (A2_b4[0] * a.x + A2_b4[1] * b.x + A2_b4[2] * c3.x),
-                        y.y + h * (A2_b4[0] * a.y + A2_b4[1] * b.y + A2_b4[2] * c3.y));
+    return make_double2(
+        ra2(y.x, rm2(h, ra2(ra2(rm2(A2_b4[0], a.x), rm2(A2_b4[1], b.x)), rm2(A2_b4[2], c3.x)))),
+        ra2(y.y, rm2(h, ra2(ra2(rm2(A2_b4[0], a.y), rm2(A2_b4[1], b.y)), rm2(A2_b4[2], c3.y)))));
   const double2 c4 = B.ks[2][q];
   if (mode == 5)
-    return make_double2(y.x + h * (A2_b5[0] * a.x + A2_b5[1] * b.x + A2_b5[2] * c3.x + A2_b5[3] * c4.x),
-                        y.y + h * (A2_b5[0] * a.y + A2_b5[1] * b.y + A2_b5[2] * c3.y + A2_b5[3] * c4.y));
+    return make_double2(
+        ra2(y.x, rm2(h, ra2(ra2(ra2(rm2(A2_b5[0], a.x), rm2(A2_b5[1], b.x)), rm2(A2_b5[2], c3.x)),
+                            rm2(A2_b5[3], c4.x)))),
+        ra2(y.y, rm2(h, ra2(ra2(ra2(rm2(A2_b5[0], a.y), rm2(A2_b5[1], b.y)), rm2(A2_b5[2], c3.y)),
+                            rm2(A2_b5[3], c4.y)))));
   const double2 c5 = B.ks[3][q];
   return make_double2(
-      y.x + h * (A2_b6[0] * a.x + A2_b6[1] * b.x + A2_b6[2] * c3.x + A2_b6[3] * c4.x + A2_b6[4] * c5.x),
-      y.y + h * (A2_b6[0] * a.y + A2_b6[1] * b.y + A2_b6[2] * c3.y + A2_b6[3] * c4.y + A2_b6[4] * c5.y));
+      ra2(y.x, rm2(h, ra2(ra2(ra2(ra2(rm2(A2_b6[0], a.x), rm2(A2_b6[1], b.x)), rm2(A2_b6[2], c3.x)),
+                              rm2(A2_b6[3], c4.x)),
+                          rm2(A2_b6[4], c5.x)))),
+      ra2(y.y, rm2(h, ra2(ra2(ra2(ra2(rm2(A2_b6[0], a.y), rm2(A2_b6[1], b.y)), rm2(A2_b6[2], c3.y)),
+                              rm2(A2_b6[3], c4.y)),
+                          rm2(A2_b6[4], c5.y)))));
 }
 
 // ---------------------------------------------------------------------------
@@ -681,14 +697,18 @@ k2_combine(RK2 rk, Work2 w, const Ctl2* __restrict__ ctl, size_t n3) {
   int bad = 0;
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n3; q += (size_t)gridDim.x * blockDim.x) {
     const double2 a = k1[q], c = rk.ks[1][q], e = rk.ks[2][q], f = rk.ks[3][q], g = rk.ks[4][q], yy = y[q];
-    const double dix = A2_c[0] * a.x + A2_c[1] * c.x + A2_c[2] * e.x + A2_c[3] * f.x + A2_c[4] * g.x;
-    const double diy = A2_c[0] * a.y + A2_c[1] * c.y + A2_c[2] * e.y + A2_c[3] * f.y + A2_c[4] * g.y;
-    const double2 nv = make_double2(yy.x + h * dix, yy.y + h * diy);
+    const double dix = ra2(ra2(ra2(ra2(rm2(A2_c[0], a.x), rm2(A2_c[1], c.x)), rm2(A2_c[2], e.x)), rm2(A2_c[3], f.x)),
+                           rm2(A2_c[4], g.x));
+    const double diy = ra2(ra2(ra2(ra2(rm2(A2_c[0], a.y), rm2(A2_c[1], c.y)), rm2(A2_c[2], e.y)), rm2(A2_c[3], f.y)),
+                           rm2(A2_c[4], g.y));
+    const double2 nv = make_double2(ra2(yy.x, rm2(h, dix)), ra2(yy.y, rm2(h, diy)));
     yn[q] = nv;
-    const double ex = h * (A2_ec[0] * a.x + A2_ec[1] * c.x + A2_ec[2] * e.x + A2_ec[3] * f.x + A2_ec[4] * g.x);
-    const double ey = h * (A2_ec[0] * a.y + A2_ec[1] * c.y + A2_ec[2] * e.y + A2_ec[3] * f.y + A2_ec[4] * g.y);
-    const double rx = fabs(ex) / fabs(er * fabs(nv.x) + ea);
-    const double ry = fabs(ey) / fabs(er * fabs(nv.y) + ea);
+    const double ex = rm2(h, ra2(ra2(ra2(ra2(rm2(A2_ec[0], a.x), rm2(A2_ec[1], c.x)), rm2(A2_ec[2], e.x)),
+                                     rm2(A2_ec[3], f.x)), rm2(A2_ec[4], g.x)));
+    const double ey = rm2(h, ra2(ra2(ra2(ra2(rm2(A2_ec[0], a.y), rm2(A2_ec[1], c.y)), rm2(A2_ec[2], e.y)),
+                                     rm2(A2_ec[3], f.y)), rm2(A2_ec[4], g.y)));
+    const double rx = fabs(ex) / fabs(ra2(rm2(er, fabs(nv.x)), ea));
+    const double ry = fabs(ey) / fabs(ra2(rm2(er, fabs(nv.y)), ea));
     bad |= (!(rx == rx) || !(ry == ry) || isinf(nv.x) || isinf(nv.y)) ? 1 : 0;
     rm = fmax(rm, fmax(rx, ry));
   }

@@ -212,8 +212,10 @@ static __device__ __noinline__ void breaking_leader(const DevMember& d, BrkDev* 
   bk->npk = bk->n_touched;
 }
 
+// returns false (Rb untouched) when no node breaks: the force is then identically
+// zero, as the reference's FFT of a zero flux gives, and the assembly skips it
 template <int M>
-__device__ __noinline__ void breaking_rhs(Ctx<M>& X, double t, const double2* PE, const double* Heta, int hs,
+__device__ __noinline__ bool breaking_rhs(Ctx<M>& X, double t, const double2* PE, const double* Heta, int hs,
                                           const double2* AEadj, double2* Rb) {
   const DevMember& d = X.d;
   BrkDev* bk = d.bk;
@@ -226,17 +228,20 @@ __device__ __noinline__ void breaking_rhs(Ctx<M>& X, double t, const double2* PE
   member_sync(d.C);
   // criterion scan over this CTA's physical points (1d/breaking.c:36-61,72)
   const int w0 = d.xbstart, w1 = d.xbstart + d.lenIF;   // window [w0, w1)
+  bool above = false;
   HW_FOREACH(X) {
     (void)idx;
     if (p >= w0 && p < w1) {
       const double e = PE[p].x;
-      if (e > d.MaxEtaInit) atomicOr(&bk->any_above, 1);
+      if (e > d.MaxEtaInit) above = true;
       if (p >= w0 + 1 && p <= w1 - 2 && !(e < d.MaxEtaInit) && e > PE[p + 1].x && e > PE[p - 1].x) {
         const int slot = atomicAdd(&bk->npk, 1);
         if (slot < N) bk->pk[slot] = p;
       }
     }
   }
+  // one flag update per warp
+  if (__any_sync(0xffffffffu, above) && (X.tid & 31) == 0) atomicOr(&bk->any_above, 1);
   member_sync(d.C);
   if (leader) {
     if (bk->npk > N) bk->npk = N;
@@ -244,13 +249,7 @@ __device__ __noinline__ void breaking_rhs(Ctx<M>& X, double t, const double2* PE
     __threadfence();
   }
   member_sync(d.C);
-  if (bk->npk == 0) {   // B identically zero: FFT(0) = 0, as the reference computes it
-    HW_FOREACH(X) {
-      (void)idx;
-      Rb[p] = make_double2(0.0, 0.0);
-    }
-    return;
-  }
+  if (bk->npk == 0) return false;   // B identically zero: FFT(0) = 0, as the reference computes it
   // d_t eta = Re F^-1(dH1_eta + adjusted nonlinear eta term)
   const double2* ZU = d.zs + N;
   const double2* HS = d.sc[6];
@@ -287,6 +286,7 @@ __device__ __noinline__ void breaking_rhs(Ctx<M>& X, double t, const double2* PE
     X.buf[pidx(idx)] = make_double2(rb, 0.0);
   }
   fft_forward_split(X, [&](int, int, int p, double2 z, double2 zp) { Rb[p] = split_re(z, zp); });
+  return true;
 }
 
 }  // namespace hwdev

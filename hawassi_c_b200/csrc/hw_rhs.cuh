@@ -11,6 +11,71 @@
 
 namespace hwdev {
 
+// Fehlberg coefficients (GSL rkf45)
+__device__ constexpr double RK_ah[5] = {1.0 / 4.0, 3.0 / 8.0, 12.0 / 13.0, 1.0, 1.0 / 2.0};
+__device__ constexpr double RK_b3[2] = {3.0 / 32.0, 9.0 / 32.0};
+__device__ constexpr double RK_b4[3] = {1932.0 / 2197.0, -7200.0 / 2197.0, 7296.0 / 2197.0};
+__device__ constexpr double RK_b5[4] = {8341.0 / 4104.0, -32832.0 / 4104.0, 29440.0 / 4104.0, -845.0 / 4104.0};
+__device__ constexpr double RK_b6[5] = {-6080.0 / 20520.0, 41040.0 / 20520.0, -28352.0 / 20520.0, 9295.0 / 20520.0,
+                                        -5643.0 / 20520.0};
+__device__ constexpr double RK_c1 = 902880.0 / 7618050.0;
+__device__ constexpr double RK_c3 = 3953664.0 / 7618050.0;
+__device__ constexpr double RK_c4 = 3855735.0 / 7618050.0;
+__device__ constexpr double RK_c5 = -1371249.0 / 7618050.0;
+__device__ constexpr double RK_c6 = 277020.0 / 7618050.0;
+__device__ constexpr double RK_ec1 = 1.0 / 360.0;
+__device__ constexpr double RK_ec3 = -128.0 / 4275.0;
+__device__ constexpr double RK_ec4 = -2197.0 / 75240.0;
+__device__ constexpr double RK_ec5 = 1.0 / 50.0;
+__device__ constexpr double RK_ec6 = 2.0 / 55.0;
+
+// the stage input of an RK stage: zs = y + h sum_j b_sj k_j (s = 2..6)
+struct StageSrc {
+  const double2* y;
+  const double2* k[5];
+  int s;
+  double h;
+};
+
+// IEEE products and sums without fused multiply-add: the stepper's arithmetic
+// rounds like GSL's (compiled without contraction)
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
+
+// one element of the stage input, in GSL rkf45's expression forms
+__device__ __forceinline__ double2 stage_val(const StageSrc& st, int q) {
+  const double2 y = st.y[q], a = st.k[0][q];
+  const double h = st.h;
+  if (st.s == 2) {
+    const double f = rmul(RK_ah[0], h);
+    return make_double2(radd(y.x, rmul(f, a.x)), radd(y.y, rmul(f, a.y)));
+  }
+  const double2 b = st.k[1][q];
+  if (st.s == 3)
+    return make_double2(radd(y.x, rmul(h, radd(rmul(RK_b3[0], a.x), rmul(RK_b3[1], b.x)))),
+                        radd(y.y, rmul(h, radd(rmul(RK_b3[0], a.y), rmul(RK_b3[1], b.y)))));
+  const double2 c3 = st.k[2][q];
+  if (st.s == 4)
+    return make_double2(
+        radd(y.x, rmul(h, radd(radd(rmul(RK_b4[0], a.x), rmul(RK_b4[1], b.x)), rmul(RK_b4[2], c3.x)))),
+        radd(y.y, rmul(h, radd(radd(rmul(RK_b4[0], a.y), rmul(RK_b4[1], b.y)), rmul(RK_b4[2], c3.y)))));
+  const double2 c4 = st.k[3][q];
+  if (st.s == 5)
+    return make_double2(
+        radd(y.x, rmul(h, radd(radd(radd(rmul(RK_b5[0], a.x), rmul(RK_b5[1], b.x)), rmul(RK_b5[2], c3.x)),
+                               rmul(RK_b5[3], c4.x)))),
+        radd(y.y, rmul(h, radd(radd(radd(rmul(RK_b5[0], a.y), rmul(RK_b5[1], b.y)), rmul(RK_b5[2], c3.y)),
+                               rmul(RK_b5[3], c4.y)))));
+  const double2 c5 = st.k[4][q];
+  return make_double2(
+      radd(y.x, rmul(h, radd(radd(radd(radd(rmul(RK_b6[0], a.x), rmul(RK_b6[1], b.x)), rmul(RK_b6[2], c3.x)),
+                                  rmul(RK_b6[3], c4.x)),
+                             rmul(RK_b6[4], c5.x)))),
+      radd(y.y, rmul(h, radd(radd(radd(radd(rmul(RK_b6[0], a.y), rmul(RK_b6[1], b.y)), rmul(RK_b6[2], c3.y)),
+                                  rmul(RK_b6[3], c4.y)),
+                             rmul(RK_b6[4], c5.y)))));
+}
+
 template <int M>
 struct Ctx {
   static constexpr int T = M / kPts;
@@ -20,6 +85,7 @@ struct Ctx {
   double* red;    // reduction scratch in shared memory
   int c;          // rank of this CTA in the member's cluster
   int tid;
+  const StageSrc* stg = nullptr;   // set: zs is to be formed from y and the k's first
 };
 
 #define HW_FOREACH(X)                            \
@@ -143,7 +209,7 @@ __device__ __noinline__ void hss(Ctx<M>& X, const double2* __restrict__ A, const
 
 // breaking hooks (implemented in hw_breaking.cuh)
 template <int M>
-__device__ __noinline__ void breaking_rhs(Ctx<M>& X, double t, const double2* PE, const double* Heta, int heta_stride,
+__device__ __noinline__ bool breaking_rhs(Ctx<M>& X, double t, const double2* PE, const double* Heta, int heta_stride,
                              const double2* AEadj, double2* Rb);
 // HS2 flat-bottom fast path (hw_rhs_fast.cuh)
 template <int M>
@@ -170,9 +236,19 @@ __device__ __noinline__ void rhs_eval(Ctx<M>& X, double t, double2* __restrict__
   double2* S10 = d.sc[10]; // spectral scratch
   double2* RB = d.sc[11];  // FFT(breaking force)
   const bool hs2 = d.model >= 2, hs3 = d.model == 3, brk = d.brk != 0, flat = d.flat != 0;
+  bool rb_live = false;   // the breaking force is nonzero (some node broke)
   if (d.model == 2 && flat) {
     rhs_hs2_flat<M>(X, t, dz);
     return;
+  }
+  if (X.stg) {
+    for (int part = 0; part < 2; ++part) {
+      const int off = part * N;
+      HW_FOREACH(X) {
+        (void)idx;
+        d.zs[p + off] = stage_val(*X.stg, p + off);
+      }
+    }
   }
 
   member_sync(d.C);   // zs written by all CTAs of the member
@@ -360,7 +436,7 @@ __device__ __noinline__ void rhs_eval(Ctx<M>& X, double t, double2* __restrict__
     // (10) kinematic breaking: eddy-viscosity force on the u-equation
     if (brk) {
       member_sync(d.C);
-      breaking_rhs<M>(X, t, PE, hs3 ? &PA[0].y : &PM[0].y, 2, AE, RB);
+      rb_live = breaking_rhs<M>(X, t, PE, hs3 ? &PA[0].y : &PM[0].y, 2, AE, RB);
     }
   }
   // (11) assembly (1d/rhs.c:217-228, 373-385, 73-83) with the source term (1d/rhs.c:659)
@@ -397,7 +473,7 @@ __device__ __noinline__ void rhs_eval(Ctx<M>& X, double t, double2* __restrict__
       te = cadd(te, AE[p]);
       tu = cadd(tu, AU[p]);
     }
-    if (brk && hs2) tu = cadd(tu, RB[p]);
+    if (rb_live && hs2) tu = cadd(tu, RB[p]);
     dz[p] = make_double2((te.x + 2 * fr - de.x) * al, (te.y + 2 * fi - de.y) * al);
     dz[N + p] = make_double2((tu.x - du.x) * al, (tu.y - du.y) * al);
   }

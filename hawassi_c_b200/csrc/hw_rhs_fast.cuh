@@ -49,10 +49,23 @@ __device__ __noinline__ void rhs_hs2_flat(Ctx<M>& X, double t, double2* __restri
   auto jpart = [&](int idx) { return X.c == 0 ? ((M - idx) & (M - 1)) : (M - 1 - idx); };
   double2 va[kPts], vb[kPts];
 
-  // (0) stage input into the two slices (spectral, cyclic)
-  HW_FOREACH(X) {
-    A[pidx(idx)] = ZE[p];
-    Bf[pidx(idx)] = ZU[p];
+  // (0) stage input into the two slices (spectral, cyclic), formed here from y and
+  // the k's during an RK step (and kept in zs for the assembly)
+  if (X.stg) {
+    double2* zw = d.zs;
+    HW_FOREACH(X) {
+      (void)idx;
+      const double2 ze = stage_val(*X.stg, p), zu = stage_val(*X.stg, N + p);
+      zw[p] = ze;
+      zw[N + p] = zu;
+      A[pidx(idx)] = ze;
+      Bf[pidx(idx)] = zu;
+    }
+  } else {
+    HW_FOREACH(X) {
+      A[pidx(idx)] = ZE[p];
+      Bf[pidx(idx)] = ZU[p];
+    }
   }
   member_sync(C);
   // (1) Hermitian packing: A <- eta^ + i u^, B <- M0 u^ + i H(eta)^ (real parts only, as the reference)
@@ -132,7 +145,7 @@ __device__ __noinline__ void rhs_hs2_flat(Ctx<M>& X, double t, double2* __restri
   }
   member_sync(C);
   // (5) kinematic breaking: eddy-viscosity force on the u-equation
-  if (brk) breaking_rhs<M>(X, t, PE, &PM[0].y, 2, AE, RB);
+  const bool rb_live = brk && breaking_rhs<M>(X, t, PE, &PM[0].y, 2, AE, RB);
   // (6) assembly (1d/rhs.c:217-228) with the source term (1d/rhs.c:659)
   double pv = 0.0, ps = 0.0;
   if (d.has_influx) {
@@ -156,7 +169,7 @@ __device__ __noinline__ void rhs_hs2_flat(Ctx<M>& X, double t, double2* __restri
     const double2 de = DE[p], dd = DU[p];
     te = cadd(te, AE[p]);
     tu = cadd(tu, AU[p]);
-    if (brk) tu = cadd(tu, RB[p]);
+    if (rb_live) tu = cadd(tu, RB[p]);
     dz[p] = make_double2((te.x + 2 * fr - de.x) * al, (te.y + 2 * fi - de.y) * al);
     dz[N + p] = make_double2((tu.x - dd.x) * al, (tu.y - dd.y) * al);
   }

@@ -17,62 +17,16 @@ struct Bufs {
   double2* k[7];   // k1..k6, kout
 };
 
-// Fehlberg coefficients (GSL rkf45)
-__device__ constexpr double RK_ah[5] = {1.0 / 4.0, 3.0 / 8.0, 12.0 / 13.0, 1.0, 1.0 / 2.0};
-__device__ constexpr double RK_b3[2] = {3.0 / 32.0, 9.0 / 32.0};
-__device__ constexpr double RK_b4[3] = {1932.0 / 2197.0, -7200.0 / 2197.0, 7296.0 / 2197.0};
-__device__ constexpr double RK_b5[4] = {8341.0 / 4104.0, -32832.0 / 4104.0, 29440.0 / 4104.0, -845.0 / 4104.0};
-__device__ constexpr double RK_b6[5] = {-6080.0 / 20520.0, 41040.0 / 20520.0, -28352.0 / 20520.0, 9295.0 / 20520.0,
-                                        -5643.0 / 20520.0};
-__device__ constexpr double RK_c1 = 902880.0 / 7618050.0;
-__device__ constexpr double RK_c3 = 3953664.0 / 7618050.0;
-__device__ constexpr double RK_c4 = 3855735.0 / 7618050.0;
-__device__ constexpr double RK_c5 = -1371249.0 / 7618050.0;
-__device__ constexpr double RK_c6 = 277020.0 / 7618050.0;
-__device__ constexpr double RK_ec1 = 1.0 / 360.0;
-__device__ constexpr double RK_ec3 = -128.0 / 4275.0;
-__device__ constexpr double RK_ec4 = -2197.0 / 75240.0;
-__device__ constexpr double RK_ec5 = 1.0 / 50.0;
-__device__ constexpr double RK_ec6 = 2.0 / 55.0;
-
 // stage input zs = y + h sum_j b_sj k_j for stage s = 2..6 (GSL's expression forms)
 template <int M>
 __device__ __forceinline__ void stage_input(Ctx<M>& X, const Bufs& B, int s, double h) {
   const DevMember& d = X.d;
-  double2* zs = d.zs;
+  const StageSrc st{B.y, {B.k[0], B.k[1], B.k[2], B.k[3], B.k[4]}, s, h};
   for (int part = 0; part < 2; ++part) {
     const int off = part * d.N;
     HW_FOREACH(X) {
       (void)idx;
-      const int q = p + off;
-      const double2 y = B.y[q], a = B.k[0][q];
-      double2 r;
-      if (s == 2) {
-        r = make_double2(y.x + RK_ah[0] * h * a.x, y.y + RK_ah[0] * h * a.y);
-      } else {
-        const double2 b = B.k[1][q];
-        if (s == 3) {
-          r = make_double2(y.x + h * (RK_b3[0] * a.x + RK_b3[1] * b.x), y.y + h * (RK_b3[0] * a.y + RK_b3[1] * b.y));
-        } else {
-          const double2 c3 = B.k[2][q];
-          if (s == 4) {
-            r = make_double2(y.x + h * (RK_b4[0] * a.x + RK_b4[1] * b.x + RK_b4[2] * c3.x),
-                             y.y + h * (RK_b4[0] * a.y + RK_b4[1] * b.y + RK_b4[2] * c3.y));
-          } else {
-            const double2 c4 = B.k[3][q];
-            if (s == 5) {
-              r = make_double2(y.x + h * (RK_b5[0] * a.x + RK_b5[1] * b.x + RK_b5[2] * c3.x + RK_b5[3] * c4.x),
-                               y.y + h * (RK_b5[0] * a.y + RK_b5[1] * b.y + RK_b5[2] * c3.y + RK_b5[3] * c4.y));
-            } else {
-              const double2 c5 = B.k[4][q];
-              r = make_double2(
-                  y.x + h * (RK_b6[0] * a.x + RK_b6[1] * b.x + RK_b6[2] * c3.x + RK_b6[3] * c4.x + RK_b6[4] * c5.x),
-                  y.y + h * (RK_b6[0] * a.y + RK_b6[1] * b.y + RK_b6[2] * c3.y + RK_b6[3] * c4.y + RK_b6[4] * c5.y));
-            }
-          }
-        }
-      }
-      zs[q] = r;
+      d.zs[p + off] = stage_val(st, p + off);
     }
   }
 }
@@ -112,14 +66,18 @@ __device__ __forceinline__ double final_combine(Ctx<M>& X, const Bufs& B, double
       (void)idx;
       const int q = p + off;
       const double2 y = B.y[q], a = B.k[0][q], c = B.k[2][q], e = B.k[3][q], f = B.k[4][q], g = B.k[5][q];
-      const double dix = RK_c1 * a.x + RK_c3 * c.x + RK_c4 * e.x + RK_c5 * f.x + RK_c6 * g.x;
-      const double diy = RK_c1 * a.y + RK_c3 * c.y + RK_c4 * e.y + RK_c5 * f.y + RK_c6 * g.y;
-      const double2 yn = make_double2(y.x + h * dix, y.y + h * diy);
+      const double dix = radd(radd(radd(radd(rmul(RK_c1, a.x), rmul(RK_c3, c.x)), rmul(RK_c4, e.x)), rmul(RK_c5, f.x)),
+                              rmul(RK_c6, g.x));
+      const double diy = radd(radd(radd(radd(rmul(RK_c1, a.y), rmul(RK_c3, c.y)), rmul(RK_c4, e.y)), rmul(RK_c5, f.y)),
+                              rmul(RK_c6, g.y));
+      const double2 yn = make_double2(radd(y.x, rmul(h, dix)), radd(y.y, rmul(h, diy)));
       B.yn[q] = yn;
-      const double ex = h * (RK_ec1 * a.x + RK_ec3 * c.x + RK_ec4 * e.x + RK_ec5 * f.x + RK_ec6 * g.x);
-      const double ey = h * (RK_ec1 * a.y + RK_ec3 * c.y + RK_ec4 * e.y + RK_ec5 * f.y + RK_ec6 * g.y);
-      const double rx = fabs(ex) / fabs(d.eps_rel * fabs(yn.x) + d.eps_abs);
-      const double ry = fabs(ey) / fabs(d.eps_rel * fabs(yn.y) + d.eps_abs);
+      const double ex = rmul(h, radd(radd(radd(radd(rmul(RK_ec1, a.x), rmul(RK_ec3, c.x)), rmul(RK_ec4, e.x)),
+                                           rmul(RK_ec5, f.x)), rmul(RK_ec6, g.x)));
+      const double ey = rmul(h, radd(radd(radd(radd(rmul(RK_ec1, a.y), rmul(RK_ec3, c.y)), rmul(RK_ec4, e.y)),
+                                           rmul(RK_ec5, f.y)), rmul(RK_ec6, g.y)));
+      const double rx = fabs(ex) / fabs(radd(rmul(d.eps_rel, fabs(yn.x)), d.eps_abs));
+      const double ry = fabs(ey) / fabs(radd(rmul(d.eps_rel, fabs(yn.y)), d.eps_abs));
       bad = bad || !(rx == rx) || !(ry == ry) || isinf(yn.x) || isinf(yn.y);
       rm = fmax(rm, fmax(rx, ry));
     }
@@ -170,8 +128,11 @@ __device__ __noinline__ void evolve_apply(Ctx<M>& X, Bufs& B, StepState& S, doub
     bool final_step = false;
     if ((dt >= 0.0 && h0 > dt) || (dt < 0.0 && h0 < dt)) { h0 = dt; final_step = true; }
     for (int s = 2; s <= 6; ++s) {
-      stage_input(X, B, s, h0);
+      // the RHS forms its own stage input from y and the k's (into zs as well)
+      const StageSrc st{B.y, {B.k[0], B.k[1], B.k[2], B.k[3], B.k[4]}, s, h0};
+      X.stg = &st;
       rhs_into(X, S, t0 + RK_ah[s - 2] * h0, B.k[s - 1]);
+      X.stg = nullptr;
     }
     member_sync(d.C);
     const double rmax = final_combine(X, B, h0);
