@@ -54,6 +54,39 @@ __global__ void k_to_reference(const double2* __restrict__ src, double* __restri
   ref[3 * N + q] = u.y;
 }
 
+// every member's state at once: member m = blockIdx.y reads its current state
+// pointer from its descriptor on the device (the stepper swaps buffers), so a whole
+// ensemble moves with one host copy and one launch, without host round trips
+__global__ void k_states_to_internal(DevMember* mems, const double* __restrict__ stage,
+                                     const long long* __restrict__ off) {
+  DevMember& d = mems[blockIdx.y];
+  const double* ref = stage + off[blockIdx.y];
+  const int N = d.N, C = d.C, M = d.M, logC = d.logC;
+  double2* dst = d.y;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < N; q += gridDim.x * blockDim.x) {
+    const int p = (q & (C - 1)) * M + (q >> logC);
+    dst[p] = make_double2(ref[q], ref[N + q]);
+    dst[N + p] = make_double2(ref[2 * N + q], ref[3 * N + q]);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) d.k1_valid = 0;   // the state changed under the stepper
+}
+
+__global__ void k_states_to_reference(const DevMember* __restrict__ mems, double* __restrict__ stage,
+                                      const long long* __restrict__ off) {
+  const DevMember& d = mems[blockIdx.y];
+  double* ref = stage + off[blockIdx.y];
+  const int N = d.N, C = d.C, M = d.M, logC = d.logC;
+  const double2* src = d.y;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < N; q += gridDim.x * blockDim.x) {
+    const int p = (q & (C - 1)) * M + (q >> logC);
+    const double2 e = src[p], u = src[N + p];
+    ref[q] = e.x;
+    ref[N + q] = e.y;
+    ref[2 * N + q] = u.x;
+    ref[3 * N + q] = u.y;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // host engine
 // ---------------------------------------------------------------------------
@@ -108,6 +141,10 @@ struct hw_ctx {
   int* d_single = nullptr;    // one-member list for single-member launches
   double* d_ref = nullptr;    // 4*maxN staging for reference-layout transfers
   int maxN = 0;
+  double* d_stage = nullptr;  // all members' states, reference layout, concatenated
+  long long* d_off = nullptr; // offset of each member in d_stage
+  size_t stage_doubles = 0;
+  bool ensure_stage();
   int device = 0;
   std::string err;
 
@@ -474,6 +511,8 @@ hw_ctx::~hw_ctx() {
   for (auto& h : mem)
     if (h.dev) cudaFree(h.dev);
   for (auto& e : tw) cudaFree(e.second);
+  if (d_stage) cudaFree(d_stage);
+  if (d_off) cudaFree(d_off);
   for (auto& c : classes) {
     if (c.d_list) cudaFree(c.d_list);
     if (c.stream) cudaStreamDestroy(c.stream);
@@ -776,46 +815,52 @@ int hw_deck_table(const char* workdir, const hw_opts* opts, const char* name, do
   return int(v.size());
 }
 
+bool hw_ctx::ensure_stage() {
+  if (d_stage) return true;
+  std::vector<long long> off(mem.size());
+  size_t tot = 0;
+  for (size_t i = 0; i < mem.size(); ++i) {
+    off[i] = (long long)tot;
+    tot += size_t(4) * mem[i].N;
+  }
+  HW_CUDA(cudaMalloc(&d_stage, sizeof(double) * std::max<size_t>(tot, 1)));
+  HW_CUDA(cudaMalloc(&d_off, sizeof(long long) * std::max<size_t>(off.size(), 1)));
+  HW_CUDA(cudaMemcpy(d_off, off.data(), sizeof(long long) * off.size(), cudaMemcpyHostToDevice));
+  stage_doubles = tot;
+  return true;
+}
+
+// every member's state to the host (concatenated reference layouts): one batched
+// layout kernel and one copy, ordered after the work already on the stream
 int hw_get_states(hw_ctx* ctx, double* y_all) {
   if (!ctx || !y_all) return 1;
   std::string& err = ctx->err;
   auto body = [&]() -> bool {
+    if (!ctx->ensure_stage()) return false;
+    const dim3 grid(unsigned((ctx->maxN + 255) / 256), unsigned(ctx->mem.size()));
+    k_states_to_reference<<<grid, 256, 0, ctx->stream>>>(ctx->d_mems, ctx->d_stage, ctx->d_off);
+    HW_CUDA(cudaGetLastError());
+    HW_CUDA(cudaMemcpyAsync(y_all, ctx->d_stage, sizeof(double) * ctx->stage_doubles, cudaMemcpyDeviceToHost,
+                            ctx->stream));
     HW_CUDA(cudaStreamSynchronize(ctx->stream));
-    size_t off = 0;
-    for (size_t i = 0; i < ctx->mem.size(); ++i) {
-      HostMember& hm = ctx->mem[i];
-      HW_CUDA(cudaMemcpyAsync(&hm.d, ctx->d_mems + i, sizeof(DevMember), cudaMemcpyDeviceToHost, ctx->stream));
-      HW_CUDA(cudaStreamSynchronize(ctx->stream));
-      k_to_reference<<<(hm.N + 255) / 256, 256, 0, ctx->stream>>>(hm.d.y, ctx->d_ref, hm.N, hm.logC, hm.M);
-      HW_CUDA(cudaGetLastError());
-      HW_CUDA(cudaMemcpyAsync(y_all + off, ctx->d_ref, sizeof(double) * 4 * hm.N, cudaMemcpyDeviceToHost,
-                              ctx->stream));
-      HW_CUDA(cudaStreamSynchronize(ctx->stream));
-      off += size_t(4) * hm.N;
-    }
     return true;
   };
   return body() ? 0 : 1;
 }
 
+// every member's state from the host: one copy and one batched layout kernel on the
+// stream (the next run starts after it, with each member's dydt_in recomputed)
 int hw_set_states(hw_ctx* ctx, const double* y_all) {
   if (!ctx || !y_all) return 1;
   std::string& err = ctx->err;
   auto body = [&]() -> bool {
-    HW_CUDA(cudaStreamSynchronize(ctx->stream));
-    size_t off = 0;
-    for (size_t i = 0; i < ctx->mem.size(); ++i) {
-      HostMember& hm = ctx->mem[i];
-      HW_CUDA(cudaMemcpy(&hm.d, ctx->d_mems + i, sizeof(DevMember), cudaMemcpyDeviceToHost));
-      HW_CUDA(cudaMemcpyAsync(ctx->d_ref, y_all + off, sizeof(double) * 4 * hm.N, cudaMemcpyHostToDevice,
-                              ctx->stream));
-      k_to_internal<<<(hm.N + 255) / 256, 256, 0, ctx->stream>>>(ctx->d_ref, hm.d.y, hm.N, hm.logC, hm.M);
-      HW_CUDA(cudaGetLastError());
-      HW_CUDA(cudaStreamSynchronize(ctx->stream));
-      hm.d.k1_valid = 0;
-      HW_CUDA(cudaMemcpy(&ctx->d_mems[i].k1_valid, &hm.d.k1_valid, sizeof(int), cudaMemcpyHostToDevice));
-      off += size_t(4) * hm.N;
-    }
+    if (!ctx->ensure_stage()) return false;
+    HW_CUDA(cudaMemcpyAsync(ctx->d_stage, y_all, sizeof(double) * ctx->stage_doubles, cudaMemcpyHostToDevice,
+                            ctx->stream));
+    const dim3 grid(unsigned((ctx->maxN + 255) / 256), unsigned(ctx->mem.size()));
+    k_states_to_internal<<<grid, 256, 0, ctx->stream>>>(ctx->d_mems, ctx->d_stage, ctx->d_off);
+    HW_CUDA(cudaGetLastError());
+    for (auto& hm : ctx->mem) hm.d.k1_valid = 0;
     return true;
   };
   return body() ? 0 : 1;

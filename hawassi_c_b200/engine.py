@@ -280,6 +280,10 @@ class Engine:
         return out
 
     def set_states(self, y_all):
+        """All member states from one host buffer (concatenated reference layouts).
+        The copy is queued on the engine's stream: a pinned buffer must stay
+        unchanged until the next synchronising call (run(sync=True), get_states)."""
+        y_all = np.ascontiguousarray(y_all, dtype=np.float64)
         self._check(load_library().hw_set_states(self._h, _dp(y_all)), "set_states")
 
     def class_timing(self):
