@@ -86,6 +86,7 @@ struct DevMember {
   const int* gidx;      // spline interval of each gauge (-1: outside the grid)
   double* gout;         // [n][2 ngauge]: eta, d eta / dt at the gauges per output sample
   double* gtim;         // [n]: time of each output sample
+  double* fields;       // [n][3][N]: eta, u, phi per output sample (nullptr: not kept)
   // control state
   double t, h, t1;      // current time, step, target of a single evolve_apply
   int i_out, i_stop;    // next output index, stop index (exclusive)

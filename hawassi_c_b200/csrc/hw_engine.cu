@@ -116,6 +116,7 @@ struct HostMember {
   DevMember d{};
   void* dev = nullptr;       // arena base
   size_t dev_bytes = 0;
+  double* fields = nullptr;  // per-sample eta, u, phi when the member keeps fields
   double t0 = 0, h0 = 0;
 };
 
@@ -508,8 +509,10 @@ bool hw_ctx::reset() {
 
 hw_ctx::~hw_ctx() {
   if (stream) cudaStreamSynchronize(stream);
-  for (auto& h : mem)
+  for (auto& h : mem) {
     if (h.dev) cudaFree(h.dev);
+    if (h.fields) cudaFree(h.fields);
+  }
   for (auto& e : tw) cudaFree(e.second);
   if (d_stage) cudaFree(d_stage);
   if (d_off) cudaFree(d_off);
@@ -949,6 +952,143 @@ int hw_gauges(hw_ctx* ctx, int member, double* eta, double* dteta, double* tim, 
   if (tim && cudaMemcpy(tim, h.d.gtim, sizeof(double) * rows, cudaMemcpyDeviceToHost) != cudaSuccess) {
     ctx->err = "gauge read-back failed";
     return -1;
+  }
+  return rows;
+}
+
+int hw_enable_fields(hw_ctx* ctx, int member, int enable) {
+  if (!valid_member(ctx, member)) return 1;
+  std::string& err = ctx->err;
+  auto body = [&]() -> bool {
+    HostMember& hm = ctx->mem[size_t(member)];
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (enable && !hm.fields) {
+      const size_t cnt = size_t(std::max(hm.m.n, 1)) * 3 * size_t(hm.N);
+      HW_CUDA(cudaMalloc(&hm.fields, sizeof(double) * cnt));
+    }
+    double* p = enable ? hm.fields : nullptr;
+    HW_CUDA(cudaMemcpy(&ctx->d_mems[member].fields, &p, sizeof(double*), cudaMemcpyHostToDevice));
+    hm.d.fields = p;
+    return true;
+  };
+  return body() ? 0 : 1;
+}
+
+// The reference's output files of one member from the device-computed samples
+// (1d/functions.c:557-760): per partition of NtoutIP = n / npartition samples a
+// Constants_NN.dat (print_xt, :784-801) and Hawassi_eta/u/phi_NN.dat (Nx doubles per
+// sample); the gauge text files (print_data_gauge, :500-522); breaking.dat.
+int hw_write_outputs(hw_ctx* ctx, int member, const char* outdir) {
+  if (!valid_member(ctx, member) || !outdir) return -1;
+  if (!ctx->sync_desc()) return -1;
+  HostMember& hm = ctx->mem[size_t(member)];
+  const hw::Member& m = hm.m;
+  const int N = hm.N, n = m.n, rows = hm.d.i_out;
+  const std::string dir(outdir);
+  std::vector<double> tim(size_t(std::max(rows, 1)));
+  if (rows > 0 && cudaMemcpy(tim.data(), hm.d.gtim, sizeof(double) * rows, cudaMemcpyDeviceToHost) != cudaSuccess) {
+    ctx->err = "output read-back failed";
+    return -1;
+  }
+  if (hm.fields && rows > 0) {
+    const int npart = std::max(m.deck.npartition, 1);
+    const int ntout = n / npart, ntrest = n - npart * ntout;
+    std::vector<double> f(size_t(rows) * 3 * N);
+    if (cudaMemcpy(f.data(), hm.fields, sizeof(double) * f.size(), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      ctx->err = "field read-back failed";
+      return -1;
+    }
+    FILE *fe = nullptr, *fu = nullptr, *fp = nullptr;
+    int ip = 0;
+    auto closeall = [&]() {
+      if (fe) std::fclose(fe);
+      if (fu) std::fclose(fu);
+      if (fp) std::fclose(fp);
+      fe = fu = fp = nullptr;
+    };
+    for (int i = 0; i < rows; ++i) {
+      if (ntout > 0 && i % ntout == 0) {
+        ++ip;
+        closeall();
+        char sfx[32];
+        std::snprintf(sfx, sizeof sfx, "%02d.dat", ip);
+        // print_xt: the rest partition is recognised by its length (N1 == Ntrest)
+        const int n1 = ip <= npart ? ntout : ntrest;
+        FILE* fc = std::fopen((dir + "/Constants_" + sfx).c_str(), "wb");
+        if (!fc) { ctx->err = "cannot write " + dir; return -1; }
+        const double NX = double(N), NT = double(n1);
+        std::fwrite(&NX, sizeof(double), 1, fc);
+        std::fwrite(m.x.data(), sizeof(double), size_t(N), fc);
+        std::fwrite(&NT, sizeof(double), 1, fc);
+        const size_t t0 = n1 == ntrest ? size_t(npart) * ntout : size_t(ip - 1) * ntout;
+        std::fwrite(m.ttrace.data() + t0, sizeof(double), size_t(n1), fc);
+        std::fwrite(m.depth.data(), sizeof(double), size_t(N), fc);
+        std::fwrite(m.k.data(), sizeof(double), size_t(N), fc);
+        std::fwrite(&m.nu_peak, sizeof(double), 1, fc);
+        std::fclose(fc);
+        fe = std::fopen((dir + "/Hawassi_eta_" + sfx).c_str(), "wb");
+        fu = std::fopen((dir + "/Hawassi_u_" + sfx).c_str(), "wb");
+        fp = std::fopen((dir + "/Hawassi_phi_" + sfx).c_str(), "wb");
+        if (!fe || !fu || !fp) { closeall(); ctx->err = "cannot write " + dir; return -1; }
+      }
+      const double* r = f.data() + size_t(i) * 3 * N;
+      std::fwrite(r, sizeof(double), size_t(N), fe);
+      std::fwrite(r + N, sizeof(double), size_t(N), fu);
+      std::fwrite(r + 2 * N, sizeof(double), size_t(N), fp);
+    }
+    closeall();
+  }
+  const int ng = hm.d.ngauge;
+  if (ng > 0 && rows > 0) {
+    std::vector<double> g(size_t(rows) * 2 * ng);
+    if (cudaMemcpy(g.data(), hm.d.gout, sizeof(double) * g.size(), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      ctx->err = "gauge read-back failed";
+      return -1;
+    }
+    FILE* f1 = std::fopen((dir + "/Hawassi_eta_gauge.txt").c_str(), "w");
+    FILE* f2 = std::fopen((dir + "/Hawassi_dteta_gauge.txt").c_str(), "w");
+    if (!f1 || !f2) {
+      if (f1) std::fclose(f1);
+      if (f2) std::fclose(f2);
+      ctx->err = "cannot write " + dir;
+      return -1;
+    }
+    std::fprintf(f1, "0 ");
+    std::fprintf(f2, "0 ");
+    for (int j = 0; j < ng; ++j) {
+      std::fprintf(f1, "%f ", m.gauge[size_t(j)]);
+      std::fprintf(f2, "%f ", m.gauge[size_t(j)]);
+    }
+    std::fprintf(f1, "\n");
+    std::fprintf(f2, "\n");
+    for (int i = 0; i < rows; ++i) {
+      std::fprintf(f1, "%f ", tim[size_t(i)]);
+      std::fprintf(f2, "%f ", tim[size_t(i)]);
+      for (int j = 0; j < ng; ++j) {
+        std::fprintf(f1, "%f ", g[size_t(i) * 2 * ng + j]);
+        std::fprintf(f2, "%f ", g[size_t(i) * 2 * ng + ng + j]);
+      }
+      std::fprintf(f1, "\n");
+      std::fprintf(f2, "\n");
+    }
+    std::fclose(f1);
+    std::fclose(f2);
+  }
+  if (m.breaking) {
+    long long len = 0;
+    if (hw_breaking_log(ctx, member, nullptr, 0, &len) < 0) return -1;
+    std::vector<double> lg(size_t(std::max(len, 1LL)));
+    if (len > 0 && hw_breaking_log(ctx, member, lg.data(), len, &len) < 0) return -1;
+    FILE* fb = std::fopen((dir + "/breaking.dat").c_str(), "w");
+    if (!fb) { ctx->err = "cannot write " + dir; return -1; }
+    for (long long i = 0; i + 1 < len;) {   // records: t, count, nodes (1d/breaking.c:434)
+      const int cnt = int(lg[size_t(i + 1)]);
+      std::fprintf(fb, "%lf %d ", lg[size_t(i)], cnt);
+      for (int q = 0; q < cnt; ++q) std::fprintf(fb, "%d ", int(lg[size_t(i + 2 + q)]));
+      std::fprintf(fb, "\n");
+      i += 2 + cnt;
+    }
+    std::fclose(fb);
   }
   return rows;
 }

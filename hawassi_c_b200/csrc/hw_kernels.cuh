@@ -44,7 +44,7 @@ __global__ void __launch_bounds__(M / kPts, HW_EVOLVE_MIN_BLOCKS(M)) k_evolve(De
           if (S.rhs >= sd.rhs_budget && S.status == kOk) S.status = kBudget;   // bounded launch
         }
         if (S.status == kOk) {
-          if (sd.ngauge > 0) gauge_stage<M>(X, B, S, iout);
+          if (sd.ngauge > 0 || sd.fields) output_stage<M>(X, B, S, iout);
           ++iout;
         }
       }

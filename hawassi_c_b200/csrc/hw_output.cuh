@@ -1,8 +1,9 @@
-// hw_output.cuh -- the output stage of ode_solver_Ham (1d/functions.c:557-760) for
-// the gauges, on the device: at every output sample the physical elevation and its
-// time derivative (real parts of the inverse transforms of eta^ and of the last
-// RHS's d eta^/dt, the reference's global dy) and their GSL natural cubic splines
-// evaluated at the gauge positions (print_data_gauge).
+// hw_output.cuh -- the output stage of ode_solver_Ham (1d/functions.c:557-760) on
+// the device: at every output sample the physical elevation and its time derivative
+// (real parts of the inverse transforms of eta^ and of the last RHS's d eta^/dt,
+// the reference's global dy), their GSL natural cubic splines evaluated at the gauge
+// positions (print_data_gauge), and, when the member keeps fields, eta, u and
+// phi = Re F^-1(-i u^ / k) for the Hawassi_{eta,u,phi}_NN.dat files.
 //
 // The spline's second-derivative coefficients solve a tridiagonal system over the
 // whole grid; on a grid of near-uniform spacing the inverse of that matrix decays
@@ -28,7 +29,7 @@ __device__ __forceinline__ double2 phys_at(double2* buf, int C, int m) {
 }
 
 template <int M>
-__device__ __noinline__ void gauge_stage(Ctx<M>& X, Bufs& B, StepState& S, int row) {
+__device__ __noinline__ void output_stage(Ctx<M>& X, Bufs& B, StepState& S, int row) {
   const DevMember& d = X.d;
   const int N = d.N, C = d.C;
   // the derivative the reference's dy holds at this sample: the RHS it evaluated
@@ -72,7 +73,14 @@ __device__ __noinline__ void gauge_stage(Ctx<M>& X, Bufs& B, StepState& S, int r
   fft_inverse<M>(A, d.tw, N, C, X.c);
   member_sync(C);
   // A: (eta, d eta / dt) at grid points c*M + i
-  if (X.c == 0) {
+  double* fr = d.fields ? d.fields + (size_t)row * 3 * N : nullptr;
+  if (fr) {
+    HW_FOREACH(X) {
+      (void)idx;
+      fr[X.c * M + idx] = A[pidx(idx)].x;
+    }
+  }
+  if (X.c == 0 && d.ngauge > 0) {
     for (int g = X.tid; g < d.ngauge; g += Ctx<M>::T) {
       const int i = d.gidx[g];
       double ve = __longlong_as_double(0x7ff8000000000000ULL), vd = ve;
@@ -149,6 +157,36 @@ __device__ __noinline__ void gauge_stage(Ctx<M>& X, Bufs& B, StepState& S, int r
       d.gout[(size_t)row * 2 * d.ngauge + d.ngauge + g] = vd;
     }
     if (X.tid == 0) d.gtim[row] = S.t;
+  }
+  if (X.c == 0 && X.tid == 0 && d.ngauge == 0) d.gtim[row] = S.t;
+  member_sync(C);
+  if (!fr) return;
+  // u and phi = Re F^-1(-i u^ / k) (1d/functions.c:571-590: the k == 0 mode is zero)
+  HW_FOREACH(X) {
+    A[pidx(idx)] = B.y[N + p];
+  }
+  member_sync(C);
+  HW_FOREACH(X) {
+    const int jp = X.c == 0 ? ((M - idx) & (M - 1)) : (M - 1 - idx);
+    const int pp = partner_pos(X, idx);
+    const double2 uh = A[pidx(idx)], up = Ap[pidx(jp)];
+    const double kq = d.k[p], kpp = d.k[pp];
+    const double2 ph = kq == 0 ? make_double2(0.0, 0.0) : mul_ik(-1 / kq, uh);
+    const double2 php = kpp == 0 ? make_double2(0.0, 0.0) : mul_ik(-1 / kpp, up);
+    va[u] = pack(herm(uh, up), herm(ph, php), d.invN);
+  }
+  member_sync(C);
+  HW_FOREACH(X) {
+    (void)p;
+    A[pidx(idx)] = va[u];
+  }
+  fft_inverse<M>(A, d.tw, N, C, X.c);
+  member_sync(C);
+  HW_FOREACH(X) {
+    (void)p;
+    const double2 v = A[pidx(idx)];
+    fr[N + X.c * M + idx] = v.x;
+    fr[2 * N + X.c * M + idx] = v.y;
   }
   member_sync(C);
 }

@@ -47,7 +47,7 @@ influxing \t= {influxing}
 propagation \t= {propagation}
 kinematic \t= no
 ngauge \t\t= {ngauge}
-npartition \t= 1
+npartition \t= {npartition}
 
 &IF BREAKING
 initiation \t= {kbc}
@@ -131,7 +131,7 @@ def write_deck(path, nx, length=None, xstart=0.0, xinflux=None, depth=1.0, bath=
                breaking=False, T_end=100.0, n_samples=2048, n_lines=1024, Hs=0.10, Tp=2.0, gamma=3.3,
                seed=0, damp=(10.0, 10.0), adjcoef=0.5, propagation="Uni+", influxing="Area",
                kbc=0.8, tc=0.2, tchar=0.5, cutfrac="default", ramp="yes 4", wavename="user_defined",
-               initial="zero", initial_wave=None, gauges=(), dt=0.02):
+               initial="zero", initial_wave=None, gauges=(), dt=0.02, npartition=1):
     """Write one deck directory.  bath: None for flat depth, or an array of nx depths."""
     os.makedirs(path, exist_ok=True)
     length = float(length if length is not None else 0.05 * nx)
@@ -144,7 +144,7 @@ def write_deck(path, nx, length=None, xstart=0.0, xinflux=None, depth=1.0, bath=
         Xinflux=repr(float(xinflux)), dx=repr(dx_for(length, nx)), dampL=repr(float(damp[0])),
         dampR=repr(float(damp[1])), bath="flat" if bath is None else "user_defined", depth=repr(float(depth)),
         adjcoef=repr(float(adjcoef)), model=model, breaking="yes" if breaking else "no", influxing=influxing,
-        propagation=propagation, ngauge=len(gauges), kbc=repr(float(kbc)), tc=repr(float(tc)),
+        propagation=propagation, ngauge=len(gauges), npartition=int(npartition), kbc=repr(float(kbc)), tc=repr(float(tc)),
         tchar=repr(float(tchar)), cutfrac=cutfrac, ramp=ramp)
     with open(os.path.join(path, "input.txt"), "w") as f:
         f.write(_INPUT.format(**fields))

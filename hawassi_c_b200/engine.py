@@ -41,7 +41,7 @@ EXPORTS = [
     "hw_mlp_set_params", "hw_mlp_grad", "hw_mlp_grad_device", "hw_mlp_train", "hw_mlp_infer",
     "hw2d_create", "hw2d_destroy", "hw2d_last_error", "hw2d_nx", "hw2d_ny", "hw2d_rhs", "hw2d_gsl_rhs",
     "hw2d_evolve_apply", "hw2d_set_state", "hw2d_get_state", "hw2d_run_to_time", "hw2d_stats",
-    "hw2d_set_stream", "hw2d_synchronize", "hw2d_launches", "hw_gauges", "hw_ngauge",
+    "hw2d_set_stream", "hw2d_synchronize", "hw2d_launches", "hw_gauges", "hw_ngauge", "hw_enable_fields", "hw_write_outputs",
 ]
 
 
@@ -83,6 +83,8 @@ def load_library():
     L.hw_rhs_noalloc.argtypes = [vp, ip, dd, vp, vp, vp]
     L.hw_gauges.argtypes = [vp, ip, dp, dp, dp, ip]
     L.hw_ngauge.argtypes = [vp, ip]
+    L.hw_enable_fields.argtypes = [vp, ip, ip]
+    L.hw_write_outputs.argtypes = [vp, ip, ctypes.c_char_p]
     L.hw_energy.argtypes = [vp, ip, dp, dp]
     L.hw_run_members.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     L.hw_set_operator_weights.argtypes = [vp, ip, ip, dp, dp]
@@ -258,6 +260,21 @@ class Engine:
         if rows < 0:
             raise EngineError(L.hw_last_error(self._h).decode())
         return tim[:rows], eta[:rows, :ng], dt[:rows, :ng]
+
+    def enable_fields(self, member=0, enable=True):
+        """Keep eta, u, phi of every output sample of the member on the device."""
+        self._check(load_library().hw_enable_fields(self._h, member, int(bool(enable))), "enable_fields")
+
+    def write_outputs(self, outdir, member=0):
+        """The reference's output files (Constants/Hawassi_*_NN.dat, gauge text files,
+        breaking.dat) of the member into outdir; returns the samples written."""
+        import os
+        os.makedirs(outdir, exist_ok=True)
+        L = load_library()
+        rows = L.hw_write_outputs(self._h, member, str(outdir).encode())
+        if rows < 0:
+            raise EngineError(L.hw_last_error(self._h).decode())
+        return rows
 
     def breaking_log(self, member=0):
         """breaking.dat records [(t, [nodes...]), ...] of the member."""

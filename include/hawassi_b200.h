@@ -158,6 +158,15 @@ int hw_deck_table(const char* workdir, const hw_opts* opts, const char* name, do
 int hw_gauges(hw_ctx* ctx, int member, double* eta, double* dteta, double* tim, int cap);
 int hw_ngauge(const hw_ctx* ctx, int member);
 
+/* Keep eta, u and phi of every output sample on the device (enable = 1, before
+ * hw_run; 3 * Nx doubles per sample of the member's deck). */
+int hw_enable_fields(hw_ctx* ctx, int member, int enable);
+/* Write the reference's output files of a member into outdir (1d/functions.c:557-801):
+ * Constants_NN.dat and Hawassi_{eta,u,phi}_NN.dat per partition (when fields are
+ * kept), Hawassi_eta_gauge.txt / Hawassi_dteta_gauge.txt (when the deck has gauges)
+ * and breaking.dat (breaking decks).  Returns the samples written or -1. */
+int hw_write_outputs(hw_ctx* ctx, int member, const char* outdir);
+
 int hw_set_stream(hw_ctx* ctx, void* cuda_stream);
 int hw_synchronize(hw_ctx* ctx);
 

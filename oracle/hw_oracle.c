@@ -1738,6 +1738,24 @@ int or_run(or_ctx* c, double* gauge_eta, double* gauge_dteta, double* tim_out, i
                 ip++;
                 char p[1024];
                 if (fe) fclose(fe); if (fu) fclose(fu); if (fp) fclose(fp);
+                /* print_xt (1d/functions.c:784-801): the rest partition is recognised by
+                 * its length, N1 == Ntrest */
+                int Ntrest = n - c->npartition * NtoutIP;
+                int N1 = ip <= c->npartition ? NtoutIP : Ntrest;
+                snprintf(p, sizeof p, "%s/Constants_%02d.dat", c->outdir, ip);
+                FILE* fc = fopen(p, "wb");
+                if (fc) {
+                    double NX = (double)Nx, NT = (double)N1;
+                    fwrite(&NX, sizeof(double), 1, fc);
+                    fwrite(c->x, sizeof(double), (size_t)Nx, fc);
+                    fwrite(&NT, sizeof(double), 1, fc);
+                    if (N1 == Ntrest) fwrite(c->ttrace + (size_t)c->npartition * NtoutIP, sizeof(double), (size_t)N1, fc);
+                    else fwrite(c->ttrace + (size_t)(ip - 1) * NtoutIP, sizeof(double), (size_t)N1, fc);
+                    fwrite(c->depth, sizeof(double), (size_t)Nx, fc);
+                    fwrite(c->k, sizeof(double), (size_t)Nx, fc);
+                    fwrite(&c->nu_peak, sizeof(double), 1, fc);
+                    fclose(fc);
+                }
                 snprintf(p, sizeof p, "%s/Hawassi_eta_%02d.dat", c->outdir, ip); fe = fopen(p, "wb");
                 snprintf(p, sizeof p, "%s/Hawassi_u_%02d.dat", c->outdir, ip); fu = fopen(p, "wb");
                 snprintf(p, sizeof p, "%s/Hawassi_phi_%02d.dat", c->outdir, ip); fp = fopen(p, "wb");

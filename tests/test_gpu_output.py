@@ -48,3 +48,62 @@ def test_gauges_pure_rhs(tmp_path, nx, cluster):
     assert np.array_equal(tim, to) or np.allclose(tim, to, rtol=1e-13, atol=0)
     assert np.abs(eta - eo).max() <= 1e-9 * np.abs(eo).max()
     assert np.abs(deta - do).max() <= 1e-8 * np.abs(do).max()
+
+
+def _read_constants(path):
+    a = np.fromfile(path, dtype=np.float64)
+    nx = int(a[0])
+    nt = int(a[1 + nx])
+    rest = a[2 + nx + nt:]
+    return dict(x=a[1:1 + nx], t=a[2 + nx:2 + nx + nt], depth=rest[:nx], k=rest[nx:2 * nx],
+                nu_peak=rest[2 * nx:2 * nx + 1])
+
+
+def test_output_files_match_golden_constants_and_oracle(golden_dir, tmp_path):
+    deck = os.path.join(golden_dir, "fbr005")
+    e = hw.Engine(deck, cluster=2)
+    e.enable_fields()
+    e.run_to_time(2.0)
+    rows = e.write_outputs(str(tmp_path / "gpu"))
+    assert rows >= 90
+    # Constants_01.dat: the reference's own output, array for array
+    gold = np.load(os.path.join(golden_dir, "fbr005_constants.npz"))
+    mine = _read_constants(str(tmp_path / "gpu" / "Constants_01.dat"))
+    for key in ("x", "t", "depth", "k", "nu_peak"):
+        assert np.array_equal(mine[key], gold[key]), key
+    # fields and gauge text against the oracle's output loop
+    os.makedirs(tmp_path / "ora", exist_ok=True)
+    o = ol.Oracle(deck, t_stop=2.0, write_fields=1, outdir=str(tmp_path / "ora"))
+    o.run()
+    o.close()
+    nx = e.nx[0]
+    for name in ("eta", "u", "phi"):
+        a = np.fromfile(str(tmp_path / "gpu" / f"Hawassi_{name}_01.dat")).reshape(-1, nx)
+        b = np.fromfile(str(tmp_path / "ora" / f"Hawassi_{name}_01.dat")).reshape(-1, nx)
+        r = min(len(a), len(b))
+        assert r >= 90
+        assert np.abs(a[:r] - b[:r]).max() <= 1e-9 * np.abs(b[:r]).max(), name
+    assert open(tmp_path / "gpu" / "Hawassi_eta_gauge.txt").readline().split() == ["0", "20.000000"]
+
+
+def test_output_partitions(tmp_path):
+    deck = small_deck(tmp_path, "part", nx=1024, T_end=2.0, n_samples=101, npartition=3,
+                      gauges=(10.0, 25.0))
+    e = hw.Engine(deck, eps_abs=1e-8, eps_rel=1e-6)
+    e.enable_fields()
+    e.run()
+    assert e.write_outputs(str(tmp_path / "gpu")) == 101
+    os.makedirs(tmp_path / "ora", exist_ok=True)
+    o = ol.Oracle(deck, eps_abs=1e-8, eps_rel=1e-6, write_fields=1, outdir=str(tmp_path / "ora"))
+    o.run()
+    o.close()
+    # 101 samples in 3 partitions of 33 and a rest of 2: files 01..04
+    for ip in range(1, 5):
+        sfx = f"{ip:02d}.dat"
+        a = open(tmp_path / "gpu" / f"Constants_{sfx}", "rb").read()
+        b = open(tmp_path / "ora" / f"Constants_{sfx}", "rb").read()
+        assert a == b, sfx
+        fa = np.fromfile(str(tmp_path / "gpu" / f"Hawassi_eta_{sfx}"))
+        fb = np.fromfile(str(tmp_path / "ora" / f"Hawassi_eta_{sfx}"))
+        assert fa.size == fb.size and fa.size == (33 if ip <= 3 else 2) * 1024
+        assert np.abs(fa - fb).max() <= 1e-9 * max(np.abs(fb).max(), 1e-300)
