@@ -477,7 +477,7 @@ def main():
     ms = ev0.elapsed_time(ev1)
     log(f"timed {args.steps} steps: {ms:.1f} ms")
     pts1, sim1 = rhs_pts(), sim_time()
-    launches = args.steps * len(eng.class_timing())
+    launches = args.steps * (len(eng.class_timing()) + 1)   # per step: k_resume + one k_evolve per class
     if world > 1:
         (ms,), (tot_pts, tot_sim) = reduce_ranks([ms], [float(pts1 - pts0), sim1 - sim0], "cuda")
     else:
