@@ -401,6 +401,8 @@ def main():
     ap.add_argument("--window", type=int, default=WINDOW)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="ensemble", choices=["ensemble", "2d"])
+    ap.add_argument("--autotune", action="store_true",
+                    help="pick the slice per grid size by timing candidates on the device first")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
@@ -438,7 +440,13 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     import hawassi_c_b200 as hw
-    eng = hw.Engine(decks, eps_abs=EPS_ABS, eps_rel=EPS_REL, device=local)
+    slices = None
+    if args.autotune:
+        from hawassi_c_b200.autotune import autotune_slices
+        slices, _ = autotune_slices(decks, window=args.window, device=local, eps_abs=EPS_ABS, eps_rel=EPS_REL,
+                                    log=log)
+        log(f"autotuned slices {slices}")
+    eng = hw.Engine(decks, eps_abs=EPS_ABS, eps_rel=EPS_REL, device=local, slices=slices)
     log("engine created")
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -554,7 +562,8 @@ def main():
             "data": "synthetic seeded decks (JONSWAP influx, flat depths) in the reference input format",
             "config": {"workload": WORKLOAD, "members_per_gpu": args.members, "window_samples": args.window,
                        "l2": "working set well above L2 (126 MB): no flush needed",
-                       "grid_sizes": sorted(set(nx))},
+                       "grid_sizes": sorted(set(nx)),
+                       "slices": ({str(k): v for k, v in slices.items()} if slices else "2048 (default)")},
             "rhs_points_per_step": tot_pts / args.steps,
             "sim_s_per_wall_s": tot_sim / (ms / 1e3),
             "sim_s_per_wall_s_per_member": tot_sim / (ms / 1e3) / (args.members * world),

@@ -149,7 +149,7 @@ struct hw_ctx {
   int device = 0;
   std::string err;
 
-  bool init(const std::vector<std::string>& dirs, const hw_opts* o);
+  bool init(const std::vector<std::string>& dirs, const hw_opts* o, const int* member_slice = nullptr);
   bool upload_member(HostMember& h);
   bool launch_class(const Class& c, const int* list, int nblocks_members, int mode, cudaStream_t s);
   bool launch_member(int mi, int mode, double t_rhs);
@@ -350,7 +350,7 @@ bool hw_ctx::upload_member(HostMember& h) {
   return true;
 }
 
-bool hw_ctx::init(const std::vector<std::string>& dirs, const hw_opts* o) {
+bool hw_ctx::init(const std::vector<std::string>& dirs, const hw_opts* o, const int* member_slice) {
   hw_opts opt{};
   if (o) opt = *o;
   device = opt.device;
@@ -383,7 +383,7 @@ bool hw_ctx::init(const std::vector<std::string>& dirs, const hw_opts* o) {
       return false;
     }
     h.N = N;
-    const int slice = opt.slice > 0 ? opt.slice : 2048;
+    const int slice = (member_slice && member_slice[i] > 0) ? member_slice[i] : (opt.slice > 0 ? opt.slice : 2048);
     int C = opt.cluster > 0 ? opt.cluster : std::max(1, N / slice);
     if ((C & (C - 1)) != 0 || N / C < 256 || N / C > 2048 || C > 16) {
       err = "invalid cluster size " + std::to_string(C) + " for Nx=" + std::to_string(N);
@@ -557,6 +557,19 @@ hw_ctx* hw_ensemble_create(const char* const* workdirs, int n, const hw_opts* op
   std::vector<std::string> dirs;
   for (int i = 0; i < n; ++i) dirs.emplace_back(workdirs[i] ? workdirs[i] : "");
   if (!c->init(dirs, opts)) {
+    g_create_err = c->err;
+    return nullptr;
+  }
+  return c.release();
+}
+
+hw_ctx* hw_ensemble_create_sliced(const char* const* workdirs, int n, const hw_opts* opts,
+                                  const int* member_slice) {
+  if (!workdirs || n <= 0) { g_create_err = "no member decks given"; return nullptr; }
+  std::unique_ptr<hw_ctx> c(new hw_ctx());
+  std::vector<std::string> dirs;
+  for (int i = 0; i < n; ++i) dirs.emplace_back(workdirs[i] ? workdirs[i] : "");
+  if (!c->init(dirs, opts, member_slice)) {
     g_create_err = c->err;
     return nullptr;
   }

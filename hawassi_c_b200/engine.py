@@ -32,7 +32,7 @@ def library_path():
 
 
 EXPORTS = [
-    "hw_create", "hw_ensemble_create", "hw_destroy", "hw_last_error", "hw_members", "hw_nx", "hw_nt",
+    "hw_create", "hw_ensemble_create", "hw_ensemble_create_sliced", "hw_destroy", "hw_last_error", "hw_members", "hw_nx", "hw_nt",
     "hw_initial_state", "hw_rhs", "hw_gsl_rhs", "hw_evolve_apply", "hw_run", "hw_run_to_time",
     "hw_get_state", "hw_set_state", "hw_reset", "hw_member_stats", "hw_last_dydt", "hw_breaking_log",
     "hw_set_stream", "hw_synchronize", "hw_deck_table", "hw_get_states", "hw_set_states",
@@ -59,6 +59,9 @@ def load_library():
     L.hw_create.argtypes = [ctypes.c_char_p, ctypes.POINTER(HwOpts)]
     L.hw_ensemble_create.restype = vp
     L.hw_ensemble_create.argtypes = [ctypes.POINTER(ctypes.c_char_p), ip, ctypes.POINTER(HwOpts)]
+    L.hw_ensemble_create_sliced.restype = vp
+    L.hw_ensemble_create_sliced.argtypes = [ctypes.POINTER(ctypes.c_char_p), ip, ctypes.POINTER(HwOpts),
+                                            ctypes.POINTER(ctypes.c_int)]
     L.hw_destroy.argtypes = [vp]
     L.hw_last_error.restype = ctypes.c_char_p
     L.hw_last_error.argtypes = [vp]
@@ -118,14 +121,24 @@ class Engine:
     (``Engine(["deck0", "deck1", ...])``) on one GPU."""
 
     def __init__(self, decks, eps_abs=0.0, eps_rel=0.0, h0=0.0, seed=0, nref=0, exact_sequence=False,
-                 cluster=0, device=0, slice=0):
+                 cluster=0, device=0, slice=0, slices=None):
+        """slices: grid points per CTA per grid size ({Nx: points}, e.g. from
+        autotune.autotune_slices) or per member (a list); others use `slice`."""
         L = load_library()
         if isinstance(decks, (str, os.PathLike)):
             decks = [decks]
         self.decks = [os.fspath(d) for d in decks]
         opts = HwOpts(eps_abs, eps_rel, h0, seed, nref, int(bool(exact_sequence)), cluster, device, slice)
         arr = (ctypes.c_char_p * len(self.decks))(*[d.encode() for d in self.decks])
-        self._h = L.hw_ensemble_create(arr, len(self.decks), ctypes.byref(opts))
+        if slices is None:
+            self._h = L.hw_ensemble_create(arr, len(self.decks), ctypes.byref(opts))
+        else:
+            if isinstance(slices, dict):
+                per = [int(slices.get(int(deck_table(d, "Nx")[0]), 0)) for d in self.decks]
+            else:
+                per = [int(v) for v in slices]
+            ms = (ctypes.c_int * len(self.decks))(*per)
+            self._h = L.hw_ensemble_create_sliced(arr, len(self.decks), ctypes.byref(opts), ms)
         if not self._h:
             raise EngineError(L.hw_last_error(None).decode())
         self.members = L.hw_members(self._h)

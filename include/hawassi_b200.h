@@ -40,6 +40,10 @@ hw_ctx* hw_create(const char* workdir, const hw_opts* opts);
 /* Batched ragged ensemble: one member per deck directory, uneven grid sizes allowed;
  * all members advance together in one launch per grid-size class. */
 hw_ctx* hw_ensemble_create(const char* const* workdirs, int n_members, const hw_opts* opts);
+/* The same with the grid points per CTA chosen per member (0: opts->slice); the
+ * autotuner (hawassi_c_b200/autotune.py) picks them per grid size by timing. */
+hw_ctx* hw_ensemble_create_sliced(const char* const* workdirs, int n_members, const hw_opts* opts,
+                                  const int* member_slice);
 
 void        hw_destroy(hw_ctx* ctx);
 const char* hw_last_error(const hw_ctx* ctx);   /* ctx may be NULL (last create error) */
