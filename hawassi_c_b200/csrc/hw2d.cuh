@@ -89,6 +89,8 @@ struct Work2 {
   double* pe;                   // eta M0u, eta M0v in physical space (2 real fields)
   double2* H1;                  // delu H1^, delv H1^ (2 fields)
   double2* EU;                  // (eta u)^, (eta v)^, deletaH2^ (3 fields)
+  // kinematic breaking only: delphiH^ as the assembly forms it (nullptr: off)
+  double2* dph;
 };
 
 // device control block of the stepper (one per engine)
@@ -96,9 +98,13 @@ struct Ctl2 {
   double t, h, h0, t1, t_direct, eps_abs, eps_rel;
   int final_step, done, status, cur, k1i, need_k1, need_kout, attempts;
   long long rhs, acc, rej;
+  // kinematic breaking on: every evolve_apply evaluates its own dydt_in and every
+  // attempt its dydt_out (mode 8) before the step control, as gsl_odeiv2 does,
+  // since each RHS past tprev advances the breaking state
+  int brk;
 };
 
-enum { kOk = 0, kNonFinite = 1, kStepFailed = 2 };
+enum { kOk = 0, kNonFinite = 1, kStepFailed = 2, kBreakCapacity = 3 };
 // RHS launch conditions
 enum { kAlways = 0, kIfK1 = 1, kIfStage = 2, kIfKout = 3 };
 
@@ -273,9 +279,13 @@ __device__ __forceinline__ double spline2(const double* __restrict__ xs, const d
   return yl + dx * (bi + dx * (ci + dx * di));
 }
 
+// modes: 0 direct RHS, 1 k1 (dydt_in), 2..6 the rkf45 stages, 7 k_out after an
+// accepted step (reused as the next k1), 8 dydt_out of the attempt's candidate
+// state at t + h before the step control (breaking runs)
 __device__ __forceinline__ double stage_time(const Ctl2* c, int mode) {
   if (mode == 0) return c->t_direct;
   if (mode == 1 || mode == 7) return c->t;
+  if (mode == 8) return c->t + c->h0;
   return c->t + A2_ah[mode - 2] * c->h0;
 }
 
@@ -285,6 +295,7 @@ __device__ __forceinline__ double ra2(double a, double b) { return __dadd_rn(a, 
 
 // stage input at element q (3n double2 per state): GSL rkf45's expression forms
 __device__ __forceinline__ double2 stage_value(const RK2& B, const Ctl2* c, int mode, size_t q) {
+  if (mode == 8) return B.y[c->cur ^ 1][q];
   const double2 y = B.y[c->cur][q];
   if (mode <= 1 || mode == 7) return y;
   const double h = c->h0;
@@ -321,6 +332,14 @@ __device__ __forceinline__ double2 stage_value(const RK2& B, const Ctl2* c, int 
 
 // ---------------------------------------------------------------------------
 // stage input z = y + h sum_j b_sj k_j of every point, a streaming pass ahead of the
+// the buffer an RHS of the given mode writes
+__device__ __forceinline__ double2* rhs_out(const RK2& rk, const Ctl2* ctl, int mode, double2* direct_out) {
+  if (mode == 0) return direct_out;
+  if (mode == 1) return rk.kk[ctl->k1i];
+  if (mode == 7 || mode == 8) return rk.kk[ctl->k1i ^ 1];
+  return rk.ks[mode - 2];
+}
+
 // first row pass (mode 1 and 7: z = y)
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
@@ -642,11 +661,7 @@ k2_rowE(Tab2 tb, Work2 w, RK2 rk, const Ctl2* __restrict__ ctl, int mode, int co
   }
   __syncthreads();
   if (!tb.chi_one) fft_slices<M>(sm, 8, tb.twx, -1);
-  double2* out;
-  if (mode == 0) out = direct_out;
-  else if (mode == 1) out = rk.kk[ctl->k1i];
-  else if (mode == 7) out = rk.kk[ctl->k1i ^ 1];
-  else out = rk.ks[mode - 2];
+  double2* out = rhs_out(rk, ctl, mode, direct_out);
   for (int k = 0; k < 2; ++k) {
     const int r = P.r[k];
     const double kyv = tb.ky[r];
@@ -668,6 +683,7 @@ k2_rowE(Tab2 tb, Work2 w, RK2 rk, const Ctl2* __restrict__ ctl, int mode, int co
       const double2 ix = slot(sm, M, 0 + k, j), iy = slot(sm, M, 2 + k, j);
       const double2 au = slot(sm, M, 4 + k, j), av = slot(sm, M, 6 + k, j);
       dphi = make_double2(dphi.x + au.x + av.x, dphi.y + au.y + av.y);
+      if (w.dph) w.dph[q] = dphi;
       const double2 S = tb.has_src ? w.src[q] : make_double2(0.0, 0.0);
       const double2 de = w.D[q], du = w.D[n + q], dv = w.D[2 * n + q];
       out[q] = make_double2((S.x + dphi.x - de.x) * a, (S.y + dphi.y - de.y) * a);
@@ -787,7 +803,7 @@ __global__ void k2_control(Ctl2* c, const Work2 w, int nparts) {
   const double tk = t0 + h_old;
   c->t = tn;
   c->h = hn;
-  if (tk == tn) c->need_kout = 1;
+  if (tk == tn && !c->brk) c->need_kout = 1;
   else c->need_k1 = 1;
   if (!(c->t < c->t1)) c->done = 1;
   else set_prologue(c);

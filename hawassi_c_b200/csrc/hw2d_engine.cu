@@ -16,6 +16,7 @@
 
 #include "../../include/hawassi_b200.h"
 #include "hw2d.cuh"
+#include "hw2d_brk.cuh"
 #include "hw2d_var.cuh"
 #include "hw_setup.hpp"
 
@@ -48,6 +49,46 @@ void set_attrs() {
   cudaFuncSetAttribute(hw2d::k2v_rowE<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(6));
   cudaFuncSetAttribute(hw2d::k2v_colF<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(8));
   cudaFuncSetAttribute(hw2d::k2v_rowG<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(8));
+  cudaFuncSetAttribute(hw2d::k2b_rowI<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(2));
+  cudaFuncSetAttribute(hw2d::k2b_colI<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(2));
+  cudaFuncSetAttribute(hw2d::k2b_sbcol<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(2));
+  cudaFuncSetAttribute(hw2d::k2b_sbrow<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(2));
+}
+
+// the breaking kernels of one RHS (row passes: row length M = nx; column passes: M = ny)
+template <int M>
+void launch_brk_row(int which, int nblocks, cudaStream_t s, const Tab2& tb, const Work2& w, const hw2d::Brk2& b,
+                    const RK2& rk, const Ctl2* ctl, int mode, int cond, double2* out) {
+  const int blk = hw2d::kGroups * (M / 8);
+  if (which == 0) hw2d::k2b_rowI<M><<<nblocks, blk, smem_bytes<M>(2), s>>>(tb, w, b, rk, ctl, mode, cond, out);
+  else hw2d::k2b_sbrow<M><<<nblocks, blk, smem_bytes<M>(2), s>>>(tb, b, rk, ctl, mode, cond, out);
+}
+template <int M>
+void launch_brk_col(int which, int nblocks, cudaStream_t s, const Tab2& tb, const Work2& w, const hw2d::Brk2& b,
+                    const Ctl2* ctl, int mode, int cond) {
+  const int blk = hw2d::kGroups * (M / 8);
+  if (which == 0) hw2d::k2b_colI<M><<<nblocks, blk, smem_bytes<M>(2), s>>>(tb, b, ctl, mode, cond);
+  else hw2d::k2b_sbcol<M><<<nblocks, blk, smem_bytes<M>(2), s>>>(tb, w, b, ctl, mode, cond);
+}
+void brk_row(int M, int which, int nb, cudaStream_t s, const Tab2& tb, const Work2& w, const hw2d::Brk2& b,
+             const RK2& rk, const Ctl2* ctl, int mode, int cond, double2* out) {
+  switch (M) {
+    case 64: launch_brk_row<64>(which, nb, s, tb, w, b, rk, ctl, mode, cond, out); break;
+    case 128: launch_brk_row<128>(which, nb, s, tb, w, b, rk, ctl, mode, cond, out); break;
+    case 256: launch_brk_row<256>(which, nb, s, tb, w, b, rk, ctl, mode, cond, out); break;
+    case 512: launch_brk_row<512>(which, nb, s, tb, w, b, rk, ctl, mode, cond, out); break;
+    default: launch_brk_row<1024>(which, nb, s, tb, w, b, rk, ctl, mode, cond, out); break;
+  }
+}
+void brk_col(int M, int which, int nb, cudaStream_t s, const Tab2& tb, const Work2& w, const hw2d::Brk2& b,
+             const Ctl2* ctl, int mode, int cond) {
+  switch (M) {
+    case 64: launch_brk_col<64>(which, nb, s, tb, w, b, ctl, mode, cond); break;
+    case 128: launch_brk_col<128>(which, nb, s, tb, w, b, ctl, mode, cond); break;
+    case 256: launch_brk_col<256>(which, nb, s, tb, w, b, ctl, mode, cond); break;
+    case 512: launch_brk_col<512>(which, nb, s, tb, w, b, ctl, mode, cond); break;
+    default: launch_brk_col<1024>(which, nb, s, tb, w, b, ctl, mode, cond); break;
+  }
 }
 
 // the five kernels of one RHS for a row length Mx and a column length My
@@ -126,6 +167,7 @@ struct hw2d_ctx {
   RK2 rk{};
   Ctl2* ctl = nullptr;     // device
   Ctl2* hctl = nullptr;    // pinned host copy
+  hw2d::Brk2 brk{};        // kinematic breaking (brk.on = 0: off)
   double* dref = nullptr;  // 6n staging for reference-layout transfers
   double2* dout = nullptr; // 3n direct RHS output
   std::vector<void*> allocs;
@@ -171,6 +213,18 @@ struct hw2d_ctx {
       if (!tb.chi_one || tb.has_src) col_dispatch(ny, 3, cols, s, tb, w, ctl, cond);
       row_dispatch(nx, 4, rows, s, tb, w, rk, ctl, ctl, mode, cond, out);
       per_rhs = ((!tb.chi_one || tb.has_src) ? 9 : 8) + 1;
+      if (brk.on) {
+        const int gb = (int)std::min<size_t>((n + 255) / 256, 4 * 148);
+        brk_row(nx, 0, rows, s, tb, w, brk, rk, ctl, mode, cond, out);
+        brk_col(ny, 0, cols, s, tb, w, brk, ctl, mode, cond);
+        hw2d::k2b_peaks<<<gb, 256, 0, s>>>(tb, w, brk, ctl, mode, cond);
+        hw2d::k2b_sort<<<1, hw2d::kBrkSortThreads, 0, s>>>(brk, ctl, mode, cond);
+        hw2d::k2b_machine<<<1, 32, 0, s>>>(tb, w, brk, ctl, mode, cond);
+        hw2d::k2b_flux<<<gb, 256, 0, s>>>(tb, w, brk, ctl, mode, cond);
+        brk_col(ny, 1, cols, s, tb, w, brk, ctl, mode, cond);
+        brk_row(nx, 1, rows, s, tb, w, brk, rk, ctl, mode, cond, out);
+        per_rhs += 8;
+      }
       return;
     }
     row_dispatch(nx, 0, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
@@ -184,6 +238,14 @@ struct hw2d_ctx {
   void attempt_launch(cudaStream_t s) {
     rhs_launch(1, hw2d::kIfK1, s, nullptr);
     for (int st = 2; st <= 6; ++st) rhs_launch(st, hw2d::kIfStage, s, nullptr);
+    if (brk.on) {
+      // gsl_odeiv2's order: dydt_out of the candidate state before the step control
+      hw2d::k2_combine<<<hw2d::kCombBlocks, hw2d::kCombThreads, 0, s>>>(rk, w, ctl, 3 * n);
+      rhs_launch(8, hw2d::kIfStage, s, nullptr);
+      hw2d::k2_control<<<1, 256, 0, s>>>(ctl, w, hw2d::kCombBlocks);
+      hw2d::k2_finalize<<<1, 1, 0, s>>>(ctl);
+      return;
+    }
     hw2d::k2_combine<<<hw2d::kCombBlocks, hw2d::kCombThreads, 0, s>>>(rk, w, ctl, 3 * n);
     hw2d::k2_control<<<1, 256, 0, s>>>(ctl, w, hw2d::kCombBlocks);
     rhs_launch(7, hw2d::kIfKout, s, nullptr);
@@ -250,6 +312,7 @@ struct hw2d_ctx {
     }
     if (hctl->status == hw2d::kNonFinite) { err = "non-finite state (the step size collapsed)"; return 1; }
     if (hctl->status == hw2d::kStepFailed) { err = "time integration failed (too many rejected steps)"; return 1; }
+    if (hctl->status == hw2d::kBreakCapacity) { err = "breaking: a capacity (peaks, crests or nodes) was exceeded"; return 1; }
     return 0;
   }
   ~hw2d_ctx() {
@@ -378,7 +441,62 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
     tb.wallchar = c->upload(std::vector<double>(t->wallchar, t->wallchar + n));
   }
 
+  hw2d::Brk2& bk = c->brk;
+  if (t->breaking) {
+    if (!var) {
+      g_err2d = "hw2d_create: breaking is built for the two-depth (varying-bottom) RHS only";
+      delete c;
+      return nullptr;
+    }
+    if (!t->bathy || !t->brchar || !t->x || !t->y || !(t->dx > 0) || !(t->dy > 0) || !(t->dt_out > 0) ||
+        !(t->rsearch > 0)) {
+      g_err2d = "hw2d_create: breaking tables missing or invalid";
+      delete c;
+      return nullptr;
+    }
+    bk.on = 1;
+    bk.bathy = c->upload(std::vector<double>(t->bathy, t->bathy + n));
+    bk.pbchar = c->upload(std::vector<double>(t->brchar, t->brchar + n));
+    bk.x = c->upload(std::vector<double>(t->x, t->x + nx));
+    bk.y = c->upload(std::vector<double>(t->y, t->y + ny));
+    bk.dx = t->dx; bk.dy = t->dy; bk.thr = t->max_eta_init; bk.tstar = t->tstar; bk.rsearch = t->rsearch;
+    bk.kbc = t->kbc; bk.tc = t->tc; bk.delb = t->delb; bk.cur_u = t->cur_u; bk.t0 = t->t0; bk.dt_out = t->dt_out;
+    bk.B = c->dalloc<double>(n);
+    bk.flux = c->dalloc<double>(n);
+    bk.P = c->dalloc<double2>(n);
+    bk.dh = c->dalloc<double2>(n);
+    bk.sb = c->dalloc<double2>(2 * n);
+    bk.peaks = c->dalloc<int>(hw2d::kBrkPeakCap);
+    bk.CB = c->dalloc<hw2d::Crest2>(hw2d::kBrkCrestCap);
+    bk.CBNew = c->dalloc<hw2d::Crest2>(hw2d::kBrkCrestCap);
+    bk.CBPrev = c->dalloc<hw2d::Crest2>(hw2d::kBrkCrestCap);
+    bk.cap_nodes = (int)std::max<size_t>(4096, n / 4);
+    bk.bn[0] = c->dalloc<int2>(bk.cap_nodes);
+    bk.bn[1] = c->dalloc<int2>(bk.cap_nodes);
+    bk.bnp = c->dalloc<int2>(bk.cap_nodes);
+    bk.cap_rec = 1 << 18;
+    bk.cap_log = (long long)std::max<size_t>(1 << 16, 4 * n);
+    bk.log_t = c->dalloc<double>(bk.cap_rec);
+    bk.log_cnt = c->dalloc<int>(bk.cap_rec);
+    bk.log_nodes = c->dalloc<int2>((size_t)bk.cap_log);
+    bk.st = c->dalloc<hw2d::BrkSt>(1);
+    const bool bok = bk.bathy && bk.pbchar && bk.x && bk.y && bk.B && bk.flux && bk.P && bk.dh && bk.sb && bk.peaks &&
+                     bk.CB && bk.CBNew && bk.CBPrev && bk.bn[0] && bk.bn[1] && bk.bnp && bk.log_t && bk.log_cnt &&
+                     bk.log_nodes && bk.st;
+    if (!bok) {
+      g_err2d = "hw2d_create: device allocation failed (breaking)";
+      delete c;
+      return nullptr;
+    }
+    hw2d::BrkSt s0{};
+    s0.sb_zero = 1;   // Sb_xhat, Sb_yhat start at zero
+    cudaMemcpy(bk.st, &s0, sizeof s0, cudaMemcpyHostToDevice);
+    cudaMemset(bk.B, 0, n * sizeof(double));
+    cudaMemset(bk.sb, 0, 2 * n * sizeof(double2));
+  }
+
   Work2& w = c->w;
+  w.dph = bk.on ? c->dalloc<double2>(n) : nullptr;
   w.z = c->dalloc<double2>(3 * n);
   w.R = c->dalloc<double2>(4 * n);
   w.Q = c->dalloc<double2>((var ? 6 : 4) * n);
@@ -404,7 +522,7 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
   c->ctl = c->dalloc<Ctl2>(1);
   bool ok = tb.kx && tb.ky && tb.c2g && tb.l2d && tb.aal && tb.damp && tb.chi && tb.twx && tb.twy && w.z && w.R &&
             w.Q && w.D && w.V && w.insig && w.insigs && w.part && c->dref && c->dout && c->ctl &&
-            (chi_one || w.W) && (!has_src || (tb.gx && tb.sx && tb.sig && w.src)) &&
+            (chi_one || w.W) && (!has_src || (tb.gx && tb.sx && tb.sig && w.src)) && (!bk.on || w.dph) &&
             (!var || (tb.gmin && tb.gplus && tb.cmin && tb.cplus && tb.omin && tb.oplus && w.phys && w.pe && w.H1 &&
                       w.EU)) && (!t->wallchar || tb.wallchar);
   for (int i = 0; i < 2; ++i) ok = ok && rk.y[i] && rk.kk[i];
@@ -422,6 +540,7 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
   h.h = c->h_first;
   h.need_k1 = 1;
   h.done = 1;
+  h.brk = bk.on;
   cudaMemcpy(c->ctl, &h, sizeof h, cudaMemcpyHostToDevice);
   cudaMemset(rk.y[0], 0, 3 * n * sizeof(double2));
   if (!c->check("hw2d_create")) {
@@ -455,7 +574,16 @@ int hw2d_rhs(hw2d_ctx* c, double t, const double* y, double* dydt) {
   c->launches += c->per_rhs + 2;
   cudaMemcpyAsync(dydt, c->dref, 6 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) return c->check("hw2d_rhs") ? 1 : 1;
-  return c->check("hw2d_rhs") ? 0 : 1;
+  if (!c->check("hw2d_rhs")) return 1;
+  if (c->brk.on) {
+    hw2d::BrkSt st{};
+    if (cudaMemcpy(&st, c->brk.st, sizeof st, cudaMemcpyDeviceToHost) != cudaSuccess) return c->check("hw2d_rhs") ? 1 : 1;
+    if (st.err & (hw2d::kBrkErrPeaks | hw2d::kBrkErrCrests | hw2d::kBrkErrNodes)) {
+      c->err = "breaking: a capacity (peaks, crests or nodes) was exceeded";
+      return 1;
+    }
+  }
+  return 0;
 }
 
 int hw2d_gsl_rhs(double t, const double* y, double* dydt, void* params) {
@@ -527,6 +655,50 @@ int hw2d_stats(const hw2d_ctx* cc, long long* r, long long* a, long long* j) {
 }
 
 long long hw2d_launches(const hw2d_ctx* c) { return c ? c->launches : 0; }
+
+int hw2d_breaking_fields(hw2d_ctx* c, double* B, double* sbx, double* sby, int* flagbr, int* ncrest) {
+  if (!c || !c->brk.on) return -1;
+  cudaSetDevice(c->device);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return c->check("hw2d_breaking_fields") ? 1 : 1;
+  const size_t n = c->n;
+  if (B && cudaMemcpy(B, c->brk.B, n * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
+  if (sbx && cudaMemcpy(sbx, c->brk.sb, n * sizeof(double2), cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
+  if (sby && cudaMemcpy(sby, c->brk.sb + n, n * sizeof(double2), cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
+  hw2d::BrkSt st{};
+  if (cudaMemcpy(&st, c->brk.st, sizeof st, cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
+  if (flagbr) *flagbr = st.flagbr;
+  if (ncrest) *ncrest = st.flagbr == 2 ? st.ncbprev : 0;
+  return 0;
+}
+
+long long hw2d_breaking_log_nodes(hw2d_ctx* c) {
+  if (!c || !c->brk.on) return -1;
+  cudaSetDevice(c->device);
+  hw2d::BrkSt st{};
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess ||
+      cudaMemcpy(&st, c->brk.st, sizeof st, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -1;
+  return st.nlog;
+}
+
+int hw2d_breaking_log(hw2d_ctx* c, double* times, int* counts, int* nodes, int cap_rec, long long cap_nodes) {
+  if (!c || !c->brk.on) return -1;
+  cudaSetDevice(c->device);
+  hw2d::BrkSt st{};
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess ||
+      cudaMemcpy(&st, c->brk.st, sizeof st, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -1;
+  const int nr = std::min(st.nrec, std::max(cap_rec, 0));
+  const long long nn = std::min(st.nlog, std::max(cap_nodes, 0LL));
+  if (times && nr > 0 && cudaMemcpy(times, c->brk.log_t, nr * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -1;
+  if (counts && nr > 0 && cudaMemcpy(counts, c->brk.log_cnt, nr * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -1;
+  if (nodes && nn > 0 && cudaMemcpy(nodes, c->brk.log_nodes, nn * sizeof(int2), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -1;
+  if (st.err & hw2d::kBrkErrLog) return -2;
+  return st.nrec;
+}
 
 int hw2d_set_stream(hw2d_ctx* c, void* s) {
   if (!c) return 1;

@@ -331,10 +331,13 @@ def shoal_bathymetry(x, y, deep=5.0, shallow=0.5, x1=100.0, x2=285.0, seed=0):
 
 def tables(nx=1024, ny=1024, Lx=300.0, Ly=300.0, depth=3.0, Hs=0.5, Tp=6.0, gamma=3.3, s_spread=10,
            n_freq=256, n_dir=64, t_end=300.0, dt=0.1, damp=30.0, x_line=45.0, nadj=1.0, model=2,
-           propagation=0, seed=0, bathymetry="flat", shallow=0.5, walls=(), refl=0.5) -> dict:
+           propagation=0, seed=0, bathymetry="flat", shallow=0.5, walls=(), refl=0.5, breaking=False,
+           kbc=0.8, tc=0.2, tchar=0.5) -> dict:
     """All tables of a 2D deck (vertical influx line at x_line).  bathymetry "flat":
     depth everywhere (rhs_AB2_2DF_uv); "shoal": `depth` offshore sloping to
-    `shallow` with a seeded shoal, two reference depths (rhs_AB2_2DB_uv)."""
+    `shallow` with a seeded shoal, two reference depths (rhs_AB2_2DB_uv).
+    breaking=True adds the kinematic-breaking tables of parambreak
+    (2d/breaking.c:1-44) with the deck's KBC, TC, Tchar (two-depth tables only)."""
     x = np.linspace(0.0, Lx, nx)          # fun_intervaltovector (2d/functions1.c:204)
     y = np.linspace(0.0, Ly, ny)
     kx = freqspace(x[-1] - x[0], nx)
@@ -377,6 +380,19 @@ def tables(nx=1024, ny=1024, Lx=300.0, Ly=300.0, depth=3.0, Hs=0.5, Tp=6.0, gamm
     extra = {k: f64(v) for k, v in var.items()} if var else {}
     if depth_field is not None:
         extra["depth"] = f64(depth_field)
+    if breaking:
+        if depth_field is None:
+            raise ValueError("breaking needs the two-depth (varying-bottom) tables")
+        # pb.Char: cfSA (min with the wall's cfSAwall, 2d/functions.c:1960-1967), zero
+        # where cfSA < 1 or ChiAdj < 1 (2d/breaking.c:10-21)
+        cf = cfsa2d(x, y, damp, damp, damp, damp)
+        if wall is not None:
+            cf = np.minimum(cf, cfw)
+        brchar = np.where((cf < 1) | (chi < 1), 0.0, cf)
+        extra.update(breaking=1, bathy=f64(-depth_field), brchar=f64(brchar), dx=float(x[1] - x[0]),
+                     dy=float(y[1] - y[0]), max_eta_init=Hs / 2.0 * 0.9, tstar=tchar * Tp,
+                     rsearch=2 * math.pi / kp / 4.0, kbc=float(kbc), tc=float(tc), delb=1.5, cur_u=0.0,
+                     t0=0.0)
     if wall is not None:
         extra["wallchar"] = f64(wall)
     return dict(**extra, nx=nx, ny=ny, model=model, propagation=propagation, cpeak=float(cpeak), kx=f64(kx), ky=f64(ky),

@@ -24,7 +24,14 @@ class Hw2dTables(ctypes.Structure):
         ("nt", ctypes.c_int), ("tsig", _dp), ("sig", _dp), ("sigskew", _dp),
         ("gam_min", _dp), ("gam_plus", _dp), ("csq_min", _dp), ("csq_plus", _dp), ("om2_min", _dp),
         ("om2_plus", _dp), ("wallchar", _dp),
+        ("breaking", ctypes.c_int), ("bathy", _dp), ("brchar", _dp), ("x", _dp), ("y", _dp),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("max_eta_init", ctypes.c_double),
+        ("tstar", ctypes.c_double), ("rsearch", ctypes.c_double), ("kbc", ctypes.c_double), ("tc", ctypes.c_double),
+        ("delb", ctypes.c_double), ("cur_u", ctypes.c_double), ("t0", ctypes.c_double), ("dt_out", ctypes.c_double),
     ]
+
+# parambreak's scalars (2d/breaking.c:1-8) as the tables dict carries them
+BREAKING_SCALARS = ("dx", "dy", "max_eta_init", "tstar", "rsearch", "kbc", "tc", "delb", "cur_u", "t0", "dt_out")
 
 
 _bound = False
@@ -54,6 +61,11 @@ def _lib():
         L.hw2d_synchronize.argtypes = [vp]
         L.hw2d_launches.restype = ctypes.c_longlong
         L.hw2d_launches.argtypes = [vp]
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.hw2d_breaking_fields.argtypes = [vp, dp, dp, dp, ip, ip]
+        L.hw2d_breaking_log.argtypes = [vp, dp, ip, ip, ctypes.c_int, ctypes.c_longlong]
+        L.hw2d_breaking_log_nodes.restype = ctypes.c_longlong
+        L.hw2d_breaking_log_nodes.argtypes = [vp]
         _bound = True
     return L
 
@@ -70,10 +82,14 @@ class Engine2D:
                   "gam_min", "gam_plus", "csq_min", "csq_plus", "om2_min", "om2_plus", "wallchar"):
             v = tables.get(k)
             keep[k] = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
+        brk = int(tables.get("breaking", 0))
+        for k in ("bathy", "brchar", "x", "y"):
+            keep[k] = np.ascontiguousarray(tables[k], dtype=np.float64) if brk else None
         self._keep = keep
+        scal = {k: float(tables.get(k, 0.0)) for k in BREAKING_SCALARS} if brk else {}
         tb = Hw2dTables(nx=int(tables["nx"]), ny=int(tables["ny"]), model=int(tables.get("model", 2)),
                         propagation=int(tables.get("propagation", 0)), cpeak=float(tables["cpeak"]),
-                        nt=int(tables.get("nt", 0) if keep["sig"] is not None else 0),
+                        nt=int(tables.get("nt", 0) if keep["sig"] is not None else 0), breaking=brk, **scal,
                         **{k: _ptr(v) for k, v in keep.items()})
         o = HwOpts(eps_abs=eps_abs, eps_rel=eps_rel, h0=h0, device=device)
         self._h = self._L.hw2d_create(ctypes.byref(tb), ctypes.byref(o))
@@ -150,3 +166,35 @@ class Engine2D:
     def synchronize(self):
         if self._L.hw2d_synchronize(self._h):
             raise self._err()
+
+    def breaking_fields(self):
+        """B, Sb_xhat, Sb_yhat (complex [ny, nx]), flagbr and the tracked crests after
+        the last RHS (the globals of 2d/breaking.c)."""
+        n = self.nx * self.ny
+        B = np.zeros(n)
+        sx, sy = np.zeros(2 * n), np.zeros(2 * n)
+        fl, nc = ctypes.c_int(), ctypes.c_int()
+        if self._L.hw2d_breaking_fields(self._h, _ptr(B), _ptr(sx), _ptr(sy), ctypes.byref(fl), ctypes.byref(nc)):
+            raise self._err()
+        shp = (self.ny, self.nx)
+        return (B.reshape(shp), (sx[0::2] + 1j * sx[1::2]).reshape(shp), (sy[0::2] + 1j * sy[1::2]).reshape(shp),
+                fl.value, nc.value)
+
+    def breaking_log(self):
+        """breaking.dat records as a list of (t, [(x index, y index), ...])."""
+        L = self._L
+        nn = int(L.hw2d_breaking_log_nodes(self._h))
+        nr = L.hw2d_breaking_log(self._h, None, None, None, 0, 0)
+        if nr < 0:
+            raise EngineError("hw2d_breaking_log: " + ("log overflow" if nr == -2 else "no breaking"))
+        t = np.zeros(max(nr, 1))
+        cnt = np.zeros(max(nr, 1), dtype=np.int32)
+        nodes = np.zeros(2 * max(nn, 1), dtype=np.int32)
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.hw2d_breaking_log(self._h, _ptr(t), cnt.ctypes.data_as(ip), nodes.ctypes.data_as(ip), nr, nn)
+        out, off = [], 0
+        for r in range(nr):
+            c = int(cnt[r])
+            out.append((float(t[r]), [tuple(v) for v in nodes[2 * off:2 * (off + c)].reshape(-1, 2).tolist()]))
+            off += c
+        return out

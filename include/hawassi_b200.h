@@ -175,7 +175,8 @@ int hw_set_stream(hw_ctx* ctx, void* cuda_stream);
 int hw_synchronize(hw_ctx* ctx);
 
 /* ------------------------------------------------------------------------ */
-/* 2D twin (HS2, no wall, no breaking): rhs_AB2_2DF_uv / rhs_AB2_2DB_uv and the*/
+/* 2D twin (HS2): rhs_AB2_2DF_uv / rhs_AB2_2DB_uv (walls, kinematic breaking  */
+/* on the two-depth tables) and the                                           */
 /* gsl_odeiv2 rkf45 loop of ode_solver_uv (2d/fun_odesolver.c:2565-2647,     */
 /* 4458-4540).  State: 6*nx*ny doubles [Re eta^|Im eta^|Re u^|Im u^|Re v^|    */
 /* Im v^], row-major i*nx + j (2d/main.c:198-201).  The operator tables are   */
@@ -214,6 +215,21 @@ typedef struct hw2d_tables {
      * 2d/functions.c:260-390); NULL for no wall.  Only with the two-depth tables
      * (the flat RHS's wall branch of fun_delphiH1hat is not built). */
     const double* wallchar;     /* [ny*nx]                                      */
+    /* kinematic breaking (2d/breaking.c: parambreak, breaking_process; fun_sbreaking
+     * 2d/fun_odesolver.c:985-1019), two-depth tables only; breaking = 0 leaves the
+     * fields below unread.  The scalars are parambreak's pb.* values. */
+    int breaking;
+    const double* bathy;        /* [ny*nx] dominfo.bathy.data (= -depth)        */
+    const double* brchar;       /* [ny*nx] pb.Char (cfSA, 0 where cfSA or ChiAdj < 1) */
+    const double* x;            /* [nx] dominfo.x                               */
+    const double* y;            /* [ny] dominfo.y                               */
+    double dx, dy;              /* dominfo.dx, dominfo.dy                       */
+    double max_eta_init;        /* pb.MaxEtaInit = 0.9 Hs / 2                   */
+    double tstar;               /* pb.Tstar = Tchar Tp                          */
+    double rsearch;             /* pb.Rsearch = 2 pi / kp / 4                   */
+    double kbc, tc, delb;       /* pb.KBC, pb.TC, pb.delb (1.5)                 */
+    double cur_u;               /* dominfo.U                                    */
+    double t0, dt_out;          /* dominfo.t[0], dominfo.dt (breaking.dat cadence) */
 } hw2d_tables;
 
 /* opts: eps_abs/eps_rel (<= 0: the 2D reference's 1e-3 / 1e-2, 2d/main.c:196-197),
@@ -240,6 +256,16 @@ int hw2d_run_to_time(hw2d_ctx* ctx, double t1);
 int hw2d_stats(const hw2d_ctx* ctx, long long* rhs_calls, long long* accepted, long long* rejected);
 /* kernels this context has launched so far (each node of a replayed graph counted) */
 long long hw2d_launches(const hw2d_ctx* ctx);
+/* Breaking state after the last RHS (the globals B, Sb_xhat, Sb_yhat, flagbr and
+ * CBPrev[0].NB of 2d/breaking.c): B [ny*nx], Sb as interleaved complex [2*ny*nx];
+ * any pointer may be NULL.  Returns -1 when the context has no breaking. */
+int hw2d_breaking_fields(hw2d_ctx* ctx, double* B, double* sbx, double* sby, int* flagbr, int* ncrest);
+/* breaking.dat (2d/breaking.c:707-718): record r is times[r] and counts[r] node
+ * pairs (x index, y index), all records' pairs concatenated in nodes.  Copies at
+ * most cap_rec records and cap_nodes pairs; returns the number of records (-1:
+ * no breaking, -2: the device log overflowed and stopped). */
+int hw2d_breaking_log(hw2d_ctx* ctx, double* times, int* counts, int* nodes, int cap_rec, long long cap_nodes);
+long long hw2d_breaking_log_nodes(hw2d_ctx* ctx);
 int hw2d_set_stream(hw2d_ctx* ctx, void* cuda_stream);
 int hw2d_synchronize(hw2d_ctx* ctx);
 

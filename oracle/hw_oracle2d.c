@@ -17,6 +17,9 @@
 #include <string.h>
 
 static const double GRAV = 9.80665;   /* 2d/var_initialization.h:246 */
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
 
 void or_fft(int n, const double* re_in, const double* im_in, double* re_out, double* im_out, int sign);
 void or_cspline_coeffs(int n, const double* x, const double* y, double* c_out);
@@ -38,10 +41,15 @@ struct or2d_ctx {
     int var;                                           /* varying bottom (two reference depths) */
     double *gmin, *gplus, *cmin, *cplus, *omin, *oplus;
     double* wallchar;                                  /* NULL: no wall */
+    struct brk2* brk;                                  /* kinematic breaking, NULL: off */
     long long rhs_calls, acc, rej;
     /* rkf45 work vectors */
     double *k1, *k2, *k3, *k4, *k5, *k6, *ytmp, *y0, *yerr, *dydt_in, *dydt_out;
 };
+
+struct brk2;
+static struct brk2* brk_create(const or2d_tables* tb);
+static void brk_destroy(struct brk2* b);
 
 static double* dup(const double* a, size_t n) {
     double* p = (double*)malloc(sizeof(double) * n);
@@ -160,6 +168,11 @@ or2d_ctx* or2d_create(const or2d_tables* tb, double eps_abs, double eps_rel) {
         if (!c->var) { set_err2("or2d_create: walls are restated for the varying-bottom RHS only"); free(c); return NULL; }
         c->wallchar = dup(tb->wallchar, n);
     }
+    if (tb->breaking) {
+        if (!c->var) { set_err2("or2d_create: breaking is restated for the varying-bottom RHS only"); free(c); return NULL; }
+        if (!tb->bathy || !tb->brchar || !tb->x || !tb->y) { set_err2("or2d_create: breaking tables missing"); free(c); return NULL; }
+        c->brk = brk_create(tb);
+    }
     size_t d = 6 * n;
     double** w[] = {&c->k1, &c->k2, &c->k3, &c->k4, &c->k5, &c->k6, &c->ytmp, &c->y0, &c->yerr, &c->dydt_in, &c->dydt_out};
     for (size_t q = 0; q < sizeof w / sizeof w[0]; q++) *w[q] = calloc(d, sizeof(double));
@@ -173,6 +186,7 @@ void or2d_destroy(or2d_ctx* c) {
                    c->y0, c->yerr, c->dydt_in, c->dydt_out, c->gmin, c->gplus, c->cmin, c->cplus, c->omin,
                    c->oplus, c->wallchar};
     for (size_t q = 0; q < sizeof f / sizeof f[0]; q++) free(f[q]);
+    brk_destroy(c->brk);
     free(c);
 }
 
@@ -265,10 +279,472 @@ static void hssgen_2depth(const or2d_ctx* c, const cx* phi, const cx* phihat, co
     free(L0m); free(L0p); free(gm); free(gp); free(gmL); free(gpL);
 }
 
+/* ------------------------------------------------------------------------ */
+/* Kinematic breaking of the 2D model: parambreak, breaking_process and its   */
+/* helpers (2d/breaking.c:1-733) and fun_sbreaking (2d/fun_odesolver.c:      */
+/* 985-1019).  The crest records keep the reference's fields and its use of  */
+/* slots (CB, CBNew, CBPrev with NB in slot 0; the continuing crests' break  */
+/* nodes and every crest's nodes written to CBPrev slots counted separately);*/
+/* node lists grow as needed where the reference's are 100 entries long.     */
+/* ------------------------------------------------------------------------ */
+typedef struct { int x, y; } v2i;
+typedef struct {
+    int xindex, yindex, xNow, yNow, kwadran, NB;
+    double Ucrest, time, theta;
+    v2i* nodes; int nnode, cap;          /* break nodes (B > 0) of a continuing crest */
+    v2i* nodes_prev; int nnode_prev, cap_prev;   /* every node inside the crest's sector */
+} crest2;
+
+struct brk2 {
+    int nx, ny, n;
+    double *bathy, *pbchar, *x, *y;
+    double dx, dy, max_eta_init, tstar, rsearch, kbc, tc, delb, cur_u, t0, dt_out;
+    double tprev;
+    int flagbr, iterbdt;
+    double *B, *U, *etah, *work;         /* B and the per-call physical fields */
+    cx *sbx, *sby;                        /* Sb_xhat, Sb_yhat (persist between calls) */
+    crest2 *CB, *CBNew, *CBPrev;
+    int capCB, capNew, capPrev;
+    v2i *bn, *bnp;                        /* Break_nodes, Break_nodes_prev */
+    int nbreak_nodes, nbreak_prev;
+    /* breaking.dat records */
+    double* log_t; int* log_cnt; int nrec, caprec;
+    v2i* log_nodes; long long nlog, caplog;
+};
+
+static struct brk2* brk_create(const or2d_tables* tb) {
+    struct brk2* b = calloc(1, sizeof(struct brk2));
+    b->nx = tb->nx; b->ny = tb->ny; b->n = tb->nx * tb->ny;
+    size_t n = (size_t)b->n;
+    b->bathy = dup(tb->bathy, n); b->pbchar = dup(tb->brchar, n);
+    b->x = dup(tb->x, b->nx); b->y = dup(tb->y, b->ny);
+    b->dx = tb->dx; b->dy = tb->dy;
+    b->max_eta_init = tb->max_eta_init; b->tstar = tb->tstar; b->rsearch = tb->rsearch;
+    b->kbc = tb->kbc; b->tc = tb->tc; b->delb = tb->delb; b->cur_u = tb->cur_u;
+    b->t0 = tb->t0; b->dt_out = tb->dt_out;
+    b->tprev = tb->t0;                    /* tprev = dominfo.t[0] (2d/main.c:120) */
+    b->B = calloc(n, sizeof(double)); b->U = calloc(n, sizeof(double));
+    b->etah = calloc(n, sizeof(double)); b->work = calloc(4 * n, sizeof(double));
+    b->sbx = calloc(n, sizeof(cx)); b->sby = calloc(n, sizeof(cx));
+    b->bn = malloc(sizeof(v2i) * n); b->bnp = malloc(sizeof(v2i) * n);
+    return b;
+}
+
+static void crest_free(crest2* a, int cap) {
+    for (int i = 0; i < cap; i++) { free(a[i].nodes); free(a[i].nodes_prev); }
+    free(a);
+}
+
+static void brk_destroy(struct brk2* b) {
+    if (!b) return;
+    free(b->bathy); free(b->pbchar); free(b->x); free(b->y);
+    free(b->B); free(b->U); free(b->etah); free(b->work); free(b->sbx); free(b->sby);
+    crest_free(b->CB, b->capCB); crest_free(b->CBNew, b->capNew); crest_free(b->CBPrev, b->capPrev);
+    free(b->bn); free(b->bnp); free(b->log_t); free(b->log_cnt); free(b->log_nodes);
+    free(b);
+}
+
+static crest2* crest_reserve(crest2* a, int* cap, int need) {
+    if (need <= *cap) return a;
+    int nc = *cap ? *cap : 16;
+    while (nc < need) nc *= 2;
+    a = realloc(a, sizeof(crest2) * nc);
+    memset(a + *cap, 0, sizeof(crest2) * (nc - *cap));
+    *cap = nc;
+    return a;
+}
+
+/* copy of the scalar fields (the reference's field-by-field copies) */
+static void crest_copy(crest2* d, const crest2* s) {
+    d->xindex = s->xindex; d->yindex = s->yindex; d->xNow = s->xNow; d->yNow = s->yNow;
+    d->Ucrest = s->Ucrest; d->theta = s->theta; d->time = s->time; d->NB = s->NB; d->kwadran = s->kwadran;
+}
+
+static int fun_sign2(double v) { return v < 0 ? -1 : 1; }   /* 2d/functions1.c:170 */
+
+/* fun_kwadran (2d/breaking.c:199-213) */
+static int fun_kwadran(double ux, double uy) {
+    if ((ux >= 0) && (uy >= 0)) return 1;
+    else if ((ux < 0) && (uy >= 0)) return 2;
+    else if ((ux < 0) && (uy < 0)) return 3;
+    return 4;
+}
+
+/* fun_exact_Cp1d_val (2d/functions.c:70-80) */
+static double exact_cp(double k, double D, double U) {
+    if (k == 0) return sqrt(GRAV * D) + U;
+    return (fun_sign2(k) * sqrt(GRAV * k * tanh(k * D)) + k * U) / k;
+}
+
+/* gradient2D (2d/functions1.c:868-885) at one point: one-sided at the edges */
+static double grad_x_at(const double* a, int nx, int i, int j, double dx) {
+    if (j == 0) return (a[i * nx + 1] - a[i * nx]) / dx;
+    if (j == nx - 1) return (a[i * nx + nx - 1] - a[i * nx + nx - 2]) / dx;
+    return (a[i * nx + j + 1] - a[i * nx + j - 1]) / (2 * dx);
+}
+static double grad_y_at(const double* a, int nx, int ny, int i, int j, double dy) {
+    if (i == 0) return (a[nx + j] - a[j]) / dy;
+    if (i == ny - 1) return (a[(ny - 1) * nx + j] - a[(ny - 2) * nx + j]) / dy;
+    return (a[(i + 1) * nx + j] - a[(i - 1) * nx + j]) / (2 * dy);
+}
+
+/* fun_peaks (2d/breaking.c:56-136), called with (ROWS, COLS) = (Nx, Ny): "row"
+ * is the x index, "col" the y index; interior points first (x outer), then the
+ * x = 0 edge, the x = Nx-1 edge, the y = 0 edge and the y = Ny-1 edge. */
+static int fun_peaks(const struct brk2* b, const double* A, int* pk) {
+    const int Nx = b->nx, Ny = b->ny;
+    const double thr = b->max_eta_init;
+    int np = 0;
+#define AT(yy, xx) A[(yy) * Nx + (xx)]
+    for (int row = 1; row < Nx - 1; row++)
+        for (int col = 1; col < Ny - 1; col++) {
+            int cnt = 0;
+            for (int i = -1; i < 2; i++)
+                for (int j = -1; j < 2; j++) cnt += (AT(col + i, row + j) - AT(col, row) <= 0.001) ? 1 : 0;
+            if (cnt == 9 && AT(col, row) > thr) { pk[2 * np] = row; pk[2 * np + 1] = col; np++; }
+        }
+    for (int e = 0; e < 4; e++) {
+        const int along_x = e >= 2;                 /* y edges run along x */
+        const int len = along_x ? Nx : Ny;
+        for (int m = 1; m < len - 1; m++) {
+            int row, col, i0, i1, j0, j1;
+            if (e == 0) { row = 0; col = m; i0 = -1; i1 = 2; j0 = 0; j1 = 2; }
+            else if (e == 1) { row = Nx - 1; col = m; i0 = -1; i1 = 2; j0 = -1; j1 = 1; }
+            else if (e == 2) { col = 0; row = m; i0 = 0; i1 = 2; j0 = -1; j1 = 2; }
+            else { col = Ny - 1; row = m; i0 = -1; i1 = 1; j0 = -1; j1 = 2; }
+            int cnt = 0;
+            for (int i = i0; i < i1; i++)
+                for (int j = j0; j < j1; j++) cnt += (AT(col + i, row + j) - AT(col, row) <= 0.001) ? 1 : 0;
+            if (cnt == 6 && AT(col, row) > thr) { pk[2 * np] = row; pk[2 * np + 1] = col; np++; }
+        }
+    }
+#undef AT
+    return np;
+}
+
+/* breaking_criterion (2d/breaking.c:215-326): candidates into CB, NB in CB[0] */
+static void brk_criterion(struct brk2* b, double t, const double* Zhat, const double* kx, const double* ky,
+                          const cx* gpx, const cx* gpy) {
+    const int Nx = b->nx, Ny = b->ny, n = b->n;
+    double* chk = b->work;
+    for (int q = 0; q < n; q++) chk[q] = b->etah[q] * b->pbchar[q];
+    double mx = chk[0];
+    for (int q = 0; q < n; q++) mx = (mx > chk[q] ? mx : chk[q]);
+    if (!(mx > b->max_eta_init)) return;
+    int* pk = malloc(sizeof(int) * 2 * (size_t)n);
+    const int npk = fun_peaks(b, chk, pk);
+    if (npk == 0) { free(pk); return; }
+    /* HilbEta: Re = Im(eta^) sign(kx + ky), Im = -Re(eta^) sign, symmetrised, inverse */
+    cx* H = malloc(sizeof(cx) * n);
+    for (int i = 0; i < Ny; i++)
+        for (int j = 0; j < Nx; j++) {
+            const int q = i * Nx + j;
+            const int s = fun_sign2(kx[j] + ky[i]);
+            H[q].re = Zhat[n + q] * s;
+            H[q].im = -Zhat[q] * s;
+        }
+    sym2(H, Nx, Ny);
+    fft2(Nx, Ny, H, +1);
+    double* Hr = b->work + n;
+    for (int q = 0; q < n; q++) Hr[q] = H[q].re / (Nx * Ny);
+    free(H);
+    int it = 0;
+    for (int p = 0; p < npk; p++) {
+        const int ix = pk[2 * p], iy = pk[2 * p + 1], q = iy * Nx + ix;
+        const double e = b->etah[q], h = Hr[q];
+        const double gxH = grad_x_at(Hr, Nx, iy, ix, b->dx), gyH = grad_y_at(Hr, Nx, Ny, iy, ix, b->dy);
+        const double gxE = grad_x_at(b->etah, Nx, iy, ix, b->dx), gyE = grad_y_at(b->etah, Nx, Ny, iy, ix, b->dy);
+        const double Kx = (e * gxH - h * gxE) / (pow(e, 2) + pow(h, 2));
+        const double Ky = (e * gyH - h * gyE) / (pow(e, 2) + pow(h, 2));
+        const double Kk = sqrt(pow(Kx, 2) + pow(Ky, 2));
+        const double Cc = exact_cp(Kk, -b->bathy[q] + e, b->cur_u);
+        if (fabs(b->U[q]) >= (b->kbc * fabs(Cc))) {
+            b->CB = crest_reserve(b->CB, &b->capCB, it + 1);
+            crest2* r = &b->CB[it];
+            r->xindex = ix; r->yindex = iy; r->xNow = ix; r->yNow = iy;
+            r->Ucrest = fabs(b->U[q]); r->time = t;
+            r->theta = fabs(atan(gpy[q].re / gpx[q].re));
+            r->kwadran = fun_kwadran(gpx[q].re, gpy[q].re);
+            it++;
+        }
+    }
+    free(pk);
+    if (b->capCB > 0) b->CB[0].NB = it;
+}
+
+/* fun_check_crest (2d/breaking.c:328-349) */
+static int check_crest(const struct brk2* b, int k, int ncbprev) {
+    const int idx = b->CB[k].xindex, idy = b->CB[k].yindex;
+    for (int l = 0; l < ncbprev; l++)
+        if (b->CBPrev[l].xindex == idx && b->CBPrev[l].yindex == idy) return 0;
+    for (int l = 0; l < ncbprev; l++)
+        for (int m = 0; m < b->CBPrev[l].nnode; m++)
+            if (b->CBPrev[l].nodes[m].x == idx && b->CBPrev[l].nodes[m].y == idy) return 0;
+    return 1;
+}
+
+/* funBr_Char (2d/breaking.c:351-441) at one point: inside the search disc and the
+ * 160-degree sector of the crest's quadrant */
+static int crest_char(const struct brk2* b, const crest2* r, int i, int j) {
+    const double xp = b->x[r->xNow], yp = b->y[r->yNow];
+    const double xc = b->x[j] - xp, yc = b->y[i] - yp;
+    if (!((pow(xc, 2) + pow(yc, 2)) <= pow(b->rsearch, 2))) return 0;
+    const double spread = 80.0, theta = r->theta;
+    double alpha, beta;
+    if (r->kwadran == 1 || r->kwadran == 3) {
+        alpha = theta - spread * M_PI / 180.0;
+        beta = (spread * M_PI / 180.0 + theta) - M_PI / 2.0;
+    } else {
+        alpha = spread * M_PI / 180.0 - theta;
+        beta = (M_PI / 2.0 - theta) - (spread * M_PI / 180.0);
+    }
+    const double XXr = (b->x[j] - xp) * cos(alpha) + (b->y[i] - yp) * sin(alpha);
+    const double YYr = (b->y[i] - yp) * cos(beta) - (b->x[j] - xp) * sin(beta);
+    switch (r->kwadran) {
+        case 1: if ((XXr < 0) || (YYr < 0)) return 0; break;
+        case 2: if ((XXr > 0) || (YYr < 0)) return 0; break;
+        case 3: if ((XXr > 0) || (YYr > 0)) return 0; break;
+        default: if ((XXr < 0) || (YYr > 0)) return 0; break;
+    }
+    return 1;
+}
+
+/* funBr_find_peak_loc + idx_max_matrix (2d/breaking.c:443-454, 2d/functions1.c:248-262) */
+static void find_peak_loc(const struct brk2* b, const crest2* r, int* ix, int* iy) {
+    const int Nx = b->nx, Ny = b->ny;
+    double temp = b->etah[0] * crest_char(b, r, 0, 0) * b->pbchar[0];
+    *ix = -1; *iy = -1;
+    for (int i = 0; i < Ny; i++)
+        for (int j = 0; j < Nx; j++) {
+            const double v = b->etah[i * Nx + j] * crest_char(b, r, i, j) * b->pbchar[i * Nx + j];
+            if (v > temp) { temp = v; *ix = j; *iy = i; }
+        }
+}
+
+/* funBr_BreakNodes_char (2d/breaking.c:456-503) */
+static void break_nodes(struct brk2* b, const crest2* r, double Ustar, double UF) {
+    const int Nx = b->nx, Ny = b->ny;
+    int id = 0, idp = 0;
+    for (int i = 0; i < Ny; i++)
+        for (int j = 0; j < Nx; j++) {
+            const int q = i * Nx + j;
+            double ch = crest_char(b, r, i, j);
+            if ((b->U[q] < UF) || (b->etah[q] < 0)) ch = 0;
+            ch = ch * b->pbchar[q];
+            if (ch == 1) {
+                b->bnp[idp].x = j; b->bnp[idp].y = i; idp++;
+                if (b->B[q] == 0) {
+                    if (b->U[q] >= (2 * Ustar)) b->B[q] = 1;
+                    else if (b->U[q] <= Ustar) b->B[q] = 0;
+                    else b->B[q] = ((b->U[q] / Ustar) - 1);
+                    if (b->B[q] > 0) { b->bn[id].x = j; b->bn[id].y = i; id++; }
+                }
+            }
+        }
+    b->nbreak_nodes = id;
+    b->nbreak_prev = idp;
+}
+
+static void set_nodes(v2i** dst, int* cnt, int* cap, const v2i* src, int m) {
+    if (m > *cap) { *dst = realloc(*dst, sizeof(v2i) * m); *cap = m; }
+    memcpy(*dst, src, sizeof(v2i) * m);
+    *cnt = m;
+}
+
+/* breaking_process (2d/breaking.c:505-733) */
+static void brk_process(or2d_ctx* c, double t, const double* Zhat, const cx* eta, const cx* u, const cx* v) {
+    struct brk2* b = c->brk;
+    const int n = c->n;
+    const double fact = (double)c->nx * c->ny;
+    for (int q = 0; q < n; q++) {
+        b->etah[q] = eta[q].re / fact;
+        b->U[q] = sqrt(pow(u[q].re / fact, 2) + pow(v[q].re / fact, 2));
+    }
+    b->CB = crest_reserve(b->CB, &b->capCB, 1);
+    b->CB[0].NB = 0;
+    memset(b->B, 0, sizeof(double) * n);
+    brk_criterion(b, t, Zhat, c->kx, c->ky, u, v);
+    const int NCB = b->CB[0].NB;
+    if ((NCB > 0) && (b->flagbr == 0)) {
+        b->flagbr = 1;
+        b->CBNew = crest_reserve(b->CBNew, &b->capNew, NCB);
+        for (int j = 0; j < NCB; j++) crest_copy(&b->CBNew[j], &b->CB[j]);
+    } else if ((NCB == 0) && (b->flagbr == 2)) {
+        const int ncp = b->CBPrev[0].NB;
+        b->CBNew = crest_reserve(b->CBNew, &b->capNew, ncp > 0 ? ncp : 1);
+        for (int j = 0; j < ncp; j++) crest_copy(&b->CBNew[j], &b->CBPrev[j]);
+        b->CBNew[0].NB = ncp;
+    } else if ((NCB > 0) && (b->flagbr == 2)) {
+        const int ncp = b->CBPrev[0].NB;
+        b->CBNew = crest_reserve(b->CBNew, &b->capNew, ncp + NCB);
+        for (int j = 0; j < ncp; j++) crest_copy(&b->CBNew[j], &b->CBPrev[j]);
+        int add = 0;
+        for (int k = 0; k < NCB; k++)
+            if (check_crest(b, k, ncp) == 1) {
+                crest2* d = &b->CBNew[ncp + add];
+                const crest2* s = &b->CB[k];
+                d->xindex = s->xindex; d->yindex = s->yindex; d->xNow = s->xNow; d->yNow = s->yNow;
+                d->Ucrest = s->Ucrest; d->time = s->time; d->theta = s->theta; d->kwadran = s->kwadran;
+                add++;
+            }
+        b->CBNew[0].NB = ncp + add;
+    }
+    if ((b->flagbr == 1) || (b->flagbr == 2)) {
+        const int ncnow = b->CBNew[0].NB;
+        b->CBPrev = crest_reserve(b->CBPrev, &b->capPrev, ncnow > 0 ? ncnow : 1);
+        b->CBPrev[0].NB = 0;
+        int* term = calloc(ncnow > 0 ? ncnow : 1, sizeof(int));
+        int itpp = 0, itp = 0;
+        for (int lx = 0; lx < ncnow; lx++) {
+            crest2* r = &b->CBNew[lx];
+            term[lx] = 0;
+            if (b->flagbr == 1) {
+                r->xNow = r->xindex;
+                r->yNow = r->yindex;
+            } else {
+                int mx, my;
+                find_peak_loc(b, r, &mx, &my);
+                if (mx < 0) { term[lx] = 1; continue; }
+                r->xNow = mx;
+                r->yNow = my;
+                const int q = my * c->nx + mx;
+                r->theta = fabs(atan(v[q].re / u[q].re));
+                r->kwadran = fun_kwadran(u[q].re, v[q].re);
+            }
+            const double tbreak = r->time, UI = r->Ucrest, UF = b->tc * UI;
+            double Ustar;
+            if ((t - tbreak) >= b->tstar) Ustar = UF;
+            else if (((t - tbreak) >= 0) && (t - tbreak) < b->tstar) Ustar = UI + ((t - tbreak) / b->tstar) * (UF - UI);
+            else Ustar = UI;
+            break_nodes(b, r, Ustar, UF);
+            if (b->nbreak_prev > 0) {
+                crest2* d = &b->CBPrev[itpp];
+                set_nodes(&d->nodes_prev, &d->nnode_prev, &d->cap_prev, b->bnp, b->nbreak_prev);
+                itpp++;
+            }
+            if (b->nbreak_nodes == 0) {
+                term[lx] = 1;
+            } else {
+                term[lx] = 0;
+                crest2* d = &b->CBPrev[itp];
+                set_nodes(&d->nodes, &d->nnode, &d->cap, b->bn, b->nbreak_nodes);
+                d->xindex = r->xindex; d->yindex = r->yindex; d->xNow = r->xNow; d->yNow = r->yNow;
+                d->Ucrest = r->Ucrest; d->time = r->time; d->theta = r->theta; d->kwadran = r->kwadran;
+                itp++;
+            }
+            b->CBPrev[0].NB = itp;
+        }
+        for (int lx = 0; lx < ncnow; lx++) {
+            if (term[lx] == 0) { b->flagbr = 2; break; }
+            else b->flagbr = 0;
+        }
+        if ((t > b->t0 + b->iterbdt * b->dt_out) && (itpp > 0)) {
+            long long m = 0;
+            for (int lx = 0; lx < itpp; lx++) m += b->CBPrev[lx].nnode_prev;
+            if (b->nrec + 1 > b->caprec) {
+                b->caprec = b->caprec ? 2 * b->caprec : 64;
+                b->log_t = realloc(b->log_t, sizeof(double) * b->caprec);
+                b->log_cnt = realloc(b->log_cnt, sizeof(int) * b->caprec);
+            }
+            if (b->nlog + m > b->caplog) {
+                while (b->nlog + m > b->caplog) b->caplog = b->caplog ? 2 * b->caplog : 4096;
+                b->log_nodes = realloc(b->log_nodes, sizeof(v2i) * b->caplog);
+            }
+            b->log_t[b->nrec] = t;
+            b->log_cnt[b->nrec] = (int)m;
+            for (int lx = 0; lx < itpp; lx++) {
+                memcpy(b->log_nodes + b->nlog, b->CBPrev[lx].nodes_prev, sizeof(v2i) * b->CBPrev[lx].nnode_prev);
+                b->nlog += b->CBPrev[lx].nnode_prev;
+            }
+            b->nrec++;
+        }
+        free(term);
+    }
+    if (t > b->t0 + b->iterbdt * b->dt_out) b->iterbdt = b->iterbdt + 1;
+}
+
+/* fun_gradient (2d/functions.c:392-460): periodic forward and backward
+ * differences, the forward ones clipped to <= 0, the backward ones to >= 0, summed */
+static void fun_gradient2(const double* f, int Nx, int Ny, double dx, double dy, double* gx, double* gy) {
+    for (int i = 0; i < Ny; i++)
+        for (int j = 0; j < Nx; j++) {
+            const int q = i * Nx + j;
+            double Fx = (j < Nx - 1) ? (f[q + 1] - f[q]) / dx : (f[i * Nx] - f[q]) / dx;
+            double Fy = (i < Ny - 1) ? (f[q + Nx] - f[q]) / dy : (f[j] - f[q]) / dy;
+            double Bx = (j > 0) ? (f[q] - f[q - 1]) / dx : (f[q] - f[i * Nx + Nx - 1]) / dx;
+            double By = (i > 0) ? (f[q] - f[q - Nx]) / dy : (f[q] - f[(Ny - 1) * Nx + j]) / dy;
+            if (Fx > 0) Fx = 0;
+            if (Fy > 0) Fy = 0;
+            if (Bx < 0) Bx = 0;
+            if (By < 0) By = 0;
+            gx[q] = Fx + Bx;
+            gy[q] = Fy + By;
+        }
+}
+
+/* fun_sbreaking (2d/fun_odesolver.c:985-1019); delphiH_hat is symmetrised in
+ * place (ifftw_2d_c2r, 2d/functions1.c:523-559), which the RHS's assembly then sees */
+static void brk_force(or2d_ctx* c, const cx* eta, cx* dphi) {
+    struct brk2* b = c->brk;
+    const int Nx = c->nx, Ny = c->ny, n = c->n;
+    const double fact = (double)Nx * Ny;
+    sym2(dphi, Nx, Ny);
+    cx* d = malloc(sizeof(cx) * n);
+    memcpy(d, dphi, sizeof(cx) * n);
+    fft2(Nx, Ny, d, +1);
+    double* flux = b->work;
+    double* gx = b->work + n;
+    double* gy = b->work + 2 * n;
+    for (int q = 0; q < n; q++) {
+        const double dp = d[q].re / (Nx * Ny);
+        flux[q] = -b->B[q] * pow(b->delb, 2) * (eta[q].re / fact - b->bathy[q]) * pow(dp, 2);
+    }
+    fun_gradient2(flux, Nx, Ny, b->dx, b->dy, gx, gy);
+    for (int q = 0; q < n; q++) {
+        const double hq = eta[q].re / fact - b->bathy[q];
+        b->sbx[q].re = gx[q] / hq; b->sbx[q].im = 0;
+        b->sby[q].re = gy[q] / hq; b->sby[q].im = 0;
+    }
+    fft2(Nx, Ny, b->sbx, -1);
+    fft2(Nx, Ny, b->sby, -1);
+    free(d);
+}
+
+void or2d_set_tprev(or2d_ctx* c, double tprev) {
+    if (c && c->brk) c->brk->tprev = tprev;
+}
+
+int or2d_brk_fields(const or2d_ctx* c, double* B, double* sbx, double* sby, int* flagbr, int* ncrest) {
+    if (!c || !c->brk) return -1;
+    const struct brk2* b = c->brk;
+    if (B) memcpy(B, b->B, sizeof(double) * b->n);
+    if (sbx) memcpy(sbx, b->sbx, sizeof(cx) * b->n);
+    if (sby) memcpy(sby, b->sby, sizeof(cx) * b->n);
+    if (flagbr) *flagbr = b->flagbr;
+    if (ncrest) *ncrest = (b->flagbr == 2 && b->capPrev > 0) ? b->CBPrev[0].NB : 0;
+    return 0;
+}
+
+int or2d_brk_log(const or2d_ctx* c, double* times, int* cnt, int* nodes, int cap_rec, int cap_nodes) {
+    if (!c || !c->brk) return -1;
+    const struct brk2* b = c->brk;
+    long long off = 0;
+    for (int r = 0; r < b->nrec && r < cap_rec; r++) {
+        if (times) times[r] = b->log_t[r];
+        if (cnt) cnt[r] = b->log_cnt[r];
+        for (int m = 0; m < b->log_cnt[r]; m++, off++)
+            if (nodes && off < cap_nodes) { nodes[2 * off] = b->log_nodes[off].x; nodes[2 * off + 1] = b->log_nodes[off].y; }
+    }
+    return b->nrec;
+}
+
+long long or2d_brk_log_nodes(const or2d_ctx* c) { return (c && c->brk) ? c->brk->nlog : -1; }
+
 /* rhs_AB2_2DB_uv (2d/fun_odesolver.c:4542-4626) with fun_termshat_AB1_2DB_uv
  * (:2874-2960) and fun_termshat_AB2_2DB_uv (:3327-3510), ninterp = 2; walls enter
- * through dominfo.wallchar in the H2 products (:3416-3430); no friction, coupling
- * or breaking. */
+ * through dominfo.wallchar in the H2 products (:3416-3430); kinematic breaking
+ * (breaking_process, fun_sbreaking) when the tables ask for it; no friction or
+ * coupling. */
 static int rhs_2db(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
     const int Nx = c->nx, Ny = c->ny, n = c->n;
     const double factIFFT = (double)Nx * Ny;
@@ -360,22 +836,36 @@ static int rhs_2db(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
     fun_adjust(c, ikyH2adj, iky);
     cx* Source_hat = malloc(sizeof(cx) * n);
     fun_source(c, t, Source_hat);
+    cx* dphi = malloc(sizeof(cx) * n);   /* delphiH_hat (2d/fun_odesolver.c:4564-4570) */
+    for (int q = 0; q < n; q++) {
+        dphi[q].re = deluH1[q].re + delvH1[q].re + deluH2adj[q].re + delvH2adj[q].re;
+        dphi[q].im = deluH1[q].im + delvH1[q].im + deluH2adj[q].im + delvH2adj[q].im;
+    }
+    /* breaking (:4578-4584): B cleared on every call, the update only past tprev;
+     * Sb_xhat / Sb_yhat keep their last values otherwise */
+    static const cx zero = {0.0, 0.0};
+    if (c->brk) {
+        memset(c->brk->B, 0, sizeof(double) * n);
+        if (c->brk->tprev < t) {
+            brk_process(c, t, Zhat, eta, u, v);
+            brk_force(c, eta, dphi);
+        }
+    }
     for (int i = 0; i < Ny; i++)
         for (int j = 0; j < Nx; j++) {
             const int q = i * Nx + j;
             const double a = c->aal[q];
-            const double dre = deluH1[q].re + delvH1[q].re + deluH2adj[q].re + delvH2adj[q].re;
-            const double dim = deluH1[q].im + delvH1[q].im + deluH2adj[q].im + delvH2adj[q].im;
-            dt_Zhat[q] = (Source_hat[q].re + dre - dampeta[q].re) * a;
-            dt_Zhat[n + q] = (Source_hat[q].im + dim - dampeta[q].im) * a;
-            dt_Zhat[2 * n + q] = (GRAV * kx[j] * Zhat[n + q] - ikxH2adj[q].re - dampu[q].re) * a;
-            dt_Zhat[3 * n + q] = (-GRAV * kx[j] * Zhat[q] - ikxH2adj[q].im - dampu[q].im) * a;
-            dt_Zhat[4 * n + q] = (GRAV * ky[i] * Zhat[n + q] - ikyH2adj[q].re - dampv[q].re) * a;
-            dt_Zhat[5 * n + q] = (-GRAV * ky[i] * Zhat[q] - ikyH2adj[q].im - dampv[q].im) * a;
+            const cx sbx = c->brk ? c->brk->sbx[q] : zero, sby = c->brk ? c->brk->sby[q] : zero;
+            dt_Zhat[q] = (Source_hat[q].re + dphi[q].re - dampeta[q].re) * a;
+            dt_Zhat[n + q] = (Source_hat[q].im + dphi[q].im - dampeta[q].im) * a;
+            dt_Zhat[2 * n + q] = (GRAV * kx[j] * Zhat[n + q] + sbx.re - ikxH2adj[q].re - dampu[q].re) * a;
+            dt_Zhat[3 * n + q] = (-GRAV * kx[j] * Zhat[q] + sbx.im - ikxH2adj[q].im - dampu[q].im) * a;
+            dt_Zhat[4 * n + q] = (GRAV * ky[i] * Zhat[n + q] + sby.re - ikyH2adj[q].re - dampv[q].re) * a;
+            dt_Zhat[5 * n + q] = (-GRAV * ky[i] * Zhat[q] + sby.im - ikyH2adj[q].im - dampv[q].im) * a;
         }
     cx* fr[] = {eta, u, v, dampeta, dampu, dampv, deluH1, delvH1, M0u, M0v, Lphi, etaM0u, eta_u, etaM0v, eta_v,
                 deletaH2, etaM0uhat, etaM0vhat, LetaM0u, LetaM0v, ikx, iky, delu, delv, deluH2adj, delvH2adj,
-                ikxH2adj, ikyH2adj, Source_hat};
+                ikxH2adj, ikyH2adj, Source_hat, dphi};
     for (size_t q = 0; q < sizeof fr / sizeof fr[0]; q++) free(fr[q]);
     for (int q = 0; q < 6 * n; q++)
         if (!isfinite(dt_Zhat[q])) return 1;
@@ -592,6 +1082,7 @@ int or2d_evolve_apply(or2d_ctx* c, double* t, double t1, double* h, double* y) {
     const double dt = t1 - t0;
     if ((dt < 0.0 && h0 > 0.0) || (dt > 0.0 && h0 < 0.0)) { set_err2("step direction"); return 1; }
     memcpy(c->y0, y, sizeof(double) * dim);
+    if (c->brk) c->brk->tprev = t0;   /* tprev = t after every evolve_apply (2d/fun_odesolver.c:2646) */
     if (or2d_rhs(c, t0, y, c->dydt_in)) { set_err2("non-finite RHS"); return 1; }
     for (int attempt = 0; attempt < 1000; attempt++) {
         int final_step = 0;
@@ -615,6 +1106,7 @@ int or2d_evolve_apply(or2d_ctx* c, double* t, double t1, double* h, double* y) {
         }
         c->acc++;
         *h = h0;
+        if (c->brk) c->brk->tprev = *t;
         return 0;
     }
     set_err2("too many rejected steps");

@@ -50,6 +50,20 @@ typedef struct or2d_tables {
     const double* om2_min;      /* [ny*nx] Oprt.InterpD.Om2dSq_min             */
     const double* om2_plus;     /* [ny*nx] Oprt.InterpD.Om2dSq_plus            */
     const double* wallchar;     /* [ny*nx] dominfo.wallchar, NULL: no wall (varying bottom only) */
+    /* kinematic breaking (2d/breaking.c; fun_sbreaking 2d/fun_odesolver.c:985-1019), varying
+     * bottom only; breaking = 0 leaves every field below unread */
+    int breaking;
+    const double* bathy;        /* [ny*nx] dominfo.bathy.data (= -depth)        */
+    const double* brchar;       /* [ny*nx] pb.Char: cfSA, 0 where cfSA < 1 or ChiAdj < 1 */
+    const double* x;            /* [nx] dominfo.x                               */
+    const double* y;            /* [ny] dominfo.y                               */
+    double dx, dy;              /* dominfo.dx, dominfo.dy                       */
+    double max_eta_init;        /* pb.MaxEtaInit = 0.9 Hs / 2                   */
+    double tstar;               /* pb.Tstar = Tchar Tp                          */
+    double rsearch;             /* pb.Rsearch = 2 pi / kp / 4                   */
+    double kbc, tc, delb;       /* pb.KBC, pb.TC, pb.delb (1.5)                 */
+    double cur_u;               /* dominfo.U (ambient current)                  */
+    double t0, dt_out;          /* dominfo.t[0], dominfo.dt (breaking.dat cadence) */
 } or2d_tables;
 
 /* Copies every table.  eps <= 0 selects the reference's 2D values (abs 1e-3,
@@ -66,6 +80,19 @@ int or2d_evolve_apply(or2d_ctx* c, double* t, double t1, double* h, double* y);
 /* evolve_apply until t == t1 (the inner loop of ode_solver_uv) */
 int or2d_run_to(or2d_ctx* c, double* t, double t1, double* h, double* y);
 void or2d_stats(const or2d_ctx* c, long long* rhs_calls, long long* accepted, long long* rejected);
+/* Breaking state (2d/breaking.c globals).  tprev is the reference's global of that
+ * name: or2d_evolve_apply sets it to t on entry (ode_solver_uv sets it after every
+ * evolve_apply, 2d/fun_odesolver.c:2646); the breaking update of an RHS runs only
+ * when its t exceeds tprev. */
+void or2d_set_tprev(or2d_ctx* c, double tprev);
+/* B (the last RHS's breaking coefficient), Sb_xhat/Sb_yhat as [ny*nx] complex
+ * pairs (re, im interleaved), flagbr and the number of tracked crests. */
+int or2d_brk_fields(const or2d_ctx* c, double* B, double* sbx, double* sby, int* flagbr, int* ncrest);
+/* breaking.dat records: times[r], node counts cnt[r], nodes as (x, y) pairs in
+ * order.  Returns the number of records (copies at most cap_rec records and
+ * cap_nodes node pairs). */
+int or2d_brk_log(const or2d_ctx* c, double* times, int* cnt, int* nodes, int cap_rec, int cap_nodes);
+long long or2d_brk_log_nodes(const or2d_ctx* c);
 /* 2D complex DFT (FFTW sign convention, unnormalised), for tests. */
 void or2d_fft(int nx, int ny, const double* re_in, const double* im_in, double* re_out, double* im_out, int sign);
 /* the reference's fftwcomplex_2d_sym applied in place to a complex [ny*nx] array */

@@ -41,7 +41,13 @@ class Or2dTables(ctypes.Structure):
         ("nt", ctypes.c_int), ("tsig", _dpt), ("sig", _dpt), ("sigskew", _dpt),
         ("gam_min", _dpt), ("gam_plus", _dpt), ("csq_min", _dpt), ("csq_plus", _dpt), ("om2_min", _dpt),
         ("om2_plus", _dpt), ("wallchar", _dpt),
+        ("breaking", ctypes.c_int), ("bathy", _dpt), ("brchar", _dpt), ("x", _dpt), ("y", _dpt),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("max_eta_init", ctypes.c_double),
+        ("tstar", ctypes.c_double), ("rsearch", ctypes.c_double), ("kbc", ctypes.c_double), ("tc", ctypes.c_double),
+        ("delb", ctypes.c_double), ("cur_u", ctypes.c_double), ("t0", ctypes.c_double), ("dt_out", ctypes.c_double),
     ]
+
+BRK_SCALARS = ("dx", "dy", "max_eta_init", "tstar", "rsearch", "kbc", "tc", "delb", "cur_u", "t0", "dt_out")
 
 
 def build():
@@ -85,6 +91,11 @@ def lib():
         L.or2d_stats.argtypes = [vp] + [ctypes.POINTER(ctypes.c_longlong)] * 3
         L.or2d_fft.argtypes = [ip, ip, dp, dp, dp, dp, ip]
         L.or2d_sym.argtypes = [ip, ip, dp, dp]
+        L.or2d_set_tprev.argtypes = [vp, ctypes.c_double]
+        L.or2d_brk_fields.argtypes = [vp, dp, dp, dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        L.or2d_brk_log.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ip, ip]
+        L.or2d_brk_log_nodes.restype = ctypes.c_longlong
+        L.or2d_brk_log_nodes.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -198,10 +209,14 @@ class Oracle2D:
                   "gam_min", "gam_plus", "csq_min", "csq_plus", "om2_min", "om2_plus", "wallchar"):
             v = tables.get(k)
             keep[k] = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
+        brk = int(tables.get("breaking", 0))
+        for k in ("bathy", "brchar", "x", "y"):
+            keep[k] = np.ascontiguousarray(tables[k], dtype=np.float64) if brk else None
         self._keep = keep
+        scal = {k: float(tables.get(k, 0.0)) for k in BRK_SCALARS} if brk else {}
         tb = Or2dTables(nx=int(tables["nx"]), ny=int(tables["ny"]), model=int(tables.get("model", 2)),
                         propagation=int(tables.get("propagation", 0)), cpeak=float(tables["cpeak"]),
-                        nt=int(tables.get("nt", 0) if keep["sig"] is not None else 0),
+                        nt=int(tables.get("nt", 0) if keep["sig"] is not None else 0), breaking=brk, **scal,
                         **{k: (None if v is None else _p(v)) for k, v in keep.items()})
         self.h = L.or2d_create(ctypes.byref(tb), eps_abs, eps_rel)
         if not self.h:
@@ -243,6 +258,37 @@ class Oracle2D:
         a, b, c = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
         lib().or2d_stats(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
         return {"rhs_calls": a.value, "accepted": b.value, "rejected": c.value}
+
+    def set_tprev(self, t):
+        lib().or2d_set_tprev(self.h, float(t))
+
+    def breaking_fields(self):
+        """B, Sb_xhat, Sb_yhat (complex [ny, nx]), flagbr, tracked crests."""
+        B = np.zeros(self.n)
+        sx, sy = np.zeros(2 * self.n), np.zeros(2 * self.n)
+        fl, nc = ctypes.c_int(), ctypes.c_int()
+        if lib().or2d_brk_fields(self.h, _p(B), _p(sx), _p(sy), ctypes.byref(fl), ctypes.byref(nc)):
+            raise RuntimeError("oracle2d: no breaking")
+        shp = (self.ny, self.nx)
+        return (B.reshape(shp), (sx[0::2] + 1j * sx[1::2]).reshape(shp), (sy[0::2] + 1j * sy[1::2]).reshape(shp),
+                fl.value, nc.value)
+
+    def breaking_log(self):
+        """breaking.dat records as a list of (t, [(x, y), ...])."""
+        L = lib()
+        nn = int(L.or2d_brk_log_nodes(self.h))
+        nr = L.or2d_brk_log(self.h, None, None, None, 0, 0)
+        t = np.zeros(max(nr, 1))
+        cnt = np.zeros(max(nr, 1), dtype=np.int32)
+        nodes = np.zeros(2 * max(nn, 1), dtype=np.int32)
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.or2d_brk_log(self.h, _p(t), cnt.ctypes.data_as(ip), nodes.ctypes.data_as(ip), nr, nn)
+        out, off = [], 0
+        for r in range(nr):
+            c = int(cnt[r])
+            out.append((float(t[r]), [tuple(v) for v in nodes[2 * off:2 * (off + c)].reshape(-1, 2).tolist()]))
+            off += c
+        return out
 
 
 def fft2(x, sign=-1):

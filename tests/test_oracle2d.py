@@ -140,3 +140,54 @@ def test_two_depth_operator_reduces_to_flat_one():
         y[(2 * f + 1) * n:(2 * f + 2) * n] = 1e-3 * spec.imag.ravel()
     a, b = flat.rhs(0.0, y), two.rhs(0.0, y)
     assert np.linalg.norm(a - b) / np.linalg.norm(a) < 1e-2
+
+
+# --------------------------------------------------------------------------
+# kinematic breaking (2d/breaking.c, fun_sbreaking)
+# --------------------------------------------------------------------------
+def test_breaking_tables_follow_parambreak():
+    from breaking2d_case import steep_crest_case
+    tb, _ = steep_crest_case()
+    cf = decks2d.cfsa2d(tb["x"], tb["y"], 6.0, 6.0, 6.0, 6.0)
+    # pb.Char: cfSA where cfSA and ChiAdj are 1, zero in the damping zones and the influx band
+    assert np.all(tb["brchar"][cf < 1] == 0) and np.all(tb["brchar"][tb["chiadj"] < 1] == 0)
+    assert tb["brchar"].max() == 1.0 and np.all(tb["bathy"] == -tb["depth"])
+    assert abs(tb["max_eta_init"] - 0.27) < 1e-15 and abs(tb["rsearch"] * 4 * decks2d.invers_omega(2 * np.pi / 4.0, 3.0)
+                                                          - 2 * np.pi) < 1e-12
+
+
+def test_breaking_rhs_at_tprev_is_the_plain_rhs():
+    """At t == tprev (the first stage of every evolve_apply) no update runs and Sb is
+    still zero: the RHS is the one without breaking, bit for bit."""
+    from breaking2d_case import steep_crest_case
+    tb, z = steep_crest_case()
+    plain = {k: v for k, v in tb.items() if k != "breaking"}
+    a, b = Oracle2D(tb, 1e-6, 1e-4), Oracle2D(plain, 1e-6, 1e-4)
+    a.set_tprev(0.3)
+    assert np.array_equal(a.rhs(0.3, z), b.rhs(0.3, z))
+    B, sx, sy, flag, nc = a.breaking_fields()
+    assert flag == 0 and nc == 0 and not B.any() and not sx.any()
+
+
+def test_breaking_starts_tracks_and_logs():
+    """The steep crest: candidates at the first update, crests tracked with break
+    nodes (flagbr 2), a nonzero eddy-viscosity force, records in breaking.dat."""
+    from breaking2d_case import steep_crest_case
+    tb, z = steep_crest_case()
+    o = Oracle2D(tb, 1e-6, 1e-4)
+    t, h, y = 0.3, 0.005, z.copy()
+    o.set_tprev(t)
+    seen2 = False
+    for _ in range(8):
+        t, h = o.evolve_apply(t, 0.6, h, y)
+        B, sx, sy, flag, nc = o.breaking_fields()
+        if flag == 2:
+            seen2 = True
+            assert nc >= 1 and (B > 0).any() and np.abs(sx).max() > 0
+            assert np.all((B >= 0) & (B <= 1))
+    assert seen2
+    log = o.breaking_log()
+    assert len(log) >= 1 and all(len(nodes) > 0 for _, nodes in log)
+    assert all(0 <= x < tb["nx"] and 0 <= yy < tb["ny"] for _, nodes in log for x, yy in nodes)
+    # records come from every RHS past tprev, rejected attempts' stages included
+    assert all(0.3 < tt <= t + 0.05 for tt, _ in log)
