@@ -215,12 +215,14 @@ class ClockSampler:
 # ----------------------------------------------------------------------------
 STEP_2D = 0.5
 # algorithmic HBM bytes per 2D RHS grid-point evaluation: the RK vectors of S = 6
-# doubles per point streamed 35 times per 6 RHS, plus 13 per-point table doubles
+# doubles per point streamed 35 times per 6 RHS, plus 15 per-point table doubles
 # (two-depth weights gam_min/plus, C^2 and Om^2 of both reference depths, aal,
-# damping, ChiAdj, two complex source kernels): 35/6 * 6 * 8 + 13 * 8
-BYTES_PER_RHS_PT_2D = 35.0 / 6.0 * 6 * 8 + 13 * 8
+# damping, ChiAdj, two complex source kernels, the breaking tables bathymetry and
+# pb.Char): 35/6 * 6 * 8 + 15 * 8
+BYTES_PER_RHS_PT_2D = 35.0 / 6.0 * 6 * 8 + 15 * 8
 WORKLOAD_2D = ("2D twin: 1024x1024 on 300 m x 300 m, depth 5 m offshore sloping to 0.5 m with a seeded shoal "
-               "(two reference depths), harbour breakwater of reflection 0.5, HS2, vertical line source of a directional JONSWAP (Hs 0.5 m, Tp 6 s, "
+               "(two reference depths), harbour breakwater of reflection 0.5, HS2 with kinematic breaking (KBC 0.8, TC 0.2, "
+               "Tchar 0.5), vertical line source of a directional JONSWAP (Hs 0.5 m, Tp 6 s, "
                "gamma 3.3, cos^2s s=10, 256x64 seeded components), 30 m damping zones, RKF45 rtol 1e-6 atol 1e-8")
 
 
@@ -343,12 +345,12 @@ def main_2d(args, rank, world, local):
     traffic = None
     try:
         for line in open(os.path.join(ROOT, "profiles", "k2v_rhs_2d_1024.md")):
-            if line.startswith("dram_bytes_per_rhs_pt:"):
+            if line.startswith("dram_bytes_per_rhs_pt_breaking:"):
                 traffic = float(line.split(":")[1]) * pts / max(1, args.steps) / (world or 1)
     except OSError:
         pass
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": traffic, "kernel": "k2v_rowA..k2_rowE (one RHS = 9 fused FFT passes)",
+            "traffic": traffic, "kernel": "k2v_rowA..k2b_sbrow (one RHS = 9 fused FFT passes + the breaking kernels)",
             "launch": f"one step = {STEP_2D} simulated s, {pts / max(1, args.steps):.3e} RHS grid points, "
                       f"{BYTES_PER_RHS_PT_2D:.1f} algorithmic B/point",
             "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback"}

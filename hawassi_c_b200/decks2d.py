@@ -406,10 +406,12 @@ def config5(seed=0, bathymetry="shoal", **kw) -> dict:
     0.5 m with a seeded shoal (two reference depths; bathymetry="flat" gives a flat
     3 m bottom and no wall), a harbour breakwater (x 200-206 m, y 90-210 m) of
     reflection coefficient 0.5, directional JONSWAP Hs 0.5 m Tp 6 s gamma 3.3,
-    cos^2s spreading s = 10, 256 x 64 seeded components, HS2, 30 m damping zones,
-    influx line at x = 45 m."""
+    cos^2s spreading s = 10, 256 x 64 seeded components, HS2 with kinematic
+    breaking (KBC 0.8, TC 0.2, Tchar 0.5; two-depth tables only), 30 m damping
+    zones, influx line at x = 45 m."""
     if bathymetry == "flat":
         return tables(seed=seed, **kw)
+    kw.setdefault("breaking", True)
     kw.setdefault("depth", 5.0)
     kw.setdefault("walls", ((200.0, 90.0, 206.0, 210.0),))
     kw.setdefault("refl", 0.5)
