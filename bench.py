@@ -233,10 +233,12 @@ def _cpu_rhs_2d(tables, threads, seconds):
     import numpy as np
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib as ol
-    o = ol.Oracle2D(tables, EPS_ABS, EPS_REL)
     n = tables["nx"] * tables["ny"]
+    # one oracle context per thread: the breaking state and work arrays are per context
+    ctxs = [ol.Oracle2D(tables, EPS_ABS, EPS_REL) for _ in range(threads)]
 
     def work(seed):
+        o = ctxs[seed]
         rng = np.random.default_rng(seed)
         y = 1e-3 * rng.standard_normal(6 * n) * np.tile(tables["aal"].ravel(), 6)
         calls, t0 = 0, time.perf_counter()

@@ -173,10 +173,16 @@ or2d_ctx* or2d_create(const or2d_tables* tb, double eps_abs, double eps_rel) {
         if (!tb->bathy || !tb->brchar || !tb->x || !tb->y) { set_err2("or2d_create: breaking tables missing"); free(c); return NULL; }
         c->brk = brk_create(tb);
     }
-    size_t d = 6 * n;
+    return c;
+}
+
+/* the rkf45 work vectors, allocated by the first evolve_apply (an RHS-only
+ * context, as the CPU baseline's threads use, needs none) */
+static void ensure_rk(or2d_ctx* c) {
+    if (c->k1) return;
+    size_t d = 6 * (size_t)c->n;
     double** w[] = {&c->k1, &c->k2, &c->k3, &c->k4, &c->k5, &c->k6, &c->ytmp, &c->y0, &c->yerr, &c->dydt_in, &c->dydt_out};
     for (size_t q = 0; q < sizeof w / sizeof w[0]; q++) *w[q] = calloc(d, sizeof(double));
-    return c;
 }
 
 void or2d_destroy(or2d_ctx* c) {
@@ -1076,6 +1082,7 @@ static int hadjust(const or2d_ctx* c, const double* y, const double* yerr, doubl
 }
 
 int or2d_evolve_apply(or2d_ctx* c, double* t, double t1, double* h, double* y) {
+    ensure_rk(c);
     const int dim = 6 * c->n;
     const double t0 = *t;
     double h0 = *h;
