@@ -17,6 +17,7 @@
 
 #include "../../include/hawassi_b200.h"
 #include "hw_kernels.h"
+#include "hw_kin.h"
 #include "hw_setup.hpp"
 
 using namespace hwdev;
@@ -118,6 +119,7 @@ struct HostMember {
   size_t dev_bytes = 0;
   double* fields = nullptr;  // per-sample eta, u, phi when the member keeps fields
   double t0 = 0, h0 = 0;
+  hwkin::Kin* kin = nullptr; // kinematics tables (made by the first kinematics call)
 };
 
 struct Class {
@@ -512,6 +514,7 @@ hw_ctx::~hw_ctx() {
   for (auto& h : mem) {
     if (h.dev) cudaFree(h.dev);
     if (h.fields) cudaFree(h.fields);
+    if (h.kin) hwkin::kin_destroy(h.kin);
   }
   for (auto& e : tw) cudaFree(e.second);
   if (d_stage) cudaFree(d_stage);
@@ -770,6 +773,49 @@ int hw_last_dydt(hw_ctx* ctx, int m, double* dydt) {
     HW_CUDA(cudaMemcpyAsync(dydt, ctx->d_ref, sizeof(double) * 4 * hm.N, cudaMemcpyDeviceToHost, ctx->stream));
     HW_CUDA(cudaStreamSynchronize(ctx->stream));
     return true;
+  };
+  return body() ? 0 : 1;
+}
+
+namespace {
+bool ensure_kin(hw_ctx* ctx, int m) {
+  HostMember& hm = ctx->mem[size_t(m)];
+  if (hm.kin) return true;
+  hm.kin = hwkin::kin_create(hm.m, ctx->err);
+  return hm.kin != nullptr;
+}
+}  // namespace
+
+int hw_kinematics_dims(hw_ctx* ctx, int m, int* nx_out, int* nz_out) {
+  if (!valid_member(ctx, m) || !ensure_kin(ctx, m)) return 1;
+  hwkin::kin_dims(ctx->mem[size_t(m)].kin, nx_out, nz_out);
+  return 0;
+}
+
+int hw_kinematics_grid(hw_ctx* ctx, int m, double* x_out, double* z_out) {
+  if (!valid_member(ctx, m) || !ensure_kin(ctx, m)) return 1;
+  hwkin::kin_grid(ctx->mem[size_t(m)].kin, x_out, z_out);
+  return 0;
+}
+
+int hw_kinematics(hw_ctx* ctx, int m, double tprev, double* eta_cut, double* P, double* dxphi, double* dzphi,
+                  double* dtdxphi, double* dtdzphi) {
+  if (!valid_member(ctx, m) || !ensure_kin(ctx, m)) return 1;
+  std::string& err = ctx->err;
+  auto body = [&]() -> bool {
+    HostMember& hm = ctx->mem[size_t(m)];
+    HW_CUDA(cudaMemcpyAsync(&hm.d, ctx->d_mems + m, sizeof(DevMember), cudaMemcpyDeviceToHost, ctx->stream));
+    HW_CUDA(cudaStreamSynchronize(ctx->stream));
+    // the state and the RHS the output stage reads (the global dy: kout in the exact
+    // sequence, k1 after a reuse in the pure one), in the reference layout
+    const double2* src = hm.d.k1_valid ? hm.d.kb[0] : hm.d.kb[6];
+    double* yb = hwkin::kin_state_buffer(hm.kin, 0);
+    double* db = hwkin::kin_state_buffer(hm.kin, 1);
+    k_to_reference<<<(hm.N + 255) / 256, 256, 0, ctx->stream>>>(hm.d.y, yb, hm.N, hm.logC, hm.M);
+    k_to_reference<<<(hm.N + 255) / 256, 256, 0, ctx->stream>>>(src, db, hm.N, hm.logC, hm.M);
+    HW_CUDA(cudaGetLastError());
+    if (!hwkin::kin_run(hm.kin, yb, db, hm.d.t, tprev, ctx->stream, err)) return false;
+    return hwkin::kin_fetch(hm.kin, eta_cut, P, dxphi, dzphi, dtdxphi, dtdzphi, ctx->stream, err);
   };
   return body() ? 0 : 1;
 }

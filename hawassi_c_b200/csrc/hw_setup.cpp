@@ -257,8 +257,8 @@ bool parse_input(const std::string& dir, Deck& d, std::string& err) {
     if (std::fscanf(f, "%*s %*s %lf \n %*s %*s %lf %lf \n", &d.parKBC, &d.parTC, &d.parTchar) < 0) {}
   }
   if (in.skip_lines(1, 128)) {
-    if (std::fscanf(f, "%*s %*s %lf \n %*s %*s %lf \n", &xi1, &xi2) < 0) {}
-    if (std::fscanf(f, "%*s %*s %d \n %*s %*s %d \n", &ns, &nd) < 0) {}
+    if (std::fscanf(f, "%*s %*s %lf \n %*s %*s %lf \n", &xi1, &xi2) == 2) { d.xinterv1 = xi1; d.xinterv2 = xi2; }
+    if (std::fscanf(f, "%*s %*s %d \n %*s %*s %d \n", &ns, &nd) == 2) { d.nsurf = ns; d.ndeep = nd; }
   }
   if (in.skip_lines(1, 128)) {
     scan_word(f, d.cut_temp);
@@ -855,5 +855,8 @@ bool build_member(const std::string& dir, const SetupOptions& opt, Member& m, st
   }
   return true;
 }
+
+double linear_wavenumber(double w, double d) { return invers_omega(w, d); }
+int closest_index(const std::vector<double>& a, double ref) { return closest(a, ref); }
 
 }  // namespace hw

@@ -25,6 +25,8 @@ struct Deck {
   int ngauge = 0, npartition = 0;
   double T0 = 0, Tend = 0, dt = 0, Tp = 0, Hs = 0, gamJS = 0;
   double Xstart = 0, Xend = 0, Xinflux = 0, dx = 0, dampL = 0, dampR = 0;
+  double xinterv1 = 0, xinterv2 = 0;   // &IF KINEMATIC block (1d/read_input.c:42-44)
+  int nsurf = 0, ndeep = 0;
 };
 
 // All per-member tables in the reference's natural index order (FFTW order for
@@ -73,5 +75,10 @@ void host_dft(std::vector<double>& re, std::vector<double>& im, int sign);
 std::vector<double> natural_spline_c(const std::vector<double>& x, const std::vector<double>& y);
 double natural_spline_eval(const std::vector<double>& x, const std::vector<double>& y,
                            const std::vector<double>& c, double t);
+
+// invers_omega (1d/functions.c:984-1020) and closest (1d/functions.c:1761), as the
+// set-up uses them, for the kinematics tables
+double linear_wavenumber(double w, double d);
+int closest_index(const std::vector<double>& a, double ref);
 
 }  // namespace hw

@@ -45,7 +45,7 @@ breaking\t= {breaking}
 friction \t= no
 influxing \t= {influxing}
 propagation \t= {propagation}
-kinematic \t= no
+kinematic \t= {kinematic}
 ngauge \t\t= {ngauge}
 npartition \t= {npartition}
 
@@ -54,10 +54,10 @@ initiation \t= {kbc}
 termination = {tc} {tchar}
 
 &IF KINEMATIC
-xstart\t\t= 40
-xend\t\t= 60
-nsurf \t\t= 50
-ndeep \t\t= 40
+xstart\t\t= {kx1}
+xend\t\t= {kx2}
+nsurf \t\t= {nsurf}
+ndeep \t\t= {ndeep}
 
 &MORE OPTIONS FOR EXPERT ONLY
 cutfrac\t\t  = {cutfrac}
@@ -131,8 +131,11 @@ def write_deck(path, nx, length=None, xstart=0.0, xinflux=None, depth=1.0, bath=
                breaking=False, T_end=100.0, n_samples=2048, n_lines=1024, Hs=0.10, Tp=2.0, gamma=3.3,
                seed=0, damp=(10.0, 10.0), adjcoef=0.5, propagation="Uni+", influxing="Area",
                kbc=0.8, tc=0.2, tchar=0.5, cutfrac="default", ramp="yes 4", wavename="user_defined",
-               initial="zero", initial_wave=None, gauges=(), dt=0.02, npartition=1):
-    """Write one deck directory.  bath: None for flat depth, or an array of nx depths."""
+               initial="zero", initial_wave=None, gauges=(), dt=0.02, npartition=1, kinematic=False,
+               kin_window=(40.0, 60.0), nsurf=50, ndeep=40):
+    """Write one deck directory.  bath: None for flat depth, or an array of nx depths.
+    kinematic: the kinematics output on the overlay window kin_window (x range, m)
+    with nsurf surface and ndeep deep levels (read_kinematics, 1d/functions.c:3555)."""
     os.makedirs(path, exist_ok=True)
     length = float(length if length is not None else 0.05 * nx)
     xend = xstart + length
@@ -145,7 +148,8 @@ def write_deck(path, nx, length=None, xstart=0.0, xinflux=None, depth=1.0, bath=
         dampR=repr(float(damp[1])), bath="flat" if bath is None else "user_defined", depth=repr(float(depth)),
         adjcoef=repr(float(adjcoef)), model=model, breaking="yes" if breaking else "no", influxing=influxing,
         propagation=propagation, ngauge=len(gauges), npartition=int(npartition), kbc=repr(float(kbc)), tc=repr(float(tc)),
-        tchar=repr(float(tchar)), cutfrac=cutfrac, ramp=ramp)
+        tchar=repr(float(tchar)), cutfrac=cutfrac, ramp=ramp, kinematic="yes" if kinematic else "no",
+        kx1=repr(float(kin_window[0])), kx2=repr(float(kin_window[1])), nsurf=int(nsurf), ndeep=int(ndeep))
     with open(os.path.join(path, "input.txt"), "w") as f:
         f.write(_INPUT.format(**fields))
     if wavename == "user_defined":

@@ -85,6 +85,9 @@ def load_library():
     L.hw_deck_table.argtypes = [ctypes.c_char_p, ctypes.POINTER(HwOpts), ctypes.c_char_p, dp, ip]
     L.hw_rhs_noalloc.argtypes = [vp, ip, dd, vp, vp, vp]
     L.hw_gauges.argtypes = [vp, ip, dp, dp, dp, ip]
+    L.hw_kinematics_dims.argtypes = [vp, ip, ctypes.POINTER(ip), ctypes.POINTER(ip)]
+    L.hw_kinematics_grid.argtypes = [vp, ip, dp, dp]
+    L.hw_kinematics.argtypes = [vp, ip, dd, dp, dp, dp, dp, dp, dp]
     L.hw_ngauge.argtypes = [vp, ip]
     L.hw_enable_fields.argtypes = [vp, ip, ip]
     L.hw_write_outputs.argtypes = [vp, ip, ctypes.c_char_p]
@@ -258,6 +261,23 @@ class Engine:
         y = np.zeros(4 * self.nx[member])
         self._check(load_library().hw_last_dydt(self._h, member, _dp(y)), "last_dydt")
         return y
+
+    def kinematics(self, tprev, member=0):
+        """kinematic_modul at the member's current time (deck with kinematic yes): dict of
+        eta_cut [nx_out], P, dxphi, dzphi, dtdxphi, dtdzphi [nx_out, nz_out], x_out, z_out."""
+        L = load_library()
+        a, b = ctypes.c_int(), ctypes.c_int()
+        self._check(L.hw_kinematics_dims(self._h, member, ctypes.byref(a), ctypes.byref(b)), "hw_kinematics_dims")
+        nxo, nz = a.value, b.value
+        xo, zo = np.zeros(nxo), np.zeros(nz)
+        self._check(L.hw_kinematics_grid(self._h, member, _dp(xo), _dp(zo)), "hw_kinematics_grid")
+        out = {k: np.zeros(nxo * nz) for k in ("P", "dxphi", "dzphi", "dtdxphi", "dtdzphi")}
+        ec = np.zeros(nxo)
+        self._check(L.hw_kinematics(self._h, member, float(tprev), _dp(ec), _dp(out["P"]), _dp(out["dxphi"]),
+                                    _dp(out["dzphi"]), _dp(out["dtdxphi"]), _dp(out["dtdzphi"])), "hw_kinematics")
+        res = {k: v.reshape(nxo, nz) for k, v in out.items()}
+        res.update(eta_cut=ec, x_out=xo, z_out=zo)
+        return res
 
     def gauges(self, member=0):
         """Gauge series the device computed at every output sample reached so far:

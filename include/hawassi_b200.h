@@ -107,6 +107,22 @@ int hw_last_dydt(hw_ctx* ctx, int member, double* dydt);
  * written, *len receives the number of doubles. */
 int hw_breaking_log(hw_ctx* ctx, int member, double* out, long long cap, long long* len);
 
+/* Kinematics of a member whose deck has "kinematic yes" (kinematic_modul,
+ * 1d/kinematic_modul.c:1-247; grid of read_kinematics, 1d/functions.c:3555-3669):
+ * at the member's current time, from its state and the last RHS (the reference's
+ * etaf, u_hatf, dtetaf, dtphi_hatf), on the overlay window [xinterv1, xinterv2]
+ * (nx_out points) and the nz_out levels zoutIP (surface layer plus the deeper
+ * Riemann-sum levels, ascending).  Outputs are [nx_out][nz_out], x-major, as the
+ * reference's fwrite of Ptot, dxPhi, dzPhi, dt_dxPHI, dt_dzPHI: NaN above the
+ * surface or below the bed; the accelerations are (velocity - 0) / (t - tprev)
+ * with the caller's tprev, as the reference computes them.  eta_cut [nx_out].
+ * Any output pointer may be NULL.  Returns 0, nonzero with hw_last_error set
+ * (e.g. kinematic no, runup). */
+int hw_kinematics_dims(hw_ctx* ctx, int member, int* nx_out, int* nz_out);
+int hw_kinematics_grid(hw_ctx* ctx, int member, double* x_out, double* z_out);
+int hw_kinematics(hw_ctx* ctx, int member, double tprev, double* eta_cut, double* P, double* dxphi,
+                  double* dzphi, double* dtdxphi, double* dtdzphi);
+
 /* All members' states, concatenated in member order (4*Nx doubles each), host buffers. */
 int hw_get_states(hw_ctx* ctx, double* y_all);
 int hw_set_states(hw_ctx* ctx, const double* y_all);

@@ -405,7 +405,12 @@ struct or_ctx {
     unsigned long long seed;
     char outdir[512];
     int write_fields;
+
+    /* kinematics (read_kinematics, 1d/functions.c:3555-3669) */
+    int kin, kin_i1, kin_i2, kin_nx, kin_nz;
+    double *kin_z, kin_maxD, kin_minD, kin_maxEta, kin_minEta;
 };
+static int kin_setup(or_ctx* c);
 
 static void blog_append(or_ctx* c, const char* fmt, ...) {
     char buf[256]; va_list ap;
@@ -960,7 +965,7 @@ static void ctx_free(or_ctx* c) {
                   c->temp_wave, c->temp_u, c->Csqr, c->L, c->M0im, c->Csq_min, c->Csq_mid, c->Csq_plus, c->gam_min, c->gam_mid, c->gam_plus,
                   c->CrestBreak, c->CrestBreakNew, c->CrestBreakPrev, c->ID_Node_end, c->Break_nodes, c->B, c->blog, c->dy, c->Rb_hat,
                   c->y0, c->yerr, c->dydt_in, c->dydt_out, c->k1, c->k2, c->k3, c->k4, c->k5, c->k6, c->ytmp,
-                  c->CsqK, c->gamK};
+                  c->CsqK, c->gamK, c->kin_z};
     for (size_t i = 0; i < sizeof ps / sizeof ps[0]; i++) free(ps[i]);
     cspline_free(&c->sp_in); cspline_free(&c->sp_skew);
     plan_free(&c->plan);
@@ -1104,6 +1109,10 @@ or_ctx* or_create(const char* dir, const or_opts* o) {
     define_operator(c, c->nu_peak);
     ALLOC(c->dy, 4 * Nx);
     plan_make(&c->plan, Nx);
+    if (strcmp(c->kinematic, "yes") == 0) {
+        c->kin = 1;
+        if (kin_setup(c)) goto fail;
+    }
     int D = 4 * Nx;
     ALLOC(c->y0, D); ALLOC(c->yerr, D); ALLOC(c->dydt_in, D); ALLOC(c->dydt_out, D);
     ALLOC(c->k1, D); ALLOC(c->k2, D); ALLOC(c->k3, D); ALLOC(c->k4, D); ALLOC(c->k5, D); ALLOC(c->k6, D); ALLOC(c->ytmp, D);
@@ -1826,4 +1835,212 @@ int or_table(const or_ctx* c, const char* nm, double* out, int cap) {
 #undef R
 #undef C
     return -1;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Kinematics: read_kinematics (1d/functions.c:3555-3669) and kinematic_modul */
+/* (1d/kinematic_modul.c:1-247): velocity potential derivatives and pressure */
+/* under the surface on the overlay window [xinterv1, xinterv2] x zoutIP.    */
+/* ------------------------------------------------------------------------ */
+/* sinhcosh2IP (1d/functions.c:1889-1928): two-depth interpolation weights of
+ * cosh/sinh(kappa D) between Dmin and Dplus, kappa the linear wavenumber of nupeak */
+static void sinhcosh2ip(int sizD, const double* D, double Dmin, double Dplus, const double* k, double nupeak,
+                        double* gmin, double* gplus) {
+    for (int j = 0; j < sizD; j++) {
+        const double kap = (D[j] == 0) ? k[2] : invers_omega(nupeak, D[j]);
+        const double cmin = cosh(kap * Dmin), cplus = cosh(kap * Dplus), cD = cosh(kap * D[j]);
+        const double smin = sinh(kap * Dmin), splus = sinh(kap * Dplus), sD = sinh(kap * D[j]);
+        const double det = cmin * splus - cplus * smin;
+        gmin[j] = (splus * cD - cplus * sD) / det;
+        gplus[j] = (-(smin * cD) + cmin * sD) / det;
+    }
+}
+
+static int kin_setup(or_ctx* c) {
+    const int Nx = c->Nx;
+    if (c->nsurf < 2 || c->ndeep < 1) { set_err("kinematics: nsurf must be >= 2 and ndeep >= 1"); return -1; }
+    for (int i = 0; i < Nx; i++)
+        if (c->depth[i] == 0) { set_err("kinematics: runup (zero depth) is not supported"); return -1; }
+    double zs1, zs2;
+    if (strcmp(c->min_z, "default") == 0) {
+        zs1 = -2.5 * c->Hs_in;
+        if (strcmp(c->initial, "user_defined") == 0) zs1 = -0.6 * c->Hs_in;
+    } else zs1 = atof(c->min_z);
+    if (strcmp(c->max_z, "default") == 0) {
+        zs2 = 2.5 * c->Hs_in;
+        if (strcmp(c->initial, "user_defined") == 0) zs2 = 0.6 * c->Hs_in;
+    } else zs2 = atof(c->max_z);
+    c->kin_maxD = search_max_val(c->depth, Nx);
+    c->kin_minD = search_min_val(c->depth, Nx);
+    c->kin_i1 = closest(c->x, c->xinterv1, Nx);
+    c->kin_i2 = closest(c->x, c->xinterv2, Nx);
+    c->kin_nx = c->kin_i2 - c->kin_i1 + 1;
+    if (c->kin_nx < 1) { set_err("kinematics: empty overlay window"); return -1; }
+    c->kin_maxEta = zs2;
+    c->kin_minEta = zs1;
+    const int ns = c->nsurf, nd = c->ndeep, nz = ns + nd;
+    double* zs = malloc(sizeof(double) * ns);
+    double* zd = malloc(sizeof(double) * nd);
+    const double dzs = (zs2 - zs1) / (ns - 1);
+    const double kpk = invers_omega(c->nu_peak, c->kin_maxD);
+    for (int j = 0; j < ns; j++) zs[j] = zs1 + j * dzs;
+    /* deeper levels: Riemann upper sum of the cosh profile (1d/functions.c:3627-3637) */
+    const double Flux = 1 / (kpk * sinh(kpk * c->kin_maxD)) * (cosh(kpk * (c->kin_maxD + zs1)) - 1);
+    const double tol = Flux / nd;
+    zd[0] = -1 * (zs1 - dzs);
+    for (int i = 1; i < nd; i++)
+        zd[i] = zd[i - 1] + (tol / (sinh(kpk * (c->kin_maxD - zd[i - 1])) / sinh(kpk * c->kin_maxD)));
+    c->kin_nz = nz;
+    c->kin_z = malloc(sizeof(double) * nz);
+    for (int i = 0; i < ns; i++) c->kin_z[i] = zs[i];
+    for (int i = ns; i < nz; i++) c->kin_z[i] = -1 * zd[i - ns];
+    for (int i = 0; i < nz; i++)            /* sorting (1d/functions1.c) */
+        for (int j = i + 1; j < nz; j++)
+            if (c->kin_z[j] < c->kin_z[i]) { double tt = c->kin_z[i]; c->kin_z[i] = c->kin_z[j]; c->kin_z[j] = tt; }
+    free(zs); free(zd);
+    return 0;
+}
+
+int or_kin_dims(const or_ctx* c, int* nxout, int* nzout) {
+    if (!c || !c->kin) return -1;
+    if (nxout) *nxout = c->kin_nx;
+    if (nzout) *nzout = c->kin_nz;
+    return 0;
+}
+
+int or_kin_grid(const or_ctx* c, double* xout, double* zout) {
+    if (!c || !c->kin) return -1;
+    if (xout) for (int i = 0; i < c->kin_nx; i++) xout[i] = c->x[c->kin_i1 + i];
+    if (zout) memcpy(zout, c->kin_z, sizeof(double) * c->kin_nz);
+    return 0;
+}
+
+/* gradient (1d/functions1.c): one-sided at the ends */
+static void gradient1(const double* a, double d, int n, double* g) {
+    g[0] = (a[1] - a[0]) / d;
+    g[n - 1] = (a[n - 1] - a[n - 2]) / d;
+    for (int i = 1; i < n - 1; i++) g[i] = (a[i + 1] - a[i - 1]) / (2 * d);
+}
+
+int or_kinematics(or_ctx* c, double t, double tprev, const double* y, const double* dy, double* eta_cut, double* P,
+                  double* dxphi, double* dzphi, double* ax, double* az) {
+    if (!c || !c->kin) { set_err("kinematics: the deck has kinematic no"); return -1; }
+    const int Nx = c->Nx, nxo = c->kin_nx, nz = c->kin_nz, NH = 100;
+    const double* k = c->k;
+    /* the output stage's fields (1d/functions.c:570-596) */
+    cpx *eh = cnew(Nx), *uh = cnew(Nx), *dh = cnew(Nx), *dph = cnew(Nx);
+    double *eta = dnew(Nx), *dteta = dnew(Nx);
+    for (int j = 0; j < Nx; j++) {
+        eh[j].re = y[j]; eh[j].im = y[Nx + j];
+        uh[j].re = y[2 * Nx + j]; uh[j].im = y[3 * Nx + j];
+        dh[j].re = dy[j]; dh[j].im = dy[Nx + j];
+        if (k[j] == 0) { dph[j].re = 0; dph[j].im = 0; }
+        else {   /* prod_1ik(-1/k, du^): (0 - (-1/k) Im) + i (0 + (-1/k) Re) */
+            const double a = -1 / k[j];
+            dph[j].re = (0 * dy[2 * Nx + j]) - (a * dy[3 * Nx + j]);
+            dph[j].im = (0 * dy[3 * Nx + j]) + (a * dy[2 * Nx + j]);
+        }
+    }
+    ifft_cr_nx(c, eh, eta);
+    ifft_cr_nx(c, dh, dteta);
+    /* kinematic_modul */
+    const double nupeak = c->nu_peak;
+    const double Hplus = c->kin_maxEta + c->kin_maxD, Hmin = c->kin_minEta + c->kin_minD;
+    const double dhtot = (Hplus - Hmin) / NH;
+    double Htot[101], gHm0[101], gHp0[101], DZtot[101], gDm0[101], gDp0[101];
+    for (int i = 0; i < NH + 1; i++) Htot[i] = Hmin + i * dhtot;
+    sinhcosh2ip(NH + 1, Htot, Hmin, Hplus, k, nupeak, gHm0, gHp0);
+    double cHm[101], cHp[101], cDm[101], cDp[101];
+    or_cspline_coeffs(NH + 1, Htot, gHm0, cHm);
+    or_cspline_coeffs(NH + 1, Htot, gHp0, cHp);
+    const double DZmin0 = 0, DZplus0 = Hplus;
+    for (int i = 0; i < NH + 1; i++) DZtot[i] = DZmin0 + i * (DZplus0 - DZmin0) / NH;
+    sinhcosh2ip(NH + 1, DZtot, DZmin0, DZplus0, k, nupeak, gDm0, gDp0);
+    or_cspline_coeffs(NH + 1, DZtot, gDm0, cDm);
+    or_cspline_coeffs(NH + 1, DZtot, gDp0, cDp);
+    cpx* phi = cnew(Nx);
+    double *H = dnew(Nx), *gH = dnew(Nx), *gD = dnew(Nx), *coshH = dnew(Nx), *tanhH = dnew(Nx);
+    for (int j = 0; j < Nx; j++) {
+        H[j] = (eta[j] + c->depth[j]);
+        const double gm = or_cspline_eval(NH + 1, Htot, gHm0, cHm, H[j]);
+        const double gp = or_cspline_eval(NH + 1, Htot, gHp0, cHp, H[j]);
+        coshH[j] = gm * cosh(k[j] * Hmin) + gp * cosh(k[j] * Hplus);
+        tanhH[j] = gm * tanh(k[j] * Hmin) + gp * tanh(k[j] * Hplus);
+        if (k[j] == 0) { phi[j].re = 0; phi[j].im = 0; }
+        else { phi[j].re = (uh[j].im) / k[j]; phi[j].im = -(uh[j].re) / k[j]; }
+    }
+    gradient1(H, c->dx, Nx, gH);
+    gradient1(c->depth, c->dx, Nx, gD);
+    const int flatb = (c->kin_minD == c->kin_maxD);
+    double *DZ = dnew(Nx), *coshZ = dnew(Nx), *sinhZ = dnew(Nx);
+    cpx *fa = cnew(Nx), *ft = cnew(Nx), *fx = cnew(Nx), *fz = cnew(Nx);
+    double *fac = dnew(Nx), *tdt = dnew(Nx), *tdx = dnew(Nx), *tdz = dnew(Nx);
+    for (int zz = 0; zz < nz; zz++) {
+        const double zo = c->kin_z[zz];
+        if (flatb) {
+            for (int j = 0; j < Nx; j++) {
+                coshZ[j] = cosh(k[j] * (zo + c->depth[0]));
+                sinhZ[j] = sinh(k[j] * (zo + c->depth[0]));
+            }
+        } else {
+            for (int j = 0; j < Nx; j++) {
+                DZ[j] = c->depth[j] + zo;
+                if (DZ[j] < 0) DZ[j] = 0;
+            }
+            const double DZplus = search_max_val(DZ, Nx);
+            double DZmin = search_min_val(DZ, Nx);
+            if (DZmin < 0) DZmin = 0;
+            if (DZmin == DZplus) {
+                for (int j = 0; j < Nx; j++) {
+                    coshZ[j] = cosh(k[j] * (zo + c->depth[0]));
+                    sinhZ[j] = sinh(k[j] * (zo + c->depth[0]));
+                }
+            } else {
+                for (int j = 0; j < Nx; j++) {
+                    double gm = or_cspline_eval(NH + 1, DZtot, gDm0, cDm, DZ[j]);
+                    double gp = or_cspline_eval(NH + 1, DZtot, gDp0, cDp, DZ[j]);
+                    if (DZ[j] == DZmin) { gm = 1; gp = 0; }
+                    if (DZ[j] == DZplus) { gm = 0; gp = 1; }
+                    coshZ[j] = gm * cosh(k[j] * DZmin) + gp * cosh(k[j] * DZplus);
+                    sinhZ[j] = gm * sinh(k[j] * DZmin) + gp * sinh(k[j] * DZplus);
+                }
+            }
+        }
+        for (int j = 0; j < Nx; j++) {
+            const double ratio = coshZ[j] / coshH[j];
+            fa[j].re = phi[j].re * ratio * (-k[j] * tanhH[j]);
+            fa[j].im = phi[j].im * ratio * (-k[j] * tanhH[j]);
+            ft[j].re = dph[j].re * ratio;
+            ft[j].im = dph[j].im * ratio;
+            fz[j].re = phi[j].re * k[j] * sinhZ[j] / coshH[j];
+            fz[j].im = phi[j].im * k[j] * sinhZ[j] / coshH[j];
+            fx[j].re = -k[j] * phi[j].im * ratio;
+            fx[j].im = k[j] * phi[j].re * ratio;
+        }
+        ifft_cr_nx(c, fa, fac);
+        ifft_cr_nx(c, ft, tdt);
+        ifft_cr_nx(c, fz, tdz);
+        ifft_cr_nx(c, fx, tdx);
+        for (int xo = 0; xo < nxo; xo++) {
+            const int j = c->kin_i1 + xo;
+            double vt, vx, vz;
+            if ((zo > eta[j]) || (zo < -c->depth[j])) { vt = NAN; vz = NAN; vx = NAN; }
+            else {
+                vt = tdt[j] + dteta[j] * fac[j];
+                vx = tdx[j] + gH[j] * fac[j] + gD[j] * tdz[j];
+                vz = tdz[j];
+            }
+            const size_t o = (size_t)xo * nz + zz;
+            dxphi[o] = vx;
+            dzphi[o] = vz;
+            P[o] = -vt - G * zo - 0.5 * (pow(vx, 2) + 2 * vz);
+            ax[o] = (vx - 0) / (t - tprev);
+            az[o] = (vz - 0) / (t - tprev);
+        }
+    }
+    for (int xo = 0; xo < nxo; xo++) eta_cut[xo] = eta[c->kin_i1 + xo];
+    void* ps[] = {eh, uh, dh, dph, eta, dteta, phi, H, gH, gD, coshH, tanhH, DZ, coshZ, sinhZ, fa, ft, fx, fz, fac, tdt,
+                  tdx, tdz};
+    for (size_t i = 0; i < sizeof ps / sizeof ps[0]; i++) free(ps[i]);
+    return 0;
 }

@@ -64,6 +64,16 @@ const char* or_breaking_log(const or_ctx* c);
 /* Reset breaking state and counters (new run on the same tables). */
 void   or_reset(or_ctx* c);
 
+/* Kinematics (kinematic_modul, 1d/kinematic_modul.c) on the overlay window
+ * [xinterv1, xinterv2] x zoutIP of a deck with "kinematic yes": sizes, grid,
+ * and the fields at time t for the state y and its RHS dy (reference layout),
+ * with the reference's tprev.  Outputs are [nx_out][nz_out] (x-major) except
+ * eta_cut [nx_out].  Returns 0, or -1 when the deck has no kinematics. */
+int    or_kin_dims(const or_ctx* c, int* nx_out, int* nz_out);
+int    or_kin_grid(const or_ctx* c, double* xout, double* zout);
+int    or_kinematics(or_ctx* c, double t, double tprev, const double* y, const double* dy, double* eta_cut,
+                     double* P, double* dxphi, double* dzphi, double* dtdxphi, double* dtdzphi);
+
 /* Plain FFT utilities (FFTW sign convention, unnormalised), exposed for tests. */
 void   or_fft(int n, const double* re_in, const double* im_in, double* re_out, double* im_out, int sign);
 

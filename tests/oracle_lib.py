@@ -81,6 +81,9 @@ def lib():
         L.or_mlp_nparams.restype = ip
         L.or_mlp_loss_grad.restype = ctypes.c_double
         L.or_mlp_loss_grad.argtypes = [dp, ctypes.POINTER(ctypes.c_float), ip, dp]
+        L.or_kin_dims.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        L.or_kin_grid.argtypes = [vp, dp, dp]
+        L.or_kinematics.argtypes = [vp, ctypes.c_double, ctypes.c_double, dp, dp, dp, dp, dp, dp, dp, dp]
         L.or2d_create.restype = vp
         L.or2d_create.argtypes = [ctypes.POINTER(Or2dTables), ctypes.c_double, ctypes.c_double]
         L.or2d_destroy.argtypes = [vp]
@@ -142,6 +145,27 @@ class Oracle:
         y = np.zeros(4 * self.nx)
         lib().or_initial_state(self.h, _p(y))
         return y
+
+    def kinematics(self, t, tprev, y, dy):
+        """kinematic_modul at t for the state y and its RHS dy: dict of eta_cut [nx_out],
+        P, dxphi, dzphi, dtdxphi, dtdzphi [nx_out, nz_out], x_out, z_out."""
+        L = lib()
+        a, b = ctypes.c_int(), ctypes.c_int()
+        if L.or_kin_dims(self.h, ctypes.byref(a), ctypes.byref(b)):
+            raise RuntimeError("oracle: the deck has no kinematics")
+        nxo, nz = a.value, b.value
+        xo, zo = np.zeros(nxo), np.zeros(nz)
+        L.or_kin_grid(self.h, _p(xo), _p(zo))
+        out = {k: np.zeros(nxo * nz) for k in ("P", "dxphi", "dzphi", "dtdxphi", "dtdzphi")}
+        ec = np.zeros(nxo)
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        dy = np.ascontiguousarray(dy, dtype=np.float64)
+        if L.or_kinematics(self.h, float(t), float(tprev), _p(y), _p(dy), _p(ec), _p(out["P"]), _p(out["dxphi"]),
+                           _p(out["dzphi"]), _p(out["dtdxphi"]), _p(out["dtdzphi"])):
+            raise RuntimeError("oracle: " + L.or_last_error().decode())
+        res = {k: v.reshape(nxo, nz) for k, v in out.items()}
+        res.update(eta_cut=ec, x_out=xo, z_out=zo)
+        return res
 
     def rhs(self, t, y):
         y = np.ascontiguousarray(y, dtype=np.float64)
