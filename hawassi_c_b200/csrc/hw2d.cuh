@@ -464,6 +464,11 @@ k2_colB(Tab2 tb, Work2 w, const Ctl2* __restrict__ ctl, int cond) {
       const double eta = P1.x * invN, lphi = P1.y * invN;
       const double u = P2.x * invN, m0u = P2.y * invN;
       const double v = P3.x * invN, m0v = P3.y * invN;
+      if (w.phys) {   // kept for the breaking kernels
+        w.phys[q] = eta;
+        w.phys[n + q] = u;
+        w.phys[2 * n + q] = v;
+      }
       const double dmp = tb.damp[q];
       // Q1 = dampeta + i dampu, Q2 = dampv + i deletaH2, Q3 = etaM0u + i eta u, Q4 = etaM0v + i eta v
       put(sm, M, 0 + k, y, make_double2(dmp * eta, dmp * u));

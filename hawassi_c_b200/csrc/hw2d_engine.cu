@@ -213,18 +213,7 @@ struct hw2d_ctx {
       if (!tb.chi_one || tb.has_src) col_dispatch(ny, 3, cols, s, tb, w, ctl, cond);
       row_dispatch(nx, 4, rows, s, tb, w, rk, ctl, ctl, mode, cond, out);
       per_rhs = ((!tb.chi_one || tb.has_src) ? 9 : 8) + 1;
-      if (brk.on) {
-        const int gb = (int)std::min<size_t>((n + 255) / 256, 4 * 148);
-        brk_row(nx, 0, rows, s, tb, w, brk, rk, ctl, mode, cond, out);
-        brk_col(ny, 0, cols, s, tb, w, brk, ctl, mode, cond);
-        hw2d::k2b_peaks<<<gb, 256, 0, s>>>(tb, w, brk, ctl, mode, cond);
-        hw2d::k2b_sort<<<1, hw2d::kBrkSortThreads, 0, s>>>(brk, ctl, mode, cond);
-        hw2d::k2b_machine<<<1, 32, 0, s>>>(tb, w, brk, ctl, mode, cond);
-        hw2d::k2b_flux<<<gb, 256, 0, s>>>(tb, w, brk, ctl, mode, cond);
-        brk_col(ny, 1, cols, s, tb, w, brk, ctl, mode, cond);
-        brk_row(nx, 1, rows, s, tb, w, brk, rk, ctl, mode, cond, out);
-        per_rhs += 8;
-      }
+      if (brk.on) brk_launch(mode, cond, s, out);
       return;
     }
     row_dispatch(nx, 0, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
@@ -233,6 +222,21 @@ struct hw2d_ctx {
     if (!tb.chi_one || tb.has_src) col_dispatch(ny, 3, cols, s, tb, w, ctl, cond);
     row_dispatch(nx, 4, rows, s, tb, w, rk, ctl, ctl, mode, cond, out);
     per_rhs = ((!tb.chi_one || tb.has_src) ? 5 : 4) + 1;
+    if (brk.on) brk_launch(mode, cond, s, out);
+  }
+  // the breaking kernels after the assembly pass (both bottoms)
+  void brk_launch(int mode, int cond, cudaStream_t s, double2* out) {
+    const int rows = ny / 2, cols = nx / 2;
+    const int gb = (int)std::min<size_t>((n + 255) / 256, 4 * 148);
+    brk_row(nx, 0, rows, s, tb, w, brk, rk, ctl, mode, cond, out);
+    brk_col(ny, 0, cols, s, tb, w, brk, ctl, mode, cond);
+    hw2d::k2b_peaks<<<gb, 256, 0, s>>>(tb, w, brk, ctl, mode, cond);
+    hw2d::k2b_sort<<<1, hw2d::kBrkSortThreads, 0, s>>>(brk, ctl, mode, cond);
+    hw2d::k2b_machine<<<1, 32, 0, s>>>(tb, w, brk, ctl, mode, cond);
+    hw2d::k2b_flux<<<gb, 256, 0, s>>>(tb, w, brk, ctl, mode, cond);
+    brk_col(ny, 1, cols, s, tb, w, brk, ctl, mode, cond);
+    brk_row(nx, 1, rows, s, tb, w, brk, rk, ctl, mode, cond, out);
+    per_rhs += 8;
   }
   long long kernels_per_attempt() const { return 7LL * per_rhs + 3; }
   void attempt_launch(cudaStream_t s) {
@@ -443,11 +447,6 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
 
   hw2d::Brk2& bk = c->brk;
   if (t->breaking) {
-    if (!var) {
-      g_err2d = "hw2d_create: breaking is built for the two-depth (varying-bottom) RHS only";
-      delete c;
-      return nullptr;
-    }
     if (!t->bathy || !t->brchar || !t->x || !t->y || !(t->dx > 0) || !(t->dy > 0) || !(t->dt_out > 0) ||
         !(t->rsearch > 0)) {
       g_err2d = "hw2d_create: breaking tables missing or invalid";
@@ -500,6 +499,7 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
   w.z = c->dalloc<double2>(3 * n);
   w.R = c->dalloc<double2>(4 * n);
   w.Q = c->dalloc<double2>((var ? 6 : 4) * n);
+  if (!var && bk.on) w.phys = c->dalloc<double>(3 * n);   // eta, u, v for the breaking kernels
   if (var) {
     w.phys = c->dalloc<double>(3 * n);
     w.pe = c->dalloc<double>(2 * n);
@@ -522,7 +522,7 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
   c->ctl = c->dalloc<Ctl2>(1);
   bool ok = tb.kx && tb.ky && tb.c2g && tb.l2d && tb.aal && tb.damp && tb.chi && tb.twx && tb.twy && w.z && w.R &&
             w.Q && w.D && w.V && w.insig && w.insigs && w.part && c->dref && c->dout && c->ctl &&
-            (chi_one || w.W) && (!has_src || (tb.gx && tb.sx && tb.sig && w.src)) && (!bk.on || w.dph) &&
+            (chi_one || w.W) && (!has_src || (tb.gx && tb.sx && tb.sig && w.src)) && (!bk.on || (w.dph && w.phys)) &&
             (!var || (tb.gmin && tb.gplus && tb.cmin && tb.cplus && tb.omin && tb.oplus && w.phys && w.pe && w.H1 &&
                       w.EU)) && (!t->wallchar || tb.wallchar);
   for (int i = 0; i < 2; ++i) ok = ok && rk.y[i] && rk.kk[i];

@@ -337,7 +337,7 @@ def tables(nx=1024, ny=1024, Lx=300.0, Ly=300.0, depth=3.0, Hs=0.5, Tp=6.0, gamm
     depth everywhere (rhs_AB2_2DF_uv); "shoal": `depth` offshore sloping to
     `shallow` with a seeded shoal, two reference depths (rhs_AB2_2DB_uv).
     breaking=True adds the kinematic-breaking tables of parambreak
-    (2d/breaking.c:1-44) with the deck's KBC, TC, Tchar (two-depth tables only)."""
+    (2d/breaking.c:1-44) with the deck's KBC, TC, Tchar."""
     x = np.linspace(0.0, Lx, nx)          # fun_intervaltovector (2d/functions1.c:204)
     y = np.linspace(0.0, Ly, ny)
     kx = freqspace(x[-1] - x[0], nx)
@@ -382,14 +382,16 @@ def tables(nx=1024, ny=1024, Lx=300.0, Ly=300.0, depth=3.0, Hs=0.5, Tp=6.0, gamm
         extra["depth"] = f64(depth_field)
     if breaking:
         if depth_field is None:
-            raise ValueError("breaking needs the two-depth (varying-bottom) tables")
+            depth_field_b = np.full((ny, nx), float(depth))
+        else:
+            depth_field_b = depth_field
         # pb.Char: cfSA (min with the wall's cfSAwall, 2d/functions.c:1960-1967), zero
         # where cfSA < 1 or ChiAdj < 1 (2d/breaking.c:10-21)
         cf = cfsa2d(x, y, damp, damp, damp, damp)
         if wall is not None:
             cf = np.minimum(cf, cfw)
         brchar = np.where((cf < 1) | (chi < 1), 0.0, cf)
-        extra.update(breaking=1, bathy=f64(-depth_field), brchar=f64(brchar), dx=float(x[1] - x[0]),
+        extra.update(breaking=1, bathy=f64(-depth_field_b), brchar=f64(brchar), dx=float(x[1] - x[0]),
                      dy=float(y[1] - y[0]), max_eta_init=Hs / 2.0 * 0.9, tstar=tchar * Tp,
                      rsearch=2 * math.pi / kp / 4.0, kbc=float(kbc), tc=float(tc), delb=1.5, cur_u=0.0,
                      t0=0.0)
@@ -407,7 +409,7 @@ def config5(seed=0, bathymetry="shoal", **kw) -> dict:
     3 m bottom and no wall), a harbour breakwater (x 200-206 m, y 90-210 m) of
     reflection coefficient 0.5, directional JONSWAP Hs 0.5 m Tp 6 s gamma 3.3,
     cos^2s spreading s = 10, 256 x 64 seeded components, HS2 with kinematic
-    breaking (KBC 0.8, TC 0.2, Tchar 0.5; two-depth tables only), 30 m damping
+    breaking (KBC 0.8, TC 0.2, Tchar 0.5), 30 m damping
     zones, influx line at x = 45 m."""
     if bathymetry == "flat":
         return tables(seed=seed, **kw)

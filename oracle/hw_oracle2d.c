@@ -169,7 +169,7 @@ or2d_ctx* or2d_create(const or2d_tables* tb, double eps_abs, double eps_rel) {
         c->wallchar = dup(tb->wallchar, n);
     }
     if (tb->breaking) {
-        if (!c->var) { set_err2("or2d_create: breaking is restated for the varying-bottom RHS only"); free(c); return NULL; }
+        if (c->model != 2) { set_err2("or2d_create: breaking is restated for the HS2 RHS only"); free(c); return NULL; }
         if (!tb->bathy || !tb->brchar || !tb->x || !tb->y) { set_err2("or2d_create: breaking tables missing"); free(c); return NULL; }
         c->brk = brk_create(tb);
     }
@@ -880,8 +880,8 @@ static int rhs_2db(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
 
 /* rhs_AB1_2DF_uv / rhs_AB2_2DF_uv (2d/fun_odesolver.c:4404-4540) with the term
  * functions fun_delphiH1hat (no wall, :2270-2283), fun_termshat_AB1_2DF_uv
- * (:2962-3027) and fun_termshat_AB2_2DF_uv (:3136-3325); no friction, coupling,
- * breaking or wall. */
+ * (:2962-3027) and fun_termshat_AB2_2DF_uv (:3136-3325), kinematic breaking when the
+ * tables ask for it (HS2); no friction, coupling or wall. */
 int or2d_rhs(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
     if (c->var) return rhs_2db(c, t, Zhat, dt_Zhat);
     const int Nx = c->nx, Ny = c->ny, n = c->n;
@@ -987,25 +987,41 @@ int or2d_rhs(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
     cx* Source_hat = malloc(sizeof(cx) * n);
     fun_source(c, t, Source_hat);
 
+    cx* dphi = malloc(sizeof(cx) * n);   /* delphiH_hat (2d/fun_odesolver.c:4480-4486) */
+    for (int q = 0; q < n; q++) {
+        dphi[q] = delphiH1hat[q];
+        if (c->model == 2) {
+            dphi[q].re = delphiH1hat[q].re + deluH2adj[q].re + delvH2adj[q].re;
+            dphi[q].im = delphiH1hat[q].im + deluH2adj[q].im + delvH2adj[q].im;
+        }
+    }
+    /* breaking (:4494-4502), as in the varying-bottom RHS */
+    static const cx zero = {0.0, 0.0};
+    if (c->brk) {
+        memset(c->brk->B, 0, sizeof(double) * n);
+        if (c->brk->tprev < t) {
+            brk_process(c, t, Zhat, eta, u, v);
+            brk_force(c, eta, dphi);
+        }
+    }
     for (int i = 0; i < Ny; i++)
         for (int j = 0; j < Nx; j++) {
             const int q = i * Nx + j;
             const double a = c->aal[q];
-            cx dphi = delphiH1hat[q];
             cx ix = {0, 0}, iy = {0, 0};
             if (c->model == 2) {
-                dphi.re = delphiH1hat[q].re + deluH2adj[q].re + delvH2adj[q].re;
-                dphi.im = delphiH1hat[q].im + deluH2adj[q].im + delvH2adj[q].im;
                 ix = ikxH2adj[q];
                 iy = ikyH2adj[q];
             }
-            dt_Zhat[q] = (Source_hat[q].re + dphi.re - dampeta[q].re) * a;
-            dt_Zhat[n + q] = (Source_hat[q].im + dphi.im - dampeta[q].im) * a;
-            dt_Zhat[2 * n + q] = (GRAV * kx[j] * Zhat[n + q] - ix.re - dampu[q].re) * a;
-            dt_Zhat[3 * n + q] = (-GRAV * kx[j] * Zhat[q] - ix.im - dampu[q].im) * a;
-            dt_Zhat[4 * n + q] = (GRAV * ky[i] * Zhat[n + q] - iy.re - dampv[q].re) * a;
-            dt_Zhat[5 * n + q] = (-GRAV * ky[i] * Zhat[q] - iy.im - dampv[q].im) * a;
+            const cx sbx = c->brk ? c->brk->sbx[q] : zero, sby = c->brk ? c->brk->sby[q] : zero;
+            dt_Zhat[q] = (Source_hat[q].re + dphi[q].re - dampeta[q].re) * a;
+            dt_Zhat[n + q] = (Source_hat[q].im + dphi[q].im - dampeta[q].im) * a;
+            dt_Zhat[2 * n + q] = (GRAV * kx[j] * Zhat[n + q] + sbx.re - ix.re - dampu[q].re) * a;
+            dt_Zhat[3 * n + q] = (-GRAV * kx[j] * Zhat[q] + sbx.im - ix.im - dampu[q].im) * a;
+            dt_Zhat[4 * n + q] = (GRAV * ky[i] * Zhat[n + q] + sby.re - iy.re - dampv[q].re) * a;
+            dt_Zhat[5 * n + q] = (-GRAV * ky[i] * Zhat[q] + sby.im - iy.im - dampv[q].im) * a;
         }
+    free(dphi);
 
     free(delphiH1hat); free(eta); free(u); free(v); free(Lphi); free(M0u); free(M0v);
     free(dampeta); free(dampu); free(dampv); free(etaM0u); free(eta_u); free(etaM0v); free(eta_v);

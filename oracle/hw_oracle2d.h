@@ -50,8 +50,8 @@ typedef struct or2d_tables {
     const double* om2_min;      /* [ny*nx] Oprt.InterpD.Om2dSq_min             */
     const double* om2_plus;     /* [ny*nx] Oprt.InterpD.Om2dSq_plus            */
     const double* wallchar;     /* [ny*nx] dominfo.wallchar, NULL: no wall (varying bottom only) */
-    /* kinematic breaking (2d/breaking.c; fun_sbreaking 2d/fun_odesolver.c:985-1019), varying
-     * bottom only; breaking = 0 leaves every field below unread */
+    /* kinematic breaking (2d/breaking.c; fun_sbreaking 2d/fun_odesolver.c:985-1019), HS2
+     * (flat or two-depth bottom); breaking = 0 leaves every field below unread */
     int breaking;
     const double* bathy;        /* [ny*nx] dominfo.bathy.data (= -depth)        */
     const double* brchar;       /* [ny*nx] pb.Char: cfSA, 0 where cfSA < 1 or ChiAdj < 1 */

@@ -41,9 +41,9 @@ def check_fields(eng, ora, tol=1e-8):
     return fo
 
 
-@pytest.mark.parametrize("nx,ny", [(64, 64), (128, 64)])
-def test_breaking_evolve_parity(nx, ny):
-    tb, z = steep_crest_case(nx, ny)
+@pytest.mark.parametrize("nx,ny,bottom", [(64, 64, "shoal"), (128, 64, "shoal"), (64, 128, "flat")])
+def test_breaking_evolve_parity(nx, ny, bottom):
+    tb, z = steep_crest_case(nx, ny, bathymetry=bottom)
     eng, ora = Engine2D(tb, EPS_ABS, EPS_REL), Oracle2D(tb, EPS_ABS, EPS_REL)
     t0, h0 = 0.3, 0.005
     eng.set_state(t0, h0, z)
