@@ -685,9 +685,15 @@ k2_rowE(Tab2 tb, Work2 w, RK2 rk, const Ctl2* __restrict__ ctl, int mode, int co
         const double2 du1 = make_double2(cg * zu.x, cg * zu.y), dv1 = make_double2(cg * zv.x, cg * zv.y);
         dphi = make_double2(kxv * du1.y + kyv * dv1.y, -kxv * du1.x - kyv * dv1.x);
       }
-      const double2 ix = slot(sm, M, 0 + k, j), iy = slot(sm, M, 2 + k, j);
-      const double2 au = slot(sm, M, 4 + k, j), av = slot(sm, M, 6 + k, j);
-      dphi = make_double2(dphi.x + au.x + av.x, dphi.y + au.y + av.y);
+      double2 ix = slot(sm, M, 0 + k, j), iy = slot(sm, M, 2 + k, j);
+      if (tb.model == 2) {
+        const double2 au = slot(sm, M, 4 + k, j), av = slot(sm, M, 6 + k, j);
+        dphi = make_double2(dphi.x + au.x + av.x, dphi.y + au.y + av.y);
+      } else {
+        // HS1 (rhs_AB1_2DF_uv, 2d/fun_odesolver.c:4404-4456): no H2 terms
+        ix = make_double2(0.0, 0.0);
+        iy = make_double2(0.0, 0.0);
+      }
       if (w.dph) w.dph[q] = dphi;
       const double2 S = tb.has_src ? w.src[q] : make_double2(0.0, 0.0);
       const double2 de = w.D[q], du = w.D[n + q], dv = w.D[2 * n + q];

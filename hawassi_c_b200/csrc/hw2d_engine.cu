@@ -339,8 +339,13 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
     g_err2d = "hw2d_create: nx and ny must be powers of two in [64, 1024]";
     return nullptr;
   }
-  if (t->model != 2) {
-    g_err2d = "hw2d_create: only the HS2 model is built on the device";
+  if (t->model != 1 && t->model != 2) {
+    g_err2d = "hw2d_create: the device builds HS1 (flat bottom) and HS2";
+    return nullptr;
+  }
+  const bool var_tables = t->gam_min && t->gam_plus && t->csq_min && t->csq_plus && t->om2_min && t->om2_plus;
+  if (t->model == 1 && (var_tables || t->breaking || t->wallchar)) {
+    g_err2d = "hw2d_create: HS1 is built for the flat bottom without walls or breaking (rhs_AB1_2DF_uv)";
     return nullptr;
   }
   if (t->propagation < 0 || t->propagation > 2) {

@@ -9,10 +9,10 @@ from oracle_lib import Oracle2D
 pytestmark = pytest.mark.gpu
 
 
-def tables(nx, ny, nadj=1.0, propagation=0, seed=1, source=True, bathymetry="flat", walls=()):
+def tables(nx, ny, nadj=1.0, propagation=0, seed=1, source=True, bathymetry="flat", walls=(), model=2):
     tb = decks2d.tables(nx=nx, ny=ny, Lx=0.9 * nx, Ly=0.9 * ny, depth=2.0, shallow=0.6, Hs=0.1, Tp=3.0, n_freq=24,
                         n_dir=6, t_end=6.0, dt=0.1, damp=6.0, x_line=10.0, nadj=nadj, propagation=propagation,
-                        seed=seed, bathymetry=bathymetry, walls=walls)
+                        seed=seed, bathymetry=bathymetry, walls=walls, model=model)
     if not source:
         for k in ("newgam", "skewgam", "tsig", "sig", "sigskew"):
             tb[k] = None
@@ -176,3 +176,26 @@ def test_wall_on_flat_bottom_rejected():
     tb["wallchar"] = np.ones(64 * 64)
     with pytest.raises(Exception):
         Engine2D(tb)
+
+
+@pytest.mark.parametrize("nx,ny,prop", [(64, 64, 0), (128, 64, 2)])
+def test_rhs_parity_hs1(nx, ny, prop):
+    """HS1 (rhs_AB1_2DF_uv): the linear model with damping and source."""
+    tb = tables(nx, ny, propagation=prop, model=1)
+    eng, ora = Engine2D(tb, 1e-8, 1e-6), Oracle2D(tb, 1e-8, 1e-6)
+    y = band_limited_state(tb, 0.02, 3)
+    assert rel(eng.rhs(0.8, y), ora.rhs(0.8, y)) < 1e-11
+
+
+def test_run_to_time_parity_hs1():
+    tb = tables(64, 64, model=1)
+    eng, ora = Engine2D(tb, 1e-8, 1e-6), Oracle2D(tb, 1e-8, 1e-6)
+    y = np.zeros(6 * tb["nx"] * tb["ny"])
+    eng.set_state(0.0, 0.02, y)
+    to, ho = ora.run_to(0.0, 3.0, 0.02, y)
+    eng.run_to_time(3.0)
+    tg, hg, yg = eng.state()
+    assert tg == 3.0 and rel(yg, y) < 1e-9
+    sg, so = eng.stats(), ora.stats()
+    assert sg["accepted"] == so["accepted"] and sg["rejected"] == so["rejected"]
+
