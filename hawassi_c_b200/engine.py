@@ -354,6 +354,38 @@ class Engine:
         self._check(load_library().hw_synchronize(self._h), "synchronize")
 
 
+class HwJonswap(ctypes.Structure):
+    _fields_ = [("T0", ctypes.c_double), ("Tend", ctypes.c_double), ("dt", ctypes.c_double),
+                ("Tp", ctypes.c_double), ("Hs", ctypes.c_double), ("gamma", ctypes.c_double),
+                ("nTramp", ctypes.c_double), ("seed", ctypes.c_ulonglong)]
+
+
+def jonswap_influx(specs, device=0):
+    """Seeded JONSWAP influx signals of many members in one device launch
+    (hw_jonswap_influx).  specs: dicts with T0, Tend, dt, Tp, Hs, gamma, nTramp, seed.
+    Returns one array per member (samples at T0 + j dt)."""
+    L = load_library()
+    if not getattr(L, "_js_bound", False):
+        L.hw_jonswap_influx.restype = ctypes.c_int
+        L.hw_jonswap_influx.argtypes = [ctypes.POINTER(HwJonswap), ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                        ctypes.c_longlong, ctypes.c_int]
+        L._js_bound = True
+    arr = (HwJonswap * len(specs))(*[HwJonswap(**{k: (int(v) if k == "seed" else float(v)) for k, v in sp.items()})
+                                    for sp in specs])
+    total = L.hw_jonswap_influx(arr, len(specs), None, 0, device)
+    if total < 0:
+        raise EngineError("hw_jonswap_influx: invalid specification")
+    out = np.zeros(total)
+    if L.hw_jonswap_influx(arr, len(specs), _dp(out), total, device) != total:
+        raise EngineError("hw_jonswap_influx failed")
+    res, off = [], 0
+    for sp in specs:
+        nt = int((sp["Tend"] - sp["T0"]) / sp["dt"] + 1)
+        res.append(out[off:off + nt])
+        off += nt
+    return res
+
+
 def deck_table(deck, name, seed=0, nref=0):
     """Host-side set-up table of a deck (no GPU involved)."""
     L = load_library()

@@ -107,6 +107,20 @@ int hw_last_dydt(hw_ctx* ctx, int member, double* dydt);
  * written, *len receives the number of doubles. */
 int hw_breaking_log(hw_ctx* ctx, int member, double* out, long long cap, long long* len);
 
+/* Seeded JONSWAP influx signals of many members in one device launch
+ * (jonswap_influx, 1d/influx_lib.c:137-255; srand(time(0)) replaced by a seeded
+ * splitmix64 stream, the spectrum's integer exponent 5/4 and the phase
+ * off-by-one kept).  Member m's signal has Nt_m = int((Tend - T0)/dt + 1) samples
+ * at T0 + j dt; the signals are concatenated in member order into eta_out.
+ * Returns the total sample count (writes only when cap covers it), -1 on error. */
+typedef struct hw_jonswap {
+    double T0, Tend, dt;        /* the deck's time block                        */
+    double Tp, Hs, gamma;       /* spectrum                                     */
+    double nTramp;              /* ramp length in peak periods (0: ramp "no")   */
+    unsigned long long seed;
+} hw_jonswap;
+int hw_jonswap_influx(const hw_jonswap* specs, int n, double* eta_out, long long cap, int device);
+
 /* Kinematics of a member whose deck has "kinematic yes" (kinematic_modul,
  * 1d/kinematic_modul.c:1-247; grid of read_kinematics, 1d/functions.c:3555-3669):
  * at the member's current time, from its state and the last RHS (the reference's

@@ -583,6 +583,53 @@ static double* fun_jonswap(const double* omg, double omgp, double gamJS, double 
     return out;
 }
 
+/* jonswap_influx (1d/influx_lib.c:289) with seeded phases: the JONSWAP spectrum on
+ * Nt/2 lines (fun_jonswap), random phases (the reference's off-by-one kept: line
+ * i+1 takes phase[i], phase[0] = 0), the inverse transform, the start/end ramps and
+ * the normalisation to Hs / (4 sqrt(variance)). */
+static void jonswap_synth(double T0, double lenT, double dt, double Tp, double Hs, double gamJS, double nTramp,
+                          unsigned long long seed, int Nt, double* eta) {
+    const double omgp = 2 * PI / Tp;
+    double* omsig = (double*)malloc(sizeof(double) * (size_t)Nt);
+    freqspace(omsig, lenT, Nt);
+    double* JS = fun_jonswap(omsig, omgp, gamJS, Hs, Nt);
+    double* phase = (double*)calloc((size_t)(Nt / 2 + 1), sizeof(double));
+    cpx* rh = (cpx*)calloc((size_t)Nt, sizeof(cpx));
+    unsigned long long s = seed;
+    for (int i = 0; i < Nt / 2; i++) {
+        phase[i + 1] = 2 * PI * sm64_uniform(&s);
+        rh[i + 1].re = (sqrt(JS[i]) * cos(phase[i])) / dt * 2 * pow(PI, 2);
+        rh[i + 1].im = -(sqrt(JS[i]) * sin(phase[i])) / dt * 2 * pow(PI, 2);
+        rh[Nt - 1 - i].re = rh[i + 1].re;
+        rh[Nt - 1 - i].im = -rh[i + 1].im;
+    }
+    rh[0].re = 0; rh[0].im = 0;
+    double* raw = (double*)malloc(sizeof(double) * (size_t)Nt);
+    ifft_complex_real(rh, raw, Nt);
+    double* ramp = (double*)malloc(sizeof(double) * (size_t)Nt);
+    for (int j = 0; j < Nt; j++) {
+        double tin = T0 + j * dt;
+        double A = ((tin - T0) - nTramp * Tp);
+        double B1 = A / fabs(A);
+        double B2 = (1 - cos((tin - T0) * PI / nTramp / Tp)) / 2;
+        ramp[j] = B1 > B2 ? B1 : B2;
+    }
+    double* ins = (double*)malloc(sizeof(double) * (size_t)Nt);
+    for (int j = 0; j < Nt; j++) ins[j] = ramp[j] * raw[j] * ramp[Nt - 1 - j];
+    double v = var_array(ins, Nt, mean_array(ins, Nt));
+    for (int j = 0; j < Nt; j++) eta[j] = ins[j] * Hs / (4 * sqrt(v));
+    free(omsig); free(JS); free(phase); free(rh); free(raw); free(ramp); free(ins);
+}
+
+int or_jonswap_signal(double T0, double Tend, double dt, double Tp, double Hs, double gamma, double nTramp,
+                      unsigned long long seed, double* eta_out, int cap) {
+    const double lenT = Tend - T0;
+    const int Nt = (int)((lenT) / dt + 1);
+    if (Nt < 4) return -1;
+    if (eta_out && cap >= Nt) jonswap_synth(T0, lenT, dt, Tp, Hs, gamma, nTramp, seed, Nt, eta_out);
+    return Nt;
+}
+
 /* influxlib (1d/influx_lib.c:1-109) + harmonic/jonswap synthesis */
 static int influxlib(or_ctx* c, const char* dir) {
     char path[1024], line[256];
@@ -638,40 +685,11 @@ static int influxlib(or_ctx* c, const char* dir) {
         }
         c->n = i;
     } else if (!strcmp(c->wavename, "jonswap")) {
-        /* jonswap_influx (1d/influx_lib.c:289) with seeded phases */
-        int Nt = c->Nt;
-        double* omsig = (double*)malloc(sizeof(double) * (size_t)Nt);
-        freqspace(omsig, c->lenT, Nt);
-        double* JS = fun_jonswap(omsig, c->omgp, c->gamJS, c->Hs, Nt);
-        double* phase = (double*)calloc((size_t)(Nt / 2 + 1), sizeof(double));
-        cpx* rh = (cpx*)calloc((size_t)Nt, sizeof(cpx));
-        unsigned long long s = c->seed;
-        for (int i = 0; i < Nt / 2; i++) {
-            phase[i + 1] = 2 * PI * sm64_uniform(&s);
-            rh[i + 1].re = (sqrt(JS[i]) * cos(phase[i])) / c->dt * 2 * pow(PI, 2);
-            rh[i + 1].im = -(sqrt(JS[i]) * sin(phase[i])) / c->dt * 2 * pow(PI, 2);
-            rh[Nt - 1 - i].re = rh[i + 1].re;
-            rh[Nt - 1 - i].im = -rh[i + 1].im;
-        }
-        rh[0].re = 0; rh[0].im = 0;
-        double* raw = (double*)malloc(sizeof(double) * (size_t)Nt);
-        ifft_complex_real(rh, raw, Nt);
-        double* ramp = (double*)malloc(sizeof(double) * (size_t)Nt);
-        for (int j = 0; j < Nt; j++) {
-            double tin = c->T0 + j * c->dt;
-            double A = ((tin - c->T0) - c->nTramp * c->Tp);
-            double B1 = A / fabs(A);
-            double B2 = (1 - cos((tin - c->T0) * PI / c->nTramp / c->Tp)) / 2;
-            ramp[j] = B1 > B2 ? B1 : B2;
-        }
-        double* ins = (double*)malloc(sizeof(double) * (size_t)Nt);
-        for (int j = 0; j < Nt; j++) ins[j] = ramp[j] * raw[j] * ramp[Nt - 1 - j];
-        double v = var_array(ins, Nt, mean_array(ins, Nt));
-        c->n = Nt;
-        c->wave_t = (double*)malloc(sizeof(double) * (size_t)Nt);
-        c->wave_eta = (double*)malloc(sizeof(double) * (size_t)Nt);
-        for (int j = 0; j < Nt; j++) { c->wave_t[j] = c->T0 + j * c->dt; c->wave_eta[j] = ins[j] * c->Hs / (4 * sqrt(v)); }
-        free(omsig); free(JS); free(phase); free(rh); free(raw); free(ramp); free(ins);
+        c->n = c->Nt;
+        c->wave_t = (double*)malloc(sizeof(double) * (size_t)c->Nt);
+        c->wave_eta = (double*)malloc(sizeof(double) * (size_t)c->Nt);
+        jonswap_synth(c->T0, c->lenT, c->dt, c->Tp, c->Hs, c->gamJS, c->nTramp, c->seed, c->Nt, c->wave_eta);
+        for (int j = 0; j < c->Nt; j++) c->wave_t[j] = c->T0 + j * c->dt;
     }
     if (!known) { fclose(f); set_err("unsupported wavename '%s'", c->wavename); return -1; }
     for (int i = 0; i < 13; i++) if (!fgets(line, sizeof line, f)) break;

@@ -74,6 +74,12 @@ int    or_kin_grid(const or_ctx* c, double* xout, double* zout);
 int    or_kinematics(or_ctx* c, double t, double tprev, const double* y, const double* dy, double* eta_cut,
                      double* P, double* dxphi, double* dzphi, double* dtdxphi, double* dtdzphi);
 
+/* jonswap_influx (1d/influx_lib.c:289) with the seeded splitmix64 phases: the influx
+ * signal at T0 + j dt, j < Nt = int((Tend - T0)/dt + 1).  Returns Nt (writes eta
+ * when cap >= Nt), -1 on a too short signal. */
+int    or_jonswap_signal(double T0, double Tend, double dt, double Tp, double Hs, double gamma, double nTramp,
+                         unsigned long long seed, double* eta_out, int cap);
+
 /* Plain FFT utilities (FFTW sign convention, unnormalised), exposed for tests. */
 void   or_fft(int n, const double* re_in, const double* im_in, double* re_out, double* im_out, int sign);
 

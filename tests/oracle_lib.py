@@ -81,6 +81,7 @@ def lib():
         L.or_mlp_nparams.restype = ip
         L.or_mlp_loss_grad.restype = ctypes.c_double
         L.or_mlp_loss_grad.argtypes = [dp, ctypes.POINTER(ctypes.c_float), ip, dp]
+        L.or_jonswap_signal.argtypes = [ctypes.c_double] * 7 + [ctypes.c_ulonglong, dp, ip]
         L.or_kin_dims.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.or_kin_grid.argtypes = [vp, dp, dp]
         L.or_kinematics.argtypes = [vp, ctypes.c_double, ctypes.c_double, dp, dp, dp, dp, dp, dp, dp, dp]
@@ -332,3 +333,13 @@ def sym2(x):
     im = np.ascontiguousarray(x.imag).ravel().copy()
     lib().or2d_sym(nx, ny, _p(re), _p(im))
     return (re + 1j * im).reshape(ny, nx)
+
+
+def jonswap_signal(T0, Tend, dt, Tp, Hs, gamma, nTramp, seed):
+    """The oracle's seeded jonswap_influx (1d/influx_lib.c:137-255)."""
+    L = lib()
+    nt = L.or_jonswap_signal(T0, Tend, dt, Tp, Hs, gamma, nTramp, seed, None, 0)
+    out = np.zeros(nt)
+    L.or_jonswap_signal(T0, Tend, dt, Tp, Hs, gamma, nTramp, seed, _p(out), nt)
+    return out
+
