@@ -367,9 +367,44 @@ bool hw_ctx::init(const std::vector<std::string>& dirs, const hw_opts* o, const 
   so.h0 = opt.h0;
   so.seed = opt.seed;
   so.nref = opt.nref;
+  // jonswap decks: every member's influx signal in one device launch; member i
+  // draws its phases from seed + i
+  std::vector<std::vector<double>> js_sig(dirs.size());
+  {
+    std::vector<hw_jonswap> specs;
+    std::vector<size_t> who;
+    for (size_t i = 0; i < dirs.size(); ++i) {
+      bool isj = false;
+      hw_jonswap sp{};
+      if (!hw::jonswap_params(dirs[i], &isj, &sp.T0, &sp.Tend, &sp.dt, &sp.Tp, &sp.Hs, &sp.gamma, &sp.nTramp, err)) {
+        err = dirs[i] + ": " + err;
+        return false;
+      }
+      if (!isj) continue;
+      sp.seed = opt.seed + (unsigned long long)i;
+      specs.push_back(sp);
+      who.push_back(i);
+    }
+    if (!specs.empty()) {
+      const int total = hw_jonswap_influx(specs.data(), int(specs.size()), nullptr, 0, device);
+      std::vector<double> all(total > 0 ? size_t(total) : 0);
+      if (total <= 0 || hw_jonswap_influx(specs.data(), int(specs.size()), all.data(), total, device) != total) {
+        err = "jonswap influx synthesis on the device failed";
+        return false;
+      }
+      size_t off = 0;
+      for (size_t k = 0; k < specs.size(); ++k) {
+        const int nt = int((specs[k].Tend - specs[k].T0) / specs[k].dt + 1);
+        js_sig[who[k]].assign(all.begin() + long(off), all.begin() + long(off + size_t(nt)));
+        off += size_t(nt);
+      }
+    }
+  }
   mem.resize(dirs.size());
   for (size_t i = 0; i < dirs.size(); ++i) {
     HostMember& h = mem[i];
+    so.seed = opt.seed + (unsigned long long)i;
+    so.influx_eta = js_sig[i].empty() ? nullptr : &js_sig[i];
     if (!hw::build_member(dirs[i], so, h.m, err)) {
       err = dirs[i] + ": " + err;
       return false;

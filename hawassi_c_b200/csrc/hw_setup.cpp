@@ -326,6 +326,10 @@ bool load_influx(const std::string& dir, Member& m, std::vector<double>& wt, std
       wt.push_back(t);
       we.push_back(amp * (r1 > r2 ? r1 : r2) * (std::sin(t * 2 * kPi / d.Tp)));
     }
+  } else if (d.wavename == "jonswap" && opt.influx_eta && int(opt.influx_eta->size()) == Nt) {
+    wt.resize(Nt);
+    we = *opt.influx_eta;
+    for (int j = 0; j < Nt; ++j) wt[j] = d.T0 + j * d.dt;
   } else if (d.wavename == "jonswap") {
     const double omgp = 2 * kPi / d.Tp;
     std::vector<double> om = freqspace(lenT, Nt);
@@ -853,6 +857,24 @@ bool build_member(const std::string& dir, const SetupOptions& opt, Member& m, st
       m.y0[j] = er[j]; m.y0[j + Nx] = ei[j]; m.y0[j + 2 * Nx] = ur[j]; m.y0[j + 3 * Nx] = ui[j];
     }
   }
+  return true;
+}
+
+bool jonswap_params(const std::string& dir, bool* is_jonswap, double* T0, double* Tend, double* dt, double* Tp,
+                    double* Hs, double* gamma, double* nTramp, std::string& err) {
+  Deck d;
+  if (!parse_input(dir, d, err)) return false;
+  *is_jonswap = d.wavename == "jonswap";
+  if (!*is_jonswap) return true;
+  InputFile in(dir + "/input.txt");
+  FILE* f = in.get();
+  in.skip_lines(5, 256);
+  if (std::fscanf(f, "%*s %*s %lf \n %*s %*s %lf \n %*s %*s %lf\n", T0, Tend, dt) != 3 ||
+      std::fscanf(f, "%*s %*s %lf \n %*s %*s %lf \n %*s %*s %lf\n", Tp, Hs, gamma) != 3) {
+    err = "malformed time/spectrum block in input.txt";
+    return false;
+  }
+  *nTramp = d.rampbool == "no" ? 0.0 : d.nTramp;
   return true;
 }
 

@@ -15,7 +15,16 @@ struct SetupOptions {
   double h0 = 0.0;        // <= 0: reference 1e-4 (1d/functions.c:541)
   unsigned long long seed = 0;  // phase seed for wavename = jonswap
   int nref = 0;           // 0/3: three reference depths (Up3IP); 2: Up2IP; >3: log-spaced K refs
+  // wavename = jonswap: the influx signal already synthesised (on the device, for a
+  // whole ensemble at once); nullptr: synthesise it here
+  const std::vector<double>* influx_eta = nullptr;
 };
+
+// The time and spectrum block of a jonswap deck (1d/influx_lib.c:1-109) with the ramp
+// length (0 when ramp_influx is no, 1d/main.cc:47-49).  Returns false with err on a
+// malformed deck; *is_jonswap false for other wavenames.
+bool jonswap_params(const std::string& dir, bool* is_jonswap, double* T0, double* Tend, double* dt, double* Tp,
+                    double* Hs, double* gamma, double* nTramp, std::string& err);
 
 // Deck values as read from input.txt (1d/read_input.c:1-60, 1d/influx_lib.c:1-109).
 struct Deck {

@@ -23,7 +23,9 @@ typedef struct hw_opts {
     double eps_abs;          /* <= 0: the reference's 1e-5 (1d/functions.c:529) */
     double eps_rel;          /* <= 0: the reference's 1e-4 (1d/functions.c:530) */
     double h0;               /* <= 0: the reference's first step 1e-4 (1d/functions.c:541) */
-    unsigned long long seed; /* phase seed for wavename = jonswap (reference: srand(time(0))) */
+    unsigned long long seed; /* phase seed for wavename = jonswap (reference: srand(time(0)));
+                                member m of an ensemble uses seed + m, its signal synthesised
+                                on the device with every other jonswap member's */
     int nref;                /* varying depth: 0 or 3 = three reference depths (Up3IP), 2 = Up2IP,
                                 4..16 = that many log-spaced reference depths, each point on its
                                 bracketing pair (no counterpart in the reference) */

@@ -30,3 +30,25 @@ def test_jonswap_influx_matches_oracle():
         # normalised to Hs = 4 std
         assert abs(4 * g.std() - sp["Hs"]) < 1e-12
     assert sizes == {0, 1}
+
+
+def test_ensemble_jonswap_decks_use_device_signals(tmp_path):
+    """An ensemble of jonswap decks: member m's signal comes from the device synthesis
+    with seed + m; its RHS during the influx equals the oracle's built with that seed."""
+    import hawassi_c_b200 as hw
+    from hawassi_c_b200 import decks
+    from decks_util import random_state, rel_l2
+    paths = []
+    for m in range(3):
+        paths.append(decks.write_deck(str(tmp_path / f"js{m}"), nx=1024, length=51.2, xinflux=8.0, depth=1.0,
+                                      model="HS2", T_end=20.0, Hs=0.08, Tp=1.3 + 0.2 * m, gamma=3.3,
+                                      wavename="jonswap", damp=(4.0, 4.0), dt=0.02))
+    base = 77
+    e = hw.Engine(paths, eps_abs=1e-8, eps_rel=1e-6, seed=base, device=0)
+    y = random_state(1024, 3)
+    for m, p in enumerate(paths):
+        o = ol.Oracle(p, eps_abs=1e-8, eps_rel=1e-6, seed=base + m)
+        ref = o.rhs(9.7, y)
+        assert rel_l2(e.rhs(9.7, y, member=m), ref) < 1e-11
+        o.close()
+    e.close()
