@@ -19,9 +19,15 @@ offset by rank), no data-path collective: weak scaling.
     python bench.py --workload 2d [--steps K] [--warmup W] [--impl ours|reference]
 
 measures the 2D twin instead: 1024 x 1024 on 300 m x 300 m, depth 5 m sloping to
-0.5 m with a shoal (two reference depths), HS2, directional JONSWAP line source
-(Hs 0.5 m, Tp 6 s, s = 10, 256 x 64 seeded components), RKF45 rtol 1e-6 /
-atol 1e-8; one step advances 0.5 simulated s.
+0.5 m with a shoal (two reference depths), HS2 with kinematic breaking,
+directional JONSWAP line source (Hs 0.5 m, Tp 6 s, s = 10, 256 x 64 seeded
+components), RKF45 rtol 1e-6 / atol 1e-8; one step advances 0.5 simulated s.
+
+    python bench.py --workload fbr005 [--steps K] [--warmup W] [--impl ours|reference]
+
+runs the reference's own test deck 1dFBr005Bor (the deck its published "Relative
+time consuming" figure comes from) with the reference's tolerances and reports
+simulated seconds per wall second; one step advances 250 output samples (5 s).
 """
 import argparse
 import json
@@ -395,6 +401,156 @@ def main_2d(args, rank, world, local):
         dist.destroy_process_group()
     return 0
 
+# ----------------------------------------------------------------------------
+# The reference's published benchmark deck (1dFBr005Bor)
+# ----------------------------------------------------------------------------
+FBR_DECK = os.path.join(ROOT, "tests", "golden", "fbr005")
+FBR_STEP_SAMPLES = 250            # one bench step = 250 output samples = 5 simulated s
+FBR_PUBLISHED_SIM_PER_WALL = 1.0 / 1.09714   # logfile.txt:35 "Relative time consuming" (hardware not recorded)
+WORKLOAD_FBR = ("the reference's own test deck 1dFBr005Bor: 1D HS2, flat h = 1 m, kinematic breaking, IVP from "
+                "initial.dat, Nx = 4096 on [-215, 215] m, output every 0.02 s to t = 120 s, the reference's "
+                "tolerances (abs 1e-5, rel 1e-4) and first step 1e-4")
+
+
+def _fbr_cpu(max_seconds):
+    """The oracle port on one host thread through the deck's output samples from t0
+    for ~max_seconds: (simulated s, wall s, RHS grid points)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as ol
+    o = ol.Oracle(FBR_DECK)
+    tt = o.table("ttrace")
+    y = o.initial_state()
+    t, h = float(tt[0]), 1e-4
+    c0, w0 = o.stats()[0], time.perf_counter()
+    for ti in tt[1:]:
+        while t < ti:
+            t, h = o.evolve_apply(t, ti, h, y)
+        if time.perf_counter() - w0 > max_seconds:
+            break
+    wall = time.perf_counter() - w0
+    pts = (o.stats()[0] - c0) * o.nx
+    o.close()
+    return t - float(tt[0]), wall, pts
+
+
+def run_reference_fbr(args, rank, world):
+    if rank != 0:
+        return 0
+    sim, wall, pts = _fbr_cpu(8.0 * (args.steps + args.warmup))
+    value = sim / wall
+    line = {
+        "metric": "sim-s/wall-s", "value": value, "unit": "simulated s per wall s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / max(1, args.steps + args.warmup),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": value / FBR_PUBLISHED_SIM_PER_WALL,
+        "dtype": "f64", "data": "the reference's shipped deck (tests/golden/fbr005)",
+        "config": {"workload": WORKLOAD_FBR}, "impl": "reference", "rhs_pts_per_s": pts / wall,
+        "cpu_baseline": {"value": value, "unit": "simulated s per wall s", "cores": 1, "kind": "port",
+                         "sample": f"the first {sim:.2f} simulated s from t0 on one thread"},
+        "e2e": {"value": value, "unit": "simulated s per wall s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main_fbr(args, rank, world, local):
+    """The whole deck on one GPU (one member, replicas only under torchrun): each step
+    advances FBR_STEP_SAMPLES output samples through hw_run, the gauge and breaking
+    stages included."""
+    import numpy as np
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sim, wall, _ = _fbr_cpu(15.0)
+        cpu = {"value": sim / wall, "unit": "simulated s per wall s", "cores": 1, "kind": "port",
+               "sample": f"the first {sim:.2f} simulated s of the deck from t0 on one thread (~15 s)"}
+        log(f"cpu baseline {cpu['value']:.3f} sim-s/wall-s")
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    import hawassi_c_b200 as hw
+    eng = hw.Engine(FBR_DECK, device=local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    eng.set_stream(stream.cuda_stream)
+    nt = eng.nt[0]
+    need = (args.warmup + 2 * args.steps) * FBR_STEP_SAMPLES
+    if need >= nt:
+        raise SystemExit(f"fbr005: {args.warmup} + 2 x {args.steps} steps of {FBR_STEP_SAMPLES} samples exceed "
+                         f"the deck's {nt} samples")
+    i = 0
+    for _ in range(args.warmup):
+        i += FBR_STEP_SAMPLES
+        eng.run(i, sync=False)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    s0 = eng.stats()
+    t_start = eng.state()[0]
+    barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        i += FBR_STEP_SAMPLES
+        eng.run(i, sync=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    t_end = eng.state()[0]
+    s1 = eng.stats()
+    sim = t_end - t_start
+    pts = float((s1["rhs_calls"] - s0["rhs_calls"]) * eng.nx[0])
+    if world > 1:
+        (ms,), (sim, pts) = reduce_ranks([ms], [sim, pts], "cuda")
+    value = sim / (ms / 1e3)
+    # end to end through the public API: the state in from pinned host memory and
+    # out again every step
+    host = torch.empty(4 * eng.nx[0], dtype=torch.float64, pin_memory=True)
+    hv = host.numpy()
+    eng.get_states(hv)
+    r0, ta = eng.stats()["rhs_calls"], eng.state()[0]
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        eng.set_states(hv)
+        i += FBR_STEP_SAMPLES
+        eng.run(i, sync=False)
+        eng.get_states(hv)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ems = e0.elapsed_time(e1)
+    e2e_sim = eng.state()[0] - ta
+    e2e = {"value": e2e_sim / (ems / 1e3), "unit": "simulated s per wall s",
+           "h2d_bytes_per_step": 4 * eng.nx[0] * 8, "d2h_bytes_per_step": 4 * eng.nx[0] * 8}
+    if rank == 0:
+        line = {
+            "metric": "sim-s/wall-s", "value": value, "unit": "simulated s per wall s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": value / FBR_PUBLISHED_SIM_PER_WALL, "dtype": "f64",
+            "data": "the reference's shipped deck (tests/golden/fbr005)",
+            "config": {"workload": WORKLOAD_FBR, "step_samples": FBR_STEP_SAMPLES,
+                       "l2": "single member (512 KB state) resident in L2: latency-bound, no roofline claim"},
+            "rhs_pts_per_s": pts / (ms / 1e3), "rhs_calls": s1["rhs_calls"] - s0["rhs_calls"],
+            "accepted": s1["accepted"] - s0["accepted"], "rejected": s1["rejected"] - s0["rejected"],
+            "published_sim_s_per_wall_s": FBR_PUBLISHED_SIM_PER_WALL,
+            "roofline": None, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "gpu_launches": args.steps * (len(eng.class_timing()) + 1),   # per step: k_resume + k_evolve
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -404,7 +560,7 @@ def main():
     ap.add_argument("--members", type=int, default=MEMBERS)
     ap.add_argument("--window", type=int, default=WINDOW)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "2d"])
+    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "2d", "fbr005"])
     ap.add_argument("--autotune", action="store_true",
                     help="pick the slice per grid size by timing candidates on the device first")
     args = ap.parse_args()
@@ -417,6 +573,10 @@ def main():
         if args.impl == "reference":
             return run_reference_2d(args, rank, world)
         return main_2d(args, rank, world, local)
+    if args.workload == "fbr005":
+        if args.impl == "reference":
+            return run_reference_fbr(args, rank, world)
+        return main_fbr(args, rank, world, local)
     if args.impl == "reference":
         return run_reference(args, rank, world)
 
