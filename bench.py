@@ -470,14 +470,14 @@ def main_fbr(args, rank, world, local):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     import hawassi_c_b200 as hw
-    eng = hw.Engine(FBR_DECK, device=local)
+    eng = hw.Engine(FBR_DECK, device=local, slice=args.slice)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     eng.set_stream(stream.cuda_stream)
     nt = eng.nt[0]
-    need = (args.warmup + 2 * args.steps) * FBR_STEP_SAMPLES
+    need = (args.warmup + args.steps) * FBR_STEP_SAMPLES
     if need >= nt:
-        raise SystemExit(f"fbr005: {args.warmup} + 2 x {args.steps} steps of {FBR_STEP_SAMPLES} samples exceed "
+        raise SystemExit(f"fbr005: {args.warmup} + {args.steps} steps of {FBR_STEP_SAMPLES} samples exceed "
                          f"the deck's {nt} samples")
     i = 0
     for _ in range(args.warmup):
@@ -511,12 +511,18 @@ def main_fbr(args, rank, world, local):
     if world > 1:
         (ms,), (sim, pts) = reduce_ranks([ms], [sim, pts], "cuda")
     value = sim / (ms / 1e3)
-    # end to end through the public API: the state in from pinned host memory and
-    # out again every step
+    # end to end through the public API over the same simulated window: back to t0,
+    # the warm-up samples again, then the state in from pinned host memory and out
+    # again every step
+    eng.reset()
+    i = 0
+    for _ in range(args.warmup):
+        i += FBR_STEP_SAMPLES
+        eng.run(i, sync=False)
     host = torch.empty(4 * eng.nx[0], dtype=torch.float64, pin_memory=True)
     hv = host.numpy()
     eng.get_states(hv)
-    r0, ta = eng.stats()["rhs_calls"], eng.state()[0]
+    ta = eng.state()[0]
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(args.steps):
@@ -536,7 +542,7 @@ def main_fbr(args, rank, world, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": value / FBR_PUBLISHED_SIM_PER_WALL, "dtype": "f64",
             "data": "the reference's shipped deck (tests/golden/fbr005)",
-            "config": {"workload": WORKLOAD_FBR, "step_samples": FBR_STEP_SAMPLES,
+            "config": {"workload": WORKLOAD_FBR, "step_samples": FBR_STEP_SAMPLES, "slice": args.slice or 2048,
                        "l2": "single member (512 KB state) resident in L2: latency-bound, no roofline claim"},
             "rhs_pts_per_s": pts / (ms / 1e3), "rhs_calls": s1["rhs_calls"] - s0["rhs_calls"],
             "accepted": s1["accepted"] - s0["accepted"], "rejected": s1["rejected"] - s0["rejected"],
@@ -561,6 +567,8 @@ def main():
     ap.add_argument("--window", type=int, default=WINDOW)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="ensemble", choices=["ensemble", "2d", "fbr005"])
+    ap.add_argument("--slice", type=int, default=0,
+                    help="fbr005: grid points per CTA of the member's cluster (0: 2048)")
     ap.add_argument("--autotune", action="store_true",
                     help="pick the slice per grid size by timing candidates on the device first")
     args = ap.parse_args()
