@@ -407,6 +407,9 @@ def main_2d(args, rank, world, local):
 FBR_DECK = os.path.join(ROOT, "tests", "golden", "fbr005")
 FBR_STEP_SAMPLES = 250            # one bench step = 250 output samples = 5 simulated s
 FBR_PUBLISHED_SIM_PER_WALL = 1.0 / 1.09714   # logfile.txt:35 "Relative time consuming" (hardware not recorded)
+# one member of 4096 points: 8 CTAs of 512 points (the shortest phases) measured fastest
+# on B200 against 1024- and 2048-point slices (9.09 / 8.33 / 7.99 sim-s per wall-s)
+FBR_SLICE = 512
 WORKLOAD_FBR = ("the reference's own test deck 1dFBr005Bor: 1D HS2, flat h = 1 m, kinematic breaking, IVP from "
                 "initial.dat, Nx = 4096 on [-215, 215] m, output every 0.02 s to t = 120 s, the reference's "
                 "tolerances (abs 1e-5, rel 1e-4) and first step 1e-4")
@@ -470,7 +473,8 @@ def main_fbr(args, rank, world, local):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     import hawassi_c_b200 as hw
-    eng = hw.Engine(FBR_DECK, device=local, slice=args.slice)
+    slice_ = args.slice or FBR_SLICE
+    eng = hw.Engine(FBR_DECK, device=local, slice=slice_)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     eng.set_stream(stream.cuda_stream)
@@ -542,7 +546,7 @@ def main_fbr(args, rank, world, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": value / FBR_PUBLISHED_SIM_PER_WALL, "dtype": "f64",
             "data": "the reference's shipped deck (tests/golden/fbr005)",
-            "config": {"workload": WORKLOAD_FBR, "step_samples": FBR_STEP_SAMPLES, "slice": args.slice or 2048,
+            "config": {"workload": WORKLOAD_FBR, "step_samples": FBR_STEP_SAMPLES, "slice": slice_,
                        "l2": "single member (512 KB state) resident in L2: latency-bound, no roofline claim"},
             "rhs_pts_per_s": pts / (ms / 1e3), "rhs_calls": s1["rhs_calls"] - s0["rhs_calls"],
             "accepted": s1["accepted"] - s0["accepted"], "rejected": s1["rejected"] - s0["rejected"],
@@ -568,7 +572,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="ensemble", choices=["ensemble", "2d", "fbr005"])
     ap.add_argument("--slice", type=int, default=0,
-                    help="fbr005: grid points per CTA of the member's cluster (0: 2048)")
+                    help="fbr005: grid points per CTA of the member's cluster (0: 512)")
     ap.add_argument("--autotune", action="store_true",
                     help="pick the slice per grid size by timing candidates on the device first")
     args = ap.parse_args()
