@@ -561,6 +561,134 @@ def main_fbr(args, rank, world, local):
     return 0
 
 
+# ----------------------------------------------------------------------------
+# Config 2: one 1D run on a slope with 16 reference depths, HS3 and breaking
+# ----------------------------------------------------------------------------
+C2_STEP_SAMPLES = 20              # one bench step = 20 output samples (~1.95 simulated s)
+C2_NREF = 16
+WORKLOAD_C2 = ("1D plain FP64, varying bathymetry and breaking: L = 400 m, Nx = 16384, depth 1.0 m flat for "
+               "150 m then a 1:30 slope to 0.05 m, dispersion interpolated over 16 reference depths, HS3, "
+               "kinematic breaking (KBC 0.8, TC 0.2, Tchar 0.5), seeded JONSWAP influx Hs 0.15 m Tp 2.5 s "
+               "gamma 3.3 (1024 lines), RKF45 rtol 1e-6 atol 1e-8, t_end 200 s")
+
+
+def _c2_deck():
+    from hawassi_c_b200 import decks
+    p = os.path.join(tempfile.gettempdir(), "hw_bench_c2")
+    if not os.path.exists(os.path.join(p, "input.txt")):
+        decks.config2_deck(p, seed=0)
+    return p
+
+
+def _c2_cpu(deck, max_seconds):
+    """The oracle port (16 reference depths) on one host thread from t0 for ~max_seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as ol
+    o = ol.Oracle(deck, eps_abs=EPS_ABS, eps_rel=EPS_REL, nref=C2_NREF)
+    tt = o.table("ttrace")
+    y = o.initial_state()
+    t, h = float(tt[0]), 1e-4
+    c0, w0 = o.stats()[0], time.perf_counter()
+    for ti in tt[1:]:
+        while t < ti and time.perf_counter() - w0 <= max_seconds:
+            t, h = o.evolve_apply(t, ti, h, y)
+        if time.perf_counter() - w0 > max_seconds:
+            break
+    wall = time.perf_counter() - w0
+    pts = (o.stats()[0] - c0) * o.nx
+    o.close()
+    return t - float(tt[0]), wall, pts
+
+
+def main_c2(args, rank, world, local):
+    deck = _c2_deck()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sim, wall, pts = _c2_cpu(deck, 15.0)
+        cpu = {"value": pts / wall, "unit": "RHS grid-point evaluations/s", "cores": 1, "kind": "port",
+               "sample": f"the first {sim:.3f} simulated s of the run from t0 on one thread (~15 s), "
+                         f"{sim / wall:.4f} sim-s/wall-s"}
+        log(f"cpu baseline {cpu['value']:.3e} pts/s, {sim / wall:.4f} sim-s/wall-s")
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    import hawassi_c_b200 as hw
+    eng = hw.Engine(deck, eps_abs=EPS_ABS, eps_rel=EPS_REL, nref=C2_NREF, device=local, slice=args.slice)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    eng.set_stream(stream.cuda_stream)
+    i = 0
+    for _ in range(args.warmup):
+        i += C2_STEP_SAMPLES
+        eng.run(i, sync=False)
+    torch.cuda.synchronize()
+    s0, t0 = eng.stats(), eng.state()[0]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        i += C2_STEP_SAMPLES
+        eng.run(i, sync=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    s1, t1 = eng.stats(), eng.state()[0]
+    nx = eng.nx[0]
+    pts = float((s1["rhs_calls"] - s0["rhs_calls"]) * nx)
+    sim = t1 - t0
+    if world > 1:
+        (ms,), (pts, sim) = reduce_ranks([ms], [pts, sim], "cuda")
+    value = pts / (ms / 1e3)
+    eng.reset()
+    i = 0
+    for _ in range(args.warmup):
+        i += C2_STEP_SAMPLES
+        eng.run(i, sync=False)
+    host = torch.empty(4 * nx, dtype=torch.float64, pin_memory=True)
+    hv = host.numpy()
+    eng.get_states(hv)
+    r0 = eng.stats()["rhs_calls"]
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        eng.set_states(hv)
+        i += C2_STEP_SAMPLES
+        eng.run(i, sync=False)
+        eng.get_states(hv)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ems = e0.elapsed_time(e1)
+    e2e = {"value": float((eng.stats()["rhs_calls"] - r0) * nx) / (ems / 1e3), "unit": "RHS grid-point evaluations/s",
+           "h2d_bytes_per_step": 4 * nx * 8, "d2h_bytes_per_step": 4 * nx * 8}
+    if rank == 0:
+        line = {
+            "metric": "RHS grid-pt evals/s", "value": value, "unit": "RHS grid-point evaluations/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic seeded deck (slope bathymetry, JONSWAP influx) in the reference input format",
+            "config": {"workload": WORKLOAD_C2, "step_samples": C2_STEP_SAMPLES, "slice": args.slice or 2048,
+                       "l2": "single member (2 MB state, 16 reference tables) resident in L2"},
+            "sim_s_per_wall_s": sim / (ms / 1e3), "rhs_calls": s1["rhs_calls"] - s0["rhs_calls"],
+            "accepted": s1["accepted"] - s0["accepted"], "rejected": s1["rejected"] - s0["rejected"],
+            "roofline": None, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "gpu_launches": args.steps * (len(eng.class_timing()) + 1),
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -570,7 +698,7 @@ def main():
     ap.add_argument("--members", type=int, default=MEMBERS)
     ap.add_argument("--window", type=int, default=WINDOW)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "2d", "fbr005"])
+    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "2d", "fbr005", "c2"])
     ap.add_argument("--slice", type=int, default=0,
                     help="fbr005: grid points per CTA of the member's cluster (0: 512)")
     ap.add_argument("--autotune", action="store_true",
@@ -585,6 +713,24 @@ def main():
         if args.impl == "reference":
             return run_reference_2d(args, rank, world)
         return main_2d(args, rank, world, local)
+    if args.workload == "c2":
+        if args.impl == "reference":
+            if rank != 0:
+                return 0
+            sim, wall, pts = _c2_cpu(_c2_deck(), 5.0 * (args.steps + args.warmup))
+            value = pts / wall
+            print(json.dumps({
+                "metric": "RHS grid-pt evals/s", "value": value, "unit": "RHS grid-point evaluations/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * wall / max(1, args.steps + args.warmup), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic seeded deck",
+                "config": {"workload": WORKLOAD_C2}, "impl": "reference", "sim_s_per_wall_s": sim / wall,
+                "cpu_baseline": {"value": value, "unit": "RHS grid-point evaluations/s", "cores": 1, "kind": "port",
+                                 "sample": f"the first {sim:.3f} simulated s from t0 on one thread"},
+                "e2e": {"value": value, "unit": "RHS grid-point evaluations/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}), flush=True)
+            return 0
+        return main_c2(args, rank, world, local)
     if args.workload == "fbr005":
         if args.impl == "reference":
             return run_reference_fbr(args, rank, world)
