@@ -690,7 +690,7 @@ k2_rowE(Tab2 tb, Work2 w, RK2 rk, const Ctl2* __restrict__ ctl, int mode, int co
         const double2 au = slot(sm, M, 4 + k, j), av = slot(sm, M, 6 + k, j);
         dphi = make_double2(dphi.x + au.x + av.x, dphi.y + au.y + av.y);
       } else {
-        // HS1 (rhs_AB1_2DF_uv, 2d/fun_odesolver.c:4404-4456): no H2 terms
+        // HS1 (rhs_AB1_2DF_uv / rhs_AB1_2DB_uv, 2d/fun_odesolver.c:4350-4456): no H2 terms
         ix = make_double2(0.0, 0.0);
         iy = make_double2(0.0, 0.0);
       }

@@ -344,10 +344,11 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
     return nullptr;
   }
   const bool var_tables = t->gam_min && t->gam_plus && t->csq_min && t->csq_plus && t->om2_min && t->om2_plus;
-  if (t->model == 1 && (var_tables || t->breaking || t->wallchar)) {
-    g_err2d = "hw2d_create: HS1 is built for the flat bottom without walls or breaking (rhs_AB1_2DF_uv)";
+  if (t->model == 1 && (t->breaking || t->wallchar)) {
+    g_err2d = "hw2d_create: HS1 is built without walls or breaking (rhs_AB1_2DF_uv, rhs_AB1_2DB_uv)";
     return nullptr;
   }
+  (void)var_tables;
   if (t->propagation < 0 || t->propagation > 2) {
     g_err2d = "hw2d_create: propagation must be 0 (Uni+), 1 (Uni-) or 2 (Bi)";
     return nullptr;

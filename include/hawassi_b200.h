@@ -219,7 +219,7 @@ typedef struct hw2d_ctx hw2d_ctx;
 
 typedef struct hw2d_tables {
     int nx, ny;                 /* powers of two, 64..1024                      */
-    int model;                  /* evolinfo.model: 2 = HS2; 1 = HS1 (flat bottom) */
+    int model;                  /* evolinfo.model: 2 = HS2; 1 = HS1 (no walls or breaking) */
     int propagation;            /* 0 = Uni+, 1 = Uni-, 2 = Bi (vertical line)   */
     double cpeak;               /* Oprt.Cpeak                                   */
     const double* kx;           /* [nx] dominfo.kx                              */

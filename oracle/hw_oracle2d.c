@@ -158,7 +158,7 @@ or2d_ctx* or2d_create(const or2d_tables* tb, double eps_abs, double eps_rel) {
         }
     }
     if (tb->gam_min && tb->gam_plus && tb->csq_min && tb->csq_plus && tb->om2_min && tb->om2_plus) {
-        if (c->model != 2) { set_err2("or2d_create: the varying-bottom RHS is restated for HS2 only"); free(c); return NULL; }
+        if (c->model == 1 && tb->wallchar) { set_err2("or2d_create: walls are restated for HS2 only"); free(c); return NULL; }
         c->var = 1;
         c->gmin = dup(tb->gam_min, n); c->gplus = dup(tb->gam_plus, n);
         c->cmin = dup(tb->csq_min, n); c->cplus = dup(tb->csq_plus, n);
@@ -788,6 +788,28 @@ static int rhs_2db(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
         }
     fft2(Nx, Ny, dampeta, -1); fft2(Nx, Ny, dampu, -1); fft2(Nx, Ny, dampv, -1);
     free(eta_hat); free(u_hat); free(v_hat); free(Csqr_uhat); free(Csqr_vhat);
+
+    if (c->model == 1) {
+        /* rhs_AB1_2DB_uv (2d/fun_odesolver.c:4350-4402): the linear model */
+        cx* Source_hat = malloc(sizeof(cx) * n);
+        fun_source(c, t, Source_hat);
+        for (int i = 0; i < Ny; i++)
+            for (int j = 0; j < Nx; j++) {
+                const int q = i * Nx + j;
+                const double a = c->aal[q];
+                dt_Zhat[q] = (Source_hat[q].re + deluH1[q].re + delvH1[q].re - dampeta[q].re) * a;
+                dt_Zhat[n + q] = (Source_hat[q].im + deluH1[q].im + delvH1[q].im - dampeta[q].im) * a;
+                dt_Zhat[2 * n + q] = (GRAV * kx[j] * Zhat[n + q] - dampu[q].re) * a;
+                dt_Zhat[3 * n + q] = (-GRAV * kx[j] * Zhat[q] - dampu[q].im) * a;
+                dt_Zhat[4 * n + q] = (GRAV * ky[i] * Zhat[n + q] - dampv[q].re) * a;
+                dt_Zhat[5 * n + q] = (-GRAV * ky[i] * Zhat[q] - dampv[q].im) * a;
+            }
+        cx* fr1[] = {eta, u, v, dampeta, dampu, dampv, deluH1, delvH1, Source_hat};
+        for (size_t q = 0; q < sizeof fr1 / sizeof fr1[0]; q++) free(fr1[q]);
+        for (int q = 0; q < 6 * n; q++)
+            if (!isfinite(dt_Zhat[q])) return 1;
+        return 0;
+    }
 
     /* AB2: the physical fields again (same transforms as AB1), M0 u = delu H1 */
     cx *M0u = malloc(sizeof(cx) * n), *M0v = malloc(sizeof(cx) * n), *Lphi = malloc(sizeof(cx) * n);

@@ -178,10 +178,10 @@ def test_wall_on_flat_bottom_rejected():
         Engine2D(tb)
 
 
-@pytest.mark.parametrize("nx,ny,prop", [(64, 64, 0), (128, 64, 2)])
-def test_rhs_parity_hs1(nx, ny, prop):
-    """HS1 (rhs_AB1_2DF_uv): the linear model with damping and source."""
-    tb = tables(nx, ny, propagation=prop, model=1)
+@pytest.mark.parametrize("nx,ny,prop,bottom", [(64, 64, 0, "flat"), (128, 64, 2, "flat"), (64, 128, 0, "shoal")])
+def test_rhs_parity_hs1(nx, ny, prop, bottom):
+    """HS1 (rhs_AB1_2DF_uv / rhs_AB1_2DB_uv): the linear model with damping and source."""
+    tb = tables(nx, ny, propagation=prop, model=1, bathymetry=bottom)
     eng, ora = Engine2D(tb, 1e-8, 1e-6), Oracle2D(tb, 1e-8, 1e-6)
     y = band_limited_state(tb, 0.02, 3)
     assert rel(eng.rhs(0.8, y), ora.rhs(0.8, y)) < 1e-11
