@@ -31,8 +31,8 @@
 
 namespace hw2d {
 
-constexpr int kBrkPeakCap = 4096;    // peaks sorted per update (one CTA)
-constexpr int kBrkCrestCap = 4096;   // records in CB, CBNew, CBPrev
+constexpr int kBrkPeakCap = 16384;   // peaks sorted per update (one CTA, 64 KB of shared memory)
+constexpr int kBrkCrestCap = 16384;  // records in CB, CBNew, CBPrev
 constexpr int kBrkSortThreads = 1024;
 
 struct Crest2 {
@@ -273,7 +273,7 @@ __global__ void k2b_peaks(Tab2 tb, Work2 w, Brk2 b, const Ctl2* __restrict__ ctl
 // sort: the peak ranks in ascending order (fun_peaks' visiting order)
 __global__ void __launch_bounds__(kBrkSortThreads) k2b_sort(Brk2 b, const Ctl2* __restrict__ ctl, int mode, int cond) {
   if (!rhs_active(ctl, cond) || !brk_update(ctl, mode)) return;
-  __shared__ int s[kBrkPeakCap];
+  extern __shared__ int s[];          // kBrkPeakCap ints
   const int np = b.st->npeaks;
   if (np > kBrkPeakCap) {
     if (threadIdx.x == 0) b.st->err |= kBrkErrPeaks;

@@ -141,6 +141,8 @@ void set_all_attrs() {
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64 || done[dev]) return;
   set_attrs<64>(); set_attrs<128>(); set_attrs<256>(); set_attrs<512>(); set_attrs<1024>();
+  cudaFuncSetAttribute(hw2d::k2b_sort, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(hw2d::kBrkPeakCap * sizeof(int)));
   done[dev] = true;
 }
 
@@ -231,7 +233,7 @@ struct hw2d_ctx {
     brk_row(nx, 0, rows, s, tb, w, brk, rk, ctl, mode, cond, out);
     brk_col(ny, 0, cols, s, tb, w, brk, ctl, mode, cond);
     hw2d::k2b_peaks<<<gb, 256, 0, s>>>(tb, w, brk, ctl, mode, cond);
-    hw2d::k2b_sort<<<1, hw2d::kBrkSortThreads, 0, s>>>(brk, ctl, mode, cond);
+    hw2d::k2b_sort<<<1, hw2d::kBrkSortThreads, hw2d::kBrkPeakCap * sizeof(int), s>>>(brk, ctl, mode, cond);
     hw2d::k2b_machine<<<1, 32, 0, s>>>(tb, w, brk, ctl, mode, cond);
     hw2d::k2b_flux<<<gb, 256, 0, s>>>(tb, w, brk, ctl, mode, cond);
     brk_col(ny, 1, cols, s, tb, w, brk, ctl, mode, cond);
