@@ -156,7 +156,8 @@ extern "C" int hw_jonswap_influx(const hw_jonswap* specs, int n, double* eta_out
     d.off = total;
     total += d.Nt;
   }
-  if (!eta_out || cap < total) return (int)std::min<long long>(total, 0x7fffffff);
+  if (total > 0x7fffffffLL) return -1;   // the count must fit the return value
+  if (!eta_out || cap < total) return (int)total;
   if (cudaSetDevice(device) != cudaSuccess) return -1;
   JsDev* dps = nullptr;
   double2* X = nullptr;
