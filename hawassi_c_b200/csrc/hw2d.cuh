@@ -71,6 +71,7 @@ struct Tab2 {
   const double* omin;           // Om2dSq_min, Om2dSq_plus (spectral)
   const double* oplus;
   const double* wallchar;       // dominfo.wallchar (harbour walls), nullptr: none
+  const double* c2d;            // Oprt.C2d (flat bottom with walls only)
 };
 
 struct Work2 {
@@ -91,6 +92,8 @@ struct Work2 {
   double2* EU;                  // (eta u)^, (eta v)^, deletaH2^ (3 fields)
   // kinematic breaking only: delphiH^ as the assembly forms it (nullptr: off)
   double2* dph;
+  // flat bottom with walls: the round trip of (C u^, C v^) (delphiH1^ lands in H1)
+  double2* WP;
 };
 
 // device control block of the stepper (one per engine)
@@ -473,8 +476,15 @@ k2_colB(Tab2 tb, Work2 w, const Ctl2* __restrict__ ctl, int cond) {
       // Q1 = dampeta + i dampu, Q2 = dampv + i deletaH2, Q3 = etaM0u + i eta u, Q4 = etaM0v + i eta v
       put(sm, M, 0 + k, y, make_double2(dmp * eta, dmp * u));
       put(sm, M, 2 + k, y, make_double2(dmp * v, 0.5 * ((u * u + v * v) - lphi * lphi)));
-      put(sm, M, 4 + k, y, make_double2(eta * m0u, eta * u));
-      put(sm, M, 6 + k, y, make_double2(eta * m0v, eta * v));
+      if (tb.wallchar) {   // the H2 products carry wallchar (2d/fun_odesolver.c:3239-3249)
+        const double wc = tb.wallchar[q];
+        put(sm, M, 2 + k, y, make_double2(dmp * v, 0.5 * ((u * u + v * v) - lphi * lphi) * wc));
+        put(sm, M, 4 + k, y, make_double2(eta * m0u * wc, eta * u * wc));
+        put(sm, M, 6 + k, y, make_double2(eta * m0v * wc, eta * v * wc));
+      } else {
+        put(sm, M, 4 + k, y, make_double2(eta * m0u, eta * u));
+        put(sm, M, 6 + k, y, make_double2(eta * m0v, eta * v));
+      }
     }
   }
   fft_slices<M>(sm, 8, tb.twy, -1);
@@ -680,6 +690,8 @@ k2_rowE(Tab2 tb, Work2 w, RK2 rk, const Ctl2* __restrict__ ctl, int mode, int co
         // delu H1^ + delv H1^ from the two-depth operator (2d/fun_odesolver.c:4560-4563)
         const double2 h1u = w.H1[q], h1v = w.H1[n + q];
         dphi = make_double2(h1u.x + h1v.x, h1u.y + h1v.y);
+      } else if (tb.wallchar) {
+        dphi = w.H1[q];   // the wall branch's delphiH1^ (k2w_row3)
       } else {
         // delphiH1^ = -i (kx C^2/g u^ + ky C^2/g v^)
         const double2 du1 = make_double2(cg * zu.x, cg * zu.y), dv1 = make_double2(cg * zv.x, cg * zv.y);

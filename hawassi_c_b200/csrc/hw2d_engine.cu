@@ -18,6 +18,7 @@
 #include "hw2d.cuh"
 #include "hw2d_brk.cuh"
 #include "hw2d_var.cuh"
+#include "hw2d_wall.cuh"
 #include "hw_setup.hpp"
 
 using hw2d::Ctl2;
@@ -53,6 +54,27 @@ void set_attrs() {
   cudaFuncSetAttribute(hw2d::k2b_colI<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(2));
   cudaFuncSetAttribute(hw2d::k2b_sbcol<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(2));
   cudaFuncSetAttribute(hw2d::k2b_sbrow<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(2));
+  cudaFuncSetAttribute(hw2d::k2w_row1<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(2));
+  cudaFuncSetAttribute(hw2d::k2w_col2<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(2));
+  cudaFuncSetAttribute(hw2d::k2w_row3<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(2));
+}
+
+// the flat bottom's wall round trip (row M = nx, column M = ny)
+template <int M>
+void launch_wall(int which, int nblocks, cudaStream_t s, const Tab2& tb, const Work2& w, const Ctl2* ctl, int cond) {
+  const int blk = hw2d::kGroups * (M / 8);
+  if (which == 0) hw2d::k2w_row1<M><<<nblocks, blk, smem_bytes<M>(2), s>>>(tb, w, ctl, cond);
+  else if (which == 1) hw2d::k2w_col2<M><<<nblocks, blk, smem_bytes<M>(2), s>>>(tb, w, ctl, cond);
+  else hw2d::k2w_row3<M><<<nblocks, blk, smem_bytes<M>(2), s>>>(tb, w, ctl, cond);
+}
+void wall_pass(int M, int which, int nb, cudaStream_t s, const Tab2& tb, const Work2& w, const Ctl2* ctl, int cond) {
+  switch (M) {
+    case 64: launch_wall<64>(which, nb, s, tb, w, ctl, cond); break;
+    case 128: launch_wall<128>(which, nb, s, tb, w, ctl, cond); break;
+    case 256: launch_wall<256>(which, nb, s, tb, w, ctl, cond); break;
+    case 512: launch_wall<512>(which, nb, s, tb, w, ctl, cond); break;
+    default: launch_wall<1024>(which, nb, s, tb, w, ctl, cond); break;
+  }
 }
 
 // the breaking kernels of one RHS (row passes: row length M = nx; column passes: M = ny)
@@ -218,12 +240,17 @@ struct hw2d_ctx {
       if (brk.on) brk_launch(mode, cond, s, out);
       return;
     }
+    if (tb.wallchar) {
+      wall_pass(nx, 0, rows, s, tb, w, ctl, cond);
+      wall_pass(ny, 1, cols, s, tb, w, ctl, cond);
+      wall_pass(nx, 2, rows, s, tb, w, ctl, cond);
+    }
     row_dispatch(nx, 0, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
     col_dispatch(ny, 1, cols, s, tb, w, ctl, cond);
     row_dispatch(nx, 2, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
     if (!tb.chi_one || tb.has_src) col_dispatch(ny, 3, cols, s, tb, w, ctl, cond);
     row_dispatch(nx, 4, rows, s, tb, w, rk, ctl, ctl, mode, cond, out);
-    per_rhs = ((!tb.chi_one || tb.has_src) ? 5 : 4) + 1;
+    per_rhs = ((!tb.chi_one || tb.has_src) ? 5 : 4) + 1 + (tb.wallchar ? 3 : 0);
     if (brk.on) brk_launch(mode, cond, s, out);
   }
   // the breaking kernels after the assembly pass (both bottoms)
@@ -445,12 +472,14 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
     tb.oplus = c->upload(std::vector<double>(t->om2_plus, t->om2_plus + n));
   }
   if (t->wallchar) {
-    if (!var) {
-      g_err2d = "hw2d_create: walls are built for the two-depth (varying-bottom) RHS only";
+    if (!var && t->refl_coef >= 1) {
+      g_err2d = "hw2d_create: fully reflecting walls on the flat bottom (the flux branch of fun_delphiH1hat) "
+                "are not built";
       delete c;
       return nullptr;
     }
     tb.wallchar = c->upload(std::vector<double>(t->wallchar, t->wallchar + n));
+    if (!var) tb.c2d = c->upload(std::vector<double>(t->c2d, t->c2d + n));
   }
 
   hw2d::Brk2& bk = c->brk;
@@ -508,6 +537,10 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
   w.R = c->dalloc<double2>(4 * n);
   w.Q = c->dalloc<double2>((var ? 6 : 4) * n);
   if (!var && bk.on) w.phys = c->dalloc<double>(3 * n);   // eta, u, v for the breaking kernels
+  if (!var && t->wallchar) {   // the flat bottom's wall round trip
+    w.WP = c->dalloc<double2>(n);
+    w.H1 = c->dalloc<double2>(n);
+  }
   if (var) {
     w.phys = c->dalloc<double>(3 * n);
     w.pe = c->dalloc<double>(2 * n);
@@ -531,6 +564,7 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
   bool ok = tb.kx && tb.ky && tb.c2g && tb.l2d && tb.aal && tb.damp && tb.chi && tb.twx && tb.twy && w.z && w.R &&
             w.Q && w.D && w.V && w.insig && w.insigs && w.part && c->dref && c->dout && c->ctl &&
             (chi_one || w.W) && (!has_src || (tb.gx && tb.sx && tb.sig && w.src)) && (!bk.on || (w.dph && w.phys)) &&
+            (var || !t->wallchar || (w.WP && w.H1 && tb.c2d)) &&
             (!var || (tb.gmin && tb.gplus && tb.cmin && tb.cplus && tb.omin && tb.oplus && w.phys && w.pe && w.H1 &&
                       w.EU)) && (!t->wallchar || tb.wallchar);
   for (int i = 0; i < 2; ++i) ok = ok && rk.y[i] && rk.kk[i];

@@ -28,6 +28,7 @@ class Hw2dTables(ctypes.Structure):
         ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("max_eta_init", ctypes.c_double),
         ("tstar", ctypes.c_double), ("rsearch", ctypes.c_double), ("kbc", ctypes.c_double), ("tc", ctypes.c_double),
         ("delb", ctypes.c_double), ("cur_u", ctypes.c_double), ("t0", ctypes.c_double), ("dt_out", ctypes.c_double),
+        ("refl_coef", ctypes.c_double),
     ]
 
 # parambreak's scalars (2d/breaking.c:1-8) as the tables dict carries them
@@ -90,6 +91,7 @@ class Engine2D:
         tb = Hw2dTables(nx=int(tables["nx"]), ny=int(tables["ny"]), model=int(tables.get("model", 2)),
                         propagation=int(tables.get("propagation", 0)), cpeak=float(tables["cpeak"]),
                         nt=int(tables.get("nt", 0) if keep["sig"] is not None else 0), breaking=brk, **scal,
+                        refl_coef=float(tables.get("refl_coef", 0.0)),
                         **{k: _ptr(v) for k, v in keep.items()})
         o = HwOpts(eps_abs=eps_abs, eps_rel=eps_rel, h0=h0, device=device)
         self._h = self._L.hw2d_create(ctypes.byref(tb), ctypes.byref(o))

@@ -165,7 +165,11 @@ or2d_ctx* or2d_create(const or2d_tables* tb, double eps_abs, double eps_rel) {
         c->omin = dup(tb->om2_min, n); c->oplus = dup(tb->om2_plus, n);
     }
     if (tb->wallchar) {
-        if (!c->var) { set_err2("or2d_create: walls are restated for the varying-bottom RHS only"); free(c); return NULL; }
+        if (!c->var && tb->refl_coef >= 1) {
+            set_err2("or2d_create: fully reflecting walls on the flat bottom (the flux branch of fun_delphiH1hat) are not restated");
+            free(c);
+            return NULL;
+        }
         c->wallchar = dup(tb->wallchar, n);
     }
     if (tb->breaking) {
@@ -903,7 +907,8 @@ static int rhs_2db(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
 /* rhs_AB1_2DF_uv / rhs_AB2_2DF_uv (2d/fun_odesolver.c:4404-4540) with the term
  * functions fun_delphiH1hat (no wall, :2270-2283), fun_termshat_AB1_2DF_uv
  * (:2962-3027) and fun_termshat_AB2_2DF_uv (:3136-3325), kinematic breaking when the
- * tables ask for it (HS2); no friction, coupling or wall. */
+ * tables ask for it (HS2), walls through fun_delphiH1hat's refl_coef < 1 branch
+ * and the H2 products' wallchar; no friction or coupling. */
 int or2d_rhs(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
     if (c->var) return rhs_2db(c, t, Zhat, dt_Zhat);
     const int Nx = c->nx, Ny = c->ny, n = c->n;
@@ -921,6 +926,32 @@ int or2d_rhs(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
             delphiH1hat[q].re = kx[j] * du.im + ky[i] * dv.im;
             delphiH1hat[q].im = -kx[j] * du.re - ky[i] * dv.re;
         }
+    if (c->wallchar) {
+        /* fun_delphiH1hat's wall branch for refl_coef < 1 (2d/fun_odesolver.c:2172-2219):
+         * C u^, C v^ to physical space (symmetrised, real part over N), times wallchar,
+         * back (r2c), times C/g, then -i (kx . + ky .) */
+        cx *Cu = malloc(sizeof(cx) * n), *Cv = malloc(sizeof(cx) * n);
+        for (int q = 0; q < n; q++) {
+            Cu[q].re = (c->c2d[q]) * Zhat[2 * n + q]; Cu[q].im = (c->c2d[q]) * Zhat[3 * n + q];
+            Cv[q].re = (c->c2d[q]) * Zhat[4 * n + q]; Cv[q].im = (c->c2d[q]) * Zhat[5 * n + q];
+        }
+        sym2(Cu, Nx, Ny); sym2(Cv, Nx, Ny);
+        fft2(Nx, Ny, Cu, +1); fft2(Nx, Ny, Cv, +1);
+        for (int q = 0; q < n; q++) {
+            Cu[q].re = Cu[q].re / (Nx * Ny) * c->wallchar[q]; Cu[q].im = 0;
+            Cv[q].re = Cv[q].re / (Nx * Ny) * c->wallchar[q]; Cv[q].im = 0;
+        }
+        fft2(Nx, Ny, Cu, -1); fft2(Nx, Ny, Cv, -1);
+        for (int i = 0; i < Ny; i++)
+            for (int j = 0; j < Nx; j++) {
+                const int q = i * Nx + j;
+                cx du = {(c->c2d[q]) / GRAV * Cu[q].re, (c->c2d[q]) / GRAV * Cu[q].im};
+                cx dv = {(c->c2d[q]) / GRAV * Cv[q].re, (c->c2d[q]) / GRAV * Cv[q].im};
+                delphiH1hat[q].re = kx[j] * du.im + ky[i] * dv.im;
+                delphiH1hat[q].im = -kx[j] * du.re - ky[i] * dv.re;
+            }
+        free(Cu); free(Cv);
+    }
 
     /* spectra of the state, copies symmetrised before the inverse transforms */
     cx *eta = malloc(sizeof(cx) * n), *u = malloc(sizeof(cx) * n), *v = malloc(sizeof(cx) * n);
@@ -966,7 +997,7 @@ int or2d_rhs(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
         dampu[q].re = sevenC * ch * u[q].re / factIFFT; dampu[q].im = 0;
         dampv[q].re = sevenC * ch * v[q].re / factIFFT; dampv[q].im = 0;
         if (c->model == 2) {
-            const double wallchar = 1.0;
+            const double wallchar = c->wallchar ? c->wallchar[q] : 1.0;   /* :3239-3249 */
             etaM0u[q].re = eta[q].re * M0u[q].re / f2 * wallchar; etaM0u[q].im = 0;
             eta_u[q].re = eta[q].re * u[q].re / f2 * wallchar; eta_u[q].im = 0;
             etaM0v[q].re = eta[q].re * M0v[q].re / f2 * wallchar; etaM0v[q].im = 0;

@@ -49,7 +49,7 @@ typedef struct or2d_tables {
     const double* csq_plus;     /* [ny*nx] Oprt.InterpD.Csqr2d_plus            */
     const double* om2_min;      /* [ny*nx] Oprt.InterpD.Om2dSq_min             */
     const double* om2_plus;     /* [ny*nx] Oprt.InterpD.Om2dSq_plus            */
-    const double* wallchar;     /* [ny*nx] dominfo.wallchar, NULL: no wall (varying bottom only) */
+    const double* wallchar;     /* [ny*nx] dominfo.wallchar, NULL: no wall                  */
     /* kinematic breaking (2d/breaking.c; fun_sbreaking 2d/fun_odesolver.c:985-1019), HS2
      * (flat or two-depth bottom); breaking = 0 leaves every field below unread */
     int breaking;
@@ -64,6 +64,7 @@ typedef struct or2d_tables {
     double kbc, tc, delb;       /* pb.KBC, pb.TC, pb.delb (1.5)                 */
     double cur_u;               /* dominfo.U (ambient current)                  */
     double t0, dt_out;          /* dominfo.t[0], dominfo.dt (breaking.dat cadence) */
+    double refl_coef;           /* walls: the reflection coefficient (the flat RHS branches on 1) */
 } or2d_tables;
 
 /* Copies every table.  eps <= 0 selects the reference's 2D values (abs 1e-3,

@@ -45,6 +45,7 @@ class Or2dTables(ctypes.Structure):
         ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("max_eta_init", ctypes.c_double),
         ("tstar", ctypes.c_double), ("rsearch", ctypes.c_double), ("kbc", ctypes.c_double), ("tc", ctypes.c_double),
         ("delb", ctypes.c_double), ("cur_u", ctypes.c_double), ("t0", ctypes.c_double), ("dt_out", ctypes.c_double),
+        ("refl_coef", ctypes.c_double),
     ]
 
 BRK_SCALARS = ("dx", "dy", "max_eta_init", "tstar", "rsearch", "kbc", "tc", "delb", "cur_u", "t0", "dt_out")
@@ -242,6 +243,7 @@ class Oracle2D:
         tb = Or2dTables(nx=int(tables["nx"]), ny=int(tables["ny"]), model=int(tables.get("model", 2)),
                         propagation=int(tables.get("propagation", 0)), cpeak=float(tables["cpeak"]),
                         nt=int(tables.get("nt", 0) if keep["sig"] is not None else 0), breaking=brk, **scal,
+                        refl_coef=float(tables.get("refl_coef", 0.0)),
                         **{k: (None if v is None else _p(v)) for k, v in keep.items()})
         self.h = L.or2d_create(ctypes.byref(tb), eps_abs, eps_rel)
         if not self.h:

@@ -151,17 +151,20 @@ def _wall(nx, ny):
     return ((0.6 * Lx, 0.3 * Ly, 0.63 * Lx, 0.7 * Ly),)
 
 
-@pytest.mark.parametrize("nx,ny", [(64, 64), (128, 128)])
-def test_rhs_parity_wall(nx, ny):
-    tb = tables(nx, ny, bathymetry="shoal", walls=_wall(nx, ny))
+@pytest.mark.parametrize("nx,ny,bottom", [(64, 64, "shoal"), (128, 128, "shoal"), (64, 64, "flat"), (128, 64, "flat")])
+def test_rhs_parity_wall(nx, ny, bottom):
+    """Walls: wallchar in the H2 products on both bottoms, and on the flat bottom
+    fun_delphiH1hat's round trip of (C u^, C v^) through the wall mask."""
+    tb = tables(nx, ny, bathymetry=bottom, walls=_wall(nx, ny))
     assert (tb["wallchar"] < 1).any()
     eng, ora = Engine2D(tb, 1e-8, 1e-6), Oracle2D(tb, 1e-8, 1e-6)
     y = band_limited_state(tb, 0.02, 3)
     assert rel(eng.rhs(1.1, y), ora.rhs(1.1, y)) < 1e-11
 
 
-def test_run_to_time_parity_wall():
-    tb = tables(64, 64, bathymetry="shoal", walls=_wall(64, 64))
+@pytest.mark.parametrize("bottom", ["shoal", "flat"])
+def test_run_to_time_parity_wall(bottom):
+    tb = tables(64, 64, bathymetry=bottom, walls=_wall(64, 64))
     eng, ora = Engine2D(tb, 1e-8, 1e-6), Oracle2D(tb, 1e-8, 1e-6)
     y = np.zeros(6 * tb["nx"] * tb["ny"])
     eng.set_state(0.0, 0.02, y)
@@ -171,9 +174,10 @@ def test_run_to_time_parity_wall():
     assert tg == to and rel(yg, y) < 1e-9
 
 
-def test_wall_on_flat_bottom_rejected():
-    tb = tables(64, 64)
-    tb["wallchar"] = np.ones(64 * 64)
+def test_fully_reflecting_wall_on_flat_bottom_rejected():
+    """refl_coef = 1 takes fun_delphiH1hat's flux branch, which is not built."""
+    tb = tables(64, 64, walls=_wall(64, 64))
+    tb["refl_coef"] = 1.0
     with pytest.raises(Exception):
         Engine2D(tb)
 
