@@ -72,6 +72,9 @@ struct Tab2 {
   const double* oplus;
   const double* wallchar;       // dominfo.wallchar (harbour walls), nullptr: none
   const double* c2d;            // Oprt.C2d (flat bottom with walls only)
+  int refl_one;                 // flat bottom, refl_coef == 1: fun_delphiH1hat's flux branch
+  const double* gwx;            // fun_gradient(wallchar) (refl_one only)
+  const double* gwy;
 };
 
 struct Work2 {

@@ -57,6 +57,9 @@ void set_attrs() {
   cudaFuncSetAttribute(hw2d::k2w_row1<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(2));
   cudaFuncSetAttribute(hw2d::k2w_col2<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(2));
   cudaFuncSetAttribute(hw2d::k2w_row3<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(2));
+  cudaFuncSetAttribute(hw2d::k2w_rowV1<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(4));
+  cudaFuncSetAttribute(hw2d::k2w_colV2<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(4));
+  cudaFuncSetAttribute(hw2d::k2w_rowV3<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(2));
 }
 
 // the flat bottom's wall round trip (row M = nx, column M = ny)
@@ -65,7 +68,10 @@ void launch_wall(int which, int nblocks, cudaStream_t s, const Tab2& tb, const W
   const int blk = hw2d::kGroups * (M / 8);
   if (which == 0) hw2d::k2w_row1<M><<<nblocks, blk, smem_bytes<M>(2), s>>>(tb, w, ctl, cond);
   else if (which == 1) hw2d::k2w_col2<M><<<nblocks, blk, smem_bytes<M>(2), s>>>(tb, w, ctl, cond);
-  else hw2d::k2w_row3<M><<<nblocks, blk, smem_bytes<M>(2), s>>>(tb, w, ctl, cond);
+  else if (which == 2) hw2d::k2w_row3<M><<<nblocks, blk, smem_bytes<M>(2), s>>>(tb, w, ctl, cond);
+  else if (which == 3) hw2d::k2w_rowV1<M><<<nblocks, blk, smem_bytes<M>(4), s>>>(tb, w, ctl, cond);
+  else if (which == 4) hw2d::k2w_colV2<M><<<nblocks, blk, smem_bytes<M>(4), s>>>(tb, w, ctl, cond);
+  else hw2d::k2w_rowV3<M><<<nblocks, blk, smem_bytes<M>(2), s>>>(tb, w, ctl, cond);
 }
 void wall_pass(int M, int which, int nb, cudaStream_t s, const Tab2& tb, const Work2& w, const Ctl2* ctl, int cond) {
   switch (M) {
@@ -241,9 +247,10 @@ struct hw2d_ctx {
       return;
     }
     if (tb.wallchar) {
-      wall_pass(nx, 0, rows, s, tb, w, ctl, cond);
-      wall_pass(ny, 1, cols, s, tb, w, ctl, cond);
-      wall_pass(nx, 2, rows, s, tb, w, ctl, cond);
+      const int base = tb.refl_one ? 3 : 0;
+      wall_pass(nx, base + 0, rows, s, tb, w, ctl, cond);
+      wall_pass(ny, base + 1, cols, s, tb, w, ctl, cond);
+      wall_pass(nx, base + 2, rows, s, tb, w, ctl, cond);
     }
     row_dispatch(nx, 0, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
     col_dispatch(ny, 1, cols, s, tb, w, ctl, cond);
@@ -472,14 +479,37 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
     tb.oplus = c->upload(std::vector<double>(t->om2_plus, t->om2_plus + n));
   }
   if (t->wallchar) {
-    if (!var && t->refl_coef >= 1) {
-      g_err2d = "hw2d_create: fully reflecting walls on the flat bottom (the flux branch of fun_delphiH1hat) "
-                "are not built";
-      delete c;
-      return nullptr;
-    }
     tb.wallchar = c->upload(std::vector<double>(t->wallchar, t->wallchar + n));
     if (!var) tb.c2d = c->upload(std::vector<double>(t->c2d, t->c2d + n));
+    if (!var && t->refl_coef == 1) {
+      // fun_delphiH1hat's refl_coef == 1 branch needs fun_gradient(wallchar)
+      // (2d/functions.c:392-460, called at :741): periodic forward and backward
+      // differences, the forward ones clipped to <= 0, the backward ones to >= 0
+      if (!(t->dx > 0) || !(t->dy > 0)) {
+        g_err2d = "hw2d_create: walls with refl_coef 1 need dx and dy";
+        delete c;
+        return nullptr;
+      }
+      std::vector<double> gx(n), gy(n);
+      const double* f = t->wallchar;
+      for (int i = 0; i < ny; ++i)
+        for (int j = 0; j < nx; ++j) {
+          const size_t q = (size_t)i * nx + j;
+          double Fx = (j < nx - 1) ? (f[q + 1] - f[q]) / t->dx : (f[(size_t)i * nx] - f[q]) / t->dx;
+          double Fy = (i < ny - 1) ? (f[q + nx] - f[q]) / t->dy : (f[j] - f[q]) / t->dy;
+          double Bx = (j > 0) ? (f[q] - f[q - 1]) / t->dx : (f[q] - f[(size_t)i * nx + nx - 1]) / t->dx;
+          double By = (i > 0) ? (f[q] - f[q - nx]) / t->dy : (f[q] - f[(size_t)(ny - 1) * nx + j]) / t->dy;
+          if (Fx > 0) Fx = 0;
+          if (Fy > 0) Fy = 0;
+          if (Bx < 0) Bx = 0;
+          if (By < 0) By = 0;
+          gx[q] = Fx + Bx;
+          gy[q] = Fy + By;
+        }
+      tb.refl_one = 1;
+      tb.gwx = c->upload(gx);
+      tb.gwy = c->upload(gy);
+    }
   }
 
   hw2d::Brk2& bk = c->brk;
@@ -538,7 +568,7 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
   w.Q = c->dalloc<double2>((var ? 6 : 4) * n);
   if (!var && bk.on) w.phys = c->dalloc<double>(3 * n);   // eta, u, v for the breaking kernels
   if (!var && t->wallchar) {   // the flat bottom's wall round trip
-    w.WP = c->dalloc<double2>(n);
+    w.WP = c->dalloc<double2>((tb.refl_one ? 2 : 1) * n);
     w.H1 = c->dalloc<double2>(n);
   }
   if (var) {
@@ -564,7 +594,7 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
   bool ok = tb.kx && tb.ky && tb.c2g && tb.l2d && tb.aal && tb.damp && tb.chi && tb.twx && tb.twy && w.z && w.R &&
             w.Q && w.D && w.V && w.insig && w.insigs && w.part && c->dref && c->dout && c->ctl &&
             (chi_one || w.W) && (!has_src || (tb.gx && tb.sx && tb.sig && w.src)) && (!bk.on || (w.dph && w.phys)) &&
-            (var || !t->wallchar || (w.WP && w.H1 && tb.c2d)) &&
+            (var || !t->wallchar || (w.WP && w.H1 && tb.c2d && (!tb.refl_one || (tb.gwx && tb.gwy)))) &&
             (!var || (tb.gmin && tb.gplus && tb.cmin && tb.cplus && tb.omin && tb.oplus && w.phys && w.pe && w.H1 &&
                       w.EU)) && (!t->wallchar || tb.wallchar);
   for (int i = 0; i < 2; ++i) ok = ok && rk.y[i] && rk.kk[i];

@@ -396,6 +396,8 @@ def tables(nx=1024, ny=1024, Lx=300.0, Ly=300.0, depth=3.0, Hs=0.5, Tp=6.0, gamm
     if wall is not None:
         extra["wallchar"] = f64(wall)
         extra["refl_coef"] = float(refl)
+    extra.setdefault("dx", float(x[1] - x[0]))
+    extra.setdefault("dy", float(y[1] - y[0]))
     return dict(**extra, nx=nx, ny=ny, model=model, propagation=propagation, cpeak=float(cpeak), kx=f64(kx), ky=f64(ky),
                 c2d=f64(c2d), l2d=f64(l2d), aal=f64(aal), charac=f64(charac), chiadj=f64(chi),
                 newgam=f64(newgam), skewgam=f64(skewgam), nt=nt, tsig=f64(tsig), sig=f64(sig), sigskew=f64(sigs),

@@ -87,7 +87,7 @@ class Engine2D:
         for k in ("bathy", "brchar", "x", "y"):
             keep[k] = np.ascontiguousarray(tables[k], dtype=np.float64) if brk else None
         self._keep = keep
-        scal = {k: float(tables.get(k, 0.0)) for k in BREAKING_SCALARS} if brk else {}
+        scal = {k: float(tables.get(k, 0.0)) for k in BREAKING_SCALARS}
         tb = Hw2dTables(nx=int(tables["nx"]), ny=int(tables["ny"]), model=int(tables.get("model", 2)),
                         propagation=int(tables.get("propagation", 0)), cpeak=float(tables["cpeak"]),
                         nt=int(tables.get("nt", 0) if keep["sig"] is not None else 0), breaking=brk, **scal,

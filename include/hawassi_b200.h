@@ -244,8 +244,8 @@ typedef struct hw2d_tables {
     const double* om2_min;      /* [ny*nx] Oprt.InterpD.Om2dSq_min              */
     const double* om2_plus;     /* [ny*nx] Oprt.InterpD.Om2dSq_plus             */
     /* harbour walls: dominfo.wallchar (1 - cutoff(refl_coef) inside the walls,
-     * 2d/functions.c:260-390); NULL for no wall.  On the flat bottom walls take
-     * fun_delphiH1hat's refl_coef < 1 branch (2d/fun_odesolver.c:2172-2219). */
+     * 2d/functions.c:260-390); NULL for no wall.  On the flat bottom walls also
+     * enter fun_delphiH1hat (2d/fun_odesolver.c:2100-2219, both branches). */
     const double* wallchar;     /* [ny*nx]                                      */
     /* kinematic breaking (2d/breaking.c: parambreak, breaking_process; fun_sbreaking
      * 2d/fun_odesolver.c:985-1019), two-depth tables only; breaking = 0 leaves the
@@ -255,15 +255,16 @@ typedef struct hw2d_tables {
     const double* brchar;       /* [ny*nx] pb.Char (cfSA, 0 where cfSA or ChiAdj < 1) */
     const double* x;            /* [nx] dominfo.x                               */
     const double* y;            /* [ny] dominfo.y                               */
-    double dx, dy;              /* dominfo.dx, dominfo.dy                       */
+    double dx, dy;              /* dominfo.dx, dominfo.dy (also read by walls with
+                                   refl_coef == 1 on the flat bottom)            */
     double max_eta_init;        /* pb.MaxEtaInit = 0.9 Hs / 2                   */
     double tstar;               /* pb.Tstar = Tchar Tp                          */
     double rsearch;             /* pb.Rsearch = 2 pi / kp / 4                   */
     double kbc, tc, delb;       /* pb.KBC, pb.TC, pb.delb (1.5)                 */
     double cur_u;               /* dominfo.U                                    */
     double t0, dt_out;          /* dominfo.t[0], dominfo.dt (breaking.dat cadence) */
-    double refl_coef;           /* walls: refl_coef (the flat RHS's fun_delphiH1hat branches
-                                   on refl_coef == 1; that flux branch is not built) */
+    double refl_coef;           /* walls: refl_coef (the flat RHS's fun_delphiH1hat takes its
+                                   flux branch when it is 1)                     */
 } hw2d_tables;
 
 /* opts: eps_abs/eps_rel (<= 0: the 2D reference's 1e-3 / 1e-2, 2d/main.c:196-197),

@@ -41,6 +41,8 @@ struct or2d_ctx {
     int var;                                           /* varying bottom (two reference depths) */
     double *gmin, *gplus, *cmin, *cplus, *omin, *oplus;
     double* wallchar;                                  /* NULL: no wall */
+    int refl_one;                                      /* flat bottom, refl_coef == 1 */
+    double *gwx, *gwy;                                 /* fun_gradient(wallchar) (refl_one) */
     struct brk2* brk;                                  /* kinematic breaking, NULL: off */
     long long rhs_calls, acc, rej;
     /* rkf45 work vectors */
@@ -49,6 +51,7 @@ struct or2d_ctx {
 
 struct brk2;
 static struct brk2* brk_create(const or2d_tables* tb);
+static void fun_gradient2(const double* f, int Nx, int Ny, double dx, double dy, double* gx, double* gy);
 static void brk_destroy(struct brk2* b);
 
 static double* dup(const double* a, size_t n) {
@@ -165,12 +168,13 @@ or2d_ctx* or2d_create(const or2d_tables* tb, double eps_abs, double eps_rel) {
         c->omin = dup(tb->om2_min, n); c->oplus = dup(tb->om2_plus, n);
     }
     if (tb->wallchar) {
-        if (!c->var && tb->refl_coef >= 1) {
-            set_err2("or2d_create: fully reflecting walls on the flat bottom (the flux branch of fun_delphiH1hat) are not restated");
-            free(c);
-            return NULL;
-        }
         c->wallchar = dup(tb->wallchar, n);
+        if (!c->var && tb->refl_coef == 1) {
+            if (!(tb->dx > 0) || !(tb->dy > 0)) { set_err2("or2d_create: walls with refl_coef 1 need dx, dy"); free(c); return NULL; }
+            c->refl_one = 1;
+            c->gwx = malloc(sizeof(double) * n); c->gwy = malloc(sizeof(double) * n);
+            fun_gradient2(c->wallchar, c->nx, c->ny, tb->dx, tb->dy, c->gwx, c->gwy);   /* 2d/functions.c:741 */
+        }
     }
     if (tb->breaking) {
         if (c->model != 2) { set_err2("or2d_create: breaking is restated for the HS2 RHS only"); free(c); return NULL; }
@@ -194,7 +198,7 @@ void or2d_destroy(or2d_ctx* c) {
     double* f[] = {c->kx, c->ky, c->c2d, c->l2d, c->aal, c->charac, c->chiadj, c->newgam, c->skewgam, c->tsig,
                    c->sig, c->sigskew, c->csig, c->csigskew, c->k1, c->k2, c->k3, c->k4, c->k5, c->k6, c->ytmp,
                    c->y0, c->yerr, c->dydt_in, c->dydt_out, c->gmin, c->gplus, c->cmin, c->cplus, c->omin,
-                   c->oplus, c->wallchar};
+                   c->oplus, c->wallchar, c->gwx, c->gwy};
     for (size_t q = 0; q < sizeof f / sizeof f[0]; q++) free(f[q]);
     brk_destroy(c->brk);
     free(c);
@@ -926,7 +930,38 @@ int or2d_rhs(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
             delphiH1hat[q].re = kx[j] * du.im + ky[i] * dv.im;
             delphiH1hat[q].im = -kx[j] * du.re - ky[i] * dv.re;
         }
-    if (c->wallchar) {
+    if (c->wallchar && c->refl_one) {
+        /* fun_delphiH1hat's branch for refl_coef == 1 (2d/fun_odesolver.c:2105-2170):
+         * Flux = Re F^-1 S(C^2/g u^) / N (both components), divC2u from the symmetrised
+         * spectra, delphiH1^ = F(divC2u wallchar) - F(Flux . grad wallchar) */
+        cx *A = malloc(sizeof(cx) * n), *B = malloc(sizeof(cx) * n), *D = malloc(sizeof(cx) * n);
+        for (int q = 0; q < n; q++) {
+            const double c2 = pow(c->c2d[q], 2);
+            A[q].re = c2 * Zhat[2 * n + q] / GRAV; A[q].im = c2 * Zhat[3 * n + q] / GRAV;
+            B[q].re = c2 * Zhat[4 * n + q] / GRAV; B[q].im = c2 * Zhat[5 * n + q] / GRAV;
+        }
+        sym2(A, Nx, Ny); sym2(B, Nx, Ny);   /* ifftw_2d_c2r symmetrises its input in place */
+        for (int i = 0; i < Ny; i++)
+            for (int j = 0; j < Nx; j++) {
+                const int q = i * Nx + j;
+                D[q].re = -(-kx[j] * A[q].im - ky[i] * B[q].im);
+                D[q].im = -(kx[j] * A[q].re + ky[i] * B[q].re);
+            }
+        sym2(D, Nx, Ny);
+        fft2(Nx, Ny, A, +1); fft2(Nx, Ny, B, +1); fft2(Nx, Ny, D, +1);
+        cx *W = malloc(sizeof(cx) * n), *F = malloc(sizeof(cx) * n);
+        for (int q = 0; q < n; q++) {
+            const double fx = A[q].re / (Nx * Ny), fy = B[q].re / (Nx * Ny), dv = D[q].re / (Nx * Ny);
+            W[q].re = dv * c->wallchar[q]; W[q].im = 0;
+            F[q].re = fx * c->gwx[q] + fy * c->gwy[q]; F[q].im = 0;
+        }
+        fft2(Nx, Ny, W, -1); fft2(Nx, Ny, F, -1);
+        for (int q = 0; q < n; q++) {
+            delphiH1hat[q].re = W[q].re - F[q].re;
+            delphiH1hat[q].im = W[q].im - F[q].im;
+        }
+        free(A); free(B); free(D); free(W); free(F);
+    } else if (c->wallchar) {
         /* fun_delphiH1hat's wall branch for refl_coef < 1 (2d/fun_odesolver.c:2172-2219):
          * C u^, C v^ to physical space (symmetrised, real part over N), times wallchar,
          * back (r2c), times C/g, then -i (kx . + ky .) */

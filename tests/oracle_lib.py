@@ -239,7 +239,7 @@ class Oracle2D:
         for k in ("bathy", "brchar", "x", "y"):
             keep[k] = np.ascontiguousarray(tables[k], dtype=np.float64) if brk else None
         self._keep = keep
-        scal = {k: float(tables.get(k, 0.0)) for k in BRK_SCALARS} if brk else {}
+        scal = {k: float(tables.get(k, 0.0)) for k in BRK_SCALARS}
         tb = Or2dTables(nx=int(tables["nx"]), ny=int(tables["ny"]), model=int(tables.get("model", 2)),
                         propagation=int(tables.get("propagation", 0)), cpeak=float(tables["cpeak"]),
                         nt=int(tables.get("nt", 0) if keep["sig"] is not None else 0), breaking=brk, **scal,

@@ -174,12 +174,23 @@ def test_run_to_time_parity_wall(bottom):
     assert tg == to and rel(yg, y) < 1e-9
 
 
-def test_fully_reflecting_wall_on_flat_bottom_rejected():
-    """refl_coef = 1 takes fun_delphiH1hat's flux branch, which is not built."""
-    tb = tables(64, 64, walls=_wall(64, 64))
-    tb["refl_coef"] = 1.0
-    with pytest.raises(Exception):
-        Engine2D(tb)
+@pytest.mark.parametrize("nx,ny", [(64, 64), (128, 64)])
+def test_fully_reflecting_wall_flat_bottom(nx, ny):
+    """refl_coef = 1: fun_delphiH1hat's flux branch (divergence through the mask,
+    fluxes through its gradient)."""
+    tb = decks2d.tables(nx=nx, ny=ny, Lx=0.9 * nx, Ly=0.9 * ny, depth=2.0, Hs=0.1, Tp=3.0, n_freq=24, n_dir=6,
+                        t_end=6.0, dt=0.1, damp=6.0, x_line=10.0, seed=1, walls=_wall(nx, ny), refl=1.0)
+    assert tb["refl_coef"] == 1.0 and (tb["wallchar"] == 0).any()
+    eng, ora = Engine2D(tb, 1e-8, 1e-6), Oracle2D(tb, 1e-8, 1e-6)
+    y = band_limited_state(tb, 0.02, 5)
+    assert rel(eng.rhs(0.9, y), ora.rhs(0.9, y)) < 1e-11
+    if nx == 64:
+        y = np.zeros(6 * nx * ny)
+        eng.set_state(0.0, 0.02, y)
+        to, ho = ora.run_to(0.0, 2.0, 0.02, y)
+        eng.run_to_time(2.0)
+        tg, hg, yg = eng.state()
+        assert tg == to and rel(yg, y) < 1e-9
 
 
 @pytest.mark.parametrize("nx,ny,prop,bottom", [(64, 64, 0, "flat"), (128, 64, 2, "flat"), (64, 128, 0, "shoal")])
