@@ -572,19 +572,26 @@ WORKLOAD_C2 = ("1D plain FP64, varying bathymetry and breaking: L = 400 m, Nx = 
                "gamma 3.3 (1024 lines), RKF45 rtol 1e-6 atol 1e-8, t_end 200 s")
 
 
-def _c2_deck():
+WORKLOAD_C1 = ("1D plain FP64: periodic tank L = 200 m, Nx = 4096, flat depth 1.0 m, HS2, no breaking, seeded "
+               "JONSWAP influx at x = 20 m (Hs 0.10 m, Tp 2.0 s, gamma 3.3, 1024 lines), 10 m damping zones, "
+               "RKF45 rtol 1e-6 atol 1e-8, t_end 100 s")
+# single runs: (deck writer, reference depths, samples per step, slice, workload text)
+SINGLE = {"c1": ("config1_deck", 0, 40, 512, WORKLOAD_C1), "c2": ("config2_deck", C2_NREF, C2_STEP_SAMPLES, 0, WORKLOAD_C2)}
+
+
+def _c2_deck(which="c2"):
     from hawassi_c_b200 import decks
-    p = os.path.join(tempfile.gettempdir(), "hw_bench_c2")
+    p = os.path.join(tempfile.gettempdir(), f"hw_bench_{which}")
     if not os.path.exists(os.path.join(p, "input.txt")):
-        decks.config2_deck(p, seed=0)
+        getattr(decks, SINGLE[which][0])(p, seed=0)
     return p
 
 
-def _c2_cpu(deck, max_seconds):
-    """The oracle port (16 reference depths) on one host thread from t0 for ~max_seconds."""
+def _c2_cpu(deck, max_seconds, nref=C2_NREF):
+    """The oracle port on one host thread from t0 for ~max_seconds."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib as ol
-    o = ol.Oracle(deck, eps_abs=EPS_ABS, eps_rel=EPS_REL, nref=C2_NREF)
+    o = ol.Oracle(deck, eps_abs=EPS_ABS, eps_rel=EPS_REL, nref=nref)
     tt = o.table("ttrace")
     y = o.initial_state()
     t, h = float(tt[0]), 1e-4
@@ -601,10 +608,12 @@ def _c2_cpu(deck, max_seconds):
 
 
 def main_c2(args, rank, world, local):
-    deck = _c2_deck()
+    which = args.workload
+    _, nref, step_samples, slice_default, workload_text = SINGLE[which]
+    deck = _c2_deck(which)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        sim, wall, pts = _c2_cpu(deck, 15.0)
+        sim, wall, pts = _c2_cpu(deck, 15.0, nref)
         cpu = {"value": pts / wall, "unit": "RHS grid-point evaluations/s", "cores": 1, "kind": "port",
                "sample": f"the first {sim:.3f} simulated s of the run from t0 on one thread (~15 s), "
                          f"{sim / wall:.4f} sim-s/wall-s"}
@@ -616,13 +625,14 @@ def main_c2(args, rank, world, local):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     import hawassi_c_b200 as hw
-    eng = hw.Engine(deck, eps_abs=EPS_ABS, eps_rel=EPS_REL, nref=C2_NREF, device=local, slice=args.slice)
+    slice_ = args.slice or slice_default
+    eng = hw.Engine(deck, eps_abs=EPS_ABS, eps_rel=EPS_REL, nref=nref, device=local, slice=slice_)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     eng.set_stream(stream.cuda_stream)
     i = 0
     for _ in range(args.warmup):
-        i += C2_STEP_SAMPLES
+        i += step_samples
         eng.run(i, sync=False)
     torch.cuda.synchronize()
     s0, t0 = eng.stats(), eng.state()[0]
@@ -633,7 +643,7 @@ def main_c2(args, rank, world, local):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        i += C2_STEP_SAMPLES
+        i += step_samples
         eng.run(i, sync=False)
     e1.record(stream)
     torch.cuda.synchronize()
@@ -651,7 +661,7 @@ def main_c2(args, rank, world, local):
     eng.reset()
     i = 0
     for _ in range(args.warmup):
-        i += C2_STEP_SAMPLES
+        i += step_samples
         eng.run(i, sync=False)
     host = torch.empty(4 * nx, dtype=torch.float64, pin_memory=True)
     hv = host.numpy()
@@ -661,7 +671,7 @@ def main_c2(args, rank, world, local):
     e0.record(stream)
     for _ in range(args.steps):
         eng.set_states(hv)
-        i += C2_STEP_SAMPLES
+        i += step_samples
         eng.run(i, sync=False)
         eng.get_states(hv)
     e1.record(stream)
@@ -675,8 +685,8 @@ def main_c2(args, rank, world, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic seeded deck (slope bathymetry, JONSWAP influx) in the reference input format",
-            "config": {"workload": WORKLOAD_C2, "step_samples": C2_STEP_SAMPLES, "slice": args.slice or 2048,
-                       "l2": "single member (2 MB state, 16 reference tables) resident in L2"},
+            "config": {"workload": workload_text, "step_samples": step_samples, "slice": slice_ or 2048,
+                       "l2": "single member resident in L2: latency-bound, no roofline claim"},
             "sim_s_per_wall_s": sim / (ms / 1e3), "rhs_calls": s1["rhs_calls"] - s0["rhs_calls"],
             "accepted": s1["accepted"] - s0["accepted"], "rejected": s1["rejected"] - s0["rejected"],
             "roofline": None, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
@@ -698,7 +708,7 @@ def main():
     ap.add_argument("--members", type=int, default=MEMBERS)
     ap.add_argument("--window", type=int, default=WINDOW)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "2d", "fbr005", "c2"])
+    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "2d", "fbr005", "c1", "c2"])
     ap.add_argument("--slice", type=int, default=0,
                     help="fbr005: grid points per CTA of the member's cluster (0: 512)")
     ap.add_argument("--autotune", action="store_true",
@@ -713,18 +723,20 @@ def main():
         if args.impl == "reference":
             return run_reference_2d(args, rank, world)
         return main_2d(args, rank, world, local)
-    if args.workload == "c2":
+    if args.workload in SINGLE:
         if args.impl == "reference":
             if rank != 0:
                 return 0
-            sim, wall, pts = _c2_cpu(_c2_deck(), 5.0 * (args.steps + args.warmup))
+            sim, wall, pts = _c2_cpu(_c2_deck(args.workload), 5.0 * (args.steps + args.warmup),
+                                     SINGLE[args.workload][1])
             value = pts / wall
             print(json.dumps({
                 "metric": "RHS grid-pt evals/s", "value": value, "unit": "RHS grid-point evaluations/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": 1e3 * wall / max(1, args.steps + args.warmup), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic seeded deck",
-                "config": {"workload": WORKLOAD_C2}, "impl": "reference", "sim_s_per_wall_s": sim / wall,
+                "config": {"workload": SINGLE[args.workload][4]}, "impl": "reference",
+                "sim_s_per_wall_s": sim / wall,
                 "cpu_baseline": {"value": value, "unit": "RHS grid-point evaluations/s", "cores": 1, "kind": "port",
                                  "sample": f"the first {sim:.3f} simulated s from t0 on one thread"},
                 "e2e": {"value": value, "unit": "RHS grid-point evaluations/s", "h2d_bytes_per_step": 0,
