@@ -684,7 +684,7 @@ def main_c2(args, rank, world, local):
             "metric": "RHS grid-pt evals/s", "value": value, "unit": "RHS grid-point evaluations/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic seeded deck (slope bathymetry, JONSWAP influx) in the reference input format",
+            "data": "synthetic seeded deck (JONSWAP influx) in the reference input format",
             "config": {"workload": workload_text, "step_samples": step_samples, "slice": slice_ or 2048,
                        "l2": "single member resident in L2: latency-bound, no roofline claim"},
             "sim_s_per_wall_s": sim / (ms / 1e3), "rhs_calls": s1["rhs_calls"] - s0["rhs_calls"],
