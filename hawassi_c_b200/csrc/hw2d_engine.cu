@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -17,6 +18,7 @@
 #include "../../include/hawassi_b200.h"
 #include "hw2d.cuh"
 #include "hw2d_brk.cuh"
+#include "hw2d_out.cuh"
 #include "hw2d_var.cuh"
 #include "hw2d_wall.cuh"
 #include "hw_setup.hpp"
@@ -60,6 +62,27 @@ void set_attrs() {
   cudaFuncSetAttribute(hw2d::k2w_rowV1<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(4));
   cudaFuncSetAttribute(hw2d::k2w_colV2<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(4));
   cudaFuncSetAttribute(hw2d::k2w_rowV3<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(2));
+  cudaFuncSetAttribute(hw2d::k2o_row<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(4));
+  cudaFuncSetAttribute(hw2d::k2o_col<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(4));
+}
+
+// the output stage's two passes (row M = nx, column M = ny)
+template <int M>
+void launch_out(int which, int nblocks, cudaStream_t s, const Tab2& tb, const double2* z, double2* P, double* phys,
+                float* f32) {
+  const int blk = hw2d::kGroups * (M / 8);
+  if (which == 0) hw2d::k2o_row<M><<<nblocks, blk, smem_bytes<M>(4), s>>>(tb, z, P);
+  else hw2d::k2o_col<M><<<nblocks, blk, smem_bytes<M>(4), s>>>(tb, P, phys, f32);
+}
+void out_pass(int M, int which, int nb, cudaStream_t s, const Tab2& tb, const double2* z, double2* P, double* phys,
+              float* f32) {
+  switch (M) {
+    case 64: launch_out<64>(which, nb, s, tb, z, P, phys, f32); break;
+    case 128: launch_out<128>(which, nb, s, tb, z, P, phys, f32); break;
+    case 256: launch_out<256>(which, nb, s, tb, z, P, phys, f32); break;
+    case 512: launch_out<512>(which, nb, s, tb, z, P, phys, f32); break;
+    default: launch_out<1024>(which, nb, s, tb, z, P, phys, f32); break;
+  }
 }
 
 // the flat bottom's wall round trip (row M = nx, column M = ny)
@@ -204,6 +227,15 @@ struct hw2d_ctx {
   cudaGraphExec_t attempt = nullptr;
   cudaStream_t graph_stream = nullptr;
   double h_first = 0.0;
+  // output stage (allocated at first use)
+  double2* oP = nullptr;    // 2n packed transforms
+  double* ophys = nullptr;  // 3n eta, u, v
+  float* of32 = nullptr;    // 3n float copies
+  float* hf32 = nullptr;    // pinned host copy of of32
+  int* ogpt = nullptr;      // gauge grid points
+  double* ogval = nullptr;  // 3 values per gauge
+  double* hgval = nullptr;  // pinned host copy of ogval
+  int ogcap = 0;
   long long launches = 0;   // kernels issued (graph nodes counted one by one)
   int per_rhs = 5;
   std::string err;
@@ -355,7 +387,38 @@ struct hw2d_ctx {
     if (hctl->status == hw2d::kBreakCapacity) { err = "breaking: a capacity (peaks, crests or nodes) was exceeded"; return 1; }
     return 0;
   }
+  bool ensure_out(int ngauge) {
+    if (!oP) {
+      oP = dalloc<double2>(2 * n);
+      ophys = dalloc<double>(3 * n);
+      of32 = dalloc<float>(3 * n);
+      if (!oP || !ophys || !of32 || cudaMallocHost(&hf32, 3 * n * sizeof(float)) != cudaSuccess) {
+        err = "output buffers: out of memory";
+        return false;
+      }
+    }
+    if (ngauge > ogcap) {
+      if (hgval) cudaFreeHost(hgval);
+      hgval = nullptr;
+      ogpt = dalloc<int>(ngauge);
+      ogval = dalloc<double>(3 * (size_t)ngauge);
+      if (!ogpt || !ogval || cudaMallocHost(&hgval, 3 * (size_t)ngauge * sizeof(double)) != cudaSuccess) {
+        err = "gauge buffers: out of memory";
+        return false;
+      }
+      ogcap = ngauge;
+    }
+    return true;
+  }
+  // eta, u, v of the current state (hctl must be current) into ophys (and of32)
+  void fields_launch(cudaStream_t s, bool keep_f32) {
+    out_pass(nx, 0, ny / 2, s, tb, rk.y[hctl->cur], oP, ophys, nullptr);
+    out_pass(ny, 1, nx / 2, s, tb, rk.y[hctl->cur], oP, ophys, keep_f32 ? of32 : nullptr);
+    launches += 2;
+  }
   ~hw2d_ctx() {
+    if (hf32) cudaFreeHost(hf32);
+    if (hgval) cudaFreeHost(hgval);
     if (attempt) cudaGraphExecDestroy(attempt);
     if (graph_stream) cudaStreamDestroy(graph_stream);
     for (void* p : allocs) cudaFree(p);
@@ -770,6 +833,176 @@ int hw2d_breaking_log(hw2d_ctx* c, double* times, int* counts, int* nodes, int c
     return -1;
   if (st.err & hw2d::kBrkErrLog) return -2;
   return st.nrec;
+}
+
+int hw2d_fields(hw2d_ctx* c, double* eta, double* u, double* v) {
+  if (!c) return 1;
+  cudaSetDevice(c->device);
+  if (!c->ensure_out(0) || !c->read_ctl()) return 1;
+  c->fields_launch(c->stream, false);
+  if (!c->check("hw2d_fields")) return 1;
+  double* dst[3] = {eta, u, v};
+  for (int f = 0; f < 3; ++f)
+    if (dst[f] && cudaMemcpyAsync(dst[f], c->ophys + f * c->n, c->n * sizeof(double), cudaMemcpyDeviceToHost,
+                                  c->stream) != cudaSuccess)
+      return c->check("hw2d_fields") ? 1 : 1;
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return c->check("hw2d_fields") ? 1 : 1;
+  return 0;
+}
+
+namespace {
+
+// the file set of ode_solver_uv's output loop; every file is closed on the way out
+struct OutFiles {
+  FILE* part[3] = {nullptr, nullptr, nullptr};   // Hawassi_eta/u/v_NN.dat
+  FILE* gauge[3] = {nullptr, nullptr, nullptr};  // Hawassi_eta/u/v_gauge.dat
+  void close_part() {
+    for (FILE*& f : part)
+      if (f) { fclose(f); f = nullptr; }
+  }
+  ~OutFiles() {
+    close_part();
+    for (FILE*& f : gauge)
+      if (f) { fclose(f); f = nullptr; }
+  }
+};
+
+// print_xt (2d/fun_odesolver.c:2532-2563)
+bool write_constant(const std::string& path, const hw2d_outputs* o, int nx, int ny, int ntpart) {
+  FILE* f = fopen(path.c_str(), "wb");
+  if (!f) return false;
+  std::vector<double> th(ntpart);
+  for (int j = 0; j < ntpart; ++j) th[j] = (0 + j) * o->dt;
+  const double NX = nx, NT = ntpart, NY = ny;
+  const size_t n = (size_t)nx * ny;
+  bool ok = fwrite(&NX, sizeof(double), 1, f) == 1 && fwrite(o->x, sizeof(double), nx, f) == (size_t)nx &&
+            fwrite(&NY, sizeof(double), 1, f) == 1 && fwrite(o->y, sizeof(double), ny, f) == (size_t)ny &&
+            fwrite(&NT, sizeof(double), 1, f) == 1 &&
+            fwrite(th.data(), sizeof(double), ntpart, f) == (size_t)ntpart &&
+            fwrite(&o->hs, sizeof(double), 1, f) == 1 && fwrite(&o->kp, sizeof(double), 1, f) == 1 &&
+            fwrite(&o->wp, sizeof(double), 1, f) == 1 && fwrite(o->kx, sizeof(double), nx, f) == (size_t)nx &&
+            fwrite(o->ky, sizeof(double), ny, f) == (size_t)ny && fwrite(o->bathy, sizeof(double), n, f) == n &&
+            fwrite(o->cfsa, sizeof(double), n, f) == n;
+  if (ok && o->chiadjphi) ok = fwrite(o->chiadjphi, sizeof(double), n, f) == n;
+  return fclose(f) == 0 && ok;
+}
+
+}  // namespace
+
+int hw2d_run_outputs(hw2d_ctx* c, const hw2d_outputs* o) {
+  if (!c || !o) return -1;
+  cudaSetDevice(c->device);
+  auto fail = [&](const std::string& m) {
+    c->err = m;
+    return -1;
+  };
+  if (!o->outdir || o->nt < 1 || !o->tout) return fail("outputs: outdir, nt and tout are required");
+  if (o->npartition < 1 || o->nt / o->npartition < 1) return fail("outputs: npartition must be in [1, nt]");
+  if (!o->x || !o->y || !o->kx || !o->ky || !o->bathy || !o->cfsa)
+    return fail("outputs: x, y, kx, ky, bathy and cfsa are required (Constant_01.dat)");
+  if (o->ngauge < 0 || (o->ngauge > 0 && (!o->xgauge || !o->ygauge || !(o->dx > 0) || !(o->dy > 0))))
+    return fail("outputs: gauges need xgauge, ygauge, dx and dy");
+  const int nx = c->nx, ny = c->ny, ng = o->ngauge;
+  const size_t n = c->n;
+  const int ntpart = o->nt / o->npartition;
+  // index_gauge (2d/functions.c:774-781): the nearest grid point
+  std::vector<int> gx(ng), gy(ng), gpt(ng);
+  for (int j = 0; j < ng; ++j) {
+    const double fx = std::round((o->xgauge[j] - o->x[0]) / o->dx), fy = std::round((o->ygauge[j] - o->y[0]) / o->dy);
+    if (!(fx >= 0 && fx < nx && fy >= 0 && fy < ny)) return fail("Gauges are outside of the domain!");
+    gx[j] = (int)fx;
+    gy[j] = (int)fy;
+    gpt[j] = gy[j] * nx + gx[j];
+  }
+  if (!c->ensure_out(ng)) return -1;
+  if (ng > 0 && cudaMemcpy(c->ogpt, gpt.data(), ng * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+    return c->check("gauge upload") ? -1 : -1;
+  const std::string pre(o->outdir);
+  OutFiles files;
+  static const char* kField[3] = {"eta", "u", "v"};
+  if (ng > 0)
+    for (int f = 0; f < 3; ++f) {
+      files.gauge[f] = fopen((pre + "Hawassi_" + kField[f] + "_gauge.dat").c_str(), "wb");
+      if (!files.gauge[f]) return fail("cannot open " + pre + "Hawassi_" + kField[f] + "_gauge.dat");
+    }
+  int ipart = 1;
+  char name[64];
+  for (int i = 0; i < o->nt; ++i) {
+    if (c->run(o->tout[i], false)) return -1;
+    const double t = c->hctl->t;
+    const bool first = (i % ntpart) == 0;
+    const bool uv = o->uv_every_sample || first;
+    c->fields_launch(c->stream, true);
+    if (ng > 0) {
+      hw2d::k2o_gauge<<<(ng + 127) / 128, 128, 0, c->stream>>>(c->ophys, c->ogpt, ng, n, c->ogval);
+      c->launches += 1;
+      cudaMemcpyAsync(c->hgval, c->ogval, 3 * (size_t)ng * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    }
+    cudaMemcpyAsync(c->hf32, c->of32, (uv ? 3 : 1) * n * sizeof(float), cudaMemcpyDeviceToHost, c->stream);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess || !c->check("output stage")) return -1;
+    if (first) {
+      // the reference opens the next partition's files without closing the last ones
+      files.close_part();
+      for (int f = 0; f < 3; ++f) {
+        snprintf(name, sizeof name, "Hawassi_%s_%02d.dat", kField[f], ipart);
+        files.part[f] = fopen((pre + name).c_str(), "wb");
+        if (!files.part[f]) return fail("cannot open " + pre + name);
+      }
+      if (i == 0) {
+        snprintf(name, sizeof name, "Constant_%02d.dat", ipart);
+        if (!write_constant(pre + name, o, nx, ny, ntpart)) return fail("cannot write " + pre + name);
+      }
+      ++ipart;
+    }
+    bool ok = fwrite(c->hf32, sizeof(float), n, files.part[0]) == n;
+    if (uv)
+      ok = ok && fwrite(c->hf32 + n, sizeof(float), n, files.part[1]) == n &&
+           fwrite(c->hf32 + 2 * n, sizeof(float), n, files.part[2]) == n;
+    for (FILE* f : files.part) ok = ok && fflush(f) == 0;
+    if (ng > 0) {
+      // print_data_gauges_uv (2d/fun_odesolver.c:427-476)
+      for (int f = 0; f < 3; ++f) {
+        FILE* g = files.gauge[f];
+        if (i == 0) {
+          fprintf(g, "0 ");
+          for (int j = 0; j < ng; ++j) fprintf(g, "%f ", o->x[gx[j]]);
+          fprintf(g, "\n");
+          fprintf(g, "0 ");
+          for (int j = 0; j < ng; ++j) fprintf(g, "%f ", o->y[gy[j]]);
+          fprintf(g, "\n");
+        }
+        fprintf(g, "%f ", t);
+        for (int j = 0; j < ng; ++j) fprintf(g, "%f ", c->hgval[3 * j + f]);
+        fprintf(g, "\n");
+        ok = ok && fflush(g) == 0;
+      }
+    }
+    if (!ok) return fail("output files: write failed");
+    if (std::isnan(c->hf32[n - 1])) {
+      snprintf(name, sizeof name, "Time stepping failed at t=%fs.", t);
+      return fail(name);
+    }
+  }
+  if (c->brk.on) {
+    // breaking.dat (2d/breaking.c:707-718): "t" then " x y " per break node, one line a record
+    const int nrec = hw2d_breaking_log(c, nullptr, nullptr, nullptr, 0, 0);
+    if (nrec < 0) return fail(nrec == -2 ? "breaking log overflowed" : "breaking log read failed");
+    const long long nn = hw2d_breaking_log_nodes(c);
+    std::vector<double> tr(nrec);
+    std::vector<int> cnt(nrec), nodes(2 * (size_t)std::max(nn, 0LL));
+    if (hw2d_breaking_log(c, tr.data(), cnt.data(), nodes.data(), nrec, nn) != nrec)
+      return fail("breaking log read failed");
+    FILE* f = fopen((pre + "breaking.dat").c_str(), "w");
+    if (!f) return fail("cannot open " + pre + "breaking.dat");
+    size_t k = 0;
+    for (int r = 0; r < nrec; ++r) {
+      fprintf(f, "%lf ", tr[r]);
+      for (int j = 0; j < cnt[r] && k < (size_t)nn; ++j, ++k) fprintf(f, " %d %d ", nodes[2 * k], nodes[2 * k + 1]);
+      fprintf(f, "\n");
+    }
+    if (fclose(f) != 0) return fail("cannot write " + pre + "breaking.dat");
+  }
+  return o->nt;
 }
 
 int hw2d_set_stream(hw2d_ctx* c, void* s) {

@@ -398,10 +398,27 @@ def tables(nx=1024, ny=1024, Lx=300.0, Ly=300.0, depth=3.0, Hs=0.5, Tp=6.0, gamm
         extra["refl_coef"] = float(refl)
     extra.setdefault("dx", float(x[1] - x[0]))
     extra.setdefault("dy", float(y[1] - y[0]))
+    # what the output stage writes to Constant_01.dat besides the grids (print_xt)
+    extra.setdefault("bathy", f64(-(depth_field if depth_field is not None else np.full((ny, nx), float(depth)))))
+    cf_out = cfsa2d(x, y, damp, damp, damp, damp)
+    if wall is not None:
+        cf_out = np.minimum(cf_out, cfw)
+    extra.update(cfsa=f64(cf_out), hs=float(Hs), kp=float(kp), wp=float(wp))
     return dict(**extra, nx=nx, ny=ny, model=model, propagation=propagation, cpeak=float(cpeak), kx=f64(kx), ky=f64(ky),
                 c2d=f64(c2d), l2d=f64(l2d), aal=f64(aal), charac=f64(charac), chiadj=f64(chi),
                 newgam=f64(newgam), skewgam=f64(skewgam), nt=nt, tsig=f64(tsig), sig=f64(sig), sigskew=f64(sigs),
                 dt_out=dt, x=x, y=y)
+
+
+def outputs(tb, tout, npartition=1, gauges=None, uv_every_sample=False, chiadjphi=None) -> dict:
+    """The output-stage arguments of ode_solver_uv for a tables dict (keyword
+    arguments of Engine2D.run_outputs): output times, partitions, the grids and the
+    Constant_01.dat tables, gauges as (x, y) pairs."""
+    tout = np.asarray(tout, dtype=np.float64)
+    return dict(tout=tout, dt=float(tout[1] - tout[0]) if tout.size > 1 else 0.0, npartition=int(npartition),
+                x=tb["x"], y=tb["y"], dx=tb["dx"], dy=tb["dy"], kx=tb["kx"], ky=tb["ky"], bathy=tb["bathy"],
+                cfsa=tb["cfsa"], chiadjphi=chiadjphi, hs=tb["hs"], kp=tb["kp"], wp=tb["wp"], gauges=gauges,
+                uv_every_sample=uv_every_sample)
 
 
 def config5(seed=0, bathymetry="shoal", **kw) -> dict:

@@ -7,6 +7,7 @@ and exposes ``rhs`` (rhs_AB2_2DF_uv, 2d/fun_odesolver.c:4458), ``evolve_apply``
 ode_solver_uv, :2641-2647) with the state resident on the device.
 """
 import ctypes
+import os
 
 import numpy as np
 
@@ -30,6 +31,36 @@ class Hw2dTables(ctypes.Structure):
         ("delb", ctypes.c_double), ("cur_u", ctypes.c_double), ("t0", ctypes.c_double), ("dt_out", ctypes.c_double),
         ("refl_coef", ctypes.c_double),
     ]
+
+
+class Hw2dOutputs(ctypes.Structure):
+    _fields_ = [
+        ("outdir", ctypes.c_char_p), ("nt", ctypes.c_int), ("tout", _dp), ("dt", ctypes.c_double),
+        ("npartition", ctypes.c_int), ("uv_every_sample", ctypes.c_int),
+        ("hs", ctypes.c_double), ("kp", ctypes.c_double), ("wp", ctypes.c_double),
+        ("x", _dp), ("y", _dp), ("dx", ctypes.c_double), ("dy", ctypes.c_double),
+        ("kx", _dp), ("ky", _dp), ("bathy", _dp), ("cfsa", _dp), ("chiadjphi", _dp),
+        ("ngauge", ctypes.c_int), ("xgauge", _dp), ("ygauge", _dp),
+    ]
+
+
+def output_spec(struct, outdir, tout, dt, npartition, x, y, dx, dy, kx, ky, bathy, cfsa, chiadjphi=None,
+                hs=0.0, kp=0.0, wp=0.0, gauges=None, uv_every_sample=False):
+    """Fill an outputs structure (hw2d_outputs layout); returns it and the arrays it
+    points into, which the caller keeps alive for the call."""
+    keep = {k: np.ascontiguousarray(v, dtype=np.float64) for k, v in
+            dict(tout=tout, x=x, y=y, kx=kx, ky=ky, bathy=bathy, cfsa=cfsa).items()}
+    keep["chiadjphi"] = None if chiadjphi is None else np.ascontiguousarray(chiadjphi, dtype=np.float64)
+    g = np.zeros((0, 2)) if gauges is None else np.asarray(gauges, dtype=np.float64).reshape(-1, 2)
+    keep["xgauge"], keep["ygauge"] = np.ascontiguousarray(g[:, 0]), np.ascontiguousarray(g[:, 1])
+    keep["outdir"] = os.path.join(str(outdir), "").encode()
+    spec = struct(outdir=keep["outdir"], nt=len(keep["tout"]), dt=float(dt), npartition=int(npartition),
+                  uv_every_sample=int(bool(uv_every_sample)), hs=float(hs), kp=float(kp), wp=float(wp),
+                  dx=float(dx), dy=float(dy), ngauge=len(g),
+                  **{k: _ptr(keep[k]) if len(g) or k not in ("xgauge", "ygauge") else None
+                     for k in ("tout", "x", "y", "kx", "ky", "bathy", "cfsa", "chiadjphi", "xgauge", "ygauge")})
+    return spec, keep
+
 
 # parambreak's scalars (2d/breaking.c:1-8) as the tables dict carries them
 BREAKING_SCALARS = ("dx", "dy", "max_eta_init", "tstar", "rsearch", "kbc", "tc", "delb", "cur_u", "t0", "dt_out")
@@ -67,6 +98,8 @@ def _lib():
         L.hw2d_breaking_log.argtypes = [vp, dp, ip, ip, ctypes.c_int, ctypes.c_longlong]
         L.hw2d_breaking_log_nodes.restype = ctypes.c_longlong
         L.hw2d_breaking_log_nodes.argtypes = [vp]
+        L.hw2d_fields.argtypes = [vp, dp, dp, dp]
+        L.hw2d_run_outputs.argtypes = [vp, ctypes.POINTER(Hw2dOutputs)]
         _bound = True
     return L
 
@@ -200,3 +233,24 @@ class Engine2D:
             out.append((float(t[r]), [tuple(v) for v in nodes[2 * off:2 * (off + c)].reshape(-1, 2).tolist()]))
             off += c
         return out
+
+    def fields(self):
+        """eta, u, v ([ny, nx] each) of the device state: ifftw_2d_c2r of each spectrum
+        (2d/functions1.c:523-557), as ode_solver_uv forms them at an output time."""
+        out = [np.empty(self.n) for _ in range(3)]
+        if self._L.hw2d_fields(self._h, *[_ptr(a) for a in out]):
+            raise self._err()
+        return tuple(a.reshape(self.ny, self.nx) for a in out)
+
+    def run_outputs(self, outdir, tout, dt, npartition, x, y, dx, dy, kx, ky, bathy, cfsa, chiadjphi=None,
+                    hs=0.0, kp=0.0, wp=0.0, gauges=None, uv_every_sample=False):
+        """ode_solver_uv's time loop with its output files (hw2d_run_outputs) from the
+        device state; gauges is a sequence of (x, y) as gauges.dat lists them.
+        Returns the samples written."""
+        spec, keep = output_spec(Hw2dOutputs, outdir, tout, dt, npartition, x, y, dx, dy, kx, ky, bathy, cfsa,
+                                 chiadjphi, hs, kp, wp, gauges, uv_every_sample)
+        r = self._L.hw2d_run_outputs(self._h, ctypes.byref(spec))
+        del keep
+        if r < 0:
+            raise self._err()
+        return r

@@ -301,6 +301,50 @@ int hw2d_breaking_fields(hw2d_ctx* ctx, double* B, double* sbx, double* sby, int
  * no breaking, -2: the device log overflowed and stopped). */
 int hw2d_breaking_log(hw2d_ctx* ctx, double* times, int* counts, int* nodes, int cap_rec, long long cap_nodes);
 long long hw2d_breaking_log_nodes(hw2d_ctx* ctx);
+
+/* Output stage of ode_solver_uv (2d/fun_odesolver.c:2565-2843).
+ * eta, u, v in physical space of the current device state: ifftw_2d_c2r of a copy
+ * of each spectrum (2d/functions1.c:523-557; the loop's :2648-2666), [ny*nx] each,
+ * row-major; any pointer may be NULL. */
+int hw2d_fields(hw2d_ctx* ctx, double* eta, double* u, double* v);
+
+typedef struct hw2d_outputs {
+    const char* outdir;         /* prefix of every file name (arg2, with its '/')      */
+    int nt;                     /* dominfo.Nt output samples                           */
+    const double* tout;         /* [nt] dominfo.t, the output times (tinterv)          */
+    double dt;                  /* dominfo.dt (time axis of Constant_01.dat)           */
+    int npartition;             /* "No of Partition": files hold Nt / npartition samples */
+    int uv_every_sample;        /* 0: u, v of each partition's first sample only (kinematic
+                                   "no", :2736-2748); 1: every sample (what kinematic "yes"
+                                   writes ahead of the kinematics module, :2756-2767) */
+    double hs, kp, wp;          /* seainfo.Hs, kp, wp                                  */
+    const double* x;            /* [nx] dominfo.x                                      */
+    const double* y;            /* [ny] dominfo.y                                      */
+    double dx, dy;              /* dominfo.dx, dominfo.dy (gauge indices)              */
+    const double* kx;           /* [nx] dominfo.kx                                     */
+    const double* ky;           /* [ny] dominfo.ky                                     */
+    const double* bathy;        /* [ny*nx] dominfo.bathy.data                          */
+    const double* cfsa;         /* [ny*nx] cfSA                                        */
+    const double* chiadjphi;    /* [ny*nx] ChiAdjPhi; NULL when wavename is zero       */
+    int ngauge;                 /* gauges.dat lines (0: no gauge files)                */
+    const double* xgauge;       /* [ngauge]                                            */
+    const double* ygauge;       /* [ngauge]                                            */
+} hw2d_outputs;
+
+/* The time loop of ode_solver_uv from the current device state (the reference
+ * starts it at t = tout[0] with h = (tout[1] - tout[0]) / 5: hw2d_set_state).  For
+ * every sample i it evolves to tout[i] on the device, transforms eta, u, v there
+ * and writes, with the reference's names under outdir:
+ *   Constant_01.dat        print_xt (:2532-2563) at i = 0 (:2687-2718)
+ *   Hawassi_eta_NN.dat     float32 eta [ny][nx] of every sample of partition NN (:2727-2734)
+ *   Hawassi_u_NN.dat, Hawassi_v_NN.dat   float32 u, v (uv_every_sample)
+ *   Hawassi_{eta,u,v}_gauge.dat          print_data_gauges_uv text (:427-476)
+ *   breaking.dat           the breaking records (2d/breaking.c:707-718), at the end
+ * Kinematics, runup, coupling and the gnuplot frames are not part of it.  Like the
+ * reference (:2819-2823; fun_max2darray's running comparison ends NaN exactly when
+ * the last grid point is NaN), it stops when the last grid point of eta is NaN.  Returns the samples written, or -1 (hw2d_last_error). */
+int hw2d_run_outputs(hw2d_ctx* ctx, const hw2d_outputs* spec);
+
 int hw2d_set_stream(hw2d_ctx* ctx, void* cuda_stream);
 int hw2d_synchronize(hw2d_ctx* ctx);
 

@@ -1231,3 +1231,165 @@ int or2d_run_to(or2d_ctx* c, double* t, double t1, double* h, double* y) {
     }
     return 0;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Output stage of ode_solver_uv                                             */
+/* ------------------------------------------------------------------------ */
+
+/* ifftw_2d_c2r (2d/functions1.c:523-557) on a copy of one spectrum */
+static void c2r2(int nx, int ny, const double* re, const double* im, double* out) {
+    int n = nx * ny;
+    cx* a = malloc(sizeof(cx) * n);
+    for (int q = 0; q < n; q++) { a[q].re = re[q]; a[q].im = im[q]; }
+    sym2(a, nx, ny);
+    fft2(nx, ny, a, +1);
+    for (int q = 0; q < n; q++) out[q] = a[q].re / (nx * ny);
+    free(a);
+}
+
+void or2d_fields(int nx, int ny, const double* y, double* eta, double* u, double* v) {
+    int n = nx * ny;
+    double* dst[3] = {eta, u, v};
+    for (int f = 0; f < 3; f++)
+        if (dst[f]) c2r2(nx, ny, y + 2 * f * n, y + (2 * f + 1) * n, dst[f]);
+}
+
+static FILE* open_named(const char* dir, const char* name, const char* mode) {
+    char path[1024];
+    snprintf(path, sizeof path, "%s%s", dir, name);
+    return fopen(path, mode);
+}
+
+/* print_xt (2d/fun_odesolver.c:2532-2563) */
+static void print_xt2(FILE* fpc, const or2d_outputs* o, int nx, int ny, int ntpart, const double* th) {
+    double NX = (double)nx, NT = (double)ntpart, NY = (double)ny;
+    fwrite(&NX, sizeof(double), 1, fpc);
+    fwrite(o->x, sizeof(double), nx, fpc);
+    fwrite(&NY, sizeof(double), 1, fpc);
+    fwrite(o->y, sizeof(double), ny, fpc);
+    fwrite(&NT, sizeof(double), 1, fpc);
+    fwrite(th, sizeof(double), ntpart, fpc);
+    fwrite(&o->hs, sizeof(double), 1, fpc);
+    fwrite(&o->kp, sizeof(double), 1, fpc);
+    fwrite(&o->wp, sizeof(double), 1, fpc);
+    fwrite(o->kx, sizeof(double), nx, fpc);
+    fwrite(o->ky, sizeof(double), ny, fpc);
+    for (int kk = 0; kk < ny; kk++) fwrite(o->bathy + (size_t)kk * nx, sizeof(double), nx, fpc);
+    for (int kk = 0; kk < ny; kk++) fwrite(o->cfsa + (size_t)kk * nx, sizeof(double), nx, fpc);
+    if (o->chiadjphi)
+        for (int kk = 0; kk < ny; kk++) fwrite(o->chiadjphi + (size_t)kk * nx, sizeof(double), nx, fpc);
+}
+
+int or2d_run_outputs(or2d_ctx* c, double* t, double* h, double* y, const or2d_outputs* o) {
+    const int nx = c->nx, ny = c->ny, n = c->n, ng = o->ngauge;
+    if (o->nt < 1 || o->npartition < 1 || o->nt / o->npartition < 1) { set_err2("npartition"); return -1; }
+    const int ntpart = o->nt / o->npartition;   /* 2d/fun_odesolver.c:2582 */
+    int* ix = malloc(sizeof(int) * (ng > 0 ? ng : 1));
+    int* iy = malloc(sizeof(int) * (ng > 0 ? ng : 1));
+    for (int j = 0; j < ng; j++) {   /* index_gauge, 2d/functions.c:774-781 */
+        ix[j] = (int)round((o->xgauge[j] - o->x[0]) / o->dx);
+        iy[j] = (int)round((o->ygauge[j] - o->y[0]) / o->dy);
+        if (ix[j] >= nx || iy[j] >= ny || ix[j] < 0 || iy[j] < 0) {
+            set_err2("Gauges are outside of the domain!");
+            free(ix); free(iy);
+            return -1;
+        }
+    }
+    double* eta = malloc(sizeof(double) * n);
+    double* u = malloc(sizeof(double) * n);
+    double* v = malloc(sizeof(double) * n);
+    FILE *fg1 = NULL, *fg2 = NULL, *fg3 = NULL, *feta = NULL, *fu = NULL, *fv = NULL;
+    if (ng > 0) {
+        fg1 = open_named(o->outdir, "Hawassi_eta_gauge.dat", "wb");
+        fg2 = open_named(o->outdir, "Hawassi_u_gauge.dat", "wb");
+        fg3 = open_named(o->outdir, "Hawassi_v_gauge.dat", "wb");
+    }
+    int ipart = 1, ret = o->nt;
+    for (int i = 0; i < o->nt; i++) {
+        double ti = o->tout[i];
+        while (*t < ti) {
+            if (or2d_evolve_apply(c, t, ti, h, y)) { ret = -1; goto done; }
+        }
+        or2d_fields(nx, ny, y, eta, u, v);
+        if ((i % ntpart) == 0) {
+            char s1[64];
+            if (feta) { fclose(feta); fclose(fu); fclose(fv); }
+            snprintf(s1, sizeof s1, "Hawassi_eta_%02d.dat", ipart); feta = open_named(o->outdir, s1, "wb");
+            snprintf(s1, sizeof s1, "Hawassi_u_%02d.dat", ipart); fu = open_named(o->outdir, s1, "wb");
+            snprintf(s1, sizeof s1, "Hawassi_v_%02d.dat", ipart); fv = open_named(o->outdir, s1, "wb");
+            if (i == 0) {
+                double* th = malloc(sizeof(double) * ntpart);
+                for (int j = 0; j < ntpart; j++) th[j] = (i + j) * o->dt;
+                snprintf(s1, sizeof s1, "Constant_%02d.dat", ipart);
+                FILE* fcon = open_named(o->outdir, s1, "wb");
+                print_xt2(fcon, o, nx, ny, ntpart, th);
+                fclose(fcon);
+                free(th);
+            }
+            ipart++;
+        }
+        for (int kk = 0; kk < ny; kk++)
+            for (int ll = 0; ll < nx; ll++) {
+                float fe = (float)eta[kk * nx + ll];
+                fwrite(&fe, sizeof(float), 1, feta);
+            }
+        fflush(feta);
+        if (o->uv_every_sample || (i % ntpart) == 0) {
+            for (int kk = 0; kk < ny; kk++)
+                for (int ll = 0; ll < nx; ll++) {
+                    float fu1 = (float)u[kk * nx + ll], fv1 = (float)v[kk * nx + ll];
+                    fwrite(&fu1, sizeof(float), 1, fu);
+                    fwrite(&fv1, sizeof(float), 1, fv);
+                }
+            fflush(fu);
+            fflush(fv);
+        }
+        if (ng > 0) {   /* print_data_gauges_uv, 2d/fun_odesolver.c:427-476 */
+            FILE* g[3] = {fg1, fg2, fg3};
+            const double* fld[3] = {eta, u, v};
+            if (i == 0) {
+                for (int f = 0; f < 3; f++) {
+                    fprintf(g[f], "0 ");
+                    for (int j = 0; j < ng; j++) fprintf(g[f], "%f ", o->x[ix[j]]);
+                    fprintf(g[f], "\n");
+                }
+                for (int f = 0; f < 3; f++) {
+                    fprintf(g[f], "0 ");
+                    for (int j = 0; j < ng; j++) fprintf(g[f], "%f ", o->y[iy[j]]);
+                    fprintf(g[f], "\n");
+                }
+            }
+            for (int f = 0; f < 3; f++) fprintf(g[f], "%f ", *t);
+            for (int j = 0; j < ng; j++)
+                for (int f = 0; f < 3; f++) fprintf(g[f], "%f ", fld[f][iy[j] * nx + ix[j]]);
+            for (int f = 0; f < 3; f++) { fprintf(g[f], "\n"); fflush(g[f]); }
+        }
+        /* fun_max2darray's running comparison (2d/functions1.c:130-139), then the
+         * NaN test of 2d/fun_odesolver.c:2819-2823 */
+        double mx = eta[0];
+        for (int q = 0; q < n; q++) mx = (mx > eta[q] ? mx : eta[q]);
+        if (isnan(mx)) { set_err2("Time stepping failed at t=%fs.", *t); ret = -1; goto done; }
+    }
+    if (c->brk) {   /* breaking.dat lines (2d/breaking.c:712-720) */
+        int nrec = or2d_brk_log(c, NULL, NULL, NULL, 0, 0);
+        long long nn = or2d_brk_log_nodes(c);
+        double* tr = malloc(sizeof(double) * (nrec > 0 ? nrec : 1));
+        int* cnt = malloc(sizeof(int) * (nrec > 0 ? nrec : 1));
+        int* nodes = malloc(sizeof(int) * 2 * (nn > 0 ? nn : 1));
+        or2d_brk_log(c, tr, cnt, nodes, nrec, (int)nn);
+        FILE* fb = open_named(o->outdir, "breaking.dat", "w");
+        long long k = 0;
+        for (int r = 0; r < nrec; r++) {
+            fprintf(fb, "%lf ", tr[r]);
+            for (int j = 0; j < cnt[r]; j++, k++) fprintf(fb, " %d %d ", nodes[2 * k], nodes[2 * k + 1]);
+            fprintf(fb, "\n");
+        }
+        fclose(fb);
+        free(tr); free(cnt); free(nodes);
+    }
+done:
+    if (feta) { fclose(feta); fclose(fu); fclose(fv); }
+    if (fg1) { fclose(fg1); fclose(fg2); fclose(fg3); }
+    free(eta); free(u); free(v); free(ix); free(iy);
+    return ret;
+}

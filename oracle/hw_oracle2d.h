@@ -99,6 +99,34 @@ void or2d_fft(int nx, int ny, const double* re_in, const double* im_in, double* 
 /* the reference's fftwcomplex_2d_sym applied in place to a complex [ny*nx] array */
 void or2d_sym(int nx, int ny, double* re, double* im);
 
+/* eta, u, v in physical space of a state y (6*nx*ny, reference layout):
+ * ifftw_2d_c2r of a copy of each spectrum (2d/functions1.c:523-557, called by
+ * ode_solver_uv at 2d/fun_odesolver.c:2648-2666).  Any output may be NULL. */
+void or2d_fields(int nx, int ny, const double* y, double* eta, double* u, double* v);
+
+/* the output files of ode_solver_uv's time loop (fields named as in the engine's
+ * hw2d_outputs) */
+typedef struct or2d_outputs {
+    const char* outdir;
+    int nt;
+    const double* tout;
+    double dt;
+    int npartition;
+    int uv_every_sample;
+    double hs, kp, wp;
+    const double *x, *y;
+    double dx, dy;
+    const double *kx, *ky, *bathy, *cfsa, *chiadjphi;
+    int ngauge;
+    const double *xgauge, *ygauge;
+} or2d_outputs;
+
+/* ode_solver_uv (2d/fun_odesolver.c:2565-2843) without kinematics, runup,
+ * coupling and plots, from (t, h, y): evolve to every output time, write
+ * Constant_01.dat, Hawassi_{eta,u,v}_NN.dat, the gauge files and breaking.dat.
+ * Returns the samples written or -1 (or2d_last_error). */
+int or2d_run_outputs(or2d_ctx* c, double* t, double* h, double* y, const or2d_outputs* o);
+
 #ifdef __cplusplus
 }
 #endif

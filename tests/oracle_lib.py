@@ -101,6 +101,8 @@ def lib():
         L.or2d_brk_log.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ip, ip]
         L.or2d_brk_log_nodes.restype = ctypes.c_longlong
         L.or2d_brk_log_nodes.argtypes = [vp]
+        L.or2d_fields.argtypes = [ip, ip, dp, dp, dp, dp]
+        L.or2d_run_outputs.argtypes = [vp, dp, dp, dp, ctypes.POINTER(Or2dOutputs)]
         _lib = L
     return _lib
 
@@ -316,6 +318,52 @@ class Oracle2D:
             out.append((float(t[r]), [tuple(v) for v in nodes[2 * off:2 * (off + c)].reshape(-1, 2).tolist()]))
             off += c
         return out
+
+
+class Or2dOutputs(ctypes.Structure):
+    """or2d_outputs (oracle/hw_oracle2d.h)."""
+    _fields_ = [
+        ("outdir", ctypes.c_char_p), ("nt", ctypes.c_int), ("tout", ctypes.POINTER(ctypes.c_double)),
+        ("dt", ctypes.c_double), ("npartition", ctypes.c_int), ("uv_every_sample", ctypes.c_int),
+        ("hs", ctypes.c_double), ("kp", ctypes.c_double), ("wp", ctypes.c_double),
+        ("x", ctypes.POINTER(ctypes.c_double)), ("y", ctypes.POINTER(ctypes.c_double)),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double),
+        ("kx", ctypes.POINTER(ctypes.c_double)), ("ky", ctypes.POINTER(ctypes.c_double)),
+        ("bathy", ctypes.POINTER(ctypes.c_double)), ("cfsa", ctypes.POINTER(ctypes.c_double)),
+        ("chiadjphi", ctypes.POINTER(ctypes.c_double)),
+        ("ngauge", ctypes.c_int), ("xgauge", ctypes.POINTER(ctypes.c_double)),
+        ("ygauge", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
+def run_outputs2d(ora, t, h, z, outdir, tout, dt, npartition, x, y, dx, dy, kx, ky, bathy, cfsa, chiadjphi=None,
+                  hs=0.0, kp=0.0, wp=0.0, gauges=None, uv_every_sample=False):
+    """or2d_run_outputs on an Oracle2D from (t, h, z); the state z is advanced in
+    place.  Returns (samples written, t, h)."""
+    keep = {k: np.ascontiguousarray(v, dtype=np.float64) for k, v in
+            dict(tout=tout, x=x, y=y, kx=kx, ky=ky, bathy=bathy, cfsa=cfsa).items()}
+    keep["chiadjphi"] = None if chiadjphi is None else np.ascontiguousarray(chiadjphi, dtype=np.float64)
+    g = np.zeros((0, 2)) if gauges is None else np.asarray(gauges, dtype=np.float64).reshape(-1, 2)
+    keep["xgauge"], keep["ygauge"] = np.ascontiguousarray(g[:, 0]), np.ascontiguousarray(g[:, 1])
+    od = os.path.join(str(outdir), "").encode()
+    spec = Or2dOutputs(outdir=od, nt=len(keep["tout"]), dt=float(dt), npartition=int(npartition),
+                       uv_every_sample=int(bool(uv_every_sample)), hs=float(hs), kp=float(kp), wp=float(wp),
+                       dx=float(dx), dy=float(dy), ngauge=len(g),
+                       **{k: (None if keep[k] is None or (k in ("xgauge", "ygauge") and not len(g)) else _p(keep[k]))
+                          for k in ("tout", "x", "y", "kx", "ky", "bathy", "cfsa", "chiadjphi", "xgauge", "ygauge")})
+    tt, hh = ctypes.c_double(t), ctypes.c_double(h)
+    r = lib().or2d_run_outputs(ora.h, ctypes.byref(tt), ctypes.byref(hh), _p(z), ctypes.byref(spec))
+    if r < 0:
+        raise RuntimeError("oracle2d: " + lib().or2d_last_error().decode())
+    return r, tt.value, hh.value
+
+
+def fields2d(nx, ny, y):
+    """eta, u, v ([ny, nx]) of a state: ifftw_2d_c2r of each spectrum."""
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    out = [np.zeros(nx * ny) for _ in range(3)]
+    lib().or2d_fields(nx, ny, _p(y), *[_p(a) for a in out])
+    return tuple(a.reshape(ny, nx) for a in out)
 
 
 def fft2(x, sign=-1):
