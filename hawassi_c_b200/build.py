@@ -20,7 +20,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 SOURCES = ["hw_engine.cu", "hw_setup.cpp", "hw_inst_256.cu", "hw_inst_512.cu", "hw_inst_1024.cu",
            "hw_inst_2048.cu", "hw_noalloc.cu", "hw_mlp.cu", "hw2d_engine.cu", "hw_kin.cu", "hw_influx.cu"]
 HEADERS = ["hw_fft.cuh", "hw_device.cuh", "hw_rhs.cuh", "hw_stepper.cuh", "hw_breaking.cuh",
-           "hw_kernels.cuh", "hw_kernels.h", "hw_setup.hpp", "hw_rhs_fast.cuh", "hw2d.cuh", "hw2d_var.cuh", "hw2d_brk.cuh", "hw2d_wall.cuh", "hw2d_out.cuh", "hw_output.cuh", "hw_kin.h"]
+           "hw_kernels.cuh", "hw_kernels.h", "hw_setup.hpp", "hw_rhs_fast.cuh", "hw2d.cuh", "hw2d_var.cuh", "hw2d_brk.cuh", "hw2d_wall.cuh", "hw2d_out.cuh", "hw2d_hs3.cuh", "hw_output.cuh", "hw_kin.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC"]

@@ -97,6 +97,10 @@ struct Work2 {
   double2* dph;
   // flat bottom with walls: the round trip of (C u^, C v^) (delphiH1^ lands in H1)
   double2* WP;
+  // HS3 on the flat bottom: eta, L phi in physical space (2 real fields) and the
+  // HS2 terms with (eta^2 M0u)^, (eta^2 M0v)^ between passes C3 and I3 (6 fields)
+  double* p3;
+  double2* T3;
 };
 
 // device control block of the stepper (one per engine)
@@ -701,7 +705,7 @@ k2_rowE(Tab2 tb, Work2 w, RK2 rk, const Ctl2* __restrict__ ctl, int mode, int co
         dphi = make_double2(kxv * du1.y + kyv * dv1.y, -kxv * du1.x - kyv * dv1.x);
       }
       double2 ix = slot(sm, M, 0 + k, j), iy = slot(sm, M, 2 + k, j);
-      if (tb.model == 2) {
+      if (tb.model != 1) {   // HS2, HS3 (the cubic terms are summed into the same slices)
         const double2 au = slot(sm, M, 4 + k, j), av = slot(sm, M, 6 + k, j);
         dphi = make_double2(dphi.x + au.x + av.x, dphi.y + au.y + av.y);
       } else {

@@ -18,6 +18,7 @@
 #include "../../include/hawassi_b200.h"
 #include "hw2d.cuh"
 #include "hw2d_brk.cuh"
+#include "hw2d_hs3.cuh"
 #include "hw2d_out.cuh"
 #include "hw2d_var.cuh"
 #include "hw2d_wall.cuh"
@@ -62,6 +63,10 @@ void set_attrs() {
   cudaFuncSetAttribute(hw2d::k2w_rowV1<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(4));
   cudaFuncSetAttribute(hw2d::k2w_colV2<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(4));
   cudaFuncSetAttribute(hw2d::k2w_rowV3<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(2));
+  cudaFuncSetAttribute(hw2d::k2_colB3<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(10));
+  cudaFuncSetAttribute(hw2d::k2_rowC3<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(10));
+  cudaFuncSetAttribute(hw2d::k2_colH3<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(6));
+  cudaFuncSetAttribute(hw2d::k2_rowI3<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(8));
   cudaFuncSetAttribute(hw2d::k2o_row<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(4));
   cudaFuncSetAttribute(hw2d::k2o_col<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(4));
 }
@@ -153,6 +158,8 @@ void launch_row(int which, int nblocks, cudaStream_t s, const Tab2& tb, const Wo
   else if (which == 12) hw2d::k2v_rowC<M><<<nblocks, blk, smem_bytes<M>(12), s>>>(tb, w, ctl, cond);
   else if (which == 14) hw2d::k2v_rowE<M><<<nblocks, blk, smem_bytes<M>(6), s>>>(tb, w, ctl, cond);
   else if (which == 16) hw2d::k2v_rowG<M><<<nblocks, blk, smem_bytes<M>(8), s>>>(tb, w, ctl, cond);
+  else if (which == 20) hw2d::k2_rowC3<M><<<nblocks, blk, smem_bytes<M>(10), s>>>(tb, w, ctl, cond);
+  else if (which == 22) hw2d::k2_rowI3<M><<<nblocks, blk, smem_bytes<M>(8), s>>>(tb, w, ctl, cond);
   else hw2d::k2_rowE<M><<<nblocks, blk, smem_bytes<M>(8), s>>>(tb, w, rk, ctl, mode, cond, out);
 }
 template <int M>
@@ -162,6 +169,8 @@ void launch_col(int which, int nblocks, cudaStream_t s, const Tab2& tb, const Wo
   else if (which == 11) hw2d::k2v_colB<M><<<nblocks, blk, smem_bytes<M>(12), s>>>(tb, w, ctl, cond);
   else if (which == 13) hw2d::k2v_colD<M><<<nblocks, blk, smem_bytes<M>(6), s>>>(tb, w, ctl, cond);
   else if (which == 15) hw2d::k2v_colF<M><<<nblocks, blk, smem_bytes<M>(8), s>>>(tb, w, ctl, cond);
+  else if (which == 21) hw2d::k2_colB3<M><<<nblocks, blk, smem_bytes<M>(10), s>>>(tb, w, ctl, cond);
+  else if (which == 23) hw2d::k2_colH3<M><<<nblocks, blk, smem_bytes<M>(6), s>>>(tb, w, ctl, cond);
   else hw2d::k2_colD<M><<<nblocks, blk, smem_bytes<M>(10), s>>>(tb, w, ctl, cond);
 }
 
@@ -285,11 +294,18 @@ struct hw2d_ctx {
       wall_pass(nx, base + 2, rows, s, tb, w, ctl, cond);
     }
     row_dispatch(nx, 0, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
-    col_dispatch(ny, 1, cols, s, tb, w, ctl, cond);
-    row_dispatch(nx, 2, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
+    if (tb.model == 3) {   // HS3: B3, C3, H3, I3 in place of B, C
+      col_dispatch(ny, 21, cols, s, tb, w, ctl, cond);
+      row_dispatch(nx, 20, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
+      col_dispatch(ny, 23, cols, s, tb, w, ctl, cond);
+      row_dispatch(nx, 22, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
+    } else {
+      col_dispatch(ny, 1, cols, s, tb, w, ctl, cond);
+      row_dispatch(nx, 2, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
+    }
     if (!tb.chi_one || tb.has_src) col_dispatch(ny, 3, cols, s, tb, w, ctl, cond);
     row_dispatch(nx, 4, rows, s, tb, w, rk, ctl, ctl, mode, cond, out);
-    per_rhs = ((!tb.chi_one || tb.has_src) ? 5 : 4) + 1 + (tb.wallchar ? 3 : 0);
+    per_rhs = ((!tb.chi_one || tb.has_src) ? 5 : 4) + 1 + (tb.wallchar ? 3 : 0) + (tb.model == 3 ? 2 : 0);
     if (brk.on) brk_launch(mode, cond, s, out);
   }
   // the breaking kernels after the assembly pass (both bottoms)
@@ -438,11 +454,15 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
     g_err2d = "hw2d_create: nx and ny must be powers of two in [64, 1024]";
     return nullptr;
   }
-  if (t->model != 1 && t->model != 2) {
-    g_err2d = "hw2d_create: the device builds HS1 (flat bottom) and HS2";
+  if (t->model < 1 || t->model > 3) {
+    g_err2d = "hw2d_create: model must be 1 (HS1), 2 (HS2) or 3 (HS3)";
     return nullptr;
   }
   const bool var_tables = t->gam_min && t->gam_plus && t->csq_min && t->csq_plus && t->om2_min && t->om2_plus;
+  if (t->model == 3 && var_tables) {
+    g_err2d = "hw2d_create: HS3 is built for the flat bottom (rhs_AB3_2DF_uv)";
+    return nullptr;
+  }
   if (t->model == 1 && (t->breaking || t->wallchar)) {
     g_err2d = "hw2d_create: HS1 is built without walls or breaking (rhs_AB1_2DF_uv, rhs_AB1_2DB_uv)";
     return nullptr;
@@ -628,7 +648,11 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
   w.dph = bk.on ? c->dalloc<double2>(n) : nullptr;
   w.z = c->dalloc<double2>(3 * n);
   w.R = c->dalloc<double2>(4 * n);
-  w.Q = c->dalloc<double2>((var ? 6 : 4) * n);
+  w.Q = c->dalloc<double2>((var ? 6 : (t->model == 3 ? 5 : 4)) * n);
+  if (t->model == 3) {
+    w.p3 = c->dalloc<double>(2 * n);
+    w.T3 = c->dalloc<double2>(6 * n);
+  }
   if (!var && bk.on) w.phys = c->dalloc<double>(3 * n);   // eta, u, v for the breaking kernels
   if (!var && t->wallchar) {   // the flat bottom's wall round trip
     w.WP = c->dalloc<double2>((tb.refl_one ? 2 : 1) * n);
@@ -659,7 +683,7 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
             (chi_one || w.W) && (!has_src || (tb.gx && tb.sx && tb.sig && w.src)) && (!bk.on || (w.dph && w.phys)) &&
             (var || !t->wallchar || (w.WP && w.H1 && tb.c2d && (!tb.refl_one || (tb.gwx && tb.gwy)))) &&
             (!var || (tb.gmin && tb.gplus && tb.cmin && tb.cplus && tb.omin && tb.oplus && w.phys && w.pe && w.H1 &&
-                      w.EU)) && (!t->wallchar || tb.wallchar);
+                      w.EU)) && (!t->wallchar || tb.wallchar) && (t->model != 3 || (w.p3 && w.T3));
   for (int i = 0; i < 2; ++i) ok = ok && rk.y[i] && rk.kk[i];
   for (int i = 0; i < 5; ++i) ok = ok && rk.ks[i];
   if (!ok || cudaMallocHost(&c->hctl, sizeof(Ctl2)) != cudaSuccess) {

@@ -346,7 +346,7 @@ def tables(nx=1024, ny=1024, Lx=300.0, Ly=300.0, depth=3.0, Hs=0.5, Tp=6.0, gamm
     c2d = exact_cp(KX, KY, depth)
     om = exact_disp(KX, KY, depth)
     l2d = om * om / GRAV
-    cutfrac = {1: 2, 2: 4}[model]
+    cutfrac = {1: 2, 2: 4, 3: 6}[model]   # evolinfo.cutfrac (2d/functions.c:209-219)
     aal = aal2d(kx, ky, cutfrac)
     wall = None
     if walls:

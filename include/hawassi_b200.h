@@ -207,8 +207,8 @@ int hw_set_stream(hw_ctx* ctx, void* cuda_stream);
 int hw_synchronize(hw_ctx* ctx);
 
 /* ------------------------------------------------------------------------ */
-/* 2D twin (HS2): rhs_AB2_2DF_uv / rhs_AB2_2DB_uv (walls, kinematic breaking  */
-/* on the two-depth tables) and the                                           */
+/* 2D twin (HS1-HS3): rhs_AB2_2DF_uv / rhs_AB2_2DB_uv (walls, kinematic breaking, */
+/* both bottoms), rhs_AB3_2DF_uv, rhs_AB1_2D*_uv and the                      */
 /* gsl_odeiv2 rkf45 loop of ode_solver_uv (2d/fun_odesolver.c:2565-2647,     */
 /* 4458-4540).  State: 6*nx*ny doubles [Re eta^|Im eta^|Re u^|Im u^|Re v^|    */
 /* Im v^], row-major i*nx + j (2d/main.c:198-201).  The operator tables are   */
@@ -219,7 +219,8 @@ typedef struct hw2d_ctx hw2d_ctx;
 
 typedef struct hw2d_tables {
     int nx, ny;                 /* powers of two, 64..1024                      */
-    int model;                  /* evolinfo.model: 2 = HS2; 1 = HS1 (no walls or breaking) */
+    int model;                  /* evolinfo.model: 2 = HS2; 1 = HS1 (no walls or breaking);
+                                   3 = HS3 (flat bottom: rhs_AB3_2DF_uv) */
     int propagation;            /* 0 = Uni+, 1 = Uni-, 2 = Bi (vertical line)   */
     double cpeak;               /* Oprt.Cpeak                                   */
     const double* kx;           /* [nx] dominfo.kx                              */

@@ -136,7 +136,7 @@ or2d_ctx* or2d_create(const or2d_tables* tb, double eps_abs, double eps_rel) {
         set_err2("or2d_create: grid must be even and at least 4x4");
         return NULL;
     }
-    if (tb->model != 1 && tb->model != 2) { set_err2("or2d_create: model must be 1 (HS1) or 2 (HS2)"); return NULL; }
+    if (tb->model < 1 || tb->model > 3) { set_err2("or2d_create: model must be 1 (HS1), 2 (HS2) or 3 (HS3)"); return NULL; }
     or2d_ctx* c = calloc(1, sizeof(or2d_ctx));
     c->nx = tb->nx; c->ny = tb->ny; c->n = tb->nx * tb->ny;
     c->model = tb->model; c->prop = tb->propagation; c->cpeak = tb->cpeak;
@@ -162,6 +162,7 @@ or2d_ctx* or2d_create(const or2d_tables* tb, double eps_abs, double eps_rel) {
     }
     if (tb->gam_min && tb->gam_plus && tb->csq_min && tb->csq_plus && tb->om2_min && tb->om2_plus) {
         if (c->model == 1 && tb->wallchar) { set_err2("or2d_create: walls are restated for HS2 only"); free(c); return NULL; }
+        if (c->model == 3) { set_err2("or2d_create: HS3 is restated for the flat bottom (rhs_AB3_2DF_uv) only"); free(c); return NULL; }
         c->var = 1;
         c->gmin = dup(tb->gam_min, n); c->gplus = dup(tb->gam_plus, n);
         c->cmin = dup(tb->csq_min, n); c->cplus = dup(tb->csq_plus, n);
@@ -177,7 +178,7 @@ or2d_ctx* or2d_create(const or2d_tables* tb, double eps_abs, double eps_rel) {
         }
     }
     if (tb->breaking) {
-        if (c->model != 2) { set_err2("or2d_create: breaking is restated for the HS2 RHS only"); free(c); return NULL; }
+        if (c->model == 1) { set_err2("or2d_create: breaking is restated for the HS2 and HS3 RHS only"); free(c); return NULL; }
         if (!tb->bathy || !tb->brchar || !tb->x || !tb->y) { set_err2("or2d_create: breaking tables missing"); free(c); return NULL; }
         c->brk = brk_create(tb);
     }
@@ -996,7 +997,7 @@ int or2d_rhs(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
         u[q].re = Zhat[2 * n + q]; u[q].im = Zhat[3 * n + q];
         v[q].re = Zhat[4 * n + q]; v[q].im = Zhat[5 * n + q];
     }
-    if (c->model == 2) {
+    if (c->model >= 2) {
         Lphi = malloc(sizeof(cx) * n); M0u = malloc(sizeof(cx) * n); M0v = malloc(sizeof(cx) * n);
         for (int i = 0; i < Ny; i++)
             for (int j = 0; j < Nx; j++) {
@@ -1012,7 +1013,7 @@ int or2d_rhs(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
     }
     sym2(eta, Nx, Ny); sym2(u, Nx, Ny); sym2(v, Nx, Ny);
     fft2(Nx, Ny, eta, +1); fft2(Nx, Ny, u, +1); fft2(Nx, Ny, v, +1);
-    if (c->model == 2) {
+    if (c->model >= 2) {
         sym2(Lphi, Nx, Ny); sym2(M0u, Nx, Ny); sym2(M0v, Nx, Ny);
         fft2(Nx, Ny, Lphi, +1); fft2(Nx, Ny, M0u, +1); fft2(Nx, Ny, M0v, +1);
     }
@@ -1021,7 +1022,7 @@ int or2d_rhs(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
     const double sevenC = 7 * c->cpeak;
     cx *dampeta = malloc(sizeof(cx) * n), *dampu = malloc(sizeof(cx) * n), *dampv = malloc(sizeof(cx) * n);
     cx *etaM0u = NULL, *eta_u = NULL, *etaM0v = NULL, *eta_v = NULL, *deletaH2 = NULL;
-    if (c->model == 2) {
+    if (c->model >= 2) {
         etaM0u = malloc(sizeof(cx) * n); eta_u = malloc(sizeof(cx) * n);
         etaM0v = malloc(sizeof(cx) * n); eta_v = malloc(sizeof(cx) * n); deletaH2 = malloc(sizeof(cx) * n);
     }
@@ -1031,7 +1032,7 @@ int or2d_rhs(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
         dampeta[q].re = sevenC * ch * eta[q].re / factIFFT; dampeta[q].im = 0;
         dampu[q].re = sevenC * ch * u[q].re / factIFFT; dampu[q].im = 0;
         dampv[q].re = sevenC * ch * v[q].re / factIFFT; dampv[q].im = 0;
-        if (c->model == 2) {
+        if (c->model >= 2) {
             const double wallchar = c->wallchar ? c->wallchar[q] : 1.0;   /* :3239-3249 */
             etaM0u[q].re = eta[q].re * M0u[q].re / f2 * wallchar; etaM0u[q].im = 0;
             eta_u[q].re = eta[q].re * u[q].re / f2 * wallchar; eta_u[q].im = 0;
@@ -1044,7 +1045,7 @@ int or2d_rhs(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
     fft2(Nx, Ny, dampeta, -1); fft2(Nx, Ny, dampu, -1); fft2(Nx, Ny, dampv, -1);
 
     cx *ikxH2adj = NULL, *ikyH2adj = NULL, *deluH2adj = NULL, *delvH2adj = NULL;
-    if (c->model == 2) {
+    if (c->model >= 2) {
         fft2(Nx, Ny, etaM0u, -1); fft2(Nx, Ny, eta_u, -1); fft2(Nx, Ny, etaM0v, -1);
         fft2(Nx, Ny, eta_v, -1); fft2(Nx, Ny, deletaH2, -1);
         cx *ikx = malloc(sizeof(cx) * n), *iky = malloc(sizeof(cx) * n);
@@ -1072,15 +1073,86 @@ int or2d_rhs(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
         free(ikx); free(iky); free(delu); free(delv);
     }
 
+    /* HS3: the cubic terms of fun_termshat_AB3_2DF_uv (2d/fun_odesolver.c:3685-3851),
+     * each adjusted on its own (:3848-3851) and added after the H2 terms (:4670-4725) */
+    cx *deluH3adj = NULL, *delvH3adj = NULL, *ikxH3adj = NULL, *ikyH3adj = NULL;
+    if (c->model == 3) {
+        const double f3 = pow(factIFFT, 3);
+        cx *LetaM0u = malloc(sizeof(cx) * n), *LetaM0v = malloc(sizeof(cx) * n), *LetaLphi = malloc(sizeof(cx) * n);
+        cx *divgradphi = malloc(sizeof(cx) * n), *dxu = malloc(sizeof(cx) * n), *dyv = malloc(sizeof(cx) * n);
+        cx *eta2M0u = malloc(sizeof(cx) * n), *eta2M0v = malloc(sizeof(cx) * n);
+        for (int i = 0; i < Ny; i++)
+            for (int j = 0; j < Nx; j++) {
+                const int q = i * Nx + j;
+                const double L = c->l2d[q], wallchar = c->wallchar ? c->wallchar[q] : 1.0;
+                LetaM0u[q].re = L * etaM0u[q].re; LetaM0u[q].im = L * etaM0u[q].im;
+                LetaM0v[q].re = L * etaM0v[q].re; LetaM0v[q].im = L * etaM0v[q].im;
+                LetaLphi[q].re = LetaM0u[q].re + LetaM0v[q].re;
+                LetaLphi[q].im = LetaM0u[q].im + LetaM0v[q].im;
+                divgradphi[q].re = -kx[j] * Zhat[3 * n + q] - ky[i] * Zhat[5 * n + q];
+                divgradphi[q].im = kx[j] * Zhat[2 * n + q] + ky[i] * Zhat[4 * n + q];
+                eta2M0u[q].re = pow(eta[q].re, 2) * M0u[q].re / f3 * wallchar; eta2M0u[q].im = 0;
+                eta2M0v[q].re = pow(eta[q].re, 2) * M0v[q].re / f3 * wallchar; eta2M0v[q].im = 0;
+                dxu[q].re = -kx[j] * Zhat[3 * n + q]; dxu[q].im = kx[j] * Zhat[2 * n + q];
+                dyv[q].re = -ky[i] * Zhat[5 * n + q]; dyv[q].im = ky[i] * Zhat[4 * n + q];
+            }
+        sym2(LetaM0u, Nx, Ny); sym2(LetaM0v, Nx, Ny); sym2(divgradphi, Nx, Ny);
+        sym2(LetaLphi, Nx, Ny); sym2(dxu, Nx, Ny); sym2(dyv, Nx, Ny);
+        fft2(Nx, Ny, LetaM0u, +1); fft2(Nx, Ny, LetaM0v, +1); fft2(Nx, Ny, divgradphi, +1);
+        fft2(Nx, Ny, eta2M0u, -1); fft2(Nx, Ny, eta2M0v, -1);
+        fft2(Nx, Ny, LetaLphi, +1); fft2(Nx, Ny, dxu, +1); fft2(Nx, Ny, dyv, +1);
+        cx *etaLetaM0u = malloc(sizeof(cx) * n), *etaLetaM0v = malloc(sizeof(cx) * n);
+        cx *eta2dxu = malloc(sizeof(cx) * n), *eta2dyv = malloc(sizeof(cx) * n), *deletaH3 = malloc(sizeof(cx) * n);
+        for (int q = 0; q < n; q++) {
+            const double wallchar = c->wallchar ? c->wallchar[q] : 1.0;
+            etaLetaM0u[q].re = eta[q].re / factIFFT * LetaM0u[q].re / factIFFT; etaLetaM0u[q].im = 0;
+            etaLetaM0v[q].re = eta[q].re / factIFFT * LetaM0v[q].re / factIFFT; etaLetaM0v[q].im = 0;
+            eta2dxu[q].re = pow(eta[q].re, 2) * dxu[q].re / f3 * wallchar; eta2dxu[q].im = 0;
+            eta2dyv[q].re = pow(eta[q].re, 2) * dyv[q].re / f3 * wallchar; eta2dyv[q].im = 0;
+            deletaH3[q].re = (Lphi[q].re / factIFFT * eta[q].re / factIFFT * divgradphi[q].re / factIFFT
+                              + Lphi[q].re / factIFFT * LetaLphi[q].re / factIFFT);
+            deletaH3[q].im = 0;
+        }
+        fft2(Nx, Ny, etaLetaM0u, -1); fft2(Nx, Ny, etaLetaM0v, -1); fft2(Nx, Ny, eta2dxu, -1);
+        fft2(Nx, Ny, eta2dyv, -1); fft2(Nx, Ny, deletaH3, -1);
+        cx *ikx = malloc(sizeof(cx) * n), *iky = malloc(sizeof(cx) * n);
+        cx *delu = malloc(sizeof(cx) * n), *delv = malloc(sizeof(cx) * n);
+        for (int i = 0; i < Ny; i++)
+            for (int j = 0; j < Nx; j++) {
+                const int q = i * Nx + j;
+                const double L = c->l2d[q];
+                ikx[q].re = -kx[j] * deletaH3[q].im; ikx[q].im = kx[j] * deletaH3[q].re;
+                iky[q].re = -ky[i] * deletaH3[q].im; iky[q].im = ky[i] * deletaH3[q].re;
+                delu[q].re = L * etaLetaM0u[q].re + 0.5 * L * eta2dxu[q].re - 0.5 * (pow(kx[j], 2) * eta2M0u[q].re);
+                delu[q].im = L * etaLetaM0u[q].im + 0.5 * L * eta2dxu[q].im - 0.5 * (pow(kx[j], 2) * eta2M0u[q].im);
+                delv[q].re = L * etaLetaM0v[q].re + 0.5 * L * eta2dyv[q].re - 0.5 * (pow(ky[i], 2) * eta2M0v[q].re);
+                delv[q].im = L * etaLetaM0v[q].im + 0.5 * L * eta2dyv[q].im - 0.5 * (pow(ky[i], 2) * eta2M0v[q].im);
+            }
+        deluH3adj = malloc(sizeof(cx) * n); delvH3adj = malloc(sizeof(cx) * n);
+        ikxH3adj = malloc(sizeof(cx) * n); ikyH3adj = malloc(sizeof(cx) * n);
+        fun_adjust(c, deluH3adj, delu);
+        fun_adjust(c, delvH3adj, delv);
+        fun_adjust(c, ikxH3adj, ikx);
+        fun_adjust(c, ikyH3adj, iky);
+        free(ikx); free(iky); free(delu); free(delv);
+        free(LetaM0u); free(LetaM0v); free(LetaLphi); free(divgradphi); free(dxu); free(dyv);
+        free(eta2M0u); free(eta2M0v); free(etaLetaM0u); free(etaLetaM0v); free(eta2dxu); free(eta2dyv);
+        free(deletaH3);
+    }
+
     cx* Source_hat = malloc(sizeof(cx) * n);
     fun_source(c, t, Source_hat);
 
     cx* dphi = malloc(sizeof(cx) * n);   /* delphiH_hat (2d/fun_odesolver.c:4480-4486) */
     for (int q = 0; q < n; q++) {
         dphi[q] = delphiH1hat[q];
-        if (c->model == 2) {
+        if (c->model >= 2) {
             dphi[q].re = delphiH1hat[q].re + deluH2adj[q].re + delvH2adj[q].re;
             dphi[q].im = delphiH1hat[q].im + deluH2adj[q].im + delvH2adj[q].im;
+        }
+        if (c->model == 3) {
+            dphi[q].re = delphiH1hat[q].re + deluH2adj[q].re + delvH2adj[q].re + deluH3adj[q].re + delvH3adj[q].re;
+            dphi[q].im = delphiH1hat[q].im + deluH2adj[q].im + delvH2adj[q].im + deluH3adj[q].im + delvH3adj[q].im;
         }
     }
     /* breaking (:4494-4502), as in the varying-bottom RHS */
@@ -1097,13 +1169,21 @@ int or2d_rhs(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
             const int q = i * Nx + j;
             const double a = c->aal[q];
             cx ix = {0, 0}, iy = {0, 0};
-            if (c->model == 2) {
+            if (c->model >= 2) {
                 ix = ikxH2adj[q];
                 iy = ikyH2adj[q];
             }
             const cx sbx = c->brk ? c->brk->sbx[q] : zero, sby = c->brk ? c->brk->sby[q] : zero;
             dt_Zhat[q] = (Source_hat[q].re + dphi[q].re - dampeta[q].re) * a;
             dt_Zhat[n + q] = (Source_hat[q].im + dphi[q].im - dampeta[q].im) * a;
+            if (c->model == 3) {   /* rhs_AB3_2DF_uv (:4703-4725) */
+                const cx jx = ikxH3adj[q], jy = ikyH3adj[q];
+                dt_Zhat[2 * n + q] = (GRAV * kx[j] * Zhat[n + q] + sbx.re - ix.re - jx.re - dampu[q].re) * a;
+                dt_Zhat[3 * n + q] = (-GRAV * kx[j] * Zhat[q] + sbx.im - ix.im - jx.im - dampu[q].im) * a;
+                dt_Zhat[4 * n + q] = (GRAV * ky[i] * Zhat[n + q] + sby.re - iy.re - jy.re - dampv[q].re) * a;
+                dt_Zhat[5 * n + q] = (-GRAV * ky[i] * Zhat[q] + sby.im - iy.im - jy.im - dampv[q].im) * a;
+                continue;
+            }
             dt_Zhat[2 * n + q] = (GRAV * kx[j] * Zhat[n + q] + sbx.re - ix.re - dampu[q].re) * a;
             dt_Zhat[3 * n + q] = (-GRAV * kx[j] * Zhat[q] + sbx.im - ix.im - dampu[q].im) * a;
             dt_Zhat[4 * n + q] = (GRAV * ky[i] * Zhat[n + q] + sby.re - iy.re - dampv[q].re) * a;
@@ -1114,6 +1194,7 @@ int or2d_rhs(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
     free(delphiH1hat); free(eta); free(u); free(v); free(Lphi); free(M0u); free(M0v);
     free(dampeta); free(dampu); free(dampv); free(etaM0u); free(eta_u); free(etaM0v); free(eta_v);
     free(deletaH2); free(ikxH2adj); free(ikyH2adj); free(deluH2adj); free(delvH2adj); free(Source_hat);
+    free(deluH3adj); free(delvH3adj); free(ikxH3adj); free(ikyH3adj);
     for (int q = 0; q < 6 * n; q++)
         if (!isfinite(dt_Zhat[q])) return 1;
     return 0;

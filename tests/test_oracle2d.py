@@ -191,3 +191,38 @@ def test_breaking_starts_tracks_and_logs():
     assert all(0 <= x < tb["nx"] and 0 <= yy < tb["ny"] for _, nodes in log for x, yy in nodes)
     # records come from every RHS past tprev, rejected attempts' stages included
     assert all(0.3 < tt <= t + 0.05 for tt, _ in log)
+
+
+def hs3_pair(nx=64, ny=32, walls=()):
+    """HS3 tables and the same tables run as HS2 (HS3's aliasing mask), no source."""
+    tb3 = decks2d.tables(nx=nx, ny=ny, Lx=0.9 * nx, Ly=0.9 * ny, depth=2.0, Hs=0.1, Tp=3.0, n_freq=24, n_dir=6,
+                         t_end=6.0, dt=0.1, damp=6.0, x_line=10.0, nadj=1.0, seed=2, model=3, walls=walls)
+    for k in ("newgam", "skewgam", "tsig", "sig", "sigskew"):
+        tb3[k] = None
+    tb3["nt"] = 0
+    tb2 = dict(tb3)
+    tb2["model"] = 2
+    return tb2, tb3
+
+
+@pytest.mark.parametrize("walls", [(), ((20.0, 5.0, 24.0, 20.0),)])
+def test_hs3_terms_are_cubic(walls):
+    """rhs_AB3_2DF_uv - rhs_AB2_2DF_uv on the same tables is homogeneous of degree
+    three in the state: the cubic terms alone (the adjustment is linear)."""
+    tb2, tb3 = hs3_pair(walls=walls)
+    nx, ny = tb3["nx"], tb3["ny"]
+    n = nx * ny
+    o2, o3 = Oracle2D(tb2), Oracle2D(tb3)
+    rng = np.random.default_rng(11)
+    z = 0.02 * rng.standard_normal(6 * n) * np.tile(tb3["aal"].ravel(), 6) * np.sqrt(n)
+    d1 = o3.rhs(0.0, z) - o2.rhs(0.0, z)
+    d2 = o3.rhs(0.0, 2 * z) - o2.rhs(0.0, 2 * z)
+    assert np.linalg.norm(d1) > 1e-8 * np.linalg.norm(o2.rhs(0.0, z))
+    assert np.linalg.norm(d2 - 8 * d1) < 1e-8 * np.linalg.norm(d2)
+
+
+def test_hs3_is_flat_bottom_only():
+    tb = decks2d.tables(nx=64, ny=32, Lx=57.6, Ly=28.8, depth=2.0, shallow=0.6, Hs=0.1, Tp=3.0, n_freq=24, n_dir=6,
+                        t_end=6.0, dt=0.1, damp=6.0, x_line=10.0, bathymetry="shoal", model=3)
+    with pytest.raises(RuntimeError, match="flat bottom"):
+        Oracle2D(tb)
