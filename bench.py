@@ -31,6 +31,7 @@ simulated seconds per wall second; one step advances 250 output samples (5 s).
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -53,6 +54,35 @@ BYTES_PER_RHS_PT = 35.0 / 6.0 * 4 * 8 + 6 * 8
 WORKLOAD = ("batched ragged 1D ensemble: 256 members/GPU, Nx in {2048,4096,8192,16384}, L=0.05*Nx, "
             "flat depth U[0.5,2] m, JONSWAP Hs U[0.05,0.20] Tp U[1.5,3.0] gamma U[1,5], HS2 + breaking, "
             "RKF45 rtol 1e-6 atol 1e-8")
+
+
+# algorithmic FP64 work per RHS grid-point evaluation (the reference's c2c transforms
+# at 5 N log2 N flops each, with common subexpressions shared, plus ~80 pointwise
+# flops): 17 transforms for HS2 with breaking in 1D; 55 2D transforms (each 5 log2 N
+# flops per point) for the 2D twin with two reference depths, breaking and walls
+FFTS_PER_RHS_1D = 17
+FFTS_PER_RHS_2D = 55
+POINTWISE_FLOPS = 80.0
+
+
+def flops_per_rhs_pt(n_points, ffts):
+    return ffts * 5.0 * math.log2(n_points) + POINTWISE_FLOPS
+
+
+def fp64_roofline(flops, ms, device, kernel, basis):
+    """The FP64 roofline beside the HBM one: algorithmic flops of the timed launches
+    over their event-timed duration, against the FP64 FMA throughput measured on this
+    GPU (hw_fp64_peak_tflops).  None when that measurement fails."""
+    try:
+        import hawassi_c_b200 as hw
+        peak = hw.fp64_peak_tflops(device)
+        achieved = flops / (ms / 1e3) / 1e12
+        return {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "kernel": kernel, "flops": basis,
+                "peak_source": "measured on this GPU (DFMA microbenchmark, hw_fp64_peak_tflops)"}
+    except Exception as e:   # the HBM roofline and the rest of the line stand without it
+        log(f"fp64 roofline unavailable: {e}")
+        return None
 
 
 T_START = time.time()
@@ -362,6 +392,10 @@ def main_2d(args, rank, world, local):
             "launch": f"one step = {STEP_2D} simulated s, {pts / max(1, args.steps):.3e} RHS grid points, "
                       f"{BYTES_PER_RHS_PT_2D:.1f} algorithmic B/point",
             "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback"}
+    roof_fp64 = fp64_roofline(pts / max(1, world) * flops_per_rhs_pt(n, FFTS_PER_RHS_2D), ms, local,
+                              "k2v_rowA..k2b_sbrow",
+                              f"{FFTS_PER_RHS_2D} 2D c2c transforms x 5 log2(Nx Ny) + {POINTWISE_FLOPS:.0f} "
+                              "pointwise flops per RHS point")
     # end to end through the public API: host state in (pinned), evolve, host state out
     host = torch.empty(6 * n, dtype=torch.float64, pin_memory=True)
     hv = host.numpy()
@@ -391,7 +425,8 @@ def main_2d(args, rank, world, local):
                        "l2": "working set (~0.9 GB of RK vectors and pass fields) above L2: no flush needed"},
             "rhs_points_per_step": pts / args.steps,
             "sim_s_per_wall_s": STEP_2D * args.steps / (ms / 1e3),
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": l1 - l0, "clocks": clocks,
+            "roofline": roof, "roofline_fp64": roof_fp64, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": l1 - l0, "clocks": clocks,
             "rhs_calls": s1["rhs_calls"] - s0["rhs_calls"], "accepted": s1["accepted"] - s0["accepted"],
             "rejected": s1["rejected"] - s0["rejected"],
         }
@@ -794,6 +829,10 @@ def main():
     def rhs_pts():
         return sum(eng.stats(i)["rhs_calls"] * nx[i] for i in range(eng.members))
 
+    def rhs_flops():
+        return sum(eng.stats(i)["rhs_calls"] * nx[i] * flops_per_rhs_pt(nx[i], FFTS_PER_RHS_1D)
+                   for i in range(eng.members))
+
     def sim_time():
         return sum(eng.state(i)[0] for i in range(eng.members))
 
@@ -830,7 +869,7 @@ def main():
     # launch of it per grid-size class, all classes running concurrently on forked
     # streams, so the launch group of one more step is timed as a unit with events
     # on the launching stream and credited with every RHS point it evaluated.
-    pts_a = rhs_pts()
+    pts_a, flops_a = rhs_pts(), rhs_flops()
     g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     g0.record(stream)
     i_stop += args.window
@@ -860,6 +899,9 @@ def main():
                       f"{gms:.2f} ms, {grp_pts:.3e} RHS grid points, {BYTES_PER_RHS_PT:.1f} algorithmic B/point",
             "class_ms": [round(c[0], 3) for c in classes],
             "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback"}
+    roof_fp64 = fp64_roofline(rhs_flops() - flops_a, gms, local, "k_evolve<2048>",
+                              f"{FFTS_PER_RHS_1D} c2c transforms x 5 log2(Nx) + {POINTWISE_FLOPS:.0f} "
+                              "pointwise flops per RHS point, per member")
 
     # end to end through the C ABI with host buffers: H2D of every member's state, the
     # step, D2H of every state
@@ -901,7 +943,8 @@ def main():
             "rhs_points_per_step": tot_pts / args.steps,
             "sim_s_per_wall_s": tot_sim / (ms / 1e3),
             "sim_s_per_wall_s_per_member": tot_sim / (ms / 1e3) / (args.members * world),
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "roofline": roof, "roofline_fp64": roof_fp64, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches,
             "clocks": clocks, "member_status_nonzero": sum(1 for s in statuses if s != 0),
         }
         print(json.dumps(line), flush=True)

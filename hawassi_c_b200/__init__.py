@@ -14,6 +14,6 @@ mirror of the reference's call surface:
 There is no CPU fallback: without the built library or a CUDA device every
 entry point raises.
 """
-from .engine import Engine, EngineError, library_path, load_library  # noqa: F401
+from .engine import Engine, EngineError, fp64_peak_tflops, library_path, load_library  # noqa: F401
 
-__all__ = ["Engine", "EngineError", "library_path", "load_library"]
+__all__ = ["Engine", "EngineError", "fp64_peak_tflops", "library_path", "load_library"]

@@ -360,6 +360,17 @@ class HwJonswap(ctypes.Structure):
                 ("nTramp", ctypes.c_double), ("seed", ctypes.c_ulonglong)]
 
 
+def fp64_peak_tflops(device=0):
+    """FP64 FMA throughput of the device in TFLOP/s (hw_fp64_peak_tflops)."""
+    L = load_library()
+    L.hw_fp64_peak_tflops.restype = ctypes.c_double
+    L.hw_fp64_peak_tflops.argtypes = [ctypes.c_int]
+    v = float(L.hw_fp64_peak_tflops(int(device)))
+    if not v > 0:
+        raise EngineError("hw_fp64_peak_tflops failed")
+    return v
+
+
 def jonswap_influx(specs, device=0):
     """Seeded JONSWAP influx signals of many members in one device launch
     (hw_jonswap_influx).  specs: dicts with T0, Tend, dt, Tp, Hs, gamma, nTramp, seed.

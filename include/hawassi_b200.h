@@ -206,6 +206,11 @@ int hw_write_outputs(hw_ctx* ctx, int member, const char* outdir);
 int hw_set_stream(hw_ctx* ctx, void* cuda_stream);
 int hw_synchronize(hw_ctx* ctx);
 
+/* FP64 FMA throughput of the device in TFLOP/s (a DFMA microbenchmark: eight
+ * independent FMA chains per thread on every SM, best of five launches): the
+ * denominator of the FP64 roofline.  Returns a negative value on error. */
+double hw_fp64_peak_tflops(int device);
+
 /* ------------------------------------------------------------------------ */
 /* 2D twin (HS1-HS3): rhs_AB2_2DF_uv / rhs_AB2_2DB_uv (walls, kinematic breaking, */
 /* both bottoms), rhs_AB3_2DF_uv, rhs_AB1_2D*_uv and the                      */
