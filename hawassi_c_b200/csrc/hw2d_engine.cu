@@ -463,8 +463,10 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
     g_err2d = "hw2d_create: HS3 is built for the flat bottom (rhs_AB3_2DF_uv)";
     return nullptr;
   }
-  if (t->model == 1 && (t->breaking || t->wallchar)) {
-    g_err2d = "hw2d_create: HS1 is built without walls or breaking (rhs_AB1_2DF_uv, rhs_AB1_2DB_uv)";
+  if (t->model == 1 && t->breaking) {
+    // rhs_AB1_2DF_uv / rhs_AB1_2DB_uv never call breaking_process: under HS1 a breaking
+    // deck is the plain HS1 run, so the tables must say breaking = 0
+    g_err2d = "hw2d_create: HS1 runs no breaking process (rhs_AB1_2DF_uv, rhs_AB1_2DB_uv); pass breaking = 0";
     return nullptr;
   }
   (void)var_tables;

@@ -224,7 +224,7 @@ typedef struct hw2d_ctx hw2d_ctx;
 
 typedef struct hw2d_tables {
     int nx, ny;                 /* powers of two, 64..1024                      */
-    int model;                  /* evolinfo.model: 2 = HS2; 1 = HS1 (no walls or breaking);
+    int model;                  /* evolinfo.model: 2 = HS2; 1 = HS1 (no breaking process);
                                    3 = HS3 (flat bottom: rhs_AB3_2DF_uv) */
     int propagation;            /* 0 = Uni+, 1 = Uni-, 2 = Bi (vertical line)   */
     double cpeak;               /* Oprt.Cpeak                                   */

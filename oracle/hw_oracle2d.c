@@ -161,7 +161,6 @@ or2d_ctx* or2d_create(const or2d_tables* tb, double eps_abs, double eps_rel) {
         }
     }
     if (tb->gam_min && tb->gam_plus && tb->csq_min && tb->csq_plus && tb->om2_min && tb->om2_plus) {
-        if (c->model == 1 && tb->wallchar) { set_err2("or2d_create: walls are restated for HS2 only"); free(c); return NULL; }
         if (c->model == 3) { set_err2("or2d_create: HS3 is restated for the flat bottom (rhs_AB3_2DF_uv) only"); free(c); return NULL; }
         c->var = 1;
         c->gmin = dup(tb->gam_min, n); c->gplus = dup(tb->gam_plus, n);

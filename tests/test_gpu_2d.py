@@ -202,6 +202,20 @@ def test_rhs_parity_hs1(nx, ny, prop, bottom):
     assert rel(eng.rhs(0.8, y), ora.rhs(0.8, y)) < 1e-11
 
 
+@pytest.mark.parametrize("bottom,refl", [("flat", 0.5), ("flat", 1.0), ("shoal", 0.5)])
+def test_rhs_parity_hs1_wall(bottom, refl):
+    """HS1 with walls: on the flat bottom fun_delphiH1hat's wall branches (both), on the
+    two-depth bottom the walls enter through the tables only (HS1's cutoff
+    coefficients, no x10 damping)."""
+    tb = decks2d.tables(nx=64, ny=64, Lx=57.6, Ly=57.6, depth=2.0, shallow=0.6, Hs=0.1, Tp=3.0, n_freq=24,
+                        n_dir=6, t_end=6.0, dt=0.1, damp=6.0, x_line=10.0, seed=1, walls=_wall(64, 64), refl=refl,
+                        model=1, bathymetry=bottom)
+    eng, ora = Engine2D(tb, 1e-8, 1e-6), Oracle2D(tb, 1e-8, 1e-6)
+    for seed in (3, 4):
+        y = band_limited_state(tb, 0.02, seed)
+        assert rel(eng.rhs(0.8, y), ora.rhs(0.8, y)) < 1e-11
+
+
 def test_run_to_time_parity_hs1():
     tb = tables(64, 64, model=1)
     eng, ora = Engine2D(tb, 1e-8, 1e-6), Oracle2D(tb, 1e-8, 1e-6)
