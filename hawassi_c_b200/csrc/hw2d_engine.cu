@@ -459,6 +459,10 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
     return nullptr;
   }
   const bool var_tables = t->gam_min && t->gam_plus && t->csq_min && t->csq_plus && t->om2_min && t->om2_plus;
+  if (t->gam_mid || t->csq_mid || t->om2_mid) {
+    g_err2d = "hw2d_create: three reference depths (ninterp = 3, HSSgen_3depth) are not built on the device";
+    return nullptr;
+  }
   if (t->model == 3 && var_tables) {
     g_err2d = "hw2d_create: HS3 is built for the flat bottom (rhs_AB3_2DF_uv)";
     return nullptr;

@@ -316,6 +316,59 @@ def two_depth_operator(depth, kx, ky, omega_p, U=0.0, mdir=0.0):
     return out
 
 
+def three_depth_operator(depth, kx, ky, omega_p, d_mid=None, U=0.0, mdir=0.0):
+    """Tables of the three-reference-depth operator (funOprt_DispInterpolation_3p,
+    2d/functions.c:1627-1762): on 100 depths between the shallowest and deepest point,
+    the weights (gam_min, gam_mid, gam_plus) that make the blend of the three reference
+    long-wave speeds, squared frequencies and phase speeds exact at the local
+    wavenumber of the peak frequency (Cramer's rule with the reference's cofactors
+    A..I); a natural cubic spline in depth gives them per point.  d_mid defaults to
+    the mean of the extreme depths ("default" in the deck).  As for two depths, the
+    peak wavenumber is the exact inverse of the dispersion relation."""
+    from scipy.interpolate import CubicSpline
+    d_min, d_max = float(depth.min()), float(depth.max())
+    d_mid = (d_max + d_min) / 2 if d_mid is None else float(d_mid)
+    N = 100
+    dD = (d_max - d_min) / (N - 1)
+    DD = d_min + dD * np.arange(N)
+    DD[-1] += 0.1 * dD
+
+    def cp1(k, D):
+        return math.sqrt(GRAV * D) + U if k == 0 else (math.copysign(1.0, k) * math.sqrt(GRAV * k * math.tanh(k * D)) + k * U) / k
+
+    def om2(k, D):
+        return (math.copysign(1.0, k) * math.sqrt(GRAV * k * math.tanh(k * D)) + k * U) ** 2
+
+    g = np.empty((3, N))
+    c0m, c0c, c0p = math.sqrt(GRAV * d_min), math.sqrt(GRAV * d_mid), math.sqrt(GRAV * d_max)
+    for i in range(N):
+        kap = invers_omega(omega_p, DD[i])
+        cD, cm, cc, cp = cp1(kap, DD[i]), cp1(kap, d_min), cp1(kap, d_mid), cp1(kap, d_max)
+        oD, om_, oc, op_ = om2(kap, DD[i]), om2(kap, d_min), om2(kap, d_mid), om2(kap, d_max)
+        c0D = math.sqrt(GRAV * DD[i])
+        A = (oc * cp) - (op_ * cc)
+        B = -(om_ * cp) + (op_ * cm)
+        C = (om_ * cc) - (oc * cm)
+        D = -(c0c * cp) + (c0p * cc)
+        E = (c0m * cp) - (c0p * cm)
+        F = -(c0m * cc) + (c0c * cm)
+        G = (c0c * op_) - (c0p * oc)
+        H = -(c0m * op_) + (c0p * om_)
+        I = (c0m * oc) - (c0c * om_)
+        det = c0m * A + c0c * B + c0p * C
+        g[0, i] = (A * c0D + D * oD + G * cD) / det
+        g[1, i] = (B * c0D + E * oD + H * cD) / det
+        g[2, i] = (C * c0D + F * oD + I * cD) / det
+    KX, KY = np.meshgrid(kx, ky)
+    out = {}
+    for r, name, D in ((0, "min", d_min), (1, "mid", d_mid), (2, "plus", d_max)):
+        out[f"gam_{name}"] = CubicSpline(DD, g[r], bc_type="natural")(depth)
+        out[f"om2_{name}"] = exact_disp(KX, KY, D, mdir, 0.0, 0.0) ** 2
+        out[f"csq_{name}"] = exact_cp(KX, KY, D) ** 2
+    out["_knots"] = (DD, g, (d_min, d_mid, d_max))
+    return out
+
+
 def shoal_bathymetry(x, y, deep=5.0, shallow=0.5, x1=100.0, x2=285.0, seed=0):
     """Depth 0.5-5 m: deep up to x1, a linear slope to `shallow` at x2, and a seeded
     Gaussian shoal on the slope; clipped to [shallow, deep]."""
@@ -332,10 +385,11 @@ def shoal_bathymetry(x, y, deep=5.0, shallow=0.5, x1=100.0, x2=285.0, seed=0):
 def tables(nx=1024, ny=1024, Lx=300.0, Ly=300.0, depth=3.0, Hs=0.5, Tp=6.0, gamma=3.3, s_spread=10,
            n_freq=256, n_dir=64, t_end=300.0, dt=0.1, damp=30.0, x_line=45.0, nadj=1.0, model=2,
            propagation=0, seed=0, bathymetry="flat", shallow=0.5, walls=(), refl=0.5, breaking=False,
-           kbc=0.8, tc=0.2, tchar=0.5) -> dict:
+           kbc=0.8, tc=0.2, tchar=0.5, ninterp=2) -> dict:
     """All tables of a 2D deck (vertical influx line at x_line).  bathymetry "flat":
     depth everywhere (rhs_AB2_2DF_uv); "shoal": `depth` offshore sloping to
-    `shallow` with a seeded shoal, two reference depths (rhs_AB2_2DB_uv).
+    `shallow` with a seeded shoal, two reference depths (rhs_AB2_2DB_uv), or three
+    with ninterp=3 (HSSgen_3depth).
     breaking=True adds the kinematic-breaking tables of parambreak
     (2d/breaking.c:1-44) with the deck's KBC, TC, Tchar."""
     x = np.linspace(0.0, Lx, nx)          # fun_intervaltovector (2d/functions1.c:204)
@@ -360,7 +414,8 @@ def tables(nx=1024, ny=1024, Lx=300.0, Ly=300.0, depth=3.0, Hs=0.5, Tp=6.0, gamm
     if bathymetry != "flat":
         depth_field = shoal_bathymetry(x, y, deep=depth, shallow=shallow,
                                        x1=x[0] + 0.33 * (x[-1] - x[0]), x2=x[0] + 0.95 * (x[-1] - x[0]), seed=seed)
-        var = two_depth_operator(depth_field, kx, ky, wp)
+        var = (two_depth_operator if ninterp == 2 else three_depth_operator)(depth_field, kx, ky, wp)
+        var.pop("_knots", None)
     kp = invers_omega(wp, depth)
     cpeak = wp / kp                        # fun_exact_Cp1d_val(kp, depth at the influx line, 0)
     chi = chiadj_vertical(x, ny, x_line, nadj, 2 * math.pi / kp)

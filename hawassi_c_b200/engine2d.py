@@ -30,6 +30,7 @@ class Hw2dTables(ctypes.Structure):
         ("tstar", ctypes.c_double), ("rsearch", ctypes.c_double), ("kbc", ctypes.c_double), ("tc", ctypes.c_double),
         ("delb", ctypes.c_double), ("cur_u", ctypes.c_double), ("t0", ctypes.c_double), ("dt_out", ctypes.c_double),
         ("refl_coef", ctypes.c_double),
+        ("gam_mid", _dp), ("csq_mid", _dp), ("om2_mid", _dp),
     ]
 
 
@@ -113,7 +114,8 @@ class Engine2D:
         self._L = _lib()
         keep = {}
         for k in ("kx", "ky", "c2d", "l2d", "aal", "charac", "chiadj", "newgam", "skewgam", "tsig", "sig", "sigskew",
-                  "gam_min", "gam_plus", "csq_min", "csq_plus", "om2_min", "om2_plus", "wallchar"):
+                  "gam_min", "gam_plus", "csq_min", "csq_plus", "om2_min", "om2_plus", "wallchar", "gam_mid",
+                  "csq_mid", "om2_mid"):
             v = tables.get(k)
             keep[k] = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
         brk = int(tables.get("breaking", 0))

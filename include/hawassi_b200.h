@@ -271,6 +271,11 @@ typedef struct hw2d_tables {
     double t0, dt_out;          /* dominfo.t[0], dominfo.dt (breaking.dat cadence) */
     double refl_coef;           /* walls: refl_coef (the flat RHS's fun_delphiH1hat takes its
                                    flux branch when it is 1)                     */
+    /* three reference depths (ninterp = 3, HSSgen_3depth): the middle depth's tables.
+     * Not built on the device yet: hw2d_create rejects tables that set them. */
+    const double* gam_mid;      /* [ny*nx] Oprt.InterpD.Gam_mid                 */
+    const double* csq_mid;      /* [ny*nx] Oprt.InterpD.Csqr2d_mid              */
+    const double* om2_mid;      /* [ny*nx] Oprt.InterpD.Om2dSq_mid              */
 } hw2d_tables;
 
 /* opts: eps_abs/eps_rel (<= 0: the 2D reference's 1e-3 / 1e-2, 2d/main.c:196-197),

@@ -40,6 +40,7 @@ struct or2d_ctx {
     double *tsig, *sig, *sigskew, *csig, *csigskew;   /* spline second-derivative coefficients */
     int var;                                           /* varying bottom (two reference depths) */
     double *gmin, *gplus, *cmin, *cplus, *omin, *oplus;
+    double *gmid, *cmid, *omid;                        /* three reference depths, NULL: two */
     double* wallchar;                                  /* NULL: no wall */
     int refl_one;                                      /* flat bottom, refl_coef == 1 */
     double *gwx, *gwy;                                 /* fun_gradient(wallchar) (refl_one) */
@@ -166,6 +167,12 @@ or2d_ctx* or2d_create(const or2d_tables* tb, double eps_abs, double eps_rel) {
         c->gmin = dup(tb->gam_min, n); c->gplus = dup(tb->gam_plus, n);
         c->cmin = dup(tb->csq_min, n); c->cplus = dup(tb->csq_plus, n);
         c->omin = dup(tb->om2_min, n); c->oplus = dup(tb->om2_plus, n);
+        if (tb->gam_mid || tb->csq_mid || tb->om2_mid) {
+            if (!(tb->gam_mid && tb->csq_mid && tb->om2_mid)) {
+                set_err2("or2d_create: three reference depths need gam_mid, csq_mid and om2_mid"); free(c); return NULL;
+            }
+            c->gmid = dup(tb->gam_mid, n); c->cmid = dup(tb->csq_mid, n); c->omid = dup(tb->om2_mid, n);
+        }
     }
     if (tb->wallchar) {
         c->wallchar = dup(tb->wallchar, n);
@@ -198,7 +205,7 @@ void or2d_destroy(or2d_ctx* c) {
     double* f[] = {c->kx, c->ky, c->c2d, c->l2d, c->aal, c->charac, c->chiadj, c->newgam, c->skewgam, c->tsig,
                    c->sig, c->sigskew, c->csig, c->csigskew, c->k1, c->k2, c->k3, c->k4, c->k5, c->k6, c->ytmp,
                    c->y0, c->yerr, c->dydt_in, c->dydt_out, c->gmin, c->gplus, c->cmin, c->cplus, c->omin,
-                   c->oplus, c->wallchar, c->gwx, c->gwy};
+                   c->oplus, c->wallchar, c->gwx, c->gwy, c->gmid, c->cmid, c->omid};
     for (size_t q = 0; q < sizeof f / sizeof f[0]; q++) free(f[q]);
     brk_destroy(c->brk);
     free(c);
@@ -266,6 +273,39 @@ static void fun_source(const or2d_ctx* c, double t, cx* Source_hat) {
  * field (its real part used) and phihat its spectrum,
  * result = [F(gam_min Re F^-1 S(Op_min phihat)) + Op_min F(gam_min phi)
  *           + F(gam_plus Re F^-1 S(Op_plus phihat)) + Op_plus F(gam_plus phi)] / 2 */
+/* HSSgen_3depth (2d/fun_odesolver.c:588-697): the two-depth operator with the middle
+ * depth's round trip and spectral term between the outer ones' */
+static void hssgen_3depth(const or2d_ctx* c, const cx* phi, const cx* phihat, const double* Om, const double* Oc,
+                          const double* Op, cx* result) {
+    const int Nx = c->nx, Ny = c->ny, n = c->n;
+    const double factIFFT = (double)Nx * Ny;
+    const double* O[3] = {Om, Oc, Op};
+    const double* G[3] = {c->gmin, c->gmid, c->gplus};
+    cx *L0[3], *g[3], *gL[3];
+    for (int d = 0; d < 3; d++) {
+        L0[d] = malloc(sizeof(cx) * n);
+        for (int q = 0; q < n; q++) { L0[d][q].re = O[d][q] * phihat[q].re; L0[d][q].im = O[d][q] * phihat[q].im; }
+        sym2(L0[d], Nx, Ny);
+        fft2(Nx, Ny, L0[d], +1);
+    }
+    for (int d = 0; d < 3; d++) {
+        g[d] = malloc(sizeof(cx) * n); gL[d] = malloc(sizeof(cx) * n);
+        for (int q = 0; q < n; q++) {
+            g[d][q].re = G[d][q] * phi[q].re / factIFFT; g[d][q].im = 0;
+            gL[d][q].re = G[d][q] * L0[d][q].re / (Nx * Ny); gL[d][q].im = 0;
+        }
+    }
+    for (int d = 0; d < 3; d++) fft2(Nx, Ny, g[d], -1);
+    for (int d = 0; d < 3; d++) fft2(Nx, Ny, gL[d], -1);
+    for (int q = 0; q < n; q++) {
+        result[q].re = (gL[0][q].re + Om[q] * g[0][q].re + gL[1][q].re + Oc[q] * g[1][q].re + gL[2][q].re
+                        + Op[q] * g[2][q].re) / 2;
+        result[q].im = (gL[0][q].im + Om[q] * g[0][q].im + gL[1][q].im + Oc[q] * g[1][q].im + gL[2][q].im
+                        + Op[q] * g[2][q].im) / 2;
+    }
+    for (int d = 0; d < 3; d++) { free(L0[d]); free(g[d]); free(gL[d]); }
+}
+
 static void hssgen_2depth(const or2d_ctx* c, const cx* phi, const cx* phihat, const double* Om, const double* Op,
                           cx* result) {
     const int Nx = c->nx, Ny = c->ny, n = c->n;
@@ -777,8 +817,13 @@ static int rhs_2db(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
     memcpy(eta, eta_hat, sizeof(cx) * n); memcpy(u, u_hat, sizeof(cx) * n); memcpy(v, v_hat, sizeof(cx) * n);
     fft2(Nx, Ny, eta, +1); fft2(Nx, Ny, u, +1); fft2(Nx, Ny, v, +1);
     cx *Csqr_uhat = malloc(sizeof(cx) * n), *Csqr_vhat = malloc(sizeof(cx) * n);
-    hssgen_2depth(c, u, u_hat, c->cmin, c->cplus, Csqr_uhat);
-    hssgen_2depth(c, v, v_hat, c->cmin, c->cplus, Csqr_vhat);
+    if (c->gmid) {   /* ninterp = 3 (2d/fun_odesolver.c:2917-2920) */
+        hssgen_3depth(c, u, u_hat, c->cmin, c->cmid, c->cplus, Csqr_uhat);
+        hssgen_3depth(c, v, v_hat, c->cmin, c->cmid, c->cplus, Csqr_vhat);
+    } else {
+        hssgen_2depth(c, u, u_hat, c->cmin, c->cplus, Csqr_uhat);
+        hssgen_2depth(c, v, v_hat, c->cmin, c->cplus, Csqr_vhat);
+    }
     const double sevenC = 7 * c->cpeak;
     cx *dampeta = malloc(sizeof(cx) * n), *dampu = malloc(sizeof(cx) * n), *dampv = malloc(sizeof(cx) * n);
     cx *deluH1 = malloc(sizeof(cx) * n), *delvH1 = malloc(sizeof(cx) * n);
@@ -850,8 +895,13 @@ static int rhs_2db(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
         etaM0v[q].re = etaM0v[q].re * factIFFT;
     }
     cx *LetaM0u = malloc(sizeof(cx) * n), *LetaM0v = malloc(sizeof(cx) * n);
-    hssgen_2depth(c, etaM0u, etaM0uhat, c->omin, c->oplus, LetaM0u);
-    hssgen_2depth(c, etaM0v, etaM0vhat, c->omin, c->oplus, LetaM0v);
+    if (c->gmid) {   /* ninterp = 3 (:3463-3466) */
+        hssgen_3depth(c, etaM0u, etaM0uhat, c->omin, c->omid, c->oplus, LetaM0u);
+        hssgen_3depth(c, etaM0v, etaM0vhat, c->omin, c->omid, c->oplus, LetaM0v);
+    } else {
+        hssgen_2depth(c, etaM0u, etaM0uhat, c->omin, c->oplus, LetaM0u);
+        hssgen_2depth(c, etaM0v, etaM0vhat, c->omin, c->oplus, LetaM0v);
+    }
     cx *ikx = malloc(sizeof(cx) * n), *iky = malloc(sizeof(cx) * n);
     cx *delu = malloc(sizeof(cx) * n), *delv = malloc(sizeof(cx) * n);
     for (int i = 0; i < Ny; i++)

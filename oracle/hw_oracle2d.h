@@ -65,6 +65,11 @@ typedef struct or2d_tables {
     double cur_u;               /* dominfo.U (ambient current)                  */
     double t0, dt_out;          /* dominfo.t[0], dominfo.dt (breaking.dat cadence) */
     double refl_coef;           /* walls: the reflection coefficient (the flat RHS branches on 1) */
+    /* three reference depths (ninterp = 3, HSSgen_3depth): the middle depth's tables;
+     * NULL for two reference depths */
+    const double* gam_mid;      /* [ny*nx] Oprt.InterpD.Gam_mid                */
+    const double* csq_mid;      /* [ny*nx] Oprt.InterpD.Csqr2d_mid             */
+    const double* om2_mid;      /* [ny*nx] Oprt.InterpD.Om2dSq_mid             */
 } or2d_tables;
 
 /* Copies every table.  eps <= 0 selects the reference's 2D values (abs 1e-3,

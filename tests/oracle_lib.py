@@ -46,6 +46,7 @@ class Or2dTables(ctypes.Structure):
         ("tstar", ctypes.c_double), ("rsearch", ctypes.c_double), ("kbc", ctypes.c_double), ("tc", ctypes.c_double),
         ("delb", ctypes.c_double), ("cur_u", ctypes.c_double), ("t0", ctypes.c_double), ("dt_out", ctypes.c_double),
         ("refl_coef", ctypes.c_double),
+        ("gam_mid", _dpt), ("csq_mid", _dpt), ("om2_mid", _dpt),
     ]
 
 BRK_SCALARS = ("dx", "dy", "max_eta_init", "tstar", "rsearch", "kbc", "tc", "delb", "cur_u", "t0", "dt_out")
@@ -234,7 +235,8 @@ class Oracle2D:
         L = lib()
         keep = {}
         for k in ("kx", "ky", "c2d", "l2d", "aal", "charac", "chiadj", "newgam", "skewgam", "tsig", "sig", "sigskew",
-                  "gam_min", "gam_plus", "csq_min", "csq_plus", "om2_min", "om2_plus", "wallchar"):
+                  "gam_min", "gam_plus", "csq_min", "csq_plus", "om2_min", "om2_plus", "wallchar", "gam_mid",
+                  "csq_mid", "om2_mid"):
             v = tables.get(k)
             keep[k] = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
         brk = int(tables.get("breaking", 0))

@@ -226,3 +226,65 @@ def test_hs3_is_flat_bottom_only():
                         t_end=6.0, dt=0.1, damp=6.0, x_line=10.0, bathymetry="shoal", model=3)
     with pytest.raises(RuntimeError, match="flat bottom"):
         Oracle2D(tb)
+
+
+def _shoal(ninterp=2, model=2, ny=32):
+    return decks2d.tables(nx=64, ny=ny, Lx=57.6, Ly=0.9 * ny, depth=2.0, shallow=0.6, Hs=0.1, Tp=3.0, n_freq=24,
+                          n_dir=6, t_end=6.0, dt=0.1, damp=6.0, x_line=10.0, seed=4, bathymetry="shoal",
+                          ninterp=ninterp, model=model)
+
+
+def test_three_depth_weights_are_exact_at_the_knots():
+    """funOprt_DispInterpolation_3p: at every knot depth the blend of the three reference
+    depths reproduces the long-wave speed, the squared frequency and the phase speed of
+    the peak wavenumber there."""
+    import math
+    tb = _shoal()
+    depth = tb["depth"]
+    wp = 2 * math.pi / 3.0
+    op = decks2d.three_depth_operator(depth, tb["kx"], tb["ky"], wp)
+    DD, g, refs = op["_knots"]
+
+    def cp1(k, D):
+        return math.sqrt(GRAV * k * math.tanh(k * D)) / k
+
+    def om2(k, D):
+        return GRAV * k * math.tanh(k * D)
+
+    for i in range(DD.size):
+        kap = decks2d.invers_omega(wp, DD[i])
+        for f in (lambda D: math.sqrt(GRAV * D), lambda D: om2(kap, D), lambda D: cp1(kap, D)):
+            blend = sum(g[r, i] * f(refs[r]) for r in range(3))
+            assert blend == pytest.approx(f(DD[i]), rel=1e-9)
+    assert op["gam_mid"].shape == depth.shape and np.isfinite(op["gam_mid"]).all()
+
+
+@pytest.mark.parametrize("model", [1, 2])
+def test_three_depth_with_an_idle_middle_depth_is_two_depth(model):
+    """HSSgen_3depth with Gam_mid = 0 adds exact zeros to HSSgen_2depth's sum: the RHS is
+    bit-identical; with the plus weight split half onto a middle depth equal to the
+    deepest one it agrees to rounding."""
+    tb2 = _shoal(model=model)
+    n = tb2["nx"] * tb2["ny"]
+    rng = np.random.default_rng(3)
+    y = 0.02 * rng.standard_normal(6 * n) * np.tile(tb2["aal"].ravel(), 6) * np.sqrt(n)
+    ref = Oracle2D(tb2).rhs(0.7, y)
+    tb3 = dict(tb2, gam_mid=np.zeros_like(tb2["gam_plus"]), csq_mid=tb2["csq_plus"], om2_mid=tb2["om2_plus"])
+    assert np.array_equal(Oracle2D(tb3).rhs(0.7, y), ref)
+    half = 0.5 * tb2["gam_plus"]
+    tb4 = dict(tb2, gam_plus=half, gam_mid=half, csq_mid=tb2["csq_plus"], om2_mid=tb2["om2_plus"])
+    d = Oracle2D(tb4).rhs(0.7, y)
+    assert np.linalg.norm(d - ref) < 1e-13 * np.linalg.norm(ref)
+
+
+def test_three_depth_tables_run_in_the_oracle_and_are_refused_by_the_engine():
+    from hawassi_c_b200.engine import EngineError
+    from hawassi_c_b200.engine2d import Engine2D
+    tb = _shoal(ninterp=3, ny=64)
+    assert {"gam_mid", "csq_mid", "om2_mid"} <= set(tb)
+    n = tb["nx"] * tb["ny"]
+    rng = np.random.default_rng(5)
+    y = 0.02 * rng.standard_normal(6 * n) * np.tile(tb["aal"].ravel(), 6) * np.sqrt(n)
+    assert np.isfinite(Oracle2D(tb).rhs(0.3, y)).all()
+    with pytest.raises(EngineError, match="three reference depths"):
+        Engine2D(tb)
