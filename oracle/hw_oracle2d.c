@@ -162,7 +162,6 @@ or2d_ctx* or2d_create(const or2d_tables* tb, double eps_abs, double eps_rel) {
         }
     }
     if (tb->gam_min && tb->gam_plus && tb->csq_min && tb->csq_plus && tb->om2_min && tb->om2_plus) {
-        if (c->model == 3) { set_err2("or2d_create: HS3 is restated for the flat bottom (rhs_AB3_2DF_uv) only"); free(c); return NULL; }
         c->var = 1;
         c->gmin = dup(tb->gam_min, n); c->gplus = dup(tb->gam_plus, n);
         c->cmin = dup(tb->csq_min, n); c->cplus = dup(tb->csq_plus, n);
@@ -920,12 +919,94 @@ static int rhs_2db(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
     fun_adjust(c, delvH2adj, delv);
     fun_adjust(c, ikxH2adj, ikx);
     fun_adjust(c, ikyH2adj, iky);
+
+    /* HS3: the cubic terms of fun_termshat_AB3_2DB_uv (2d/fun_odesolver.c:4104-4296),
+     * the flat bottom's with L applied as HSS(.; Om2dSq) / g, the physical products
+     * fed to HSS at the unnormalised scale; each adjusted on its own and added after the
+     * H2 terms (rhs_AB3_2DB_uv, :4776-4829) */
+    cx *deluH3adj = NULL, *delvH3adj = NULL, *ikxH3adj = NULL, *ikyH3adj = NULL;
+    if (c->model == 3) {
+        const double f3 = pow(factIFFT, 3);
+        cx *LMu = malloc(sizeof(cx) * n), *LMv = malloc(sizeof(cx) * n), *LetaLphi = malloc(sizeof(cx) * n);
+        cx *divgradphi = malloc(sizeof(cx) * n), *dxu = malloc(sizeof(cx) * n), *dyv = malloc(sizeof(cx) * n);
+        cx *eta2M0u = malloc(sizeof(cx) * n), *eta2M0v = malloc(sizeof(cx) * n);
+        for (int i = 0; i < Ny; i++)
+            for (int j = 0; j < Nx; j++) {
+                const int q = i * Nx + j;
+                const double wallchar = c->wallchar ? c->wallchar[q] : 1.0;
+                LMu[q].re = LetaM0u[q].re / GRAV; LMu[q].im = LetaM0u[q].im / GRAV;
+                LMv[q].re = LetaM0v[q].re / GRAV; LMv[q].im = LetaM0v[q].im / GRAV;
+                LetaLphi[q].re = LMu[q].re + LMv[q].re; LetaLphi[q].im = LMu[q].im + LMv[q].im;
+                divgradphi[q].re = -kx[j] * Zhat[3 * n + q] - ky[i] * Zhat[5 * n + q];
+                divgradphi[q].im = kx[j] * Zhat[2 * n + q] + ky[i] * Zhat[4 * n + q];
+                eta2M0u[q].re = pow(eta[q].re, 2) * M0u[q].re / f3 * wallchar; eta2M0u[q].im = 0;
+                eta2M0v[q].re = pow(eta[q].re, 2) * M0v[q].re / f3 * wallchar; eta2M0v[q].im = 0;
+                dxu[q].re = -kx[j] * Zhat[3 * n + q]; dxu[q].im = kx[j] * Zhat[2 * n + q];
+                dyv[q].re = -ky[i] * Zhat[5 * n + q]; dyv[q].im = ky[i] * Zhat[4 * n + q];
+            }
+        sym2(LMu, Nx, Ny); sym2(LMv, Nx, Ny); sym2(divgradphi, Nx, Ny);
+        sym2(LetaLphi, Nx, Ny); sym2(dxu, Nx, Ny); sym2(dyv, Nx, Ny);
+        fft2(Nx, Ny, LMu, +1); fft2(Nx, Ny, LMv, +1); fft2(Nx, Ny, divgradphi, +1);
+        fft2(Nx, Ny, eta2M0u, -1); fft2(Nx, Ny, eta2M0v, -1);
+        fft2(Nx, Ny, LetaLphi, +1); fft2(Nx, Ny, dxu, +1); fft2(Nx, Ny, dyv, +1);
+        /* physical cubic products p[0..3] = eta L(eta M0u), eta L(eta M0v), eta^2 dx u,
+         * eta^2 dy v; deletaH3 */
+        cx *p[4], *ph[4], *deletaH3 = malloc(sizeof(cx) * n);
+        for (int k = 0; k < 4; k++) { p[k] = malloc(sizeof(cx) * n); ph[k] = malloc(sizeof(cx) * n); }
+        for (int q = 0; q < n; q++) {
+            const double wallchar = c->wallchar ? c->wallchar[q] : 1.0;
+            p[0][q].re = eta[q].re / factIFFT * LMu[q].re / factIFFT; p[0][q].im = 0;
+            p[1][q].re = eta[q].re / factIFFT * LMv[q].re / factIFFT; p[1][q].im = 0;
+            p[2][q].re = pow(eta[q].re, 2) * dxu[q].re / f3 * wallchar; p[2][q].im = 0;
+            p[3][q].re = pow(eta[q].re, 2) * dyv[q].re / f3 * wallchar; p[3][q].im = 0;
+            deletaH3[q].re = (Lphi[q].re / factIFFT * eta[q].re / factIFFT * divgradphi[q].re / factIFFT
+                              + Lphi[q].re / factIFFT * LetaLphi[q].re / factIFFT);
+            deletaH3[q].im = 0;
+        }
+        for (int k = 0; k < 4; k++) { memcpy(ph[k], p[k], sizeof(cx) * n); fft2(Nx, Ny, ph[k], -1); }
+        fft2(Nx, Ny, deletaH3, -1);
+        for (int k = 0; k < 4; k++)
+            for (int q = 0; q < n; q++) p[k][q].re = p[k][q].re * factIFFT;   /* "for operator" */
+        cx* Lp[4];
+        for (int k = 0; k < 4; k++) {
+            Lp[k] = malloc(sizeof(cx) * n);
+            if (c->gmid) hssgen_3depth(c, p[k], ph[k], c->omin, c->omid, c->oplus, Lp[k]);
+            else hssgen_2depth(c, p[k], ph[k], c->omin, c->oplus, Lp[k]);
+        }
+        cx *ikx3 = malloc(sizeof(cx) * n), *iky3 = malloc(sizeof(cx) * n);
+        cx *delu3 = malloc(sizeof(cx) * n), *delv3 = malloc(sizeof(cx) * n);
+        for (int i = 0; i < Ny; i++)
+            for (int j = 0; j < Nx; j++) {
+                const int q = i * Nx + j;
+                ikx3[q].re = -kx[j] * deletaH3[q].im; ikx3[q].im = kx[j] * deletaH3[q].re;
+                iky3[q].re = -ky[i] * deletaH3[q].im; iky3[q].im = ky[i] * deletaH3[q].re;
+                delu3[q].re = Lp[0][q].re / GRAV + 0.5 * Lp[2][q].re / GRAV - 0.5 * (pow(kx[j], 2) * eta2M0u[q].re);
+                delu3[q].im = Lp[0][q].im / GRAV + 0.5 * Lp[2][q].im / GRAV - 0.5 * (pow(kx[j], 2) * eta2M0u[q].im);
+                delv3[q].re = Lp[1][q].re / GRAV + 0.5 * Lp[3][q].re / GRAV - 0.5 * (pow(ky[i], 2) * eta2M0v[q].re);
+                delv3[q].im = Lp[1][q].im / GRAV + 0.5 * Lp[3][q].im / GRAV - 0.5 * (pow(ky[i], 2) * eta2M0v[q].im);
+            }
+        deluH3adj = malloc(sizeof(cx) * n); delvH3adj = malloc(sizeof(cx) * n);
+        ikxH3adj = malloc(sizeof(cx) * n); ikyH3adj = malloc(sizeof(cx) * n);
+        fun_adjust(c, deluH3adj, delu3);
+        fun_adjust(c, delvH3adj, delv3);
+        fun_adjust(c, ikxH3adj, ikx3);
+        fun_adjust(c, ikyH3adj, iky3);
+        for (int k = 0; k < 4; k++) { free(p[k]); free(ph[k]); free(Lp[k]); }
+        cx* f3r[] = {LMu, LMv, LetaLphi, divgradphi, dxu, dyv, eta2M0u, eta2M0v, deletaH3, ikx3, iky3, delu3, delv3};
+        for (size_t q = 0; q < sizeof f3r / sizeof f3r[0]; q++) free(f3r[q]);
+    }
     cx* Source_hat = malloc(sizeof(cx) * n);
     fun_source(c, t, Source_hat);
     cx* dphi = malloc(sizeof(cx) * n);   /* delphiH_hat (2d/fun_odesolver.c:4564-4570) */
     for (int q = 0; q < n; q++) {
         dphi[q].re = deluH1[q].re + delvH1[q].re + deluH2adj[q].re + delvH2adj[q].re;
         dphi[q].im = deluH1[q].im + delvH1[q].im + deluH2adj[q].im + delvH2adj[q].im;
+        if (c->model == 3) {
+            dphi[q].re = deluH1[q].re + delvH1[q].re + deluH2adj[q].re + delvH2adj[q].re + deluH3adj[q].re
+                         + delvH3adj[q].re;
+            dphi[q].im = deluH1[q].im + delvH1[q].im + deluH2adj[q].im + delvH2adj[q].im + deluH3adj[q].im
+                         + delvH3adj[q].im;
+        }
     }
     /* breaking (:4578-4584): B cleared on every call, the update only past tprev;
      * Sb_xhat / Sb_yhat keep their last values otherwise */
@@ -944,6 +1025,14 @@ static int rhs_2db(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
             const cx sbx = c->brk ? c->brk->sbx[q] : zero, sby = c->brk ? c->brk->sby[q] : zero;
             dt_Zhat[q] = (Source_hat[q].re + dphi[q].re - dampeta[q].re) * a;
             dt_Zhat[n + q] = (Source_hat[q].im + dphi[q].im - dampeta[q].im) * a;
+            if (c->model == 3) {
+                const cx jx = ikxH3adj[q], jy = ikyH3adj[q];
+                dt_Zhat[2 * n + q] = (GRAV * kx[j] * Zhat[n + q] + sbx.re - ikxH2adj[q].re - jx.re - dampu[q].re) * a;
+                dt_Zhat[3 * n + q] = (-GRAV * kx[j] * Zhat[q] + sbx.im - ikxH2adj[q].im - jx.im - dampu[q].im) * a;
+                dt_Zhat[4 * n + q] = (GRAV * ky[i] * Zhat[n + q] + sby.re - ikyH2adj[q].re - jy.re - dampv[q].re) * a;
+                dt_Zhat[5 * n + q] = (-GRAV * ky[i] * Zhat[q] + sby.im - ikyH2adj[q].im - jy.im - dampv[q].im) * a;
+                continue;
+            }
             dt_Zhat[2 * n + q] = (GRAV * kx[j] * Zhat[n + q] + sbx.re - ikxH2adj[q].re - dampu[q].re) * a;
             dt_Zhat[3 * n + q] = (-GRAV * kx[j] * Zhat[q] + sbx.im - ikxH2adj[q].im - dampu[q].im) * a;
             dt_Zhat[4 * n + q] = (GRAV * ky[i] * Zhat[n + q] + sby.re - ikyH2adj[q].re - dampv[q].re) * a;
@@ -951,7 +1040,7 @@ static int rhs_2db(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
         }
     cx* fr[] = {eta, u, v, dampeta, dampu, dampv, deluH1, delvH1, M0u, M0v, Lphi, etaM0u, eta_u, etaM0v, eta_v,
                 deletaH2, etaM0uhat, etaM0vhat, LetaM0u, LetaM0v, ikx, iky, delu, delv, deluH2adj, delvH2adj,
-                ikxH2adj, ikyH2adj, Source_hat, dphi};
+                ikxH2adj, ikyH2adj, Source_hat, dphi, deluH3adj, delvH3adj, ikxH3adj, ikyH3adj};
     for (size_t q = 0; q < sizeof fr / sizeof fr[0]; q++) free(fr[q]);
     for (int q = 0; q < 6 * n; q++)
         if (!isfinite(dt_Zhat[q])) return 1;

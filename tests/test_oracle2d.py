@@ -221,11 +221,25 @@ def test_hs3_terms_are_cubic(walls):
     assert np.linalg.norm(d2 - 8 * d1) < 1e-8 * np.linalg.norm(d2)
 
 
-def test_hs3_is_flat_bottom_only():
-    tb = decks2d.tables(nx=64, ny=32, Lx=57.6, Ly=28.8, depth=2.0, shallow=0.6, Hs=0.1, Tp=3.0, n_freq=24, n_dir=6,
-                        t_end=6.0, dt=0.1, damp=6.0, x_line=10.0, bathymetry="shoal", model=3)
-    with pytest.raises(RuntimeError, match="flat bottom"):
-        Oracle2D(tb)
+@pytest.mark.parametrize("ninterp", [2, 3])
+def test_hs3_terms_are_cubic_varying_bottom(ninterp):
+    """rhs_AB3_2DB_uv - rhs_AB2_2DB_uv on the same two- or three-depth tables: the cubic
+    terms alone, homogeneous of degree three."""
+    tb3 = decks2d.tables(nx=64, ny=32, Lx=57.6, Ly=28.8, depth=2.0, shallow=0.6, Hs=0.1, Tp=3.0, n_freq=24,
+                         n_dir=6, t_end=6.0, dt=0.1, damp=6.0, x_line=10.0, nadj=1.0, seed=2, bathymetry="shoal",
+                         model=3, ninterp=ninterp)
+    for k in ("newgam", "skewgam", "tsig", "sig", "sigskew"):
+        tb3[k] = None
+    tb3["nt"] = 0
+    tb2 = dict(tb3, model=2)
+    n = tb3["nx"] * tb3["ny"]
+    o2, o3 = Oracle2D(tb2), Oracle2D(tb3)
+    rng = np.random.default_rng(12)
+    z = 0.02 * rng.standard_normal(6 * n) * np.tile(tb3["aal"].ravel(), 6) * np.sqrt(n)
+    d1 = o3.rhs(0.0, z) - o2.rhs(0.0, z)
+    d2 = o3.rhs(0.0, 2 * z) - o2.rhs(0.0, 2 * z)
+    assert np.linalg.norm(d1) > 1e-8 * np.linalg.norm(o2.rhs(0.0, z))
+    assert np.linalg.norm(d2 - 8 * d1) < 1e-8 * np.linalg.norm(d2)
 
 
 def _shoal(ninterp=2, model=2, ny=32):
@@ -259,7 +273,7 @@ def test_three_depth_weights_are_exact_at_the_knots():
     assert op["gam_mid"].shape == depth.shape and np.isfinite(op["gam_mid"]).all()
 
 
-@pytest.mark.parametrize("model", [1, 2])
+@pytest.mark.parametrize("model", [1, 2, 3])
 def test_three_depth_with_an_idle_middle_depth_is_two_depth(model):
     """HSSgen_3depth with Gam_mid = 0 adds exact zeros to HSSgen_2depth's sum: the RHS is
     bit-identical; with the plus weight split half onto a middle depth equal to the
@@ -288,3 +302,5 @@ def test_three_depth_tables_run_in_the_oracle_and_are_refused_by_the_engine():
     assert np.isfinite(Oracle2D(tb).rhs(0.3, y)).all()
     with pytest.raises(EngineError, match="three reference depths"):
         Engine2D(tb)
+    with pytest.raises(EngineError, match="HS3 is built for the flat bottom"):
+        Engine2D(_shoal(ny=64, model=3))
