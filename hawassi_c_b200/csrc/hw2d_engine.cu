@@ -262,6 +262,12 @@ struct hw2d_ctx {
     if (p && cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) return nullptr;
     return p;
   }
+  // a failed runtime call: record it (with the call's own error) and return 1
+  int fail(const char* what, cudaError_t e) {
+    err = std::string(what) + ": " + cudaGetErrorString(e);
+    cudaGetLastError();
+    return 1;
+  }
   bool check(const char* what) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
@@ -388,7 +394,7 @@ struct hw2d_ctx {
       }
       launched += batch;
       for (int b = 0; b < batch; ++b)
-        if (cudaGraphLaunch(attempt, stream) != cudaSuccess) return check("graph launch") ? 1 : 1;
+        if (const cudaError_t e = cudaGraphLaunch(attempt, stream); e != cudaSuccess) return fail("graph launch", e);
       launches += batch * kernels_per_attempt();
       if (!read_ctl()) return 1;
       if (hctl->status != hw2d::kOk) break;
@@ -738,11 +744,12 @@ int hw2d_rhs(hw2d_ctx* c, double t, const double* y, double* dydt) {
   hw2d::k2_to_reference<<<592, 256, 0, c->stream>>>(c->dout, c->dref, n);
   c->launches += c->per_rhs + 2;
   cudaMemcpyAsync(dydt, c->dref, 6 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
-  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return c->check("hw2d_rhs") ? 1 : 1;
+  if (const cudaError_t e = cudaStreamSynchronize(c->stream); e != cudaSuccess) return c->fail("hw2d_rhs", e);
   if (!c->check("hw2d_rhs")) return 1;
   if (c->brk.on) {
     hw2d::BrkSt st{};
-    if (cudaMemcpy(&st, c->brk.st, sizeof st, cudaMemcpyDeviceToHost) != cudaSuccess) return c->check("hw2d_rhs") ? 1 : 1;
+    if (const cudaError_t e = cudaMemcpy(&st, c->brk.st, sizeof st, cudaMemcpyDeviceToHost); e != cudaSuccess)
+      return c->fail("hw2d_rhs", e);
     if (st.err & (hw2d::kBrkErrPeaks | hw2d::kBrkErrCrests | hw2d::kBrkErrNodes)) {
       c->err = "breaking: a capacity (peaks, crests or nodes) was exceeded";
       return 1;
@@ -772,7 +779,7 @@ int hw2d_set_state(hw2d_ctx* c, double t, double h, const double* y) {
   hw2d::k2_to_internal<<<592, 256, 0, c->stream>>>(c->dref, c->rk.y[0], c->n);
   c->launches += 1;
   cudaMemcpyAsync(c->ctl, c->hctl, sizeof(Ctl2), cudaMemcpyHostToDevice, c->stream);
-  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return c->check("hw2d_set_state") ? 1 : 1;
+  if (const cudaError_t e = cudaStreamSynchronize(c->stream); e != cudaSuccess) return c->fail("hw2d_set_state", e);
   return c->check("hw2d_set_state") ? 0 : 1;
 }
 
@@ -786,7 +793,7 @@ int hw2d_get_state(hw2d_ctx* c, double* t, double* h, double* y) {
     hw2d::k2_to_reference<<<592, 256, 0, c->stream>>>(c->rk.y[c->hctl->cur], c->dref, c->n);
     c->launches += 1;
     cudaMemcpyAsync(y, c->dref, 6 * c->n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
-    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return c->check("hw2d_get_state") ? 1 : 1;
+    if (const cudaError_t e = cudaStreamSynchronize(c->stream); e != cudaSuccess) return c->fail("hw2d_get_state", e);
   }
   return c->check("hw2d_get_state") ? 0 : 1;
 }
@@ -824,13 +831,17 @@ long long hw2d_launches(const hw2d_ctx* c) { return c ? c->launches : 0; }
 int hw2d_breaking_fields(hw2d_ctx* c, double* B, double* sbx, double* sby, int* flagbr, int* ncrest) {
   if (!c || !c->brk.on) return -1;
   cudaSetDevice(c->device);
-  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return c->check("hw2d_breaking_fields") ? 1 : 1;
+  if (const cudaError_t e = cudaStreamSynchronize(c->stream); e != cudaSuccess)
+    return c->fail("hw2d_breaking_fields", e);
   const size_t n = c->n;
-  if (B && cudaMemcpy(B, c->brk.B, n * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
-  if (sbx && cudaMemcpy(sbx, c->brk.sb, n * sizeof(double2), cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
-  if (sby && cudaMemcpy(sby, c->brk.sb + n, n * sizeof(double2), cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
+  struct Copy { void* dst; const void* src; size_t bytes; };
   hw2d::BrkSt st{};
-  if (cudaMemcpy(&st, c->brk.st, sizeof st, cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
+  const Copy copies[4] = {{B, c->brk.B, n * sizeof(double)}, {sbx, c->brk.sb, n * sizeof(double2)},
+                          {sby, c->brk.sb + n, n * sizeof(double2)}, {&st, c->brk.st, sizeof st}};
+  for (const Copy& k : copies)
+    if (k.dst)
+      if (const cudaError_t e = cudaMemcpy(k.dst, k.src, k.bytes, cudaMemcpyDeviceToHost); e != cudaSuccess)
+        return c->fail("hw2d_breaking_fields", e);
   if (flagbr) *flagbr = st.flagbr;
   if (ncrest) *ncrest = st.flagbr == 2 ? st.ncbprev : 0;
   return 0;
@@ -873,10 +884,12 @@ int hw2d_fields(hw2d_ctx* c, double* eta, double* u, double* v) {
   if (!c->check("hw2d_fields")) return 1;
   double* dst[3] = {eta, u, v};
   for (int f = 0; f < 3; ++f)
-    if (dst[f] && cudaMemcpyAsync(dst[f], c->ophys + f * c->n, c->n * sizeof(double), cudaMemcpyDeviceToHost,
-                                  c->stream) != cudaSuccess)
-      return c->check("hw2d_fields") ? 1 : 1;
-  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return c->check("hw2d_fields") ? 1 : 1;
+    if (dst[f])
+      if (const cudaError_t e = cudaMemcpyAsync(dst[f], c->ophys + f * c->n, c->n * sizeof(double),
+                                                cudaMemcpyDeviceToHost, c->stream);
+          e != cudaSuccess)
+        return c->fail("hw2d_fields", e);
+  if (const cudaError_t e = cudaStreamSynchronize(c->stream); e != cudaSuccess) return c->fail("hw2d_fields", e);
   return 0;
 }
 
@@ -945,8 +958,10 @@ int hw2d_run_outputs(hw2d_ctx* c, const hw2d_outputs* o) {
     gpt[j] = gy[j] * nx + gx[j];
   }
   if (!c->ensure_out(ng)) return -1;
-  if (ng > 0 && cudaMemcpy(c->ogpt, gpt.data(), ng * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
-    return c->check("gauge upload") ? -1 : -1;
+  if (ng > 0)
+    if (const cudaError_t e = cudaMemcpy(c->ogpt, gpt.data(), ng * sizeof(int), cudaMemcpyHostToDevice);
+        e != cudaSuccess)
+      return -c->fail("gauge upload", e);
   const std::string pre(o->outdir);
   OutFiles files;
   static const char* kField[3] = {"eta", "u", "v"};
@@ -969,7 +984,8 @@ int hw2d_run_outputs(hw2d_ctx* c, const hw2d_outputs* o) {
       cudaMemcpyAsync(c->hgval, c->ogval, 3 * (size_t)ng * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
     }
     cudaMemcpyAsync(c->hf32, c->of32, (uv ? 3 : 1) * n * sizeof(float), cudaMemcpyDeviceToHost, c->stream);
-    if (cudaStreamSynchronize(c->stream) != cudaSuccess || !c->check("output stage")) return -1;
+    if (const cudaError_t e = cudaStreamSynchronize(c->stream); e != cudaSuccess) return -c->fail("output stage", e);
+    if (!c->check("output stage")) return -1;
     if (first) {
       // the reference opens the next partition's files without closing the last ones
       files.close_part();
