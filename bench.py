@@ -14,7 +14,10 @@ sample like the reference.  Metric: RHS grid-point evaluations per second
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Multi-GPU (torchrun): each rank advances its own 256-member ensemble (seeds
-offset by rank), no data-path collective: weak scaling.
+offset by rank), no data-path collective: weak scaling.  With --shard fixed the
+ranks split ONE 256-member ensemble instead (greedy balance of Nx log2 Nx x
+expected steps, hawassi_c_b200/partition.py), gather the per-member scalars once
+after the timed region, and report strong scaling.
 
     python bench.py --workload 2d [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -88,6 +91,22 @@ def fp64_roofline(flops, ms, device, kernel, basis):
 T_START = time.time()
 
 
+def profile_traffic(workload):
+    """DRAM bytes per RHS grid point of a workload's dominant kernel, from the ncu
+    capture recorded in profiles/traffic.json (dram__bytes_read.sum +
+    dram__bytes_write.sum of a small capture of the same kernel, divided by the RHS
+    points it evaluated).  Returns (bytes per point or None, provenance text); the
+    bench scales it to the launch it times, so the figure is profile-derived, not
+    measured in this run."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            rec = json.load(f)[workload]
+        return float(rec["dram_bytes_per_rhs_pt"]), (
+            f"profile-derived: {rec['capture']} ({rec['build']}), scaled by this launch's RHS points")
+    except (OSError, KeyError, ValueError, TypeError) as e:
+        return None, f"no ncu capture recorded for this workload ({type(e).__name__})"
+
+
 def log(msg):
     print(f"[bench +{time.time() - T_START:7.1f}s] {msg}", file=sys.stderr, flush=True)
 
@@ -103,6 +122,24 @@ def reduce_ranks(max_vals, sum_vals, device):
     dist.all_reduce(tm, op=dist.ReduceOp.MAX)
     dist.all_reduce(ts, op=dist.ReduceOp.SUM)
     return [float(v) for v in tm.tolist()], [float(v) for v in ts.tolist()]
+
+
+def sample_members(decks, n):
+    """A systematic sample of n members of the ensemble (every len/n-th seed), so a
+    bounded CPU run sees the ensemble's mix of grid sizes and sea states."""
+    if n >= len(decks):
+        return list(decks)
+    step = len(decks) / n
+    return [decks[int(i * step)] for i in range(n)]
+
+
+def ensemble_config(args):
+    """The workload description both arms print (the driver compares them)."""
+    return {"workload": WORKLOAD, "members_per_gpu": args.members, "window_samples": args.window,
+            "sharding": ("one fixed ensemble split over the ranks (LPT on Nx log2 Nx x expected steps)"
+                         if args.shard == "fixed" else "one ensemble per rank (seeds offset by rank)"),
+            "l2": "working set well above L2 (126 MB): no flush needed",
+            "grid_sizes": [2048, 4096, 8192, 16384]}
 
 
 def make_decks(root, rank, members, breaking=True):
@@ -179,20 +216,23 @@ def run_reference(args, rank, world):
     ol.lib()
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
     root = os.path.join(tempfile.gettempdir(), "hw_bench_decks_r0")
-    decks = make_decks(root, 0, min(MEMBERS, cores))
+    decks = sample_members(make_decks(root, 0, args.members), cores)
     steps, _ = cpu_measure(decks, cores, args.window, args.warmup + args.steps, 1e9)
     timed = steps[args.warmup:]
     value = sum(p for p, _ in timed) / sum(t for _, t in timed)
     line = {
         "metric": "RHS grid-pt evals/s", "value": value, "unit": "RHS grid-point evaluations/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * sum(t for _, t in timed) / len(timed), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic seeded decks",
-        "config": {"workload": WORKLOAD, "members": len(decks), "window_samples": args.window},
+        "ms_per_step": 1e3 * sum(t for _, t in timed) / len(timed), "higher_is_better": True,
+        "scaling": "strong" if args.shard == "fixed" else "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic seeded decks (JONSWAP influx, flat depths) in the "
+                                                    "reference input format",
+        "config": ensemble_config(args),
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "RHS grid-point evaluations/s", "cores": cores, "kind": "port",
-                         "sample": f"{len(decks)} of the ensemble members, one per core, each advanced "
-                                   f"{args.window} output samples per step"},
+                         "sample": f"{len(decks)} of the ensemble's {args.members} members (every "
+                                   f"{max(1, args.members // len(decks))}th seed: the same mix of grid sizes), "
+                                   f"one per core, each advanced {args.window} output samples per step"},
         "e2e": {"value": value, "unit": "RHS grid-point evaluations/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -380,15 +420,11 @@ def main_2d(args, rank, world, local):
     except OSError:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    traffic = None
-    try:
-        for line in open(os.path.join(ROOT, "profiles", "k2v_rhs_2d_1024.md")):
-            if line.startswith("dram_bytes_per_rhs_pt_breaking:"):
-                traffic = float(line.split(":")[1]) * pts / max(1, args.steps) / (world or 1)
-    except OSError:
-        pass
+    per_pt, traffic_source = profile_traffic("2d")
+    traffic = per_pt * pts / max(1, args.steps) / (world or 1) if per_pt else None
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": traffic, "kernel": "k2v_rowA..k2b_sbrow (one RHS = 9 fused FFT passes + the breaking kernels)",
+            "traffic": traffic, "traffic_source": traffic_source,
+            "kernel": "k2v_rowA..k2b_sbrow (one RHS = 9 fused FFT passes + the breaking kernels)",
             "launch": f"one step = {STEP_2D} simulated s, {pts / max(1, args.steps):.3e} RHS grid points, "
                       f"{BYTES_PER_RHS_PT_2D:.1f} algorithmic B/point",
             "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback"}
@@ -746,6 +782,8 @@ def main():
     ap.add_argument("--workload", default="ensemble", choices=["ensemble", "2d", "fbr005", "c1", "c2"])
     ap.add_argument("--slice", type=int, default=0,
                     help="fbr005: grid points per CTA of the member's cluster (0: 512)")
+    ap.add_argument("--shard", default="replicas", choices=["replicas", "fixed"],
+                    help="multi-GPU ensemble: a 256-member ensemble per rank (weak) or one split over ranks (strong)")
     ap.add_argument("--autotune", action="store_true",
                     help="pick the slice per grid size by timing candidates on the device first")
     args = ap.parse_args()
@@ -785,21 +823,31 @@ def main():
     if args.impl == "reference":
         return run_reference(args, rank, world)
 
-    root = os.path.join(tempfile.gettempdir(), f"hw_bench_decks_r{rank}")
-    decks = make_decks(root, rank, args.members)
+    shard = None
+    if args.shard == "fixed":
+        from hawassi_c_b200 import partition
+        all_decks = make_decks(os.path.join(tempfile.gettempdir(), "hw_bench_decks_r0"), 0, args.members)
+        costs = partition.deck_costs(all_decks, T_END)
+        shard = partition.greedy_partition(costs, world)[rank]
+        decks = [all_decks[i] for i in shard]
+        log(f"fixed ensemble: rank {rank} runs {len(decks)} of {len(all_decks)} members")
+    else:
+        root = os.path.join(tempfile.gettempdir(), f"hw_bench_decks_r{rank}")
+        decks = make_decks(root, rank, args.members)
     log(f"{len(decks)} decks ready")
 
     # CPU baseline on the host cores (spawned before any CUDA work), rank 0 at N=1 only
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = min(len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count() or 1, 64)
-        sample = decks[:cores]
+        sample = sample_members(decks, cores)
         log(f"cpu baseline on {cores} threads")
         steps, sims = cpu_measure(sample, cores, args.window, 10 ** 6, 15.0, timeout=240)
         cpu = {"value": sum(p for p, _ in steps) / sum(t for _, t in steps), "unit": "RHS grid-point evaluations/s",
                "cores": cores, "kind": "port",
-               "sample": f"{len(sample)} ensemble members on {cores} threads, {len(steps)} windows of "
-                         f"{args.window} output samples from t0 (~15 s of CPU time, {sims:.1f} simulated s)"}
+               "sample": f"{len(sample)} of the ensemble's members (every {max(1, len(decks) // len(sample))}th "
+                         f"seed) on {cores} threads, {len(steps)} windows of {args.window} output samples from t0 "
+                         f"(~15 s of CPU time, {sims:.1f} simulated s)"}
         log(f"cpu baseline {cpu['value']:.3e} pts/s")
 
     import torch
@@ -885,16 +933,11 @@ def main():
     except OSError:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    traffic = None
-    try:
-        for line in open(os.path.join(ROOT, "profiles", "k_evolve_ensemble.md")):
-            if line.startswith("dram_bytes_per_rhs_pt:"):
-                traffic = float(line.split(":")[1]) * grp_pts   # bytes over the launch group
-    except OSError:
-        pass
+    per_pt, traffic_source = profile_traffic("ensemble")
+    traffic = per_pt * grp_pts if per_pt else None   # bytes over the launch group
     classes = eng.class_timing()
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": traffic, "kernel": "k_evolve<2048>",
+            "traffic": traffic, "traffic_source": traffic_source, "kernel": "k_evolve<2048>",
             "launch": f"one step = {len(classes)} concurrent launches (one per grid-size class), "
                       f"{gms:.2f} ms, {grp_pts:.3e} RHS grid points, {BYTES_PER_RHS_PT:.1f} algorithmic B/point",
             "class_ms": [round(c[0], 3) for c in classes],
@@ -929,17 +972,29 @@ def main():
     e2e = {"value": e_pts / (ems / 1e3), "unit": "RHS grid-point evaluations/s",
            "h2d_bytes_per_step": tot_doubles * 8, "d2h_bytes_per_step": tot_doubles * 8}
     statuses = [eng.stats(i)["status"] for i in range(eng.members)]
+    summary = None
+    if shard is not None:
+        # the one end-of-run exchange of the fixed ensemble: per-member scalars to every rank
+        from hawassi_c_b200 import partition
+        rows = []
+        for i in range(eng.members):
+            st = eng.stats(i)
+            rows.append([eng.state(i)[0], st["rhs_calls"], st["accepted"], st["rejected"], st["status"],
+                         eng.energy(member=i)])
+        tab = partition.gather_member_scalars(shard, rows, args.members, "cuda")
+        summary = {"members": int(tab.shape[0]), "sim_s": float(tab[:, 0].sum()),
+                   "rhs_calls": int(tab[:, 1].sum()), "status_nonzero": int((tab[:, 4] != 0).sum())}
 
     if rank == 0:
         line = {
             "metric": "RHS grid-pt evals/s", "value": value, "unit": "RHS grid-point evaluations/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "strong" if shard is not None else "weak", "vs_baseline": None,
+            "dtype": "f64",
             "data": "synthetic seeded decks (JONSWAP influx, flat depths) in the reference input format",
-            "config": {"workload": WORKLOAD, "members_per_gpu": args.members, "window_samples": args.window,
-                       "l2": "working set well above L2 (126 MB): no flush needed",
-                       "grid_sizes": sorted(set(nx)),
-                       "slices": ({str(k): v for k, v in slices.items()} if slices else "2048 (default)")},
+            "config": ensemble_config(args),
+            "slices": ({str(k): v for k, v in slices.items()} if slices else "2048 (default)"),
+            "ensemble_summary": summary,
             "rhs_points_per_step": tot_pts / args.steps,
             "sim_s_per_wall_s": tot_sim / (ms / 1e3),
             "sim_s_per_wall_s_per_member": tot_sim / (ms / 1e3) / (args.members * world),

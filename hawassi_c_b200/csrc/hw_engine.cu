@@ -165,8 +165,8 @@ static std::string g_create_err;
 
 // no-allocation RHS (hw_noalloc.cu)
 int hw_noalloc_max_nx();
-bool hw_noalloc_rhs_launch(const DevMember* mems, int mi, int N, int M, int C, double t, const double* y,
-                           double* dy, cudaStream_t s, std::string& err);
+bool hw_noalloc_rhs_launch(DevMember* mems, int mi, int N, int M, int C, double t, const double* y,
+                           double* dy, cudaStream_t s, int dev, std::string& err);
 
 namespace {
 
@@ -661,19 +661,25 @@ int hw_rhs(hw_ctx* ctx, int m, double t, const double* y, double* dydt) {
 
 int hw_rhs_noalloc(hw_ctx* ctx, int m, double t, const double* y_dev, double* dydt_dev, void* cuda_stream) {
   if (!valid_member(ctx, m) || !y_dev || !dydt_dev) return 1;
-  int cur = -1;
-  if (cudaGetDevice(&cur) != cudaSuccess || cur != ctx->device) {
-    cudaError_t e = cudaSetDevice(ctx->device);
-    if (e != cudaSuccess) {
-      ctx->err = std::string("hw_rhs_noalloc: cudaSetDevice: ") + cudaGetErrorString(e);
-      return 1;
-    }
+  // the caller's current device is restored on every return path
+  int prev = -1;
+  cudaError_t e = cudaGetDevice(&prev);
+  if (e != cudaSuccess) {
+    ctx->err = std::string("hw_rhs_noalloc: cudaGetDevice: ") + cudaGetErrorString(e);
+    return 1;
+  }
+  if (prev != ctx->device && (e = cudaSetDevice(ctx->device)) != cudaSuccess) {
+    ctx->err = std::string("hw_rhs_noalloc: cudaSetDevice: ") + cudaGetErrorString(e);
+    return 1;
   }
   const HostMember& h = ctx->mem[size_t(m)];
-  return hw_noalloc_rhs_launch(ctx->d_mems, m, h.N, h.M, h.C, t, y_dev, dydt_dev,
-                               static_cast<cudaStream_t>(cuda_stream), ctx->err)
-             ? 0
-             : 1;
+  const bool ok = hw_noalloc_rhs_launch(ctx->d_mems, m, h.N, h.M, h.C, t, y_dev, dydt_dev,
+                                        static_cast<cudaStream_t>(cuda_stream), ctx->device, ctx->err);
+  if (prev != ctx->device && (e = cudaSetDevice(prev)) != cudaSuccess) {
+    ctx->err = std::string("hw_rhs_noalloc: restoring the caller's device: ") + cudaGetErrorString(e);
+    return 1;
+  }
+  return ok ? 0 : 1;
 }
 
 int hw_gsl_rhs(double t, const double* y, double* dydt, void* params) {

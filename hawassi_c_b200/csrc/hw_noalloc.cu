@@ -7,8 +7,14 @@
 // name to a kernel: the name is a host-side stand-in, not a device address.  The
 // device address is fetched once per device with cudaGetSymbolAddress (with that
 // device current) on the first call and reused.
+//
+// Everything else the RHS reads or writes stays in the context: the tables, the
+// member's breaking state (crest records, B, the breaking.dat log), which a
+// breaking deck's RHS advances exactly as hw_rhs does, and the member's RHS
+// counter.
 #include <cuda_runtime.h>
 
+#include <mutex>
 #include <string>
 
 #include "hw_kernels.cuh"
@@ -21,14 +27,20 @@ constexpr int kNoAllocMaxNx = 4096;   // largest grid the static scratch covers
 constexpr int kSlots = 16;            // 2N stage input + 2N output + 12 N fields, in N double2 units
 static __device__ __align__(256) double2 g_rhs_scratch[size_t(kSlots) * kNoAllocMaxNx];
 
+constexpr int kMaxDevices = 128;
+
+// per-device set-up done by the first call on that device (the scratch array's
+// device address and the kernels' attributes), under a lock so that two host
+// threads making their first call on one device at once do it once
 struct DeviceScratch {
   bool ready = false;
   double2* ptr = nullptr;
 };
-DeviceScratch g_scratch_addr[128];
+DeviceScratch g_scratch_addr[kMaxDevices];
+std::mutex g_setup_lock;
 
 template <int M>
-__global__ void __launch_bounds__(M / kPts, (4096 / M)) k_rhs_noalloc(const DevMember* mems, int mi, double t,
+__global__ void __launch_bounds__(M / kPts, (4096 / M)) k_rhs_noalloc(DevMember* mems, int mi, double t,
                                                                       const double* __restrict__ y_ref,
                                                                       double* __restrict__ dy_ref,
                                                                       double2* scratch) {
@@ -62,25 +74,22 @@ __global__ void __launch_bounds__(M / kPts, (4096 / M)) k_rhs_noalloc(const DevM
     dy_ref[2 * N + kk] = u.x;
     dy_ref[3 * N + kk] = u.y;
   }
+  member_sync(int(cl.num_blocks()));
+  if (rank == 0 && threadIdx.x == 0) mems[mi].rhs_calls += 1;
 }
 
 template <int M>
-cudaError_t launch_noalloc(const DevMember* mems, int mi, int C, double t, const double* y, double* dy,
-                           double2* scratch, cudaStream_t s) {
-  static bool attr_done[128] = {};
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
+cudaError_t set_noalloc_attrs() {
   const int bytes = 2 * padded(M) * int(sizeof(double2));
-  if (dev >= 0 && dev < 128 && !attr_done[dev]) {
-    if ((e = cudaFuncSetAttribute(k_rhs_noalloc<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) !=
-        cudaSuccess)
-      return e;
-    if ((e = cudaFuncSetAttribute(k_rhs_noalloc<M>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) !=
-        cudaSuccess)
-      return e;
-    attr_done[dev] = true;
-  }
+  cudaError_t e = cudaFuncSetAttribute(k_rhs_noalloc<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_rhs_noalloc<M>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+}
+
+template <int M>
+cudaError_t launch_noalloc(DevMember* mems, int mi, int C, double t, const double* y, double* dy,
+                           double2* scratch, cudaStream_t s) {
+  const int bytes = 2 * padded(M) * int(sizeof(double2));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(unsigned(C));
   cfg.blockDim = dim3(M / kPts);
@@ -100,32 +109,39 @@ cudaError_t launch_noalloc(const DevMember* mems, int mi, int C, double t, const
 
 int hw_noalloc_max_nx() { return kNoAllocMaxNx; }
 
-// Launch the no-allocation RHS for member mi (grid N, slice M, cluster C) on stream s.
-// The first call on a device looks up the scratch array's device address (with that
-// device current) and caches it.
-bool hw_noalloc_rhs_launch(const DevMember* mems, int mi, int N, int M, int C, double t, const double* y,
-                           double* dy, cudaStream_t s, std::string& err) {
+// Launch the no-allocation RHS for member mi (grid N, slice M, cluster C) on stream s,
+// with the member's device (dev) current.  The first call on a device looks up the
+// scratch array's device address and sets the kernels' attributes, once, under a lock.
+bool hw_noalloc_rhs_launch(DevMember* mems, int mi, int N, int M, int C, double t, const double* y,
+                           double* dy, cudaStream_t s, int dev, std::string& err) {
   if (N > kNoAllocMaxNx) {
     err = "hw_rhs_noalloc: Nx=" + std::to_string(N) + " exceeds the " + std::to_string(kNoAllocMaxNx) +
           "-point limit of its static scratch";
     return false;
   }
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= 128) {
-    err = std::string("hw_rhs_noalloc: cudaGetDevice: ") + cudaGetErrorString(e);
+  if (dev < 0 || dev >= kMaxDevices) {
+    err = "hw_rhs_noalloc: device ordinal " + std::to_string(dev) + " out of range";
     return false;
   }
+  cudaError_t e = cudaSuccess;
   DeviceScratch& ds = g_scratch_addr[dev];
-  if (!ds.ready) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_rhs_scratch);
-    if (e != cudaSuccess) {
-      err = std::string("hw_rhs_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e);
-      return false;
+  {
+    std::lock_guard<std::mutex> lk(g_setup_lock);
+    if (!ds.ready) {
+      void* p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_rhs_scratch);
+      if (e != cudaSuccess) {
+        err = std::string("hw_rhs_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+        return false;
+      }
+      if ((e = set_noalloc_attrs<256>()) != cudaSuccess || (e = set_noalloc_attrs<512>()) != cudaSuccess ||
+          (e = set_noalloc_attrs<1024>()) != cudaSuccess || (e = set_noalloc_attrs<2048>()) != cudaSuccess) {
+        err = std::string("hw_rhs_noalloc: cudaFuncSetAttribute: ") + cudaGetErrorString(e);
+        return false;
+      }
+      ds.ptr = static_cast<double2*>(p);
+      ds.ready = true;
     }
-    ds.ptr = static_cast<double2*>(p);
-    ds.ready = true;
   }
   switch (M) {
     case 256: e = launch_noalloc<256>(mems, mi, C, t, y, dy, ds.ptr, s); break;

@@ -201,16 +201,19 @@ def config1_deck(path, seed=0, T_end=100.0, nx=4096):
                       damp=(10.0, 10.0), adjcoef=0.5)
 
 
-def ensemble_member_deck(path, seed, T_end=100.0, breaking=True):
-    """One member of the batched ensemble: Nx from {2048,4096,8192,16384}, L=0.05*Nx,
-    flat depth U[0.5,2], JONSWAP Hs U[0.05,0.20], Tp U[1.5,3.0], gamma U[1,5], HS2."""
+def ensemble_member_params(seed):
+    """The drawn parameters of ensemble member `seed`: Nx from {2048,4096,8192,16384},
+    L=0.05*Nx, flat depth U[0.5,2], JONSWAP Hs U[0.05,0.20], Tp U[1.5,3.0], gamma U[1,5]."""
     u = splitmix64_uniform(1_000_003 * (seed + 1), 6)
     nx = [2048, 4096, 8192, 16384][min(int(u[0] * 4), 3)]
-    depth = 0.5 + 1.5 * u[1]
-    Hs = 0.05 + 0.15 * u[2]
-    Tp = 1.5 + 1.5 * u[3]
-    gamma = 1.0 + 4.0 * u[4]
-    length = 0.05 * nx
+    return dict(nx=nx, length=0.05 * nx, depth=0.5 + 1.5 * u[1], Hs=0.05 + 0.15 * u[2], Tp=1.5 + 1.5 * u[3],
+                gamma=1.0 + 4.0 * u[4])
+
+
+def ensemble_member_deck(path, seed, T_end=100.0, breaking=True):
+    """One member of the batched ensemble (parameters of ensemble_member_params), HS2."""
+    pm = ensemble_member_params(seed)
+    nx, depth, Hs, Tp, gamma, length = pm["nx"], pm["depth"], pm["Hs"], pm["Tp"], pm["gamma"], pm["length"]
     return write_deck(path, nx=nx, length=length, xinflux=0.1 * length, depth=depth, model="HS2",
                       breaking=breaking, T_end=T_end, n_samples=2048, n_lines=1024, Hs=Hs, Tp=Tp, gamma=gamma,
                       seed=seed, damp=(0.05 * length, 0.05 * length), adjcoef=0.5)

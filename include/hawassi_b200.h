@@ -71,10 +71,18 @@ int hw_gsl_rhs(double t, const double* y, double* dydt, void* params);
  * DEVICE pointers (4*Nx doubles, reference layout) owned by the caller; the call
  * allocates nothing: its scratch is a 1 MiB static device array held by every GPU
  * that loads the library, so Nx is limited to 4096 (larger grids are rejected with
- * an error).  The first call on a device looks up the array's device address;
- * make that call before any stream capture.  All calls share the one array:
- * calls that overlap on the GPU (different streams, contexts or threads) race.
- * No scratch field needs to start at zero.  cuda_stream NULL: the default stream. */
+ * an error).  The first call on a device looks up the array's device address and
+ * sets the kernels' attributes (once per device, under a lock); make that call
+ * before any stream capture.  All calls share the one array: calls that overlap on
+ * the GPU (different streams, contexts or threads) race.  No scratch field needs
+ * to start at zero.  cuda_stream NULL: the default stream.  The call makes the
+ * context's device current for the launch and restores the caller's device.
+ * Side effects are hw_rhs's: the member's RHS counter grows by one and, on a
+ * breaking deck, the member's breaking state (crest records, B, the breaking
+ * log) advances, as the reference's RHS does on every call.  That state belongs
+ * to the context, so order the call against the context's own work: it runs on
+ * cuda_stream, not on the context's stream, so a call made while hw_run or
+ * hw_evolve_apply work of the same member is in flight races with it. */
 int hw_rhs_noalloc(hw_ctx* ctx, int member, double t, const double* y_dev, double* dydt_dev, void* cuda_stream);
 
 /* Replaces gsl_odeiv_evolve_apply(e, c, s, &sys, &t, t1, &h, y) with rkf45 and

@@ -3,6 +3,8 @@ test decks (run in a container where the reference checkout is mounted).
 
     python tests/golden/make_golden.py /path/to/reference
 
+The reference checkout is the first argument, or $HAWASSI_REFERENCE.
+
 Fixtures written (all are reference *outputs or inputs*, no reference code):
   fbr005/            input deck of 1d/Testcases/1dFBr005Bor/Input (input.txt,
                      initial.dat, gauges.dat)
@@ -10,6 +12,14 @@ Fixtures written (all are reference *outputs or inputs*, no reference code):
   fbr005_gauge_head.txt      Output/Hawassi_eta_gauge.txt rows with t <= 13.0
   fbr005_constants.npz       x, t, depth, k, nu_peak of Output/Constants_01.dat
   irslope_constants.npz      x, k, depth, nu_peak of 1dB001IrSlope Constants_01.dat
+  harmbar/           input deck of 1d/Testcases/1dB002HarmBar (input.txt, bath.dat,
+                     influx.dat, gauges.dat): HS2 over a submerged bar (varying
+                     bathymetry through three reference depths), Area influx of a
+                     user-defined signal, adjcoef 0.3
+  harmbar_gauges.npz         output/Hawassi_eta_gauge.txt and Hawassi_dteta_gauge.txt
+                             (gauge positions; all 5000 rows as printed with %f,
+                             stored as integers of 1e-6)
+  harmbar_constants.npz      x, t, depth, k, nu_peak of output/Constants_01.dat
 """
 import os
 import shutil
@@ -53,7 +63,37 @@ def main(ref):
     c = read_constants(os.path.join(ref, "1d", "Testcases", "1dB001IrSlope", "output", "Output", "Constants_01.dat"))
     np.savez_compressed(os.path.join(HERE, "irslope_constants.npz"),
                         x=c["x"], depth=c["depth"], k=c["k"], nu_peak=c["nu_peak"])
+    harmbar(ref)
+
+
+def read_gauge_text(path):
+    """A Hawassi_*_gauge.txt file: header '#0 x1 x2 ...' (or '0 x1 ...'), then rows t g1 g2 ..."""
+    with open(path) as f:
+        head = f.readline().replace("#", " ").split()
+    rows = np.loadtxt(path, skiprows=1)
+    return np.array([float(v) for v in head[1:]]), rows
+
+
+def harmbar(ref):
+    src = os.path.join(ref, "1d", "Testcases", "1dB002HarmBar")
+    dst = os.path.join(HERE, "harmbar")
+    os.makedirs(dst, exist_ok=True)
+    for f in ("input.txt", "bath.dat", "influx.dat", "gauges.dat"):
+        shutil.copyfile(os.path.join(src, f), os.path.join(dst, f))
+    xg, eta = read_gauge_text(os.path.join(src, "output", "Hawassi_eta_gauge.txt"))
+    _, dteta = read_gauge_text(os.path.join(src, "output", "Hawassi_dteta_gauge.txt"))
+    # the files print %f: stored exactly as integers of 1e-6 (micro_eta / 1e6 is the printed value)
+    assert np.abs(eta).max() < 2000 and np.abs(dteta).max() < 2000
+    np.savez_compressed(os.path.join(HERE, "harmbar_gauges.npz"), xgauge=xg,
+                        micro_t=np.rint(eta[:, 0] * 1e6).astype(np.int64),
+                        micro_eta=np.rint(eta[:, 1:] * 1e6).astype(np.int32),
+                        micro_dteta=np.rint(dteta[:, 1:] * 1e6).astype(np.int32))
+    c = read_constants(os.path.join(src, "output", "Constants_01.dat"))
+    np.savez_compressed(os.path.join(HERE, "harmbar_constants.npz"), **c)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("HAWASSI_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_golden.py <reference checkout> (or set HAWASSI_REFERENCE)")
+    main(ref)

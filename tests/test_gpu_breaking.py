@@ -55,11 +55,19 @@ def test_breaking_state_vs_oracle(golden_dir):
     eta_o = np.fft.ifft(y[:nx] + 1j * y[nx:2 * nx]).real
     eta_g = np.fft.ifft(yg[:nx] + 1j * yg[nx:2 * nx]).real
     assert rel_l2(eta_g, eta_o) < 1e-9
-    # total energy (quadratic Hamiltonian, same spectral form both sides) within 1e-6
-    assert e.stats()["rhs_calls"] == o.stats()[0]
+    # the breaking-run criterion: total energy within 1e-6 (the quadratic Hamiltonian,
+    # evaluated by the same function on both states) ...
+    e_gpu, e_ora = e.energy(), e.energy(y)
+    assert e_ora > 0 and abs(e_gpu - e_ora) / e_ora < 1e-6
+    # ... and the same onset step: identical RHS, accepted and rejected counts
+    st = e.stats()
+    assert (st["rhs_calls"], st["accepted"], st["rejected"]) == tuple(o.stats())
+    # ... and the same onset record (time and grid indices) as the oracle and the golden file
     gold = [l.split() for l in open(os.path.join(golden_dir, "fbr005_breaking_head.txt"))]
-    assert _log_lines(e.breaking_log())[:3] == [l.split() for l in o.breaking_log().splitlines()][:3]
-    assert gold[0] == _log_lines(e.breaking_log())[0]
+    mine = _log_lines(e.breaking_log())
+    assert mine[:3] == [l.split() for l in o.breaking_log().splitlines()][:3]
+    assert gold[0] == mine[0]
+    assert int(mine[0][1]) > 0 and mine[0][2:] == gold[0][2:]
 
 
 def test_breaking_single_rhs(golden_dir):

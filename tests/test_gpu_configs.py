@@ -1,0 +1,175 @@
+"""GPU parity at the sizes and shapes of the benchmarked configurations.
+
+* 1dB002HarmBar, the reference's own golden run (HS2 over a submerged bar: the
+  three-reference-depth operator Up3IP / HSS, Area influx of a user-defined
+  signal, adjcoef 0.3, reference tolerances, Nx = 2048): the device's gauge
+  output of the whole 196.52 s run equals Hawassi_eta_gauge.txt and
+  Hawassi_dteta_gauge.txt to print precision; the state after 30 s equals the
+  oracle's to 1e-9 with identical step counts.
+* Configuration 1 (L = 200 m, Nx = 4096, flat 1 m, HS2, JONSWAP influx, rtol 1e-6,
+  atol 1e-8) to t_end = 100 s in the 8-CTA shape of its benchmark (512-point
+  slices): eta and u within relative L2 1e-9 of the oracle, identical counts.
+* The ensemble configuration: members of every grid size, run as ONE ensemble in
+  the benchmark's default shape (2048-point slices: 16384-point members on 8-CTA
+  clusters, 8192 on 4), each compared with its own standalone oracle run through a
+  breaking onset: eta and u 1e-9, identical breaking.dat records and step counts.
+* Configuration 2 with the reference's operator (three reference depths, HS3,
+  breaking, Nx = 16384 on the 1:30 slope): identical onset record and step counts,
+  total energy within 1e-6, against the committed oracle run
+  (tests/golden/make_oracle_fixtures.py).
+"""
+import concurrent.futures as cf
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+from decks_util import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+hw = pytest.importorskip("hawassi_c_b200")
+from hawassi_c_b200 import decks  # noqa: E402
+from hawassi_c_b200.engine import deck_table  # noqa: E402
+
+PRINT = 5.01e-7   # half a unit of the files' %f
+
+
+def _physical(y):
+    n = y.size // 4
+    return np.fft.ifft(y[:n] + 1j * y[n:2 * n]).real, np.fft.ifft(y[2 * n:3 * n] + 1j * y[3 * n:]).real
+
+
+def _oracle_to(deck, t_stop, eps_abs=0.0, eps_rel=0.0):
+    """The ode_solver_Ham loop on the oracle up to the last output sample <= t_stop."""
+    o = ol.Oracle(deck, eps_abs=eps_abs, eps_rel=eps_rel)
+    tt = o.table("ttrace")
+    y = o.initial_state()
+    t, h = float(tt[0]), 1e-4
+    for ti in tt[1:]:
+        if ti > t_stop:
+            break
+        while t < ti:
+            t, h = o.evolve_apply(t, ti, h, y)
+    return o, t, h, y
+
+
+def _log_lines(recs):
+    return [[f"{t:f}", str(len(nodes))] + [str(n) for n in nodes] for t, nodes in recs]
+
+
+# ---------------------------------------------------------------- 1dB002HarmBar
+@pytest.mark.parametrize("cluster", [0, 4])
+def test_harmbar_full_run_matches_golden(golden_dir, cluster):
+    deck = os.path.join(golden_dir, "harmbar")
+    z = np.load(os.path.join(golden_dir, "harmbar_gauges.npz"))
+    e = hw.Engine(deck, cluster=cluster)
+    e.run()
+    assert e.stats()["status"] == 0
+    tim, eta, dteta = e.gauges()
+    assert tim.size == z["micro_t"].size == 5000
+    assert np.abs(tim - z["micro_t"] / 1e6).max() <= PRINT
+    assert np.abs(eta - z["micro_eta"] / 1e6).max() <= PRINT
+    assert np.abs(dteta - z["micro_dteta"] / 1e6).max() <= PRINT
+    e.close()
+
+
+def test_harmbar_state_vs_oracle(golden_dir):
+    deck = os.path.join(golden_dir, "harmbar")
+    o, t, h, y = _oracle_to(deck, 30.0)
+    e = hw.Engine(deck)
+    e.run_to_time(30.0)
+    tg, hg, yg = e.state()
+    assert tg == pytest.approx(t, rel=1e-13)
+    st = e.stats()
+    assert (st["rhs_calls"], st["accepted"], st["rejected"]) == tuple(o.stats())
+    (eo, uo), (eg, ug) = _physical(y), _physical(yg)
+    assert rel_l2(eg, eo) < 1e-9 and rel_l2(ug, uo) < 1e-9
+    e.close()
+
+
+# ---------------------------------------------------------------- configuration 1
+def test_config1_full_run(tmp_path):
+    deck = decks.config1_deck(str(tmp_path / "c1"), seed=0)
+    o, t, h, y = _oracle_to(deck, 100.0, 1e-8, 1e-6)
+    assert t == pytest.approx(100.0, abs=0.05)
+    e = hw.Engine(deck, eps_abs=1e-8, eps_rel=1e-6, slice=512)
+    e.run()
+    tg, hg, yg = e.state()
+    assert tg == pytest.approx(t, rel=1e-13)
+    st = e.stats()
+    assert (st["rhs_calls"], st["accepted"], st["rejected"]) == tuple(o.stats())
+    (eo, uo), (eg, ug) = _physical(y), _physical(yg)
+    assert np.abs(eo).max() > 0.01   # the influx has filled the tank
+    assert rel_l2(eg, eo) < 1e-9 and rel_l2(ug, uo) < 1e-9
+    e.close()
+
+
+# ---------------------------------------------------------------- ensemble members
+# seeds of the ensemble's member decks: two of each grid size; seed 225 (Nx 2048)
+# starts breaking at t = 16.90 s, inside the window
+C3_SEEDS = [225, 217, 22, 246, 117, 66, 48, 203]
+C3_T = 20.0
+
+
+def _oracle_member(deck):
+    o, t, h, y = _oracle_to(deck, C3_T, 1e-8, 1e-6)
+    return t, y, tuple(o.stats()), o.breaking_log()
+
+
+def test_ensemble_members_vs_standalone_oracle(tmp_path):
+    paths = [decks.ensemble_member_deck(str(tmp_path / f"m{s}"), s) for s in C3_SEEDS]
+    nxs = [int(deck_table(p, "Nx")[0]) for p in paths]
+    assert sorted(nxs) == [2048, 2048, 4096, 4096, 8192, 8192, 16384, 16384]
+    with cf.ThreadPoolExecutor(len(paths)) as ex:   # ctypes releases the GIL
+        refs = list(ex.map(_oracle_member, paths))
+    e = hw.Engine(paths, eps_abs=1e-8, eps_rel=1e-6)
+    e.run_to_time(C3_T)
+    n_broken = 0
+    for m, (t, y, stats, log) in enumerate(refs):
+        tg, hg, yg = e.state(m)
+        st = e.stats(m)
+        assert st["status"] == 0
+        assert tg == pytest.approx(t, rel=1e-13), m
+        assert (st["rhs_calls"], st["accepted"], st["rejected"]) == stats, m
+        mine = _log_lines(e.breaking_log(m))
+        assert mine == [l.split() for l in log.splitlines()], m
+        (eo, uo), (eg, ug) = _physical(y), _physical(yg)
+        n_broken += bool(mine)
+        assert rel_l2(eg, eo) < 1e-9 and rel_l2(ug, uo) < 1e-9, m
+    assert n_broken >= 1
+    e.close()
+
+
+# ---------------------------------------------------------------- configuration 2, K = 3
+def test_config2_k3_breaking_onset(tmp_path, golden_dir):
+    fx = np.load(os.path.join(golden_dir, "c2_k3_onset.npz"))
+    deck = decks.config2_deck(str(tmp_path / "c2"), seed=0)
+    with open(os.path.join(deck, "influx.dat"), "rb") as f:
+        assert hashlib.sha256(f.read()).hexdigest() == str(fx["influx_sha256"])
+    e = hw.Engine(deck, eps_abs=1e-8, eps_rel=1e-6, nref=3)
+    i_on, i_end = int(fx["i_onset"]), int(fx["i_end"])
+    # through the first sample with a breaking record: same counts, same record
+    e.run(i_stop=i_on + 1)
+    t, _, _ = e.state()
+    assert t == pytest.approx(float(fx["onset_t"]), rel=1e-13)
+    st = e.stats()
+    assert st["status"] == 0
+    assert (st["rhs_calls"], st["accepted"], st["rejected"]) == tuple(int(v) for v in fx["onset_stats"])
+    gold = [l.split() for l in str(fx["onset_log"]).splitlines()]
+    assert len(gold) >= 1 and _log_lines(e.breaking_log()) == gold
+    e_on = float(fx["onset_energy"])
+    assert abs(e.energy() - e_on) / e_on < 1e-6
+    # and on through the next samples of the breaking event
+    e.run(i_stop=i_end + 1)
+    st = e.stats()
+    assert (st["rhs_calls"], st["accepted"], st["rejected"]) == tuple(int(v) for v in fx["end_stats"])
+    assert _log_lines(e.breaking_log()) == [l.split() for l in str(fx["end_log"]).splitlines()]
+    e_end = float(fx["end_energy"])
+    assert abs(e.energy() - e_end) / e_end < 1e-6
+    tg, _, yg = e.state()
+    eg, ug = _physical(yg)
+    assert rel_l2(eg[::16], fx["eta16"]) < 1e-7 and rel_l2(ug[::16], fx["u16"]) < 1e-7
+    e.close()
