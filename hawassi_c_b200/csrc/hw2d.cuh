@@ -75,6 +75,10 @@ struct Tab2 {
   int refl_one;                 // flat bottom, refl_coef == 1: fun_delphiH1hat's flux branch
   const double* gwx;            // fun_gradient(wallchar) (refl_one only)
   const double* gwy;
+  // three reference depths (HSSgen_3depth): the middle depth's tables, nullptr: two
+  const double* gmid;
+  const double* cmid;
+  const double* omid;
 };
 
 struct Work2 {

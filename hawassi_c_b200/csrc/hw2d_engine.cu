@@ -18,6 +18,7 @@
 #include "../../include/hawassi_b200.h"
 #include "hw2d.cuh"
 #include "hw2d_brk.cuh"
+#include "hw2d_gen.cuh"
 #include "hw2d_hs3.cuh"
 #include "hw2d_out.cuh"
 #include "hw2d_var.cuh"
@@ -69,6 +70,35 @@ void set_attrs() {
   cudaFuncSetAttribute(hw2d::k2_rowI3<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(8));
   cudaFuncSetAttribute(hw2d::k2o_row<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(4));
   cudaFuncSetAttribute(hw2d::k2o_col<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(4));
+  cudaFuncSetAttribute(hw2d::k2g_rows<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(4));
+  cudaFuncSetAttribute(hw2d::k2g_cols<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<M>(4));
+}
+
+// the general path's transform passes over nf consecutive fields (rows: M = nx,
+// four rows per CTA; columns: M = ny, four columns per CTA)
+template <int M>
+void launch_gen(int cols, double2* f, int nf, int nx, int ny, const double2* tw, int sign, cudaStream_t s,
+                const Ctl2* ctl, int cond) {
+  const int blk = hw2d::kGroups * (M / 8);
+  if (!cols)
+    hw2d::k2g_rows<M><<<dim3(ny / hw2d::kGroups, nf), blk, smem_bytes<M>(4), s>>>(f, nx, ny, tw, sign, ctl, cond);
+  else
+    hw2d::k2g_cols<M><<<dim3(nx / 4, nf), blk, smem_bytes<M>(4), s>>>(f, nx, ny, tw, sign, ctl, cond);
+}
+void gen_pass(int M, int cols, double2* f, int nf, int nx, int ny, const double2* tw, int sign, cudaStream_t s,
+              const Ctl2* ctl, int cond) {
+  switch (M) {
+    case 64: launch_gen<64>(cols, f, nf, nx, ny, tw, sign, s, ctl, cond); break;
+    case 128: launch_gen<128>(cols, f, nf, nx, ny, tw, sign, s, ctl, cond); break;
+    case 256: launch_gen<256>(cols, f, nf, nx, ny, tw, sign, s, ctl, cond); break;
+    case 512: launch_gen<512>(cols, f, nf, nx, ny, tw, sign, s, ctl, cond); break;
+    default: launch_gen<1024>(cols, f, nf, nx, ny, tw, sign, s, ctl, cond); break;
+  }
+}
+
+// the first kernel of a general-path RHS: counts the call when it runs
+__global__ void k2g_count(hw2d::Ctl2* ctl, int cond) {
+  if (hw2d::rhs_active(ctl, cond)) ctl->rhs += 1;
 }
 
 // the output stage's two passes (row M = nx, column M = ny)
@@ -276,9 +306,184 @@ struct hw2d_ctx {
     }
     return true;
   }
+  // ---- the general varying-bottom path (hw2d_gen.cuh) ----
+  // pool of complex N-point fields; the numbered slots below
+  enum GenSlot {
+    gEH = 0, gP = 3, gCU = 6, gCV = 7, gD = 8, gH1 = 11, gM = 13, gEM0U = 16, gEU = 17, gEM0V = 18, gEV = 19,
+    gDH2 = 20, gEM0UH = 21, gEM0VH = 22, gLU = 23, gLV = 24, gADJIN = 25, gADJ = 29, gSRC = 33, gHSS = 34,
+    // HS3
+    gLMU = 43, gLMV = 44, gDIVG = 45, gLELP = 46, gDXU = 47, gDYV = 48, gE2U = 49, gE2V = 50, gPK = 51, gPH = 55,
+    gDH3 = 59, gLP = 60, gADJ3IN = 64, gADJ3 = 68, gSlotsHS2 = 43, gSlotsHS3 = 72
+  };
+  int gen = 0;              // 1: the general path serves this bottom / model
+  double2* gpool = nullptr;
+  int gcount = 0;           // kernels of the RHS being issued
+  double2* G(int i) const { return gpool + (size_t)i * n; }
+  void g_fft(double2* f, int nf, int sign, cudaStream_t s, int cond) {
+    gen_pass(nx, 0, f, nf, nx, ny, tb.twx, sign, s, ctl, cond);
+    gen_pass(ny, 1, f, nf, nx, ny, tb.twy, sign, s, ctl, cond);
+    gcount += 2;
+  }
+  void g_sym(double2* f, int nf, cudaStream_t s, int cond) {
+    hw2d::k2g_sym<<<hw2d::kGenBlocks, hw2d::kGenThreads, 0, s>>>(f, nf, nx, ny, ctl, cond);
+    ++gcount;
+  }
+  template <class Op>
+  void g_map(const Op& op, cudaStream_t s, int cond) {
+    hw2d::k2g_map<Op><<<hw2d::kGenBlocks, hw2d::kGenThreads, 0, s>>>(op, n, nx, ctl, cond);
+    ++gcount;
+  }
+  // HSSgen_2depth / HSSgen_3depth (2d/fun_odesolver.c:500-697): res from phi (the
+  // unnormalised physical field, real part used) and its spectrum phihat, with the
+  // spectral tables O of the reference depths (min, [mid,] plus)
+  void g_hss(const double2* phi, const double2* phihat, const double* omin, const double* omid, const double* oplus,
+             double2* res, cudaStream_t s, int cond) {
+    const int K = tb.gmid ? 3 : 2;
+    const double* O[3] = {omin, tb.gmid ? omid : oplus, oplus};
+    const double* Gm[3] = {tb.gmin, tb.gmid ? tb.gmid : tb.gplus, tb.gplus};
+    const double N = double(nx) * double(ny);
+    double2* L0 = G(gHSS);
+    double2* g = G(gHSS + K);
+    double2* gl = G(gHSS + 2 * K);
+    for (int d = 0; d < K; ++d) g_map(hw2d::OpScaleTable{L0 + d * n, phihat, O[d]}, s, cond);
+    g_sym(L0, K, s, cond);
+    g_fft(L0, K, +1, s, cond);
+    for (int d = 0; d < K; ++d) {
+      g_map(hw2d::OpGam{g + d * n, phi, Gm[d], N}, s, cond);
+      g_map(hw2d::OpGam{gl + d * n, L0 + d * n, Gm[d], N}, s, cond);
+    }
+    g_fft(g, 2 * K, -1, s, cond);
+    hw2d::OpHssSum sum{res, {g, g + n, g + 2 * n}, {gl, gl + n, gl + 2 * n}, {O[0], O[1], O[2]}, K};
+    g_map(sum, s, cond);
+  }
+  // fun_adjust (2d/fun_odesolver.c:810-884) of nf consecutive fields A into AChi:
+  // S(A) in place, AChi = F(ChiAdj F^-1(S(A)) / N)
+  void g_adjust(double2* A, double2* AChi, int nf, cudaStream_t s, int cond) {
+    const double N = double(nx) * double(ny);
+    g_sym(A, nf, s, cond);
+    for (int f = 0; f < nf; ++f) g_map(hw2d::OpCopy{AChi + f * n, A + f * n}, s, cond);
+    g_fft(AChi, nf, +1, s, cond);
+    for (int f = 0; f < nf; ++f) g_map(hw2d::OpChi{AChi + f * n, tb.chi, N}, s, cond);
+    g_fft(AChi, nf, -1, s, cond);
+  }
+  // one RHS of rhs_AB1/AB2/AB3_2DB_uv from the stage input w.z into out
+  void gen_rhs(int mode, int cond, cudaStream_t s, double2* out) {
+    gcount = 0;
+    k2g_count<<<1, 1, 0, s>>>(ctl, cond);
+    ++gcount;
+    const double N = double(nx) * double(ny), f2 = N * N, f3 = N * N * N, g = hw2d::kGrav;
+    const int model = tb.model;
+    // AB1: symmetrised spectra, physical fields, HSS of u^ and v^ with Csqr
+    for (int f = 0; f < 3; ++f) g_map(hw2d::OpCopy{G(gEH + f), w.z + f * n}, s, cond);
+    g_sym(G(gEH), 3, s, cond);
+    for (int f = 0; f < 3; ++f) g_map(hw2d::OpCopy{G(gP + f), G(gEH + f)}, s, cond);
+    g_fft(G(gP), 3, +1, s, cond);
+    g_hss(G(gP + 1), G(gEH + 1), tb.cmin, tb.cmid, tb.cplus, G(gCU), s, cond);
+    g_hss(G(gP + 2), G(gEH + 2), tb.cmin, tb.cmid, tb.cplus, G(gCV), s, cond);
+    g_map(hw2d::OpDampH1{G(gD), G(gD + 1), G(gD + 2), G(gH1), G(gH1 + 1), G(gP), G(gP + 1), G(gP + 2), G(gCU),
+                         G(gCV), tb.damp, tb.kx, tb.ky, N, g},
+          s, cond);
+    g_fft(G(gD), 3, -1, s, cond);
+    const double2* src = nullptr;
+    if (tb.has_src) {
+      hw2d::k2g_signal<<<(ny + 127) / 128, 128, 0, s>>>(tb, w, ctl, mode, cond);
+      ++gcount;
+      g_map(hw2d::OpSource{G(gSRC), tb.gx, tb.sx, w.insig, w.insigs, tb.fac_src}, s, cond);
+      gen_pass(ny, 1, G(gSRC), 1, nx, ny, tb.twy, -1, s, ctl, cond);   // its row transform is a set-up table
+      ++gcount;
+      src = G(gSRC);
+    }
+    hw2d::OpAssemble as{};
+    as.out = out;
+    as.dph = w.dph;
+    as.z = w.z;
+    as.src = src;
+    as.h1u = G(gH1);
+    as.h1v = G(gH1 + 1);
+    as.de = G(gD);
+    as.du = G(gD + 1);
+    as.dv = G(gD + 2);
+    as.aal = tb.aal;
+    as.kx = tb.kx;
+    as.ky = tb.ky;
+    as.g = g;
+    as.model = model;
+    as.n = n;
+    if (model >= 2) {
+      // AB2: M0u, M0v, L phi in physical space; the H2 products
+      g_map(hw2d::OpM0{G(gM), G(gM + 1), G(gM + 2), G(gH1), G(gH1 + 1)}, s, cond);
+      g_sym(G(gM), 3, s, cond);
+      g_fft(G(gM), 3, +1, s, cond);
+      g_map(hw2d::OpH2Products{G(gEM0U), G(gEU), G(gEM0V), G(gEV), G(gDH2), G(gEM0UH), G(gEM0VH), w.phys, G(gP),
+                               G(gP + 1), G(gP + 2), G(gM), G(gM + 1), G(gM + 2), tb.wallchar, N, f2, n},
+            s, cond);
+      g_fft(G(gEU), 1, -1, s, cond);
+      g_fft(G(gEV), 4, -1, s, cond);   // eta v, deletaH2, (eta M0u)^, (eta M0v)^
+      g_map(hw2d::OpScaleRe{G(gEM0U), N}, s, cond);
+      g_map(hw2d::OpScaleRe{G(gEM0V), N}, s, cond);
+      g_hss(G(gEM0U), G(gEM0UH), tb.omin, tb.omid, tb.oplus, G(gLU), s, cond);
+      g_hss(G(gEM0V), G(gEM0VH), tb.omin, tb.omid, tb.oplus, G(gLV), s, cond);
+      // adjust inputs: ikx, iky, delu, delv
+      g_map(hw2d::OpDelH2{G(gADJIN), G(gADJIN + 1), G(gADJIN + 2), G(gADJIN + 3), G(gDH2), G(gEU), G(gEV), G(gLU),
+                          G(gLV), tb.kx, tb.ky, g},
+            s, cond);
+      g_adjust(G(gADJIN), G(gADJ), 4, s, cond);
+      as.ikx = G(gADJ);
+      as.iky = G(gADJ + 1);
+      as.au = G(gADJ + 2);
+      as.av = G(gADJ + 3);
+    }
+    if (model == 3) {
+      // the cubic terms (fun_termshat_AB3_2DB_uv), L applied as HSS(.; Om2dSq) / g
+      g_map(hw2d::OpH3Pre{G(gLMU), G(gLMV), G(gLELP), G(gDIVG), G(gE2U), G(gE2V), G(gDXU), G(gDYV), G(gLU),
+                          G(gLV), w.z, G(gP), G(gM), G(gM + 1), tb.kx, tb.ky, tb.wallchar, g, f3, n},
+            s, cond);
+      g_sym(G(gLMU), 6, s, cond);           // LMu, LMv, divgradphi, LetaLphi, dxu, dyv
+      g_fft(G(gLMU), 6, +1, s, cond);
+      g_fft(G(gE2U), 2, -1, s, cond);
+      hw2d::OpH3Products pr{};
+      for (int k = 0; k < 4; ++k) {
+        pr.p[k] = G(gPK + k);
+        pr.ph[k] = G(gPH + k);
+      }
+      pr.dh3 = G(gDH3);
+      pr.eta = G(gP);
+      pr.lmu = G(gLMU);
+      pr.lmv = G(gLMV);
+      pr.dxu = G(gDXU);
+      pr.dyv = G(gDYV);
+      pr.lphi = G(gM + 2);
+      pr.divg = G(gDIVG);
+      pr.lelp = G(gLELP);
+      pr.wall = tb.wallchar;
+      pr.N = N;
+      pr.f3 = f3;
+      g_map(pr, s, cond);
+      g_fft(G(gPH), 5, -1, s, cond);        // the four products' spectra and deletaH3^
+      for (int k = 0; k < 4; ++k) g_map(hw2d::OpScaleRe{G(gPK + k), N}, s, cond);
+      for (int k = 0; k < 4; ++k) g_hss(G(gPK + k), G(gPH + k), tb.omin, tb.omid, tb.oplus, G(gLP + k), s, cond);
+      g_map(hw2d::OpDelH3{G(gADJ3IN), G(gADJ3IN + 1), G(gADJ3IN + 2), G(gADJ3IN + 3), G(gDH3), G(gLP), G(gLP + 1),
+                          G(gLP + 2), G(gLP + 3), G(gE2U), G(gE2V), tb.kx, tb.ky, g},
+            s, cond);
+      g_adjust(G(gADJ3IN), G(gADJ3), 4, s, cond);
+      as.ikx3 = G(gADJ3);
+      as.iky3 = G(gADJ3 + 1);
+      as.au3 = G(gADJ3 + 2);
+      as.av3 = G(gADJ3 + 3);
+    }
+    g_map(as, s, cond);
+    per_rhs = gcount;
+  }
+
   void rhs_launch(int mode, int cond, cudaStream_t s, double2* out) {
     const int rows = ny / 2, cols = nx / 2;
     if (mode != 0) hw2d::k2_stage<<<hw2d::kCombBlocks, 256, 0, s>>>(rk, w, ctl, mode, cond, 3 * n);
+    if (gen) {
+      gen_rhs(mode, cond, s, out);
+      per_rhs += 1;
+      if (brk.on) brk_launch(mode, cond, s, out);
+      return;
+    }
     if (tb.var) {
       row_dispatch(nx, 10, rows, s, tb, w, rk, ctl, ctl, mode, cond, nullptr);
       col_dispatch(ny, 11, cols, s, tb, w, ctl, cond);
@@ -465,12 +670,9 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
     return nullptr;
   }
   const bool var_tables = t->gam_min && t->gam_plus && t->csq_min && t->csq_plus && t->om2_min && t->om2_plus;
-  if (t->gam_mid || t->csq_mid || t->om2_mid) {
-    g_err2d = "hw2d_create: three reference depths (ninterp = 3, HSSgen_3depth) are not built on the device";
-    return nullptr;
-  }
-  if (t->model == 3 && var_tables) {
-    g_err2d = "hw2d_create: HS3 is built for the flat bottom (rhs_AB3_2DF_uv)";
+  const bool mid_tables = t->gam_mid && t->csq_mid && t->om2_mid;
+  if ((t->gam_mid || t->csq_mid || t->om2_mid) && !(mid_tables && var_tables)) {
+    g_err2d = "hw2d_create: three reference depths need all of gam, csq, om2 for the min, mid and plus depths";
     return nullptr;
   }
   if (t->model == 1 && t->breaking) {
@@ -572,6 +774,14 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
     tb.cplus = c->upload(std::vector<double>(t->csq_plus, t->csq_plus + n));
     tb.omin = c->upload(std::vector<double>(t->om2_min, t->om2_min + n));
     tb.oplus = c->upload(std::vector<double>(t->om2_plus, t->om2_plus + n));
+    if (t->gam_mid) {   // three reference depths: the general path
+      tb.gmid = c->upload(std::vector<double>(t->gam_mid, t->gam_mid + n));
+      tb.cmid = c->upload(std::vector<double>(t->csq_mid, t->csq_mid + n));
+      tb.omid = c->upload(std::vector<double>(t->om2_mid, t->om2_mid + n));
+    }
+    // the fused passes serve two reference depths under HS1 / HS2; three depths and
+    // HS3 on this bottom take the general path
+    c->gen = (t->gam_mid || t->model == 3) ? 1 : 0;
   }
   if (t->wallchar) {
     tb.wallchar = c->upload(std::vector<double>(t->wallchar, t->wallchar + n));
@@ -676,6 +886,10 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
     w.H1 = c->dalloc<double2>(2 * n);
     w.EU = c->dalloc<double2>(3 * n);
   }
+  if (c->gen) {
+    const int slots = t->model == 3 ? hw2d_ctx::gSlotsHS3 : hw2d_ctx::gSlotsHS2;
+    c->gpool = c->dalloc<double2>((size_t)slots * n);
+  }
   w.D = c->dalloc<double2>(3 * n);
   w.W = chi_one ? nullptr : c->dalloc<double2>(4 * n);
   w.V = c->dalloc<double2>(4 * n);
@@ -695,7 +909,8 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
             (chi_one || w.W) && (!has_src || (tb.gx && tb.sx && tb.sig && w.src)) && (!bk.on || (w.dph && w.phys)) &&
             (var || !t->wallchar || (w.WP && w.H1 && tb.c2d && (!tb.refl_one || (tb.gwx && tb.gwy)))) &&
             (!var || (tb.gmin && tb.gplus && tb.cmin && tb.cplus && tb.omin && tb.oplus && w.phys && w.pe && w.H1 &&
-                      w.EU)) && (!t->wallchar || tb.wallchar) && (t->model != 3 || (w.p3 && w.T3));
+                      w.EU)) && (!t->wallchar || tb.wallchar) && (t->model != 3 || (w.p3 && w.T3)) &&
+            (!c->gen || (c->gpool && (!t->gam_mid || (tb.gmid && tb.cmid && tb.omid))));
   for (int i = 0; i < 2; ++i) ok = ok && rk.y[i] && rk.kk[i];
   for (int i = 0; i < 5; ++i) ok = ok && rk.ks[i];
   if (!ok || cudaMallocHost(&c->hctl, sizeof(Ctl2)) != cudaSuccess) {

@@ -2,10 +2,12 @@
 // rhs_breaking, 1d/rhs.c:617-657), run inside every RHS evaluation exactly as
 // the reference does (the state machine sees every call, rejected stages too).
 //
-//  * criterion (parallel): eta above MaxEtaInit in the breaking window and the
-//    local maxima above it (findpeaks), collected with global atomics;
-//  * crest state machine (one leader thread of the member): local wavenumber
-//    from the Hilbert transform, u > KBC * c test, crest tracking with the
+//  * criterion (parallel): eta above MaxEtaInit in the breaking window, the
+//    local maxima above it (findpeaks) and, at each of them, the local wavenumber
+//    from the Hilbert transform and the u > KBC * c test, evaluated by the thread
+//    that found the maximum; the passing crests are collected with global atomics;
+//  * crest state machine (one leader thread of the member): the passing crests in
+//    ascending grid order (findpeaks' order), crest tracking with the
 //    CrestBreak / New / Prev records, the U*(t) ramp and B in [0, 1] along each
 //    breaking crest, and the breaking.dat record once per output interval;
 //  * eddy-viscosity force (parallel): Flux = -B delb^2 (h + eta) (d_t eta)^2,
@@ -33,6 +35,23 @@ __device__ __forceinline__ void crest_clear(Crest* a, int n) {  // set_init_CB (
   }
 }
 
+// breaking_criterion's test at a local maximum J (1d/breaking.c:72-95): local
+// wavenumber K = (eta dH/dx - H deta/dx) / (eta^2 + H^2) from the Hilbert transform
+// H of eta (centred differences, 1d/functions.c:1850), crest speed c(K, h + eta),
+// breaking if |u| > KBC |c|.  Products and sums are rounded one by one (no fused
+// multiply-add), in the reference's order, as the reference's x86-64 build rounds.
+__device__ __forceinline__ bool crest_breaks(const DevMember& d, const double2* PE, const double* Heta, int hs,
+                                             int J) {
+  const double eJ = PE[J].x, hJ = Heta[size_t(hs) * J];
+  const double dx2 = 2 * d.dx;
+  const double gH = __ddiv_rn(__dsub_rn(Heta[size_t(hs) * (J + 1)], Heta[size_t(hs) * (J - 1)]), dx2);
+  const double ge = __ddiv_rn(__dsub_rn(PE[J + 1].x, PE[J - 1].x), dx2);
+  const double KxJ = __ddiv_rn(__dsub_rn(__dmul_rn(eJ, gH), __dmul_rn(hJ, ge)),
+                               __dadd_rn(__dmul_rn(eJ, eJ), __dmul_rn(hJ, hJ)));
+  const double Cc = phase_velocity_dev(KxJ, __dadd_rn(d.depth[J], eJ));
+  return fabs(PE[J].y) > __dmul_rn(d.KBC, fabs(Cc));
+}
+
 // the sequential part of breaking_process, run by one thread
 static __device__ __noinline__ void breaking_leader(const DevMember& d, BrkDev* bk, double t, const double2* PE, const double* Heta,
                                 int hs) {
@@ -48,7 +67,7 @@ static __device__ __noinline__ void breaking_leader(const DevMember& d, BrkDev* 
   Crest* cb = bk->cb;
   Crest* cbn = bk->cbn;
   Crest* cbp = bk->cbp;
-  // ---- breaking_criterion (1d/breaking.c:63) ----
+  // ---- breaking_criterion (1d/breaking.c:63): the crests that passed the test ----
   const int npk = bk->npk;
   if (bk->any_above && npk > 0) {
     int* pk = bk->pk;
@@ -61,13 +80,8 @@ static __device__ __noinline__ void breaking_leader(const DevMember& d, BrkDev* 
     int itCB = 0;
     for (int i = 0; i < npk; ++i) {
       const int J = pk[i];
-      const double eJ = PE[J].x, hJ = Heta[size_t(hs) * J];
-      const double gH = (Heta[size_t(hs) * (J + 1)] - Heta[size_t(hs) * (J - 1)]) / (2 * d.dx);
-      const double ge = (PE[J + 1].x - PE[J - 1].x) / (2 * d.dx);
-      const double KxJ = (eJ * gH - hJ * ge) / (eJ * eJ + hJ * hJ);
-      const double Cc = phase_velocity_dev(KxJ, d.depth[J] + eJ);
       const double Up = PE[J].y;
-      if (fabs(Up) > (d.KBC * fabs(Cc)) && itCB < cap) {
+      if (itCB < cap) {
         Crest& r = cb[itCB];
         r.Bindex = J;
         r.BindexNow = J;
@@ -212,21 +226,27 @@ static __device__ __noinline__ void breaking_leader(const DevMember& d, BrkDev* 
   bk->npk = bk->n_touched;
 }
 
-// returns false (Rb untouched) when no node breaks: the force is then identically
-// zero, as the reference's FFT of a zero flux gives, and the assembly skips it
+// The parts of one RHS's breaking work, so that a caller can place them between
+// its own phases:
+//   breaking_reset  (leader) before a barrier that precedes the scan;
+//   breaking_scan   (all threads) once eta, u and H(eta) are complete member-wide;
+//   breaking_lead   (leader) after a barrier that follows the scan; it leaves the
+//                   count of nodes with B != 0 in bk->npk (0: no force);
+//   breaking_force  (all threads) after a barrier that follows the leader.
 template <int M>
-__device__ __noinline__ bool breaking_rhs(Ctx<M>& X, double t, const double2* PE, const double* Heta, int hs,
-                                          const double2* AEadj, double2* Rb) {
+__device__ __forceinline__ void breaking_reset(Ctx<M>& X) {
+  if (X.c == 0 && X.tid == 0) {
+    X.d.bk->npk = 0;
+    X.d.bk->any_above = 0;
+  }
+}
+
+// criterion scan over this CTA's physical points (1d/breaking.c:36-61,72)
+template <int M>
+__device__ __forceinline__ void breaking_scan(Ctx<M>& X, const double2* PE, const double* Heta, int hs) {
   const DevMember& d = X.d;
   BrkDev* bk = d.bk;
   const int N = d.N;
-  const bool leader = X.c == 0 && X.tid == 0;
-  if (leader) {
-    bk->npk = 0;
-    bk->any_above = 0;
-  }
-  member_sync(d.C);
-  // criterion scan over this CTA's physical points (1d/breaking.c:36-61,72)
   const int w0 = d.xbstart, w1 = d.xbstart + d.lenIF;   // window [w0, w1)
   bool above = false;
   HW_FOREACH(X) {
@@ -234,7 +254,8 @@ __device__ __noinline__ bool breaking_rhs(Ctx<M>& X, double t, const double2* PE
     if (p >= w0 && p < w1) {
       const double e = PE[p].x;
       if (e > d.MaxEtaInit) above = true;
-      if (p >= w0 + 1 && p <= w1 - 2 && !(e < d.MaxEtaInit) && e > PE[p + 1].x && e > PE[p - 1].x) {
+      if (p >= w0 + 1 && p <= w1 - 2 && !(e < d.MaxEtaInit) && e > PE[p + 1].x && e > PE[p - 1].x &&
+          crest_breaks(d, PE, Heta, hs, p)) {
         const int slot = atomicAdd(&bk->npk, 1);
         if (slot < N) bk->pk[slot] = p;
       }
@@ -242,15 +263,25 @@ __device__ __noinline__ bool breaking_rhs(Ctx<M>& X, double t, const double2* PE
   }
   // one flag update per warp
   if (__any_sync(0xffffffffu, above) && (X.tid & 31) == 0) atomicOr(&bk->any_above, 1);
-  member_sync(d.C);
-  if (leader) {
-    if (bk->npk > N) bk->npk = N;
-    breaking_leader(d, bk, t, PE, Heta, hs);
+}
+
+template <int M>
+__device__ __forceinline__ void breaking_lead(Ctx<M>& X, double t, const double2* PE, const double* Heta, int hs) {
+  if (X.c == 0 && X.tid == 0) {
+    BrkDev* bk = X.d.bk;
+    if (bk->npk > X.d.N) bk->npk = X.d.N;
+    breaking_leader(X.d, bk, t, PE, Heta, hs);
     __threadfence();
   }
-  member_sync(d.C);
-  if (bk->npk == 0) return false;   // B identically zero: FFT(0) = 0, as the reference computes it
-  // d_t eta = Re F^-1(dH1_eta + adjusted nonlinear eta term)
+}
+
+// eddy-viscosity force (rhs_breaking, 1d/rhs.c:617-657): Rb = F(d_x Flux / (h + eta)),
+// Flux = -B delb^2 (h + eta) (d_t eta)^2, d_t eta = Re F^-1(dH1_eta + AEadj)
+template <int M>
+__device__ __noinline__ void breaking_force(Ctx<M>& X, const double2* PE, const double2* AEadj, double2* Rb) {
+  const DevMember& d = X.d;
+  BrkDev* bk = d.bk;
+  const int N = d.N;
   const double2* ZU = d.zs + N;
   const double2* HS = d.sc[6];
   auto teta = [&](int q) -> double2 {
@@ -286,6 +317,22 @@ __device__ __noinline__ bool breaking_rhs(Ctx<M>& X, double t, const double2* PE
     X.buf[pidx(idx)] = make_double2(rb, 0.0);
   }
   fft_forward_split(X, [&](int, int, int p, double2 z, double2 zp) { Rb[p] = split_re(z, zp); });
+}
+
+// The whole breaking step of one RHS, after the adjusted nonlinear terms: returns
+// false (Rb untouched) when no node breaks: the force is then identically zero, as
+// the reference's FFT of a zero flux gives, and the assembly skips it
+template <int M>
+__device__ __noinline__ bool breaking_rhs(Ctx<M>& X, double t, const double2* PE, const double* Heta, int hs,
+                                          const double2* AEadj, double2* Rb) {
+  breaking_reset(X);
+  member_sync(X.d.C);
+  breaking_scan(X, PE, Heta, hs);
+  member_sync(X.d.C);
+  breaking_lead(X, t, PE, Heta, hs);
+  member_sync(X.d.C);
+  if (X.d.bk->npk == 0) return false;   // B identically zero: FFT(0) = 0, as the reference computes it
+  breaking_force(X, PE, AEadj, Rb);
   return true;
 }
 

@@ -175,6 +175,9 @@ __device__ __forceinline__ void local_fft(double2* buf, const double2* __restric
 // the thread owning position i gathers the C values at i from every CTA's slice,
 // applies the C-point DFT (forward: then the twiddles W_N^(i k1); inverse: the
 // twiddles W_N^-(i k1) first) and stores output j into CTA j's slice at i.
+// Every position is owned by exactly one thread of the cluster, which reads and
+// then rewrites it in every CTA, so the scatter needs no barrier after the gather:
+// one cluster barrier before (the slices are complete) and one after.
 template <int M, int C, int NBUF>
 __device__ __forceinline__ void cross_gs(double2* A, double2* B, const double2* __restrict__ tw, int c, int sign) {
   constexpr int T = M / kPts;
@@ -191,7 +194,6 @@ __device__ __forceinline__ void cross_gs(double2* A, double2* B, const double2* 
       if constexpr (NBUF == 2) vb[q][r] = cl.map_shared_rank(B, r)[pidx(i)];
     }
   }
-  cl.sync();
 #pragma unroll
   for (int q = 0; q < PER; ++q) {
     const int i = c * T + threadIdx.x + q * (C * T);

@@ -26,7 +26,7 @@ __global__ void __launch_bounds__(M / kPts, HW_EVOLVE_MIN_BLOCKS(M)) k_evolve(De
   const int mi = list[blockIdx.x / C];
   if (threadIdx.x == 0) sd = mems[mi];
   __syncthreads();
-  Ctx<M> X{sd, smem_buf, smem_buf + padded(M), red, rank, int(threadIdx.x)};
+  Ctx<M> X = make_ctx<M>(sd, smem_buf, red, rank);
   Bufs B;
   B.y = sd.y;
   B.yn = sd.ynew;
@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(M / kPts, (4096 / M)) k_rhs(DevMember* mems, c
   const int mi = list[blockIdx.x / C];
   if (threadIdx.x == 0) sd = mems[mi];
   __syncthreads();
-  Ctx<M> X{sd, smem_buf, smem_buf + padded(M), red, rank, int(threadIdx.x)};
+  Ctx<M> X = make_ctx<M>(sd, smem_buf, red, rank);
   rhs_eval<M>(X, t, sd.kb[6]);
   member_sync(C);
   if (rank == 0 && threadIdx.x == 0) mems[mi].rhs_calls += 1;
@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(M / kPts, (4096 / M)) k_rhs(DevMember* mems, c
 
 template <int M>
 cudaError_t set_attrs() {
-  const int bytes = 2 * padded(M) * int(sizeof(double2));
+  const int bytes = int(slice_smem_bytes(M));
   cudaError_t e;
   if ((e = cudaFuncSetAttribute(k_evolve<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
   if ((e = cudaFuncSetAttribute(k_rhs<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
@@ -101,7 +101,7 @@ cudaError_t launch(int mode, DevMember* mems, const int* list, int nmem, int C, 
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(unsigned(nmem * C));
   cfg.blockDim = dim3(M / kPts);
-  cfg.dynamicSmemBytes = 2 * size_t(padded(M)) * sizeof(double2);
+  cfg.dynamicSmemBytes = slice_smem_bytes(M);
   cfg.stream = s;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;

@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(M / kPts, (4096 / M)) k_rhs_noalloc(DevMember*
     for (int i = 0; i < kScratch; ++i) sd.sc[i] = scratch + size_t(4 + i) * N;
   }
   __syncthreads();
-  Ctx<M> X{sd, smem_buf, smem_buf + padded(M), red, rank, int(threadIdx.x)};
+  Ctx<M> X = make_ctx<M>(sd, smem_buf, red, rank);
   const int N = sd.N;
   // reference layout -> this CTA's spectral slice of the stage input
   HW_FOREACH(X) {
@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(M / kPts, (4096 / M)) k_rhs_noalloc(DevMember*
 
 template <int M>
 cudaError_t set_noalloc_attrs() {
-  const int bytes = 2 * padded(M) * int(sizeof(double2));
+  const int bytes = int(slice_smem_bytes(M));
   cudaError_t e = cudaFuncSetAttribute(k_rhs_noalloc<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_rhs_noalloc<M>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
@@ -89,7 +89,7 @@ cudaError_t set_noalloc_attrs() {
 template <int M>
 cudaError_t launch_noalloc(DevMember* mems, int mi, int C, double t, const double* y, double* dy,
                            double2* scratch, cudaStream_t s) {
-  const int bytes = 2 * padded(M) * int(sizeof(double2));
+  const int bytes = int(slice_smem_bytes(M));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(unsigned(C));
   cfg.blockDim = dim3(M / kPts);

@@ -38,8 +38,7 @@ __device__ __noinline__ void output_stage(Ctx<M>& X, Bufs& B, StepState& S, int 
   const double2* dy = B.k[6];
   if (!d.exact && !none) {
     if (!S.k1_valid) {
-      load_stage(X, B.y);
-      rhs_into(X, S, S.t, B.k[0]);
+      rhs_at(X, S, S.t, B.y, B.k[0]);
       S.k1_valid = 1;
     }
     dy = B.k[0];

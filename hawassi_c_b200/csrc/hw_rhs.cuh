@@ -29,7 +29,8 @@ __device__ constexpr double RK_ec4 = -2197.0 / 75240.0;
 __device__ constexpr double RK_ec5 = 1.0 / 50.0;
 __device__ constexpr double RK_ec6 = 2.0 / 55.0;
 
-// the stage input of an RK stage: zs = y + h sum_j b_sj k_j (s = 2..6)
+// the stage input of an RK stage: zs = y + h sum_j b_sj k_j (s = 2..6), or zs = y
+// itself (s = 1: the state a first or last derivative is evaluated at)
 struct StageSrc {
   const double2* y;
   const double2* k[5];
@@ -44,6 +45,7 @@ __device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a,
 
 // one element of the stage input, in GSL rkf45's expression forms
 __device__ __forceinline__ double2 stage_val(const StageSrc& st, int q) {
+  if (st.s == 1) return st.y[q];
   const double2 y = st.y[q], a = st.k[0][q];
   const double h = st.h;
   if (st.s == 2) {
@@ -86,7 +88,21 @@ struct Ctx {
   int c;          // rank of this CTA in the member's cluster
   int tid;
   const StageSrc* stg = nullptr;   // set: zs is to be formed from y and the k's first
+  double* rs = nullptr;            // M doubles of shared memory: one real field held across transforms
 };
+
+// dynamic shared memory of the 1D kernels of slice M: two padded FFT slices and one
+// real M-point field
+__host__ __device__ constexpr size_t slice_smem_bytes(int m) {
+  return 2 * size_t(padded(m)) * sizeof(double2) + size_t(m) * sizeof(double);
+}
+
+template <int M>
+__device__ __forceinline__ Ctx<M> make_ctx(const DevMember& d, double2* smem, double* red, int rank) {
+  Ctx<M> X{d, smem, smem + padded(M), red, rank, int(threadIdx.x)};
+  X.rs = reinterpret_cast<double*>(smem + 2 * padded(M));
+  return X;
+}
 
 #define HW_FOREACH(X)                            \
   _Pragma("unroll") for (int u = 0; u < kPts; ++u)  \
@@ -211,6 +227,14 @@ __device__ __noinline__ void hss(Ctx<M>& X, const double2* __restrict__ A, const
 template <int M>
 __device__ __noinline__ bool breaking_rhs(Ctx<M>& X, double t, const double2* PE, const double* Heta, int heta_stride,
                              const double2* AEadj, double2* Rb);
+template <int M>
+__device__ __forceinline__ void breaking_reset(Ctx<M>& X);
+template <int M>
+__device__ __forceinline__ void breaking_scan(Ctx<M>& X, const double2* PE, const double* Heta, int hs);
+template <int M>
+__device__ __forceinline__ void breaking_lead(Ctx<M>& X, double t, const double2* PE, const double* Heta, int hs);
+template <int M>
+__device__ __noinline__ void breaking_force(Ctx<M>& X, const double2* PE, const double2* AEadj, double2* Rb);
 // HS2 flat-bottom fast path (hw_rhs_fast.cuh)
 template <int M>
 __device__ __noinline__ void rhs_hs2_flat(Ctx<M>& X, double t, double2* __restrict__ dz);

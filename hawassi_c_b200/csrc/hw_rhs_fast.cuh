@@ -22,6 +22,36 @@ __device__ __forceinline__ double2 hilbert_hat(double k, double2 e) {
   return make_double2(s * e.y, -s * e.x);
 }
 
+// the influx source term of the assembly (1d/rhs.c:659-693): force = (fr, fi)
+__device__ __forceinline__ void source_term(const DevMember& d, int p, double pv, double ps, double& fr, double& fi) {
+  fr = 0.0;
+  fi = 0.0;
+  if (d.has_influx) {
+    const double2 gx = d.gamX[p], gs = d.gamXs[p];
+    if (d.prop_mode == 0) { fr = 0.5 * (pv * gx.x - ps * gs.x); fi = 0.5 * (pv * gx.y - ps * gs.y); }
+    else if (d.prop_mode == 1) { fr = 0.5 * (pv * gx.x + ps * gs.x); fi = 0.5 * (pv * gx.y + ps * gs.y); }
+    else if (d.prop_mode == 2) { fr = pv * gx.x; fi = pv * gx.y; }
+  }
+}
+
+// assembly of dz at spectral position p (1d/rhs.c:217-228): delta H1 + adjusted
+// nonlinear terms (ae, au) + breaking force (rb) + 2 force - damping (de, du), times aal
+__device__ __forceinline__ void assemble_flat(const DevMember& d, int p, double2 ae, double2 au, double2 rb, double2 de,
+                                              double2 du, double pv, double ps, double2* __restrict__ dz) {
+  const int N = d.N;
+  const double2 ze = d.zs[p], zu = d.zs[N + p];
+  const double c1 = d.c1[p], gk = d.gk[p];
+  double2 te = make_double2(c1 * zu.y, -c1 * zu.x);
+  double2 tu = make_double2(gk * ze.y, -gk * ze.x);
+  double fr, fi;
+  source_term(d, p, pv, ps, fr, fi);
+  const double al = d.aal[p];
+  te = cadd(te, ae);
+  tu = cadd(cadd(tu, au), rb);
+  dz[p] = make_double2((te.x + 2 * fr - de.x) * al, (te.y + 2 * fi - de.y) * al);
+  dz[N + p] = make_double2((tu.x - du.x) * al, (tu.y - du.y) * al);
+}
+
 template <int M>
 __device__ __noinline__ void rhs_hs2_flat(Ctx<M>& X, double t, double2* __restrict__ dz) {
   const DevMember& d = X.d;
@@ -30,12 +60,12 @@ __device__ __noinline__ void rhs_hs2_flat(Ctx<M>& X, double t, double2* __restri
   double2* Bf = X.buf2;
   const double2* ZE = d.zs;
   const double2* ZU = d.zs + N;
-  double2* PE = d.sc[0];   // physical (eta, u)          [breaking only]
-  double2* PM = d.sc[1];   // physical (., Hilbert eta)  [breaking only]
-  double2* AE = d.sc[2];   // adjusted nonlinear eta term
-  double2* AU = d.sc[3];   // adjusted nonlinear u term
+  double2* PE = d.sc[0];   // physical (eta, u)           [breaking only]
+  double2* PM = d.sc[1];   // physical (., Hilbert eta)   [breaking only]
+  double2* AE = d.sc[2];   // adjusted nonlinear eta term [breaking force live only]
+  double2* AU = d.sc[3];   // adjusted nonlinear u term   [breaking force live only]
   double2* DE = d.sc[4];   // FFT(damping eta)
-  double2* DU = d.sc[5];   // FFT(damping u)
+  double2* DU = d.sc[5];   // FFT(damping u)              [breaking force live only]
   double2* RB = d.sc[11];  // FFT(breaking force)
   const bool brk = d.brk != 0;
   const double2* Ap = A;
@@ -49,79 +79,89 @@ __device__ __noinline__ void rhs_hs2_flat(Ctx<M>& X, double t, double2* __restri
   auto jpart = [&](int idx) { return X.c == 0 ? ((M - idx) & (M - 1)) : (M - 1 - idx); };
   double2 va[kPts], vb[kPts];
 
-  // (0) stage input into the two slices (spectral, cyclic), formed here from y and
-  // the k's during an RK step (and kept in zs for the assembly)
+  // (0)-(1) stage input (spectral, cyclic) and its Hermitian packing for the first
+  // dual inverse transform: A <- eta^ + i u^, B <- M0 u^ + i H(eta)^ (real parts
+  // only, as the reference).  Every exit of this function leaves the slices unread
+  // by the other CTAs (a barrier follows the last partner reads), so they can be
+  // written at once.
+  if (brk) breaking_reset(X);
+  auto packed = [&](int p, int pp, double2 e, double2 ep, double2 w, double2 wp, double2& a, double2& b) {
+    a = pack(herm(e, ep), herm(w, wp), d.invN);
+    const double2 m0 = mul_ik(d.M0im[p], w), m0p = mul_ik(d.M0im[pp], wp);
+    const double2 s2 = brk ? herm(hilbert_hat(d.k[p], e), hilbert_hat(d.k[pp], ep)) : make_double2(0.0, 0.0);
+    b = pack(herm(m0, m0p), s2, d.invN);
+  };
   if (X.stg) {
+    // during a step the stage input is formed here from y and the k's (and kept in
+    // zs for the assembly); the value at the partner wavenumber N - k is formed from
+    // the same global vectors, so no exchange between the CTAs is needed
     double2* zw = d.zs;
     HW_FOREACH(X) {
-      (void)idx;
-      const double2 ze = stage_val(*X.stg, p), zu = stage_val(*X.stg, N + p);
-      zw[p] = ze;
-      zw[N + p] = zu;
-      A[pidx(idx)] = ze;
-      Bf[pidx(idx)] = zu;
+      const int pp = partner_pos(X, idx);
+      const double2 e = stage_val(*X.stg, p), w = stage_val(*X.stg, N + p);
+      const double2 ep = stage_val(*X.stg, pp), wp = stage_val(*X.stg, N + pp);
+      zw[p] = e;
+      zw[N + p] = w;
+      packed(p, pp, e, ep, w, wp, va[u], vb[u]);
     }
   } else {
+    // zs written by the caller: the partner values come through the slices
     HW_FOREACH(X) {
       A[pidx(idx)] = ZE[p];
       Bf[pidx(idx)] = ZU[p];
     }
+    member_sync(C);
+    HW_FOREACH(X) {
+      const int jp = jpart(idx), pp = partner_pos(X, idx);
+      packed(p, pp, A[pidx(idx)], Ap[pidx(jp)], Bf[pidx(idx)], Bp[pidx(jp)], va[u], vb[u]);
+    }
+    member_sync(C);
   }
-  member_sync(C);
-  // (1) Hermitian packing: A <- eta^ + i u^, B <- M0 u^ + i H(eta)^ (real parts only, as the reference)
-  HW_FOREACH(X) {
-    const int jp = jpart(idx), pp = partner_pos(X, idx);
-    const double2 e = A[pidx(idx)], ep = Ap[pidx(jp)], w = Bf[pidx(idx)], wp = Bp[pidx(jp)];
-    va[u] = pack(herm(e, ep), herm(w, wp), d.invN);
-    const double2 m0 = mul_ik(d.M0im[p], w), m0p = mul_ik(d.M0im[pp], wp);
-    const double2 s2 = brk ? herm(hilbert_hat(d.k[p], e), hilbert_hat(d.k[pp], ep)) : make_double2(0.0, 0.0);
-    vb[u] = pack(herm(m0, m0p), s2, d.invN);
-  }
-  member_sync(C);
   HW_FOREACH(X) {
     (void)p;
     A[pidx(idx)] = va[u];
     Bf[pidx(idx)] = vb[u];
   }
   fft_inverse2<M>(A, Bf, d.tw, N, C, X.c);
-  // (2) products in physical space (1d/functions.c:1486-1498)
-  double du[kPts];
+  // (2) products in physical space (1d/functions.c:1486-1498); the damping of u
+  // waits in shared memory for the adjustment's transform
   HW_FOREACH(X) {
     const double2 e = A[pidx(idx)], m = Bf[pidx(idx)];
     if (brk) {
       PE[p] = e;
       PM[p].y = m.y;
     }
-    du[u] = (d.dcoef[p] * e.y) * d.dchar[p];
+    X.rs[idx] = (d.dcoef[p] * e.y) * d.dchar[p];
     A[pidx(idx)] = make_double2(e.x * e.y, e.x * m.x);
     Bf[pidx(idx)] = make_double2(e.y * e.y - m.x * m.x, (d.dcoef[p] * e.x) * d.dchar[p]);
   }
   fft_forward2<M>(A, Bf, d.tw, N, C, X.c);
-  // (3) spectra of the products; H2 terms (1d/rhs.c:141-147)
+  // breaking criterion (1d/breaking.c:36-95) on eta, u, H(eta): the transform's
+  // barriers made PE / PM complete member-wide
+  if (brk) breaking_scan(X, PE, &PM[0].y, 2);
+  // (3) spectra of the products, H2 terms (1d/rhs.c:141-147) and, in the same
+  // pass, the Hermitian packing of the nonlinear adjustment (1d/rhs.c:695-715):
+  // each thread forms the terms at its wavenumber k and at N - k from the pair of
+  // transformed values it holds, so no exchange separates the two steps
   member_sync(C);
   HW_FOREACH(X) {
-    const int jp = jpart(idx);
+    const int jp = jpart(idx), pp = partner_pos(X, idx);
     const double2 z1 = A[pidx(idx)], z1p = Ap[pidx(jp)], z2 = Bf[pidx(idx)], z2p = Bp[pidx(jp)];
-    const double2 ah = split_re(z1, z1p), bh = split_im(z1, z1p), ch = split_re(z2, z2p);
     DE[p] = split_im(z2, z2p);
-    const double kp = d.k[p];
+    const double kp = d.k[p], kq = d.k[pp];
+    // at k
+    const double2 ah = split_re(z1, z1p), bh = split_im(z1, z1p), ch = split_re(z2, z2p);
     const double2 lem = cscale(bh, d.L[p]), ik = mul_ik(kp, ah), ikc = mul_ik(kp, ch);
-    va[u] = make_double2(-lem.x - ik.x, -lem.y - ik.y);
-    vb[u] = make_double2(-ikc.x / 2, -ikc.y / 2);
+    const double2 te = make_double2(-lem.x - ik.x, -lem.y - ik.y);
+    const double2 tu = make_double2(-ikc.x / 2, -ikc.y / 2);
+    // at N - k (the partner's pair is (z1p, z1))
+    const double2 ahq = split_re(z1p, z1), bhq = split_im(z1p, z1), chq = split_re(z2p, z2);
+    const double2 lemq = cscale(bhq, d.L[pp]), ikq = mul_ik(kq, ahq), ikcq = mul_ik(kq, chq);
+    const double2 teq = make_double2(-lemq.x - ikq.x, -lemq.y - ikq.y);
+    const double2 tuq = make_double2(-ikcq.x / 2, -ikcq.y / 2);
+    va[u] = pack(herm(te, teq), herm(tu, tuq), d.invN);
   }
-  member_sync(C);
-  HW_FOREACH(X) {
-    (void)p;
-    A[pidx(idx)] = va[u];
-    Bf[pidx(idx)] = vb[u];
-  }
-  member_sync(C);
-  // (4) nonlinear adjustment (1d/rhs.c:695-715): ChiAdj applied in physical space
-  HW_FOREACH(X) {
-    (void)p;
-    const int jp = jpart(idx);
-    va[u] = pack(herm(A[pidx(idx)], Ap[pidx(jp)]), herm(Bf[pidx(idx)], Bp[pidx(jp)]), d.invN);
-  }
+  if (brk) breaking_lead(X, t, PE, &PM[0].y, 2);
   member_sync(C);
   HW_FOREACH(X) {
     (void)p;
@@ -132,10 +172,28 @@ __device__ __noinline__ void rhs_hs2_flat(Ctx<M>& X, double t, double2* __restri
     const double2 v = A[pidx(idx)];
     const double ch = d.chi[p];
     A[pidx(idx)] = make_double2(v.x * ch, v.y * ch);
-    Bf[pidx(idx)] = make_double2(du[u], 0.0);
+    Bf[pidx(idx)] = make_double2(X.rs[idx], 0.0);
   }
   fft_forward2<M>(A, Bf, d.tw, N, C, X.c);
+  double pv = 0.0, ps = 0.0;
+  if (d.has_influx) {
+    pv = spline_eval(d.tt, d.ins, d.insc, d.n_in, t);
+    ps = spline_eval(d.tt, d.skw, d.skwc, d.n_in, t);
+  }
   member_sync(C);
+  // the leader's node count is visible member-wide after the transforms' barriers
+  const bool rb_live = brk && d.bk->npk > 0;
+  if (!rb_live) {
+    // (6) assembly (1d/rhs.c:217-228) straight from the adjusted spectra
+    HW_FOREACH(X) {
+      const int jp = jpart(idx);
+      const double2 z = A[pidx(idx)], zp = Ap[pidx(jp)], zb = Bf[pidx(idx)], zbp = Bp[pidx(jp)];
+      assemble_flat(d, p, split_re(z, zp), split_im(z, zp), make_double2(0.0, 0.0), DE[p], split_re(zb, zbp), pv, ps,
+                    dz);
+    }
+    member_sync(C);   // the partner reads of the slices are done
+    return;
+  }
   HW_FOREACH(X) {
     const int jp = jpart(idx);
     const double2 z = A[pidx(idx)], zp = Ap[pidx(jp)], zb = Bf[pidx(idx)], zbp = Bp[pidx(jp)];
@@ -145,33 +203,12 @@ __device__ __noinline__ void rhs_hs2_flat(Ctx<M>& X, double t, double2* __restri
   }
   member_sync(C);
   // (5) kinematic breaking: eddy-viscosity force on the u-equation
-  const bool rb_live = brk && breaking_rhs<M>(X, t, PE, &PM[0].y, 2, AE, RB);
-  // (6) assembly (1d/rhs.c:217-228) with the source term (1d/rhs.c:659)
-  double pv = 0.0, ps = 0.0;
-  if (d.has_influx) {
-    pv = spline_eval(d.tt, d.ins, d.insc, d.n_in, t);
-    ps = spline_eval(d.tt, d.skw, d.skwc, d.n_in, t);
-  }
+  breaking_force<M>(X, PE, AE, RB);
+  // (6) assembly with the force
+  member_sync(C);
   HW_FOREACH(X) {
     (void)idx;
-    const double2 ze = ZE[p], zu = ZU[p];
-    const double c1 = d.c1[p], gk = d.gk[p];
-    double2 te = make_double2(c1 * zu.y, -c1 * zu.x);
-    double2 tu = make_double2(gk * ze.y, -gk * ze.x);
-    double fr = 0.0, fi = 0.0;
-    if (d.has_influx) {
-      const double2 gx = d.gamX[p], gs = d.gamXs[p];
-      if (d.prop_mode == 0) { fr = 0.5 * (pv * gx.x - ps * gs.x); fi = 0.5 * (pv * gx.y - ps * gs.y); }
-      else if (d.prop_mode == 1) { fr = 0.5 * (pv * gx.x + ps * gs.x); fi = 0.5 * (pv * gx.y + ps * gs.y); }
-      else if (d.prop_mode == 2) { fr = pv * gx.x; fi = pv * gx.y; }
-    }
-    const double al = d.aal[p];
-    const double2 de = DE[p], dd = DU[p];
-    te = cadd(te, AE[p]);
-    tu = cadd(tu, AU[p]);
-    if (rb_live) tu = cadd(tu, RB[p]);
-    dz[p] = make_double2((te.x + 2 * fr - de.x) * al, (te.y + 2 * fi - de.y) * al);
-    dz[N + p] = make_double2((tu.x - dd.x) * al, (tu.y - dd.y) * al);
+    assemble_flat(d, p, AE[p], AU[p], RB[p], DE[p], DU[p], pv, ps, dz);
   }
 }
 

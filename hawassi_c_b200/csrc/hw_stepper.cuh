@@ -98,6 +98,15 @@ __device__ __forceinline__ void rhs_into(Ctx<M>& X, StepState& S, double t, doub
   ++S.rhs;
 }
 
+// one RHS evaluation at the state src itself (the RHS copies it into zs)
+template <int M>
+__device__ __forceinline__ void rhs_at(Ctx<M>& X, StepState& S, double t, const double2* src, double2* out) {
+  const StageSrc st{src, {nullptr, nullptr, nullptr, nullptr, nullptr}, 1, 0.0};
+  X.stg = &st;
+  rhs_into(X, S, t, out);
+  X.stg = nullptr;
+}
+
 // copy a state buffer into the stage-input buffer
 template <int M>
 __device__ __forceinline__ void load_stage(Ctx<M>& X, const double2* src) {
@@ -119,10 +128,7 @@ __device__ __noinline__ void evolve_apply(Ctx<M>& X, Bufs& B, StepState& S, doub
   double h0 = S.h;
   const double dt = t1 - t0;
   if ((dt < 0.0 && h0 > 0.0) || (dt > 0.0 && h0 < 0.0)) { S.status = kStepFailed; return; }
-  if (d.exact || !S.k1_valid) {
-    load_stage(X, B.y);
-    rhs_into(X, S, t0, B.k[0]);
-  }
+  if (d.exact || !S.k1_valid) rhs_at(X, S, t0, B.y, B.k[0]);
   int attempts = 0;
   for (;;) {
     bool final_step = false;
@@ -136,10 +142,7 @@ __device__ __noinline__ void evolve_apply(Ctx<M>& X, Bufs& B, StepState& S, doub
     }
     member_sync(d.C);
     const double rmax = final_combine(X, B, h0);
-    if (d.exact) {
-      load_stage(X, B.yn);
-      rhs_into(X, S, t0 + h0, B.k[6]);
-    }
+    if (d.exact) rhs_at(X, S, t0 + h0, B.yn, B.k[6]);
     const double tn = final_step ? t1 : t0 + h0;
     // std_control_hadjust (order 5)
     const double h_old = h0;
@@ -174,8 +177,7 @@ __device__ __noinline__ void evolve_apply(Ctx<M>& X, Bufs& B, StepState& S, doub
       // next call starts exactly at t0 + h0
       const double tk = t0 + h0;
       if (tk == tn) {
-        load_stage(X, B.yn);
-        rhs_into(X, S, tk, B.k[6]);
+        rhs_at(X, S, tk, B.yn, B.k[6]);
         double2* tmp = B.k[0]; B.k[0] = B.k[6]; B.k[6] = tmp;
         S.k1_valid = 1;
       } else {

@@ -9,10 +9,11 @@ from hawassi_c_b200 import decks2d
 GRAV = 9.80665
 
 
-def steep_crest_case(nx=64, ny=64, dt_out=0.002, x_crest=40.0, seed=1, bathymetry="shoal", model=2):
+def steep_crest_case(nx=64, ny=64, dt_out=0.002, x_crest=40.0, seed=1, bathymetry="shoal", model=2, ninterp=2,
+                     walls=()):
     tb = decks2d.tables(nx=nx, ny=ny, Lx=float(nx), Ly=float(ny), depth=3.0 if bathymetry != "flat" else 1.5,
                         shallow=0.5, Hs=0.6, Tp=4.0, n_freq=16, n_dir=4, t_end=10.0, dt=0.1, damp=6.0, x_line=8.0,
-                        seed=seed, bathymetry=bathymetry, breaking=True, model=model)
+                        seed=seed, bathymetry=bathymetry, breaking=True, model=model, ninterp=ninterp, walls=walls)
     tb["dt_out"] = dt_out
     d = -tb["bathy"]
     X, Y = np.meshgrid(tb["x"], tb["y"])

@@ -291,16 +291,10 @@ def test_three_depth_with_an_idle_middle_depth_is_two_depth(model):
     assert np.linalg.norm(d - ref) < 1e-13 * np.linalg.norm(ref)
 
 
-def test_three_depth_tables_run_in_the_oracle_and_are_refused_by_the_engine():
-    from hawassi_c_b200.engine import EngineError
-    from hawassi_c_b200.engine2d import Engine2D
+def test_three_depth_tables_run_in_the_oracle():
     tb = _shoal(ninterp=3, ny=64)
     assert {"gam_mid", "csq_mid", "om2_mid"} <= set(tb)
     n = tb["nx"] * tb["ny"]
     rng = np.random.default_rng(5)
     y = 0.02 * rng.standard_normal(6 * n) * np.tile(tb["aal"].ravel(), 6) * np.sqrt(n)
     assert np.isfinite(Oracle2D(tb).rhs(0.3, y)).all()
-    with pytest.raises(EngineError, match="three reference depths"):
-        Engine2D(tb)
-    with pytest.raises(EngineError, match="HS3 is built for the flat bottom"):
-        Engine2D(_shoal(ny=64, model=3))
