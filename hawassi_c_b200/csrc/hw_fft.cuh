@@ -442,4 +442,18 @@ __device__ __noinline__ void fft_inverse2(double2* A, double2* B, const double2*
   }
 }
 
+// The local (in-CTA) part of a distributed transform alone, for callers that do the
+// cross-CTA step themselves: sign +1 is the inverse's first half, -1 the forward's
+// second half.  Barrier on entry (the caller wrote the slices) and on exit.
+template <int M>
+__device__ __noinline__ void fft_local(double2* A, const double2* __restrict__ tw, int C, int sign) {
+  __syncthreads();
+  local_fft<M>(A, tw, C, sign);
+}
+template <int M>
+__device__ __noinline__ void fft_local2(double2* A, double2* B, const double2* __restrict__ tw, int C, int sign) {
+  __syncthreads();
+  local_fft2<M>(A, B, tw, C, sign);
+}
+
 }  // namespace hwdev

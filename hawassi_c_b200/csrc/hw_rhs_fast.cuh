@@ -52,6 +52,128 @@ __device__ __forceinline__ void assemble_flat(const DevMember& d, int p, double2
   dz[N + p] = make_double2((tu.x - du.x) * al, (tu.y - du.y) * al);
 }
 
+// Cluster members: the inverse transform's cross-CTA step, the pointwise work in
+// physical space and the next forward transform's cross-CTA step meet at the same
+// index set -- position i of every CTA's slice, i.e. the physical points r M + i
+// (r = 0..C-1) -- so the thread owning position i (the ownership of cross_gs) does
+// all three in registers: gather, twiddle, inverse C-point DFT, pointwise step,
+// forward C-point DFT, twiddle, scatter.  Two cluster barriers replace four and the
+// physical fields never pass through shared memory.
+//
+// First meeting (1d/functions.c:1486-1498): A = eta + i u, B = M0 u + i H(eta) in;
+// out A = (eta u) + i (eta M0 u), B = (u^2 - (M0 u)^2) + i (damping of eta); the
+// damping of u is kept in the thread's own part of X.rs for the second meeting;
+// eta, u and H(eta) go to global memory for the breaking criterion.
+template <int M, int C>
+__device__ __forceinline__ void cross_products(Ctx<M>& X, double2* A, double2* B, bool brk, double2* PE, double2* PM) {
+  constexpr int T = M / kPts;
+  constexpr int PER = kPts / C;
+  const DevMember& d = X.d;
+  cg::cluster_group cl = cg::this_cluster();
+  cl.sync();
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int i = X.c * T + X.tid + q * (C * T);
+    double2 va[C], vb[C], w[C > 1 ? C : 2];
+#pragma unroll
+    for (int r = 0; r < C; ++r) {
+      va[r] = cl.map_shared_rank(A, r)[pidx(i)];
+      vb[r] = cl.map_shared_rank(B, r)[pidx(i)];
+    }
+    twiddle_powers<C>(twd(d.tw, i, +1), w);
+#pragma unroll
+    for (int r = 1; r < C; ++r) {
+      va[r] = cmul(va[r], w[r]);
+      vb[r] = cmul(vb[r], w[r]);
+    }
+    dft_small<C>(va, +1);
+    dft_small<C>(vb, +1);
+#pragma unroll
+    for (int r = 0; r < C; ++r) {
+      const int n = r * M + i;
+      const double2 e = va[r], m = vb[r];
+      if (brk) {
+        PE[n] = e;
+        PM[n].y = m.y;
+      }
+      const double dc = d.dcoef[n], ch = d.dchar[n];
+      X.rs[X.tid * kPts + q * C + r] = (dc * e.y) * ch;
+      va[r] = make_double2(e.x * e.y, e.x * m.x);
+      vb[r] = make_double2(e.y * e.y - m.x * m.x, (dc * e.x) * ch);
+    }
+    dft_small<C>(va, -1);
+    dft_small<C>(vb, -1);
+    twiddle_powers<C>(twd(d.tw, i, -1), w);
+#pragma unroll
+    for (int r = 1; r < C; ++r) {
+      va[r] = cmul(va[r], w[r]);
+      vb[r] = cmul(vb[r], w[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < C; ++r) {
+      cl.map_shared_rank(A, r)[pidx(i)] = va[r];
+      cl.map_shared_rank(B, r)[pidx(i)] = vb[r];
+    }
+  }
+  cl.sync();
+}
+
+// Second meeting (1d/rhs.c:695-715): the nonlinear terms' inverse transform times
+// ChiAdj, paired with the damping of u kept by the first meeting, into the forward
+// dual transform: A in (one transform), out A = ChiAdj-adjusted terms, B = damping of u.
+template <int M, int C>
+__device__ __forceinline__ void cross_adjust(Ctx<M>& X, double2* A, double2* B) {
+  constexpr int T = M / kPts;
+  constexpr int PER = kPts / C;
+  const DevMember& d = X.d;
+  cg::cluster_group cl = cg::this_cluster();
+  cl.sync();
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int i = X.c * T + X.tid + q * (C * T);
+    double2 va[C], vb[C], w[C > 1 ? C : 2];
+#pragma unroll
+    for (int r = 0; r < C; ++r) va[r] = cl.map_shared_rank(A, r)[pidx(i)];
+    twiddle_powers<C>(twd(d.tw, i, +1), w);
+#pragma unroll
+    for (int r = 1; r < C; ++r) va[r] = cmul(va[r], w[r]);
+    dft_small<C>(va, +1);
+#pragma unroll
+    for (int r = 0; r < C; ++r) {
+      const double ch = d.chi[r * M + i];
+      va[r] = make_double2(va[r].x * ch, va[r].y * ch);
+      vb[r] = make_double2(X.rs[X.tid * kPts + q * C + r], 0.0);
+    }
+    dft_small<C>(va, -1);
+    dft_small<C>(vb, -1);
+    twiddle_powers<C>(twd(d.tw, i, -1), w);
+#pragma unroll
+    for (int r = 1; r < C; ++r) {
+      va[r] = cmul(va[r], w[r]);
+      vb[r] = cmul(vb[r], w[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < C; ++r) {
+      cl.map_shared_rank(A, r)[pidx(i)] = va[r];
+      cl.map_shared_rank(B, r)[pidx(i)] = vb[r];
+    }
+  }
+  cl.sync();
+}
+
+template <int M>
+__device__ __noinline__ void cross_products_any(Ctx<M>& X, double2* A, double2* B, bool brk, double2* PE, double2* PM) {
+  if (X.d.C == 2) cross_products<M, 2>(X, A, B, brk, PE, PM);
+  else if (X.d.C == 4) cross_products<M, 4>(X, A, B, brk, PE, PM);
+  else cross_products<M, 8>(X, A, B, brk, PE, PM);
+}
+template <int M>
+__device__ __noinline__ void cross_adjust_any(Ctx<M>& X, double2* A, double2* B) {
+  if (X.d.C == 2) cross_adjust<M, 2>(X, A, B);
+  else if (X.d.C == 4) cross_adjust<M, 4>(X, A, B);
+  else cross_adjust<M, 8>(X, A, B);
+}
+
 template <int M>
 __device__ __noinline__ void rhs_hs2_flat(Ctx<M>& X, double t, double2* __restrict__ dz) {
   const DevMember& d = X.d;
@@ -122,20 +244,27 @@ __device__ __noinline__ void rhs_hs2_flat(Ctx<M>& X, double t, double2* __restri
     A[pidx(idx)] = va[u];
     Bf[pidx(idx)] = vb[u];
   }
-  fft_inverse2<M>(A, Bf, d.tw, N, C, X.c);
   // (2) products in physical space (1d/functions.c:1486-1498); the damping of u
   // waits in shared memory for the adjustment's transform
-  HW_FOREACH(X) {
-    const double2 e = A[pidx(idx)], m = Bf[pidx(idx)];
-    if (brk) {
-      PE[p] = e;
-      PM[p].y = m.y;
+  const bool fused = C == 2 || C == 4 || C == 8;
+  if (fused) {
+    fft_local2<M>(A, Bf, d.tw, C, +1);
+    cross_products_any<M>(X, A, Bf, brk, PE, PM);
+    fft_local2<M>(A, Bf, d.tw, C, -1);
+  } else {
+    fft_inverse2<M>(A, Bf, d.tw, N, C, X.c);
+    HW_FOREACH(X) {
+      const double2 e = A[pidx(idx)], m = Bf[pidx(idx)];
+      if (brk) {
+        PE[p] = e;
+        PM[p].y = m.y;
+      }
+      X.rs[idx] = (d.dcoef[p] * e.y) * d.dchar[p];
+      A[pidx(idx)] = make_double2(e.x * e.y, e.x * m.x);
+      Bf[pidx(idx)] = make_double2(e.y * e.y - m.x * m.x, (d.dcoef[p] * e.x) * d.dchar[p]);
     }
-    X.rs[idx] = (d.dcoef[p] * e.y) * d.dchar[p];
-    A[pidx(idx)] = make_double2(e.x * e.y, e.x * m.x);
-    Bf[pidx(idx)] = make_double2(e.y * e.y - m.x * m.x, (d.dcoef[p] * e.x) * d.dchar[p]);
+    fft_forward2<M>(A, Bf, d.tw, N, C, X.c);
   }
-  fft_forward2<M>(A, Bf, d.tw, N, C, X.c);
   // breaking criterion (1d/breaking.c:36-95) on eta, u, H(eta): the transform's
   // barriers made PE / PM complete member-wide
   if (brk) breaking_scan(X, PE, &PM[0].y, 2);
@@ -167,14 +296,20 @@ __device__ __noinline__ void rhs_hs2_flat(Ctx<M>& X, double t, double2* __restri
     (void)p;
     A[pidx(idx)] = va[u];
   }
-  fft_inverse<M>(A, d.tw, N, C, X.c);
-  HW_FOREACH(X) {
-    const double2 v = A[pidx(idx)];
-    const double ch = d.chi[p];
-    A[pidx(idx)] = make_double2(v.x * ch, v.y * ch);
-    Bf[pidx(idx)] = make_double2(X.rs[idx], 0.0);
+  if (fused) {
+    fft_local<M>(A, d.tw, C, +1);
+    cross_adjust_any<M>(X, A, Bf);
+    fft_local2<M>(A, Bf, d.tw, C, -1);
+  } else {
+    fft_inverse<M>(A, d.tw, N, C, X.c);
+    HW_FOREACH(X) {
+      const double2 v = A[pidx(idx)];
+      const double ch = d.chi[p];
+      A[pidx(idx)] = make_double2(v.x * ch, v.y * ch);
+      Bf[pidx(idx)] = make_double2(X.rs[idx], 0.0);
+    }
+    fft_forward2<M>(A, Bf, d.tw, N, C, X.c);
   }
-  fft_forward2<M>(A, Bf, d.tw, N, C, X.c);
   double pv = 0.0, ps = 0.0;
   if (d.has_influx) {
     pv = spline_eval(d.tt, d.ins, d.insc, d.n_in, t);
