@@ -395,6 +395,9 @@ struct hw2d_ctx {
     }
     hw2d::OpAssemble as{};
     as.out = out;
+    as.rk = rk;
+    as.ctl = ctl;
+    as.mode = mode;
     as.dph = w.dph;
     as.z = w.z;
     as.src = src;

@@ -278,7 +278,10 @@ struct OpSource {   // the line source after its row transform (a set-up table):
   }
 };
 struct OpAssemble {   // dt Z of rhs_AB1/AB2/AB3_2DB_uv (the breaking force is added after)
-  double2* out;       // 3 fields
+  double2* out;       // 3 fields: the direct RHS's output (mode 0); the stepper's modes
+  RK2 rk;             // write the RK buffer rhs_out selects from the control block
+  const Ctl2* ctl;
+  int mode;
   double2* dph;       // delphiH^ kept for the breaking kernels (nullptr: off)
   const double2 *z, *src, *h1u, *h1v, *au, *av, *au3, *av3, *ikx, *iky, *ikx3, *iky3, *de, *du, *dv;
   const double *aal, *kx, *ky;
@@ -286,6 +289,7 @@ struct OpAssemble {   // dt Z of rhs_AB1/AB2/AB3_2DB_uv (the breaking force is a
   int model;
   size_t n;
   __device__ void operator()(size_t q, int i, int j) const {
+    double2* out = rhs_out(rk, ctl, mode, this->out);
     const double a = aal[q];
     const double2 S = src ? src[q] : make_double2(0.0, 0.0);
     const double2 ze = z[q];
