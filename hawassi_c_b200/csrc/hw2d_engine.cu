@@ -380,18 +380,20 @@ struct hw2d_ctx {
     g_fft(G(gP), 3, +1, s, cond);
     g_hss(G(gP + 1), G(gEH + 1), tb.cmin, tb.cmid, tb.cplus, G(gCU), s, cond);
     g_hss(G(gP + 2), G(gEH + 2), tb.cmin, tb.cmid, tb.cplus, G(gCV), s, cond);
-    g_map(hw2d::OpDampH1{G(gD), G(gD + 1), G(gD + 2), G(gH1), G(gH1 + 1), G(gP), G(gP + 1), G(gP + 2), G(gCU),
+    // the damping spectra and the source spectrum go where the breaking kernels read
+    // them when they rewrite dt eta^ (w.D, w.src)
+    g_map(hw2d::OpDampH1{w.D, w.D + n, w.D + 2 * n, G(gH1), G(gH1 + 1), G(gP), G(gP + 1), G(gP + 2), G(gCU),
                          G(gCV), tb.damp, tb.kx, tb.ky, N, g},
           s, cond);
-    g_fft(G(gD), 3, -1, s, cond);
+    g_fft(w.D, 3, -1, s, cond);
     const double2* src = nullptr;
     if (tb.has_src) {
       hw2d::k2g_signal<<<(ny + 127) / 128, 128, 0, s>>>(tb, w, ctl, mode, cond);
       ++gcount;
-      g_map(hw2d::OpSource{G(gSRC), tb.gx, tb.sx, w.insig, w.insigs, tb.fac_src}, s, cond);
-      gen_pass(ny, 1, G(gSRC), 1, nx, ny, tb.twy, -1, s, ctl, cond);   // its row transform is a set-up table
+      g_map(hw2d::OpSource{w.src, tb.gx, tb.sx, w.insig, w.insigs, tb.fac_src}, s, cond);
+      gen_pass(ny, 1, w.src, 1, nx, ny, tb.twy, -1, s, ctl, cond);   // its row transform is a set-up table
       ++gcount;
-      src = G(gSRC);
+      src = w.src;
     }
     hw2d::OpAssemble as{};
     as.out = out;
@@ -403,9 +405,9 @@ struct hw2d_ctx {
     as.src = src;
     as.h1u = G(gH1);
     as.h1v = G(gH1 + 1);
-    as.de = G(gD);
-    as.du = G(gD + 1);
-    as.dv = G(gD + 2);
+    as.de = w.D;
+    as.du = w.D + n;
+    as.dv = w.D + 2 * n;
     as.aal = tb.aal;
     as.kx = tb.kx;
     as.ky = tb.ky;
