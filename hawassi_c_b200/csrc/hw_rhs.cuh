@@ -88,20 +88,15 @@ struct Ctx {
   int c;          // rank of this CTA in the member's cluster
   int tid;
   const StageSrc* stg = nullptr;   // set: zs is to be formed from y and the k's first
-  double* rs = nullptr;            // M doubles of shared memory: one real field held across transforms
 };
 
-// dynamic shared memory of the 1D kernels of slice M: two padded FFT slices and one
-// real M-point field
-__host__ __device__ constexpr size_t slice_smem_bytes(int m) {
-  return 2 * size_t(padded(m)) * sizeof(double2) + size_t(m) * sizeof(double);
-}
+// dynamic shared memory of the 1D kernels of slice M: two padded FFT slices (no more:
+// what the SM does not give to shared memory serves as L1 cache)
+__host__ __device__ constexpr size_t slice_smem_bytes(int m) { return 2 * size_t(padded(m)) * sizeof(double2); }
 
 template <int M>
 __device__ __forceinline__ Ctx<M> make_ctx(const DevMember& d, double2* smem, double* red, int rank) {
-  Ctx<M> X{d, smem, smem + padded(M), red, rank, int(threadIdx.x)};
-  X.rs = reinterpret_cast<double*>(smem + 2 * padded(M));
-  return X;
+  return Ctx<M>{d, smem, smem + padded(M), red, rank, int(threadIdx.x)};
 }
 
 #define HW_FOREACH(X)                            \

@@ -62,13 +62,19 @@ __device__ __forceinline__ void assemble_flat(const DevMember& d, int p, double2
 //
 // First meeting (1d/functions.c:1486-1498): A = eta + i u, B = M0 u + i H(eta) in;
 // out A = (eta u) + i (eta M0 u), B = (u^2 - (M0 u)^2) + i (damping of eta); the
-// damping of u is kept in the thread's own part of X.rs for the second meeting;
+// damping of u waits in the member's scratch (damp_u_field) for the second meeting;
 // eta, u and H(eta) go to global memory for the breaking criterion.
+// the physical damping of u between the products and the adjustment, one double per
+// grid point in the member's scratch field 5 (used for the spectral damping of u only
+// after that); kept out of shared memory, which leaves the SM more L1 cache
+__device__ __forceinline__ double* damp_u_field(const DevMember& d) { return reinterpret_cast<double*>(d.sc[5]); }
+
 template <int M, int C>
 __device__ __forceinline__ void cross_products(Ctx<M>& X, double2* A, double2* B, bool brk, double2* PE, double2* PM) {
   constexpr int T = M / kPts;
   constexpr int PER = kPts / C;
   const DevMember& d = X.d;
+  double* du = damp_u_field(d);
   cg::cluster_group cl = cg::this_cluster();
   cl.sync();
 #pragma unroll
@@ -97,7 +103,7 @@ __device__ __forceinline__ void cross_products(Ctx<M>& X, double2* A, double2* B
         PM[n].y = m.y;
       }
       const double dc = d.dcoef[n], ch = d.dchar[n];
-      X.rs[X.tid * kPts + q * C + r] = (dc * e.y) * ch;
+      du[n] = (dc * e.y) * ch;
       va[r] = make_double2(e.x * e.y, e.x * m.x);
       vb[r] = make_double2(e.y * e.y - m.x * m.x, (dc * e.x) * ch);
     }
@@ -126,6 +132,7 @@ __device__ __forceinline__ void cross_adjust(Ctx<M>& X, double2* A, double2* B) 
   constexpr int T = M / kPts;
   constexpr int PER = kPts / C;
   const DevMember& d = X.d;
+  const double* du = damp_u_field(d);
   cg::cluster_group cl = cg::this_cluster();
   cl.sync();
 #pragma unroll
@@ -142,7 +149,7 @@ __device__ __forceinline__ void cross_adjust(Ctx<M>& X, double2* A, double2* B) 
     for (int r = 0; r < C; ++r) {
       const double ch = d.chi[r * M + i];
       va[r] = make_double2(va[r].x * ch, va[r].y * ch);
-      vb[r] = make_double2(X.rs[X.tid * kPts + q * C + r], 0.0);
+      vb[r] = make_double2(du[r * M + i], 0.0);
     }
     dft_small<C>(va, -1);
     dft_small<C>(vb, -1);
@@ -245,8 +252,9 @@ __device__ __noinline__ void rhs_hs2_flat(Ctx<M>& X, double t, double2* __restri
     Bf[pidx(idx)] = vb[u];
   }
   // (2) products in physical space (1d/functions.c:1486-1498); the damping of u
-  // waits in shared memory for the adjustment's transform
+  // waits in the member's scratch for the adjustment's transform
   const bool fused = C == 2 || C == 4 || C == 8;
+  double* du = damp_u_field(d);
   if (fused) {
     fft_local2<M>(A, Bf, d.tw, C, +1);
     cross_products_any<M>(X, A, Bf, brk, PE, PM);
@@ -259,7 +267,7 @@ __device__ __noinline__ void rhs_hs2_flat(Ctx<M>& X, double t, double2* __restri
         PE[p] = e;
         PM[p].y = m.y;
       }
-      X.rs[idx] = (d.dcoef[p] * e.y) * d.dchar[p];
+      du[p] = (d.dcoef[p] * e.y) * d.dchar[p];
       A[pidx(idx)] = make_double2(e.x * e.y, e.x * m.x);
       Bf[pidx(idx)] = make_double2(e.y * e.y - m.x * m.x, (d.dcoef[p] * e.x) * d.dchar[p]);
     }
@@ -306,7 +314,7 @@ __device__ __noinline__ void rhs_hs2_flat(Ctx<M>& X, double t, double2* __restri
       const double2 v = A[pidx(idx)];
       const double ch = d.chi[p];
       A[pidx(idx)] = make_double2(v.x * ch, v.y * ch);
-      Bf[pidx(idx)] = make_double2(X.rs[idx], 0.0);
+      Bf[pidx(idx)] = make_double2(du[p], 0.0);
     }
     fft_forward2<M>(A, Bf, d.tw, N, C, X.c);
   }
