@@ -169,13 +169,13 @@ __device__ __forceinline__ void cross_adjust(Ctx<M>& X, double2* A, double2* B) 
 }
 
 template <int M>
-__device__ __noinline__ void cross_products_any(Ctx<M>& X, double2* A, double2* B, bool brk, double2* PE, double2* PM) {
+__device__ __forceinline__ void cross_products_any(Ctx<M>& X, double2* A, double2* B, bool brk, double2* PE, double2* PM) {
   if (X.d.C == 2) cross_products<M, 2>(X, A, B, brk, PE, PM);
   else if (X.d.C == 4) cross_products<M, 4>(X, A, B, brk, PE, PM);
   else cross_products<M, 8>(X, A, B, brk, PE, PM);
 }
 template <int M>
-__device__ __noinline__ void cross_adjust_any(Ctx<M>& X, double2* A, double2* B) {
+__device__ __forceinline__ void cross_adjust_any(Ctx<M>& X, double2* A, double2* B) {
   if (X.d.C == 2) cross_adjust<M, 2>(X, A, B);
   else if (X.d.C == 4) cross_adjust<M, 4>(X, A, B);
   else cross_adjust<M, 8>(X, A, B);

@@ -94,7 +94,9 @@ struct StepState {
 
 template <int M>
 __device__ __forceinline__ void rhs_into(Ctx<M>& X, StepState& S, double t, double2* out) {
-  rhs_eval<M>(X, t, out);
+  // the flat HS2 RHS directly (one call level less on the ensemble's hot path)
+  if (X.d.model == 2 && X.d.flat) rhs_hs2_flat<M>(X, t, out);
+  else rhs_eval<M>(X, t, out);
   ++S.rhs;
 }
 

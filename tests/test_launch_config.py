@@ -9,8 +9,8 @@ SRC = os.path.join(ROOT, "hawassi_c_b200", "csrc", "hw2d_engine.cu")
 MAX_SMEM_PER_CTA = 227 * 1024   # sm_100 opt-in limit of dynamic shared memory per block
 
 
-def padded(m):   # hw_fft.cuh: a one-shift bank skew every 8 points plus one
-    return m + (m >> 3) + 1
+def padded(m):   # hw_fft.cuh: slices are swizzled in place, no pad slots
+    return m
 
 
 def test_every_pass_launches_with_its_attribute():
@@ -27,4 +27,4 @@ def test_largest_pass_fits_a_cta_at_1024_points():
     slices = max(int(v) for v in re.findall(r"smem_bytes<M>\((\d+)\)", s))
     assert slices * padded(1024) * 16 <= MAX_SMEM_PER_CTA
     src_fft = open(os.path.join(ROOT, "hawassi_c_b200", "csrc", "hw_fft.cuh")).read()
-    assert "return m + (m >> 3) + 1;" in src_fft   # the skew the bound above assumes
+    assert "constexpr int padded(int m) { return m; }" in src_fft   # the size the bound above assumes
