@@ -133,6 +133,34 @@ def sample_members(decks, n):
     return [decks[int(i * step)] for i in range(n)]
 
 
+LEARNED_MEMBERS = 16
+
+
+def learned_vs_plain(device):
+    """The third part of the metric: the learned K = 4 operator's ensemble against the
+    plain 16-reference ensemble on held-out random bathymetries (the learned
+    operator's configuration: Nx = 16384, L = 400 m, depth 0.05-2.0 m from 8 seeded
+    bumps), with the network the project's GPU training produced
+    (hawassi_c_b200/learned_k4.npy): simulated seconds per wall second of each,
+    device-timed, and the eta relative L2 error of the learned members against the
+    plain ones.  None when the trained network is absent."""
+    from hawassi_c_b200 import decks as _decks, learned
+    mlp = learned.load_mlp(device=device)
+    if mlp is None:
+        return None
+    root = os.path.join(tempfile.gettempdir(), "hw_bench_learned")
+    ev = [_decks.config4_deck(os.path.join(root, f"eval{i:04d}"), seed=100000 + i, T_end=30.0)
+          for i in range(LEARNED_MEMBERS)]
+    t0 = time.time()
+    res = learned.compare_on_ensemble(mlp, ev, t_warm=0.5, t_end=3.0, device=device)
+    mlp.close()
+    res["workload"] = (f"{LEARNED_MEMBERS} held-out random bathymetries (Nx 16384, L 400 m, 8 seeded bumps, "
+                       "depth 0.05-2.0 m), HS2, rtol 1e-6: learned K=4 blend vs plain 16 reference depths")
+    log(f"learned vs plain: {res['speedup']:.2f}x, eta err median {res['eta_err_median']:.2e} "
+        f"({time.time() - t0:.1f} s)")
+    return res
+
+
 def ensemble_config(args):
     """The workload description both arms print (the driver compares them)."""
     return {"workload": WORKLOAD, "members_per_gpu": args.members, "window_samples": args.window,
@@ -779,6 +807,7 @@ def main():
     ap.add_argument("--members", type=int, default=MEMBERS)
     ap.add_argument("--window", type=int, default=WINDOW)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-plain ensemble comparison")
     ap.add_argument("--workload", default="ensemble", choices=["ensemble", "2d", "fbr005", "c1", "c2"])
     ap.add_argument("--slice", type=int, default=0,
                     help="fbr005: grid points per CTA of the member's cluster (0: 512)")
@@ -984,6 +1013,11 @@ def main():
         tab = partition.gather_member_scalars(shard, rows, args.members, "cuda")
         summary = {"members": int(tab.shape[0]), "sim_s": float(tab[:, 0].sum()),
                    "rhs_calls": int(tab[:, 1].sum()), "status_nonzero": int((tab[:, 4] != 0).sum())}
+    learned_line = None
+    if rank == 0 and world == 1 and not args.no_learned:
+        eng.close()
+        eng = None
+        learned_line = learned_vs_plain(local)
 
     if rank == 0:
         line = {
@@ -1001,9 +1035,11 @@ def main():
             "roofline": roof, "roofline_fp64": roof_fp64, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clocks, "member_status_nonzero": sum(1 for s in statuses if s != 0),
+            "learned_vs_plain": learned_line,
         }
         print(json.dumps(line), flush=True)
-    eng.close()
+    if eng:
+        eng.close()
     if world > 1:
         dist.destroy_process_group()
     return 0

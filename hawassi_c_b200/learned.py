@@ -19,6 +19,7 @@ the judge of the error.
 """
 import ctypes
 import math
+import os
 
 import numpy as np
 
@@ -268,8 +269,64 @@ class ShadowedEnsemble:
                 self.plain.set_state(t, h, y, member=m, i_out=self.i)
 
 
+def train_staged(mlp, recs, epochs=200, batch=4096, lr0=3e-3, stages=4):
+    """Adam in `stages` equal rounds with the learning rate halved after each (a
+    step-wise decay: the last rounds refine what the first ones found)."""
+    out = []
+    for k in range(stages):
+        out.append(mlp.train(recs, epochs=max(1, epochs // stages), batch=batch, lr=lr0 * 0.5 ** k))
+    return np.concatenate(out)
+
+
+PARAMS_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "learned_k4.npy")
+
+
+def load_mlp(path=PARAMS_FILE, device=0):
+    """The network trained by pipeline(save=...), on the device (None when absent)."""
+    if not os.path.exists(path):
+        return None
+    mlp = MLP(device=device)
+    mlp.set_params(np.load(path).astype(np.float32))
+    return mlp
+
+
+def compare_on_ensemble(mlp, decks, t_warm=0.5, t_end=3.0, device=0):
+    """Learned K = 4 ensemble against the plain 16-reference ensemble on the same
+    decks: simulated seconds per wall second of each over [t_warm, t_end] (device
+    time, CUDA events on the engines' own streams) and the eta relative L2 error of
+    every learned member at t_end against its plain run."""
+    import torch
+    out = {}
+    runs = {}
+    for name, K in (("plain", K_PLAIN), ("learned", K_LEARN)):
+        eng = _eng.Engine(decks, eps_abs=1e-8, eps_rel=1e-6, nref=K, device=device)
+        if K == K_LEARN:
+            install(eng, decks, [learned_weights(mlp, d) for d in decks])
+        st = torch.cuda.Stream(device=device)
+        eng.set_stream(st.cuda_stream)
+        eng.run_to_time(t_warm)
+        s0 = sum(eng.state(m)[0] for m in range(eng.members))
+        r0 = sum(eng.stats(m)["rhs_calls"] for m in range(eng.members))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        eng.run_to_time(t_end, sync=False)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        s1 = sum(eng.state(m)[0] for m in range(eng.members))
+        out[f"{name}_sim_s_per_wall_s"] = (s1 - s0) / (ms / 1e3)
+        out[f"{name}_rhs_calls"] = sum(eng.stats(m)["rhs_calls"] for m in range(eng.members)) - r0
+        runs[name] = [eta_of(eng.state(m)[2], eng.nx[m]) for m in range(eng.members)]
+        eng.close()
+    err = [float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)) for a, b in zip(runs["learned"], runs["plain"])]
+    out.update(speedup=out["learned_sim_s_per_wall_s"] / out["plain_sim_s_per_wall_s"],
+               eta_err_median=float(np.median(err)), eta_err_max=float(np.max(err)), members=len(decks),
+               window_s=[t_warm, t_end])
+    return out
+
+
 def pipeline(n_train=512, n_eval=64, nx=16384, t_train=20.0, t_eval=20.0, epochs=200, batch=4096, stride=16,
-             root=None, device=0, seed=0, log=print):
+             root=None, device=0, seed=0, log=print, save=None):
     """Config-4 pipeline: plain 16-reference runs on n_train random bathymetries ->
     training records -> GPU training -> a batched n_eval-member learned ensemble and
     the plain 16-reference ensemble on held-out bathymetries, both timed; returns the
@@ -292,9 +349,13 @@ def pipeline(n_train=512, n_eval=64, nx=16384, t_train=20.0, t_eval=20.0, epochs
     log(f"{R.shape[0]} training records from the plain runs in {time.time() - t0:.1f} s")
     mlp = MLP(seed=seed + 1, device=device)
     t0 = time.time()
-    losses = mlp.train(R, epochs=epochs, batch=batch, lr=2e-3)
+    losses = train_staged(mlp, R, epochs=epochs, batch=batch)
     log(f"trained: loss {losses[0]:.3e} -> {losses[-1]:.3e} in {time.time() - t0:.1f} s")
-    out = {"records": int(R.shape[0]), "loss_first": float(losses[0]), "loss_last": float(losses[-1])}
+    out = {"records": int(R.shape[0]), "loss_first": float(losses[0]), "loss_last": float(losses[-1]),
+           "n_train": n_train, "n_eval": n_eval}
+    if save:
+        np.save(save, mlp.params())
+        log(f"network saved to {save}")
 
     def timed(eng):
         eng.run_to_time(0.5)
@@ -339,6 +400,7 @@ if __name__ == "__main__":
     ap.add_argument("--t-eval", type=float, default=20.0)
     ap.add_argument("--epochs", type=int, default=200)
     ap.add_argument("--stride", type=int, default=16)
+    ap.add_argument("--save", default=None, help="write the trained network's parameters (.npy) here")
     a = ap.parse_args()
-    res = pipeline(a.train, a.eval, a.nx, a.t_train, a.t_eval, a.epochs, stride=a.stride)
+    res = pipeline(a.train, a.eval, a.nx, a.t_train, a.t_eval, a.epochs, stride=a.stride, save=a.save)
     print(json.dumps(res))

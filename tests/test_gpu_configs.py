@@ -60,7 +60,7 @@ def _oracle_to(deck, t_stop, eps_abs=0.0, eps_rel=0.0):
     return o, t, h, y
 
 
-def _same_steps(st, ostats, exact=True):
+def _same_steps(st, ostats, exact=True, breaking=False):
     """Accepted and rejected steps: identical (exact), or within the spread that a
     different rounding of the same arithmetic produces over a long run.  Over
     thousands of steps one step-control decision sits within rounding of its
@@ -75,9 +75,14 @@ def _same_steps(st, ostats, exact=True):
     rhs, acc, rej = ostats
     if exact:
         assert (st["accepted"], st["rejected"]) == (acc, rej)
-    else:
+    elif not breaking:
         assert abs(st["accepted"] - acc) <= max(5, 0.002 * acc)
         assert abs(st["rejected"] - rej) <= max(10, 0.05 * rej)
+    else:
+        # after a breaking onset the steps follow the discontinuous node-by-node decisions:
+        # the two oracle builds are 8 accepted / 10 rejected steps apart at seed 66's onset
+        assert abs(st["accepted"] - acc) <= max(20, 0.01 * acc)
+        assert abs(st["rejected"] - rej) <= max(30, 0.15 * rej)
     return rhs
 
 
@@ -193,7 +198,7 @@ def test_ensemble_members_vs_standalone_oracle(tmp_path):
         st = e.stats(m)
         assert st["status"] == 0
         assert tg == pytest.approx(t, rel=1e-13), m
-        _same_steps(st, stats, exact=False)
+        _same_steps(st, stats, exact=False, breaking=m in breaking)
         (eo, uo), (eg, ug) = _physical(y), _physical(yg)
         if m in breaking:
             e_o, e_g = e.energy(y, member=m), e.energy(member=m)
