@@ -651,7 +651,7 @@ def main_fbr(args, rank, world, local):
             "accepted": s1["accepted"] - s0["accepted"], "rejected": s1["rejected"] - s0["rejected"],
             "published_sim_s_per_wall_s": FBR_PUBLISHED_SIM_PER_WALL,
             "roofline": None, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-            "gpu_launches": args.steps * (len(eng.class_timing()) + 1),   # per step: k_resume + k_evolve
+            "gpu_launches": args.steps * (2 * len(eng.class_timing()) + 1),   # per step: k_resume, k_order_class, k_evolve
         }
         print(json.dumps(line), flush=True)
     eng.close()
@@ -789,7 +789,7 @@ def main_c2(args, rank, world, local):
             "sim_s_per_wall_s": sim / (ms / 1e3), "rhs_calls": s1["rhs_calls"] - s0["rhs_calls"],
             "accepted": s1["accepted"] - s0["accepted"], "rejected": s1["rejected"] - s0["rejected"],
             "roofline": None, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-            "gpu_launches": args.steps * (len(eng.class_timing()) + 1),
+            "gpu_launches": args.steps * (2 * len(eng.class_timing()) + 1),
         }
         print(json.dumps(line), flush=True)
     eng.close()
@@ -935,7 +935,7 @@ def main():
     ms = ev0.elapsed_time(ev1)
     log(f"timed {args.steps} steps: {ms:.1f} ms")
     pts1, sim1 = rhs_pts(), sim_time()
-    launches = args.steps * (len(eng.class_timing()) + 1)   # per step: k_resume + one k_evolve per class
+    launches = args.steps * (2 * len(eng.class_timing()) + 1)   # per step: k_resume + per class k_order_class and k_evolve
     if world > 1:
         (ms,), (tot_pts, tot_sim) = reduce_ranks([ms], [float(pts1 - pts0), sim1 - sim0], "cuda")
     else:

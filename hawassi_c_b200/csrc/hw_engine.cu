@@ -27,10 +27,36 @@ namespace {
 // ---------------------------------------------------------------------------
 // kernels
 // ---------------------------------------------------------------------------
-// clear the budget status so that a bounded launch can continue where it stopped
-__global__ void k_resume(DevMember* mems, int n) {
+// clear the budget status so that a bounded launch can continue where it stopped, and
+// set every member's stop index for the coming launch
+__global__ void k_resume(DevMember* mems, int n, const int* __restrict__ stops) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n && mems[i].status == kBudget) mems[i].status = kOk;
+  if (i >= n) return;
+  if (mems[i].status == kBudget) mems[i].status = kOk;
+  mems[i].i_stop = stops[i];
+}
+
+// Longest-first order of a class's members for its next launch: the CTAs of a launch
+// start roughly in block order, so the members that took the most RHS evaluations in
+// the previous launch start first and the launch's tail is shorter.  The members are
+// independent: their order changes no result.  One block; ties keep member order.
+__global__ void k_order_class(const DevMember* __restrict__ mems, int* list, int n, long long* prev) {
+  extern __shared__ long long key[];
+  int* id = reinterpret_cast<int*>(key + n);
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    const int m = list[j];
+    id[j] = m;
+    key[j] = mems[m].rhs_calls - prev[m];
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    const long long kj = key[j];
+    const int mj = id[j];
+    int r = 0;
+    for (int k = 0; k < n; ++k) r += (key[k] > kj) || (key[k] == kj && id[k] < mj);
+    list[r] = mj;
+    prev[mj] = mems[mj].rhs_calls;
+  }
 }
 
 // reference layout (4N doubles) -> internal (2N double2, spectral permuted)
@@ -142,6 +168,8 @@ struct hw_ctx {
   cudaStream_t stream = nullptr;
   cudaEvent_t fork = nullptr;
   int* d_single = nullptr;    // one-member list for single-member launches
+  int* d_stops = nullptr;     // stop index of every member for the next launch
+  long long* d_prev_rhs = nullptr;   // each member's RHS count when its class was last ordered
   double* d_ref = nullptr;    // 4*maxN staging for reference-layout transfers
   int maxN = 0;
   double* d_stage = nullptr;  // all members' states, reference layout, concatenated
@@ -438,6 +466,9 @@ bool hw_ctx::init(const std::vector<std::string>& dirs, const hw_opts* o, const 
   for (size_t i = 0; i < mem.size(); ++i)
     HW_CUDA(cudaMemcpy(d_mems + i, &mem[i].d, sizeof(DevMember), cudaMemcpyHostToDevice));
   HW_CUDA(cudaMalloc(&d_single, sizeof(int) * mem.size()));
+  HW_CUDA(cudaMalloc(&d_stops, sizeof(int) * mem.size()));
+  HW_CUDA(cudaMalloc(&d_prev_rhs, sizeof(long long) * mem.size()));
+  HW_CUDA(cudaMemset(d_prev_rhs, 0, sizeof(long long) * mem.size()));
   std::vector<int> ids(mem.size());
   for (size_t i = 0; i < mem.size(); ++i) ids[i] = int(i);
   HW_CUDA(cudaMemcpy(d_single, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice));
@@ -475,7 +506,8 @@ bool hw_ctx::launch_member(int mi, int mode, double t_rhs) {
 }
 
 bool hw_ctx::run(int i_stop_all, double t_end, bool by_time, const int* per_member) {
-  // set stop indices on the device descriptors
+  // stop indices of the members, set on the device descriptors with one copy
+  std::vector<int> stops(mem.size());
   for (size_t i = 0; i < mem.size(); ++i) {
     const hw::Member& m = mem[i].m;
     int stop = m.n;
@@ -487,15 +519,21 @@ bool hw_ctx::run(int i_stop_all, double t_end, bool by_time, const int* per_memb
     } else if (i_stop_all >= 0) {
       stop = std::min(i_stop_all, m.n);
     }
-    HW_CUDA(cudaMemcpyAsync(&d_mems[i].i_stop, &stop, sizeof(int), cudaMemcpyHostToDevice, stream));
+    stops[i] = stop;
   }
+  // (from pageable memory: the runtime stages the vector before the call returns)
+  HW_CUDA(cudaMemcpyAsync(d_stops, stops.data(), sizeof(int) * stops.size(), cudaMemcpyHostToDevice, stream));
   // a member stopped by the per-launch RHS budget resumes here
-  k_resume<<<(unsigned(mem.size()) + 127) / 128, 128, 0, stream>>>(d_mems, int(mem.size()));
+  k_resume<<<(unsigned(mem.size()) + 127) / 128, 128, 0, stream>>>(d_mems, int(mem.size()), d_stops);
   HW_CUDA(cudaGetLastError());
   HW_CUDA(cudaEventRecord(fork, stream));
   for (auto& c : classes) {
     HW_CUDA(cudaStreamWaitEvent(c.stream, fork, 0));
     HW_CUDA(cudaEventRecord(c.t_start, c.stream));
+    const int nm = int(c.members.size());
+    k_order_class<<<1, 256, size_t(nm) * (sizeof(long long) + sizeof(int)), c.stream>>>(d_mems, c.d_list, nm,
+                                                                                      d_prev_rhs);
+    HW_CUDA(cudaGetLastError());
     cudaError_t e = launch_any(c.M, 0, d_mems, c.d_list, int(c.members.size()), c.C, 0.0, c.stream);
     if (e != cudaSuccess) { err = std::string("launch: ") + cudaGetErrorString(e); return false; }
     HW_CUDA(cudaEventRecord(c.t_stop, c.stream));
@@ -563,6 +601,8 @@ hw_ctx::~hw_ctx() {
   }
   if (d_mems) cudaFree(d_mems);
   if (d_single) cudaFree(d_single);
+  if (d_stops) cudaFree(d_stops);
+  if (d_prev_rhs) cudaFree(d_prev_rhs);
   if (d_ref) cudaFree(d_ref);
   if (fork) cudaEventDestroy(fork);
   if (own_stream) cudaStreamDestroy(own_stream);
