@@ -235,7 +235,10 @@ def test_config2_k3_breaking_onset(tmp_path, golden_dir):
     e_on = float(fx["onset_energy"])
     assert abs(e.energy() - e_on) / e_on < 1e-6
     # and on through the next samples of the breaking event, where the node-by-node
-    # breaking decisions follow the rounding of the step sequence
+    # breaking decisions follow the rounding of the step sequence: the oracle built
+    # with fused multiply-adds reaches the same onset sample and nodes (record time
+    # 72.985052 against 72.985341, onset energy 9.1e-8 apart) and ends these 10
+    # samples with an energy 7.3e-5 from the fixture's
     e.run(i_stop=i_end + 1)
     assert e.stats()["status"] == 0
     e_end = float(fx["end_energy"])
