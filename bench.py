@@ -161,6 +161,29 @@ def learned_vs_plain(device):
     return res
 
 
+def learned_vs_plain_2d(device):
+    """The 2D configuration's two paths side by side: its deck (1024 x 1024 on 300 m x
+    300 m, shoal bottom 0.5-5 m, harbour wall, HS2 with breaking, directional line
+    source) with the plain 16-reference operator and with the learned 4-reference
+    blend (the same trained network, 2D depth features): device-timed simulated
+    seconds per wall second of each over 0.25-0.75 s from the same sea state over the
+    whole domain, and the learned run's eta error against the plain one.  None when
+    the trained network is absent."""
+    from hawassi_c_b200 import decks2d, learned
+    mlp = learned.load_mlp(device=device)
+    if mlp is None:
+        return None
+    t0 = time.time()
+    res = learned.compare_2d(mlp, decks2d.config5(seed=0), t_warm=0.25, t_end=0.75, device=device,
+                             eps_abs=EPS_ABS, eps_rel=EPS_REL)
+    mlp.close()
+    res["workload"] = ("2D configuration deck (1024x1024, 300 m x 300 m, shoal 0.5-5 m, wall refl 0.5, HS2 + breaking, "
+                       "rtol 1e-6): learned K=4 blend vs plain 16 reference depths, general 2D path for both")
+    log(f"2D learned vs plain: {res['speedup']:.2f}x, eta err {res['eta_err']:.2e} "
+        f"(uniform weights {res['eta_err_uniform_weights']:.2e}) ({time.time() - t0:.1f} s)")
+    return res
+
+
 def ensemble_config(args):
     """The workload description both arms print (the driver compares them)."""
     return {"workload": WORKLOAD, "members_per_gpu": args.members, "window_samples": args.window,
@@ -1013,11 +1036,12 @@ def main():
         tab = partition.gather_member_scalars(shard, rows, args.members, "cuda")
         summary = {"members": int(tab.shape[0]), "sim_s": float(tab[:, 0].sum()),
                    "rhs_calls": int(tab[:, 1].sum()), "status_nonzero": int((tab[:, 4] != 0).sum())}
-    learned_line = None
+    learned_line = learned_line_2d = None
     if rank == 0 and world == 1 and not args.no_learned:
         eng.close()
         eng = None
         learned_line = learned_vs_plain(local)
+        learned_line_2d = learned_vs_plain_2d(local)
 
     if rank == 0:
         line = {
@@ -1036,6 +1060,7 @@ def main():
             "gpu_launches": launches,
             "clocks": clocks, "member_status_nonzero": sum(1 for s in statuses if s != 0),
             "learned_vs_plain": learned_line,
+            "learned_vs_plain_2d": learned_line_2d,
         }
         print(json.dumps(line), flush=True)
     if eng:

@@ -79,6 +79,12 @@ struct Tab2 {
   const double* gmid;
   const double* cmid;
   const double* omid;
+  // K reference depths (the plain K-reference and the learned operators): [K][N] weights,
+  // C^2 and Omega^2 of each depth; nk = 0 when the min / plus (/ mid) tables serve
+  int nk;
+  const double* gk;
+  const double* ck;
+  const double* ok;
 };
 
 struct Work2 {

@@ -336,15 +336,31 @@ struct hw2d_ctx {
   // HSSgen_2depth / HSSgen_3depth (2d/fun_odesolver.c:500-697): res from phi (the
   // unnormalised physical field, real part used) and its spectrum phihat, with the
   // spectral tables O of the reference depths (min, [mid,] plus)
+  // With K reference depths (tb.nk > 0) the same sum runs over the K depths' tables
+  // (O = the C^2 or the Omega^2 rows of ck / ok, as omega selects), in the same order.
+  int hss_base = gHSS;      // first pool slot of the operator's 3K scratch fields
   void g_hss(const double2* phi, const double2* phihat, const double* omin, const double* omid, const double* oplus,
-             double2* res, cudaStream_t s, int cond) {
-    const int K = tb.gmid ? 3 : 2;
-    const double* O[3] = {omin, tb.gmid ? omid : oplus, oplus};
-    const double* Gm[3] = {tb.gmin, tb.gmid ? tb.gmid : tb.gplus, tb.gplus};
+             double2* res, cudaStream_t s, int cond, bool omega = false) {
+    const int K = tb.nk ? tb.nk : (tb.gmid ? 3 : 2);
+    const double* O[hw2d::kMaxRef2];
+    const double* Gm[hw2d::kMaxRef2];
+    if (tb.nk) {
+      for (int d = 0; d < K; ++d) {
+        O[d] = (omega ? tb.ok : tb.ck) + (size_t)d * n;
+        Gm[d] = tb.gk + (size_t)d * n;
+      }
+    } else {
+      O[0] = omin;
+      O[1] = tb.gmid ? omid : oplus;
+      O[2] = oplus;
+      Gm[0] = tb.gmin;
+      Gm[1] = tb.gmid ? tb.gmid : tb.gplus;
+      Gm[2] = tb.gplus;
+    }
     const double N = double(nx) * double(ny);
-    double2* L0 = G(gHSS);
-    double2* g = G(gHSS + K);
-    double2* gl = G(gHSS + 2 * K);
+    double2* L0 = G(hss_base);
+    double2* g = G(hss_base + K);
+    double2* gl = G(hss_base + 2 * K);
     for (int d = 0; d < K; ++d) g_map(hw2d::OpScaleTable{L0 + d * n, phihat, O[d]}, s, cond);
     g_sym(L0, K, s, cond);
     g_fft(L0, K, +1, s, cond);
@@ -353,7 +369,14 @@ struct hw2d_ctx {
       g_map(hw2d::OpGam{gl + d * n, L0 + d * n, Gm[d], N}, s, cond);
     }
     g_fft(g, 2 * K, -1, s, cond);
-    hw2d::OpHssSum sum{res, {g, g + n, g + 2 * n}, {gl, gl + n, gl + 2 * n}, {O[0], O[1], O[2]}, K};
+    hw2d::OpHssSum sum{};
+    sum.res = res;
+    for (int d = 0; d < K; ++d) {
+      sum.g[d] = g + (size_t)d * n;
+      sum.gl[d] = gl + (size_t)d * n;
+      sum.o[d] = O[d];
+    }
+    sum.K = K;
     g_map(sum, s, cond);
   }
   // fun_adjust (2d/fun_odesolver.c:810-884) of nf consecutive fields A into AChi:
@@ -426,8 +449,8 @@ struct hw2d_ctx {
       g_fft(G(gEV), 4, -1, s, cond);   // eta v, deletaH2, (eta M0u)^, (eta M0v)^
       g_map(hw2d::OpScaleRe{G(gEM0U), N}, s, cond);
       g_map(hw2d::OpScaleRe{G(gEM0V), N}, s, cond);
-      g_hss(G(gEM0U), G(gEM0UH), tb.omin, tb.omid, tb.oplus, G(gLU), s, cond);
-      g_hss(G(gEM0V), G(gEM0VH), tb.omin, tb.omid, tb.oplus, G(gLV), s, cond);
+      g_hss(G(gEM0U), G(gEM0UH), tb.omin, tb.omid, tb.oplus, G(gLU), s, cond, true);
+      g_hss(G(gEM0V), G(gEM0VH), tb.omin, tb.omid, tb.oplus, G(gLV), s, cond, true);
       // adjust inputs: ikx, iky, delu, delv
       g_map(hw2d::OpDelH2{G(gADJIN), G(gADJIN + 1), G(gADJIN + 2), G(gADJIN + 3), G(gDH2), G(gEU), G(gEV), G(gLU),
                           G(gLV), tb.kx, tb.ky, g},
@@ -466,7 +489,8 @@ struct hw2d_ctx {
       g_map(pr, s, cond);
       g_fft(G(gPH), 5, -1, s, cond);        // the four products' spectra and deletaH3^
       for (int k = 0; k < 4; ++k) g_map(hw2d::OpScaleRe{G(gPK + k), N}, s, cond);
-      for (int k = 0; k < 4; ++k) g_hss(G(gPK + k), G(gPH + k), tb.omin, tb.omid, tb.oplus, G(gLP + k), s, cond);
+      for (int k = 0; k < 4; ++k)
+        g_hss(G(gPK + k), G(gPH + k), tb.omin, tb.omid, tb.oplus, G(gLP + k), s, cond, true);
       g_map(hw2d::OpDelH3{G(gADJ3IN), G(gADJ3IN + 1), G(gADJ3IN + 2), G(gADJ3IN + 3), G(gDH3), G(gLP), G(gLP + 1),
                           G(gLP + 2), G(gLP + 3), G(gE2U), G(gE2V), tb.kx, tb.ky, g},
             s, cond);
@@ -680,6 +704,15 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
     g_err2d = "hw2d_create: three reference depths need all of gam, csq, om2 for the min, mid and plus depths";
     return nullptr;
   }
+  const bool kref = t->nrefk != 0;
+  if (kref && (t->nrefk < 2 || t->nrefk > hw2d::kMaxRef2 || !t->gam_k || !t->csq_k || !t->om2_k)) {
+    g_err2d = "hw2d_create: K reference depths need 2 <= nrefk <= 16 and gam_k, csq_k, om2_k";
+    return nullptr;
+  }
+  if (kref && (var_tables || t->gam_mid)) {
+    g_err2d = "hw2d_create: give either the min/plus(/mid) tables or the K-reference tables, not both";
+    return nullptr;
+  }
   if (t->model == 1 && t->breaking) {
     // rhs_AB1_2DF_uv / rhs_AB1_2DB_uv never call breaking_process: under HS1 a breaking
     // deck is the plain HS1 run, so the tables must say breaking = 0
@@ -770,9 +803,16 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
     c->h_first = 1e-3;
   }
   if (o && o->h0 > 0) c->h_first = o->h0;
-  const bool var = t->gam_min && t->gam_plus && t->csq_min && t->csq_plus && t->om2_min && t->om2_plus;
+  const bool var = kref || (t->gam_min && t->gam_plus && t->csq_min && t->csq_plus && t->om2_min && t->om2_plus);
   tb.var = var ? 1 : 0;
-  if (var) {
+  if (kref) {   // K reference depths: the general path with the K-depth sum
+    const size_t kn = (size_t)t->nrefk * n;
+    tb.nk = t->nrefk;
+    tb.gk = c->upload(std::vector<double>(t->gam_k, t->gam_k + kn));
+    tb.ck = c->upload(std::vector<double>(t->csq_k, t->csq_k + kn));
+    tb.ok = c->upload(std::vector<double>(t->om2_k, t->om2_k + kn));
+    c->gen = 1;
+  } else if (var) {
     tb.gmin = c->upload(std::vector<double>(t->gam_min, t->gam_min + n));
     tb.gplus = c->upload(std::vector<double>(t->gam_plus, t->gam_plus + n));
     tb.cmin = c->upload(std::vector<double>(t->csq_min, t->csq_min + n));
@@ -892,7 +932,11 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
     w.EU = c->dalloc<double2>(3 * n);
   }
   if (c->gen) {
-    const int slots = t->model == 3 ? hw2d_ctx::gSlotsHS3 : hw2d_ctx::gSlotsHS2;
+    int slots = t->model == 3 ? hw2d_ctx::gSlotsHS3 : hw2d_ctx::gSlotsHS2;
+    if (kref && t->nrefk > 3) {   // the operator's 3K scratch fields after the model's own
+      c->hss_base = slots;
+      slots += 3 * t->nrefk;
+    }
     c->gpool = c->dalloc<double2>((size_t)slots * n);
   }
   w.D = c->dalloc<double2>(3 * n);
@@ -913,8 +957,10 @@ hw2d_ctx* hw2d_create(const hw2d_tables* t, const hw_opts* o) {
             w.Q && w.D && w.V && w.insig && w.insigs && w.part && c->dref && c->dout && c->ctl &&
             (chi_one || w.W) && (!has_src || (tb.gx && tb.sx && tb.sig && w.src)) && (!bk.on || (w.dph && w.phys)) &&
             (var || !t->wallchar || (w.WP && w.H1 && tb.c2d && (!tb.refl_one || (tb.gwx && tb.gwy)))) &&
-            (!var || (tb.gmin && tb.gplus && tb.cmin && tb.cplus && tb.omin && tb.oplus && w.phys && w.pe && w.H1 &&
-                      w.EU)) && (!t->wallchar || tb.wallchar) && (t->model != 3 || (w.p3 && w.T3)) &&
+            (!var || ((kref ? (tb.gk && tb.ck && tb.ok) : (tb.gmin && tb.gplus && tb.cmin && tb.cplus && tb.omin &&
+                                                             tb.oplus)) &&
+                      w.phys && w.pe && w.H1 && w.EU)) &&
+            (!t->wallchar || tb.wallchar) && (t->model != 3 || (w.p3 && w.T3)) &&
             (!c->gen || (c->gpool && (!t->gam_mid || (tb.gmid && tb.cmid && tb.omid))));
   for (int i = 0; i < 2; ++i) ok = ok && rk.y[i] && rk.kk[i];
   for (int i = 0; i < 5; ++i) ok = ok && rk.ks[i];

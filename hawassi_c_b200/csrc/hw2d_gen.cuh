@@ -122,11 +122,12 @@ struct OpGam {   // dst = gam re(src) / N (imaginary part 0): HSSgen's gam_j phi
   double N;
   __device__ void operator()(size_t q, int, int) const { dst[q] = make_double2(gam[q] * src[q].x / N, 0.0); }
 };
+constexpr int kMaxRef2 = 16;   // reference depths of the K-reference operator
 struct OpHssSum {   // result = (sum_j gL_j + O_j g_j) / 2 in the reference's order
   double2* res;
-  const double2* g[3];
-  const double2* gl[3];
-  const double* o[3];
+  const double2* g[kMaxRef2];
+  const double2* gl[kMaxRef2];
+  const double* o[kMaxRef2];
   int K;
   __device__ void operator()(size_t q, int, int) const {
     double re = gl[0][q].x + o[0][q] * g[0][q].x, im = gl[0][q].y + o[0][q] * g[0][q].y;

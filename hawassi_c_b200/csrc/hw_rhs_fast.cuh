@@ -231,7 +231,10 @@ __device__ __noinline__ void rhs_hs2_flat(Ctx<M>& X, double t, double2* __restri
       const double2 ep = stage_val(*X.stg, pp), wp = stage_val(*X.stg, N + pp);
       zw[p] = e;
       zw[N + p] = w;
-      packed(p, pp, e, ep, w, wp, va[u], vb[u]);
+      double2 a, b;
+      packed(p, pp, e, ep, w, wp, a, b);
+      A[pidx(idx)] = a;
+      Bf[pidx(idx)] = b;
     }
   } else {
     // zs written by the caller: the partner values come through the slices
@@ -245,11 +248,11 @@ __device__ __noinline__ void rhs_hs2_flat(Ctx<M>& X, double t, double2* __restri
       packed(p, pp, A[pidx(idx)], Ap[pidx(jp)], Bf[pidx(idx)], Bp[pidx(jp)], va[u], vb[u]);
     }
     member_sync(C);
-  }
-  HW_FOREACH(X) {
-    (void)p;
-    A[pidx(idx)] = va[u];
-    Bf[pidx(idx)] = vb[u];
+    HW_FOREACH(X) {
+      (void)p;
+      A[pidx(idx)] = va[u];
+      Bf[pidx(idx)] = vb[u];
+    }
   }
   // (2) products in physical space (1d/functions.c:1486-1498); the damping of u
   // waits in the member's scratch for the adjustment's transform

@@ -369,6 +369,79 @@ def three_depth_operator(depth, kx, ky, omega_p, d_mid=None, U=0.0, mdir=0.0):
     return out
 
 
+def kappa_of_omega(omega, depth):
+    """Wavenumber of frequency omega at each depth (Newton on omega^2 = g k tanh(k d),
+    vectorised, to rounding)."""
+    d = np.asarray(depth, dtype=np.float64)
+    k = omega / np.sqrt(GRAV * d)
+    for _ in range(60):
+        t = np.tanh(k * d)
+        k = k - (GRAV * k * t - omega ** 2) / (GRAV * t + GRAV * k * d * (1 - t * t))
+    return k
+
+
+def log_reference_depths(depth, K):
+    """K log-spaced reference depths over [min h, max h]."""
+    dmin, dmax = float(np.min(depth)), float(np.max(depth))
+    D = dmin * (dmax / dmin) ** (np.arange(K) / (K - 1))
+    D[0], D[-1] = dmin, dmax
+    return D
+
+
+def k_reference_weights(depth, omega_p, D):
+    """Per-point weights [K][...] of the K-reference operator (no counterpart in the
+    reference): each point on its bracketing pair [D_j, D_j+1] with the two-depth
+    weights of funOprt_DispInterpolation_2p (2d/functions.c:1534-1626) -- the blend of
+    the pair's phase speeds and squared frequencies exact at the point's own depth
+    for the wavenumber of the peak frequency there -- evaluated at the point itself
+    instead of through a spline over 101 depth samples.  Weights of the other depths
+    are zero."""
+    h = np.asarray(depth, dtype=np.float64)
+    K = len(D)
+    j = np.clip(np.searchsorted(D, h, side="right") - 1, 0, K - 2)
+    kap = kappa_of_omega(omega_p, h)
+
+    def cp1(k, d):
+        return np.sqrt(GRAV * np.tanh(k * d) / k)
+
+    def om2(k, d):
+        return GRAV * k * np.tanh(k * d)
+
+    Da, Db = np.asarray(D)[j], np.asarray(D)[j + 1]
+    cD, cm, cp = cp1(kap, h), cp1(kap, Da), cp1(kap, Db)
+    oD, om_, op_ = om2(kap, h), om2(kap, Da), om2(kap, Db)
+    det = cm * op_ - cp * om_
+    w = np.zeros((K,) + h.shape)
+    ia = np.indices(h.shape)
+    w[(j,) + tuple(ia)] = (op_ * cD - cp * oD) / det
+    w[(j + 1,) + tuple(ia)] = (-om_ * cD + cm * oD) / det
+    return w
+
+
+def with_k_operator(tb, D, gam):
+    """A copy of a varying-bottom tables dict whose operator is the K-reference one:
+    reference depths D (K), per-point weights gam [K][ny][nx]; the spectral tables are
+    C^2 and Omega^2 of each depth, as for the two-depth operator.  The min/plus/mid
+    tables are dropped (hw2d_tables takes one form or the other)."""
+    out = {k: v for k, v in tb.items() if not (k.startswith(("gam_", "csq_", "om2_")))}
+    KX, KY = np.meshgrid(tb["kx"], tb["ky"])
+    K = len(D)
+    out["nrefk"] = K
+    out["gam_k"] = np.ascontiguousarray(np.asarray(gam, dtype=np.float64).reshape(K, -1))
+    out["csq_k"] = np.ascontiguousarray(np.stack([(exact_cp(KX, KY, d) ** 2).ravel() for d in D]))
+    out["om2_k"] = np.ascontiguousarray(np.stack([(exact_disp(KX, KY, d) ** 2).ravel() for d in D]))
+    out["ref_depths"] = np.asarray(D, dtype=np.float64)
+    return out
+
+
+def plain_k_operator(tb, K=16):
+    """The plain K-reference operator of a varying-bottom tables dict (log-spaced
+    depths over the bottom's range, weights from k_reference_weights)."""
+    depth = tb["depth"]
+    D = log_reference_depths(depth, K)
+    return with_k_operator(tb, D, k_reference_weights(depth, tb["wp"], D))
+
+
 def shoal_bathymetry(x, y, deep=5.0, shallow=0.5, x1=100.0, x2=285.0, seed=0):
     """Depth 0.5-5 m: deep up to x1, a linear slope to `shallow` at x2, and a seeded
     Gaussian shoal on the slope; clipped to [shallow, deep]."""

@@ -31,6 +31,7 @@ class Hw2dTables(ctypes.Structure):
         ("delb", ctypes.c_double), ("cur_u", ctypes.c_double), ("t0", ctypes.c_double), ("dt_out", ctypes.c_double),
         ("refl_coef", ctypes.c_double),
         ("gam_mid", _dp), ("csq_mid", _dp), ("om2_mid", _dp),
+        ("nrefk", ctypes.c_int), ("gam_k", _dp), ("csq_k", _dp), ("om2_k", _dp),
     ]
 
 
@@ -115,7 +116,7 @@ class Engine2D:
         keep = {}
         for k in ("kx", "ky", "c2d", "l2d", "aal", "charac", "chiadj", "newgam", "skewgam", "tsig", "sig", "sigskew",
                   "gam_min", "gam_plus", "csq_min", "csq_plus", "om2_min", "om2_plus", "wallchar", "gam_mid",
-                  "csq_mid", "om2_mid"):
+                  "csq_mid", "om2_mid", "gam_k", "csq_k", "om2_k"):
             v = tables.get(k)
             keep[k] = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
         brk = int(tables.get("breaking", 0))
@@ -126,7 +127,7 @@ class Engine2D:
         tb = Hw2dTables(nx=int(tables["nx"]), ny=int(tables["ny"]), model=int(tables.get("model", 2)),
                         propagation=int(tables.get("propagation", 0)), cpeak=float(tables["cpeak"]),
                         nt=int(tables.get("nt", 0) if keep["sig"] is not None else 0), breaking=brk, **scal,
-                        refl_coef=float(tables.get("refl_coef", 0.0)),
+                        refl_coef=float(tables.get("refl_coef", 0.0)), nrefk=int(tables.get("nrefk", 0)),
                         **{k: _ptr(v) for k, v in keep.items()})
         o = HwOpts(eps_abs=eps_abs, eps_rel=eps_rel, h0=h0, device=device)
         self._h = self._L.hw2d_create(ctypes.byref(tb), ctypes.byref(o))

@@ -325,6 +325,114 @@ def compare_on_ensemble(mlp, decks, t_warm=0.5, t_end=3.0, device=0):
     return out
 
 
+# ---------------------------------------------------------------- the 2D variant
+def smooth2d(a, dx, dy, sigma):
+    """Isotropic Gaussian smoothing of a [ny][nx] field (periodic, by FFT), standard
+    deviation sigma (m)."""
+    ny, nx = a.shape
+    kx = 2 * np.pi * np.fft.fftfreq(nx, d=dx)
+    ky = 2 * np.pi * np.fft.fftfreq(ny, d=dy)
+    g = np.exp(-0.5 * sigma ** 2 * (ky[:, None] ** 2 + kx[None, :] ** 2))
+    return np.fft.ifft2(np.fft.fft2(a) * g).real
+
+
+def features2d(depth, dx, dy, kdom):
+    """(ny*nx, 5) float32 features of a 2D bottom, the 1D features' definitions with the
+    smoothing isotropic in the plane: h and h smoothed at 2, 8 and 32 m as positions
+    on the log scale of the 4 reference depths, and log(kappa_dom h)."""
+    D = reference_depths(depth, K_LEARN)
+    scale = np.log(D[-1] / D[0]) / (K_LEARN - 1) if D[-1] > D[0] else 1.0
+    hs = [depth] + [np.maximum(smooth2d(depth, dx, dy, s), 1e-3) for s in SCALES_M]
+    f = [(np.log(h / D[0]) / scale - 1.5).ravel() for h in hs] + [np.log(kdom * depth).ravel()]
+    return np.stack(f, axis=1).astype(np.float32)
+
+
+def learned_tables2d(mlp, tb):
+    """A 2D varying-bottom tables dict (decks2d.tables) with the learned K = 4 operator:
+    the network's per-point softmax weights over 4 log-spaced reference depths, the
+    dominant wavenumber from linear dispersion at the peak frequency.  The network is
+    the 1D one: the blend it picks is a function of the local depth features and
+    kappa_dom h, which the 2D bottom defines the same way."""
+    from . import decks2d
+    depth = tb["depth"]
+    dx, dy = float(tb["dx"]), float(tb["dy"])
+    kdom = kappa_linear(float(tb["wp"]), depth)
+    w = mlp.infer(features2d(depth, dx, dy, kdom))
+    return decks2d.with_k_operator(tb, reference_depths(depth, K_LEARN), w)
+
+
+def wave_field_2d(tb, seed=0, hs_frac=0.25):
+    """A sea state filling the whole 2D domain, as the initial state of a comparison:
+    eta a seeded sum of random-phase waves of significant height hs_frac times the
+    deck's (a quarter by default: no wave breaks over the shallowest bottom), their
+    wavenumbers in [0.5 kp, 2 kp] and directions within 45 degrees of the x axis
+    (kp of the peak period at the offshore depth), u = v = 0, in the spectral state
+    layout [Re eta^ | Im eta^ | Re u^ | Im u^ | Re v^ | Im v^] (FFTW order) filtered by
+    the anti-aliasing mask.  Unlike a start from rest, the waves cover the varying
+    bottom from the first step, so a short window sees the depth operator everywhere."""
+    rng = np.random.default_rng(seed)
+    nx, ny = tb["nx"], tb["ny"]
+    kx, ky = np.asarray(tb["kx"]), np.asarray(tb["ky"])
+    kp = float(tb["kp"])
+    KX, KY = np.meshgrid(kx, ky)
+    kk = np.hypot(KX, KY)
+    ang = np.abs(np.arctan2(KY, KX))
+    band = (kk > 0.5 * kp) & (kk < 2.0 * kp) & (ang < np.pi / 4)
+    spec = np.where(band, np.exp(-0.5 * ((kk - kp) / (0.3 * kp)) ** 2), 0.0)
+    ehat = spec * np.exp(2j * np.pi * rng.random(spec.shape))
+    eta = np.fft.ifft2(ehat).real
+    eta *= (hs_frac * float(tb.get("hs", 0.5)) / 4.0) / max(eta.std(), 1e-300)
+    ehat = np.fft.fft2(eta) * tb["aal"]
+    y = np.zeros(6 * nx * ny)
+    y[: nx * ny] = ehat.real.ravel()
+    y[nx * ny: 2 * nx * ny] = ehat.imag.ravel()
+    return y
+
+
+def compare_2d(mlp, tb, t_warm=0.25, t_end=0.75, device=0, eps_abs=1e-8, eps_rel=1e-6, uniform=True):
+    """The 2D learned variant beside the plain path on one varying-bottom deck: the
+    plain 16-reference operator and the learned 4-reference blend (learned_tables2d),
+    each from the same sea state over the whole domain (wave_field_2d) through t_warm
+    and then, device-timed on the engine's own stream, to t_end; simulated seconds
+    per wall second of each, RHS calls, and the eta relative L2 error of the learned
+    run at t_end against the plain one (and, for scale, of uniform weights over the
+    same 4 depths)."""
+    import torch
+    from . import decks2d
+    from .engine2d import Engine2D
+    n = tb["nx"] * tb["ny"]
+    y0 = wave_field_2d(tb)
+    lrn = learned_tables2d(mlp, tb)
+    variants = [("plain", decks2d.plain_k_operator(tb, K_PLAIN)), ("learned", lrn)]
+    if uniform:
+        variants.append(("uniform", decks2d.with_k_operator(tb, lrn["ref_depths"],
+                                                            np.full((K_LEARN,) + tb["depth"].shape, 1.0 / K_LEARN))))
+    out, etas = {}, {}
+    for name, t in variants:
+        eng = Engine2D(t, eps_abs, eps_rel, device=device)
+        st = torch.cuda.Stream(device=device)
+        eng.set_stream(st.cuda_stream)
+        eng.set_state(0.0, 0.02, y0)
+        eng.run_to_time(t_warm)
+        r0 = eng.stats()["rhs_calls"]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        eng.run_to_time(t_end)
+        e1.record(st)
+        torch.cuda.synchronize()
+        if name != "uniform":
+            out[f"{name}_sim_s_per_wall_s"] = (t_end - t_warm) / (e0.elapsed_time(e1) / 1e3)
+            out[f"{name}_rhs_calls"] = eng.stats()["rhs_calls"] - r0
+        etas[name] = eng.fields()[0]
+        eng.close()
+    err = lambda a: float(np.linalg.norm(a - etas["plain"]) / max(np.linalg.norm(etas["plain"]), 1e-300))
+    out.update(speedup=out["learned_sim_s_per_wall_s"] / out["plain_sim_s_per_wall_s"],
+               eta_err=err(etas["learned"]),
+               eta_err_uniform_weights=err(etas["uniform"]) if "uniform" in etas else None,
+               window_s=[t_warm, t_end])
+    return out
+
+
 def pipeline(n_train=512, n_eval=64, nx=16384, t_train=20.0, t_eval=20.0, epochs=200, batch=4096, stride=16,
              root=None, device=0, seed=0, log=print, save=None):
     """Config-4 pipeline: plain 16-reference runs on n_train random bathymetries ->

@@ -279,11 +279,19 @@ typedef struct hw2d_tables {
     double t0, dt_out;          /* dominfo.t[0], dominfo.dt (breaking.dat cadence) */
     double refl_coef;           /* walls: refl_coef (the flat RHS's fun_delphiH1hat takes its
                                    flux branch when it is 1)                     */
-    /* three reference depths (ninterp = 3, HSSgen_3depth): the middle depth's tables.
-     * Not built on the device yet: hw2d_create rejects tables that set them. */
+    /* three reference depths (ninterp = 3, HSSgen_3depth): the middle depth's tables
+     * (served by the general path); NULL for two reference depths */
     const double* gam_mid;      /* [ny*nx] Oprt.InterpD.Gam_mid                 */
     const double* csq_mid;      /* [ny*nx] Oprt.InterpD.Csqr2d_mid              */
     const double* om2_mid;      /* [ny*nx] Oprt.InterpD.Om2dSq_mid              */
+    /* K reference depths, 2 <= nrefk <= 16 (no counterpart in the reference: HSSgen's
+     * sum over K depths, used by the plain 16-reference operator and the learned
+     * 4-reference blend); nrefk = 0 leaves the three fields below unread, nrefk > 0
+     * replaces the min/plus/mid tables above (which must then be NULL) */
+    int nrefk;
+    const double* gam_k;        /* [K][ny*nx] per-point weight of each depth    */
+    const double* csq_k;        /* [K][ny*nx] C^2 of each reference depth       */
+    const double* om2_k;        /* [K][ny*nx] Omega^2 of each reference depth   */
 } hw2d_tables;
 
 /* opts: eps_abs/eps_rel (<= 0: the 2D reference's 1e-3 / 1e-2, 2d/main.c:196-197),

@@ -41,6 +41,8 @@ struct or2d_ctx {
     int var;                                           /* varying bottom (two reference depths) */
     double *gmin, *gplus, *cmin, *cplus, *omin, *oplus;
     double *gmid, *cmid, *omid;                        /* three reference depths, NULL: two */
+    int nk;                                            /* K reference depths (0: min/plus/mid tables) */
+    double *gk, *ck, *ok;                              /* [K][n] weights, C^2, Omega^2 */
     double* wallchar;                                  /* NULL: no wall */
     int refl_one;                                      /* flat bottom, refl_coef == 1 */
     double *gwx, *gwy;                                 /* fun_gradient(wallchar) (refl_one) */
@@ -173,6 +175,16 @@ or2d_ctx* or2d_create(const or2d_tables* tb, double eps_abs, double eps_rel) {
             c->gmid = dup(tb->gam_mid, n); c->cmid = dup(tb->csq_mid, n); c->omid = dup(tb->om2_mid, n);
         }
     }
+    if (tb->nrefk) {
+        if (tb->nrefk < 2 || tb->nrefk > 16 || !tb->gam_k || !tb->csq_k || !tb->om2_k) {
+            set_err2("or2d_create: K reference depths need 2 <= K <= 16 and gam_k, csq_k, om2_k"); free(c); return NULL;
+        }
+        c->var = 1;
+        c->nk = tb->nrefk;
+        c->gk = dup(tb->gam_k, (size_t)c->nk * n);
+        c->ck = dup(tb->csq_k, (size_t)c->nk * n);
+        c->ok = dup(tb->om2_k, (size_t)c->nk * n);
+    }
     if (tb->wallchar) {
         c->wallchar = dup(tb->wallchar, n);
         if (!c->var && tb->refl_coef == 1) {
@@ -204,7 +216,7 @@ void or2d_destroy(or2d_ctx* c) {
     double* f[] = {c->kx, c->ky, c->c2d, c->l2d, c->aal, c->charac, c->chiadj, c->newgam, c->skewgam, c->tsig,
                    c->sig, c->sigskew, c->csig, c->csigskew, c->k1, c->k2, c->k3, c->k4, c->k5, c->k6, c->ytmp,
                    c->y0, c->yerr, c->dydt_in, c->dydt_out, c->gmin, c->gplus, c->cmin, c->cplus, c->omin,
-                   c->oplus, c->wallchar, c->gwx, c->gwy, c->gmid, c->cmid, c->omid};
+                   c->oplus, c->wallchar, c->gwx, c->gwy, c->gmid, c->cmid, c->omid, c->gk, c->ck, c->ok};
     for (size_t q = 0; q < sizeof f / sizeof f[0]; q++) free(f[q]);
     brk_destroy(c->brk);
     free(c);
@@ -303,6 +315,39 @@ static void hssgen_3depth(const or2d_ctx* c, const cx* phi, const cx* phihat, co
                         + Op[q] * g[2][q].im) / 2;
     }
     for (int d = 0; d < 3; d++) { free(L0[d]); free(g[d]); free(gL[d]); }
+}
+
+/* The K-reference-depth operator (no counterpart in the reference): HSSgen_3depth's
+ * sum over K depths, result = 1/2 sum_j [F(gam_j Re F^-1 S(O_j phihat)) + O_j F(gam_j phi)],
+ * summed in the same order (j ascending, round-trip term then spectral term); with K = 2
+ * and K = 3 and the same tables it is HSSgen_2depth / HSSgen_3depth bit for bit.
+ * O = c->ck (C^2) or c->ok (Omega^2), [K][n]. */
+static void hssgen_k(const or2d_ctx* c, const cx* phi, const cx* phihat, const double* O, cx* result) {
+    const int Nx = c->nx, Ny = c->ny, n = c->n, K = c->nk;
+    const double factIFFT = (double)Nx * Ny;
+    cx* L0 = malloc(sizeof(cx) * n);
+    cx* g = malloc(sizeof(cx) * n);
+    cx* gL = malloc(sizeof(cx) * n);
+    for (int q = 0; q < n; q++) { result[q].re = 0; result[q].im = 0; }
+    for (int d = 0; d < K; d++) {
+        const double* Od = O + (size_t)d * n;
+        const double* Gd = c->gk + (size_t)d * n;
+        for (int q = 0; q < n; q++) { L0[q].re = Od[q] * phihat[q].re; L0[q].im = Od[q] * phihat[q].im; }
+        sym2(L0, Nx, Ny);
+        fft2(Nx, Ny, L0, +1);
+        for (int q = 0; q < n; q++) {
+            g[q].re = Gd[q] * phi[q].re / factIFFT; g[q].im = 0;
+            gL[q].re = Gd[q] * L0[q].re / (Nx * Ny); gL[q].im = 0;
+        }
+        fft2(Nx, Ny, g, -1);
+        fft2(Nx, Ny, gL, -1);
+        for (int q = 0; q < n; q++) {
+            result[q].re = result[q].re + gL[q].re + Od[q] * g[q].re;
+            result[q].im = result[q].im + gL[q].im + Od[q] * g[q].im;
+        }
+    }
+    for (int q = 0; q < n; q++) { result[q].re /= 2; result[q].im /= 2; }
+    free(L0); free(g); free(gL);
 }
 
 static void hssgen_2depth(const or2d_ctx* c, const cx* phi, const cx* phihat, const double* Om, const double* Op,
@@ -816,7 +861,10 @@ static int rhs_2db(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
     memcpy(eta, eta_hat, sizeof(cx) * n); memcpy(u, u_hat, sizeof(cx) * n); memcpy(v, v_hat, sizeof(cx) * n);
     fft2(Nx, Ny, eta, +1); fft2(Nx, Ny, u, +1); fft2(Nx, Ny, v, +1);
     cx *Csqr_uhat = malloc(sizeof(cx) * n), *Csqr_vhat = malloc(sizeof(cx) * n);
-    if (c->gmid) {   /* ninterp = 3 (2d/fun_odesolver.c:2917-2920) */
+    if (c->nk) {
+        hssgen_k(c, u, u_hat, c->ck, Csqr_uhat);
+        hssgen_k(c, v, v_hat, c->ck, Csqr_vhat);
+    } else if (c->gmid) {   /* ninterp = 3 (2d/fun_odesolver.c:2917-2920) */
         hssgen_3depth(c, u, u_hat, c->cmin, c->cmid, c->cplus, Csqr_uhat);
         hssgen_3depth(c, v, v_hat, c->cmin, c->cmid, c->cplus, Csqr_vhat);
     } else {
@@ -894,7 +942,10 @@ static int rhs_2db(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
         etaM0v[q].re = etaM0v[q].re * factIFFT;
     }
     cx *LetaM0u = malloc(sizeof(cx) * n), *LetaM0v = malloc(sizeof(cx) * n);
-    if (c->gmid) {   /* ninterp = 3 (:3463-3466) */
+    if (c->nk) {
+        hssgen_k(c, etaM0u, etaM0uhat, c->ok, LetaM0u);
+        hssgen_k(c, etaM0v, etaM0vhat, c->ok, LetaM0v);
+    } else if (c->gmid) {   /* ninterp = 3 (:3463-3466) */
         hssgen_3depth(c, etaM0u, etaM0uhat, c->omin, c->omid, c->oplus, LetaM0u);
         hssgen_3depth(c, etaM0v, etaM0vhat, c->omin, c->omid, c->oplus, LetaM0v);
     } else {
@@ -970,7 +1021,8 @@ static int rhs_2db(or2d_ctx* c, double t, const double* Zhat, double* dt_Zhat) {
         cx* Lp[4];
         for (int k = 0; k < 4; k++) {
             Lp[k] = malloc(sizeof(cx) * n);
-            if (c->gmid) hssgen_3depth(c, p[k], ph[k], c->omin, c->omid, c->oplus, Lp[k]);
+            if (c->nk) hssgen_k(c, p[k], ph[k], c->ok, Lp[k]);
+            else if (c->gmid) hssgen_3depth(c, p[k], ph[k], c->omin, c->omid, c->oplus, Lp[k]);
             else hssgen_2depth(c, p[k], ph[k], c->omin, c->oplus, Lp[k]);
         }
         cx *ikx3 = malloc(sizeof(cx) * n), *iky3 = malloc(sizeof(cx) * n);

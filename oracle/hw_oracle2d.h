@@ -70,6 +70,14 @@ typedef struct or2d_tables {
     const double* gam_mid;      /* [ny*nx] Oprt.InterpD.Gam_mid                */
     const double* csq_mid;      /* [ny*nx] Oprt.InterpD.Csqr2d_mid             */
     const double* om2_mid;      /* [ny*nx] Oprt.InterpD.Om2dSq_mid             */
+    /* K reference depths (no counterpart in the reference: the generalisation of
+     * HSSgen_2depth / _3depth to K depths that the plain 16-reference and the learned
+     * 4-reference operators use); nrefk = 0 leaves these unread, nrefk >= 2 replaces
+     * the min/plus/mid tables above */
+    int nrefk;
+    const double* gam_k;        /* [K][ny*nx] per-point weights                */
+    const double* csq_k;        /* [K][ny*nx] C^2 of each reference depth      */
+    const double* om2_k;        /* [K][ny*nx] Omega^2 of each reference depth  */
 } or2d_tables;
 
 /* Copies every table.  eps <= 0 selects the reference's 2D values (abs 1e-3,

@@ -47,6 +47,7 @@ class Or2dTables(ctypes.Structure):
         ("delb", ctypes.c_double), ("cur_u", ctypes.c_double), ("t0", ctypes.c_double), ("dt_out", ctypes.c_double),
         ("refl_coef", ctypes.c_double),
         ("gam_mid", _dpt), ("csq_mid", _dpt), ("om2_mid", _dpt),
+        ("nrefk", ctypes.c_int), ("gam_k", _dpt), ("csq_k", _dpt), ("om2_k", _dpt),
     ]
 
 BRK_SCALARS = ("dx", "dy", "max_eta_init", "tstar", "rsearch", "kbc", "tc", "delb", "cur_u", "t0", "dt_out")
@@ -236,7 +237,7 @@ class Oracle2D:
         keep = {}
         for k in ("kx", "ky", "c2d", "l2d", "aal", "charac", "chiadj", "newgam", "skewgam", "tsig", "sig", "sigskew",
                   "gam_min", "gam_plus", "csq_min", "csq_plus", "om2_min", "om2_plus", "wallchar", "gam_mid",
-                  "csq_mid", "om2_mid"):
+                  "csq_mid", "om2_mid", "gam_k", "csq_k", "om2_k"):
             v = tables.get(k)
             keep[k] = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
         brk = int(tables.get("breaking", 0))
@@ -248,6 +249,7 @@ class Oracle2D:
                         propagation=int(tables.get("propagation", 0)), cpeak=float(tables["cpeak"]),
                         nt=int(tables.get("nt", 0) if keep["sig"] is not None else 0), breaking=brk, **scal,
                         refl_coef=float(tables.get("refl_coef", 0.0)),
+                        nrefk=int(tables.get("nrefk", 0)),
                         **{k: (None if v is None else _p(v)) for k, v in keep.items()})
         self.h = L.or2d_create(ctypes.byref(tb), eps_abs, eps_rel)
         if not self.h:

@@ -108,3 +108,60 @@ def test_rhs_parity_1024_two_depth_wall_breaking():
     Be, _, _, fe, ne = eng.breaking_fields()
     Bo, _, _, fo, no = ora.breaking_fields()
     assert (fe, ne) == (fo, no) and np.array_equal(Be > 0, Bo > 0)
+
+
+# ------------------------------------------------ K reference depths (plain and learned)
+@pytest.mark.parametrize("K,model", [(4, 2), (16, 2), (4, 3), (16, 1)])
+def test_k_reference_rhs_parity(K, model):
+    """The K-reference operator (the plain 16-reference one and the 4-depth form the
+    learned blend uses) on the general path: one RHS 1e-11 against the oracle's
+    K-depth HSSgen sum."""
+    tb = decks2d.plain_k_operator(shoal(64, 64, ninterp=2, model=model), K)
+    eng, ora = Engine2D(tb, 1e-8, 1e-6), Oracle2D(tb, 1e-8, 1e-6)
+    for seed, t in ((1, 0.7), (2, 3.3)):
+        y = band_limited_state(tb, 0.02, seed)
+        assert rel(eng.rhs(t, y), ora.rhs(t, y)) < 1e-11
+
+
+def test_k_reference_run_parity():
+    """The graph-replayed loop with 16 reference depths to t = 1.5 s from rest: the
+    same step counts, state 1e-9."""
+    tb = decks2d.plain_k_operator(shoal(64, 64, ninterp=2), 16)
+    eng, ora = Engine2D(tb, 1e-8, 1e-6), Oracle2D(tb, 1e-8, 1e-6)
+    n = tb["nx"] * tb["ny"]
+    h0 = 0.02
+    eng.set_state(0.0, h0, np.zeros(6 * n))
+    y = np.zeros(6 * n)
+    t, h = ora.run_to(0.0, 1.5, h0, y)
+    eng.run_to_time(1.5)
+    te, he, ye = eng.state()
+    assert abs(te - t) < 1e-12 and abs(he - h) <= 1e-6 * abs(h)
+    so, se = ora.stats(), eng.stats()
+    assert (se["accepted"], se["rejected"]) == (so["accepted"], so["rejected"])
+    assert np.abs(y).max() > 0 and rel(ye, y) < 1e-9
+
+
+def test_learned_operator_2d_gain():
+    """The learned K = 4 blend on a 2D bottom (the committed network, 2D features):
+    against the plain 16-reference run its eta error is well below that of uniform
+    weights over the same 4 depths, the method without the network."""
+    from hawassi_c_b200 import learned
+    mlp = learned.load_mlp()
+    assert mlp is not None
+    tb = decks2d.tables(nx=128, ny=128, Lx=115.2, Ly=115.2, depth=2.0, shallow=0.3, Hs=0.1, Tp=2.5, n_freq=24,
+                        n_dir=6, t_end=8.0, dt=0.1, damp=8.0, x_line=12.0, seed=5, bathymetry="shoal")
+    plain = decks2d.plain_k_operator(tb, 16)
+    lrn = learned.learned_tables2d(mlp, tb)
+    D4 = lrn["ref_depths"]
+    uni = decks2d.with_k_operator(tb, D4, np.full((4,) + tb["depth"].shape, 0.25))
+    n = tb["nx"] * tb["ny"]
+    etas = {}
+    for name, t in (("plain", plain), ("learned", lrn), ("uniform", uni)):
+        e = Engine2D(t, 1e-8, 1e-6)
+        e.set_state(0.0, 0.02, np.zeros(6 * n))
+        e.run_to_time(6.0)
+        etas[name] = e.fields()[0]
+        e.close()
+    err = {k: rel(etas[k], etas["plain"]) for k in ("learned", "uniform")}
+    assert np.abs(etas["plain"]).max() > 0
+    assert err["learned"] < 0.2 * err["uniform"], err

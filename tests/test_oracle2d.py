@@ -298,3 +298,48 @@ def test_three_depth_tables_run_in_the_oracle():
     rng = np.random.default_rng(5)
     y = 0.02 * rng.standard_normal(6 * n) * np.tile(tb["aal"].ravel(), 6) * np.sqrt(n)
     assert np.isfinite(Oracle2D(tb).rhs(0.3, y)).all()
+
+
+# ------------------------------------------------------------ K reference depths
+def _k_tables(tb, names):
+    kt = {k: v for k, v in tb.items() if not k.startswith(("gam_", "csq_", "om2_"))}
+    kt["nrefk"] = len(names)
+    kt["gam_k"] = np.stack([tb[f"gam_{m}"].ravel() for m in names])
+    kt["csq_k"] = np.stack([tb[f"csq_{m}"].ravel() for m in names])
+    kt["om2_k"] = np.stack([tb[f"om2_{m}"].ravel() for m in names])
+    return kt
+
+
+@pytest.mark.parametrize("ninterp,model", [(2, 2), (2, 3), (3, 2), (3, 3)])
+def test_k_reference_form_is_hssgen_bit_for_bit(ninterp, model):
+    """The K-depth sum with the two- or three-depth tables is HSSgen_2depth /
+    HSSgen_3depth exactly (same products, same summation order)."""
+    tb = decks2d.tables(nx=64, ny=64, Lx=57.6, Ly=57.6, depth=2.0, shallow=0.6, Hs=0.1, Tp=3.0, n_freq=16,
+                        n_dir=4, t_end=4.0, dt=0.1, damp=6.0, x_line=10.0, seed=1, bathymetry="shoal",
+                        ninterp=ninterp, model=model)
+    names = ["min", "mid", "plus"] if ninterp == 3 else ["min", "plus"]
+    kt = _k_tables(tb, names)
+    n = 64 * 64
+    y = 0.02 * np.random.default_rng(3).standard_normal(6 * n) * np.tile(tb["aal"].ravel(), 6) * 64
+    a = Oracle2D(tb, 1e-8, 1e-6).rhs(0.9, y)
+    b = Oracle2D(kt, 1e-8, 1e-6).rhs(0.9, y)
+    assert np.array_equal(a, b)
+
+
+def test_k_reference_weights():
+    """The plain K-reference weights: two non-zero weights per point (the bracketing
+    pair), weight 1 on a point that sits at a reference depth, and with K = 2 the
+    two-depth operator's weights up to its spline over 101 depth samples."""
+    tb = decks2d.tables(nx=64, ny=64, Lx=57.6, Ly=57.6, depth=2.0, shallow=0.6, Hs=0.1, Tp=3.0, n_freq=16,
+                        n_dir=4, t_end=4.0, dt=0.1, damp=6.0, x_line=10.0, seed=1, bathymetry="shoal")
+    depth = tb["depth"]
+    D = decks2d.log_reference_depths(depth, 16)
+    w = decks2d.k_reference_weights(depth, tb["wp"], D)
+    assert w.shape == (16,) + depth.shape
+    assert ((w != 0).sum(axis=0) <= 2).all()
+    assert np.abs(w.sum(axis=0) - 1).max() < 1e-3
+    wd = decks2d.k_reference_weights(np.array(D[5:9]), tb["wp"], D)
+    assert np.allclose(wd[5:9].diagonal(), 1.0, atol=1e-12)
+    w2 = decks2d.plain_k_operator(tb, 2)["gam_k"]
+    assert np.abs(w2[0] - tb["gam_min"].ravel()).max() < 1e-4
+    assert np.abs(w2[1] - tb["gam_plus"].ravel()).max() < 1e-4
