@@ -834,6 +834,9 @@ def main():
     ap.add_argument("--workload", default="ensemble", choices=["ensemble", "2d", "fbr005", "c1", "c2"])
     ap.add_argument("--slice", type=int, default=0,
                     help="fbr005: grid points per CTA of the member's cluster (0: 512)")
+    ap.add_argument("--resident", type=int, default=0,
+                    help="ensemble evolve grid: 0 one cluster per member, -1 persistent clusters "
+                         "pulling members from a queue (the class's share), n > 0 at most n per class")
     ap.add_argument("--shard", default="replicas", choices=["replicas", "fixed"],
                     help="multi-GPU ensemble: a 256-member ensemble per rank (weak) or one split over ranks (strong)")
     ap.add_argument("--autotune", action="store_true",
@@ -915,7 +918,7 @@ def main():
         slices, _ = autotune_slices(decks, window=args.window, device=local, eps_abs=EPS_ABS, eps_rel=EPS_REL,
                                     log=log)
         log(f"autotuned slices {slices}")
-    eng = hw.Engine(decks, eps_abs=EPS_ABS, eps_rel=EPS_REL, device=local, slices=slices)
+    eng = hw.Engine(decks, eps_abs=EPS_ABS, eps_rel=EPS_REL, device=local, slices=slices, resident=args.resident)
     log("engine created")
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)

@@ -155,6 +155,8 @@ struct Class {
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
   cudaEvent_t t_start = nullptr, t_stop = nullptr;   // timing of the last evolve launch
+  int* d_queue = nullptr;   // work-queue counter of the persistent evolve grid
+  int grid = 0;             // resident clusters of the persistent grid (0: one per member)
 };
 
 }  // namespace
@@ -204,13 +206,24 @@ std::vector<double> permute(const std::vector<double>& v, int N, int C, int M) {
   return r;
 }
 
-cudaError_t launch_any(int M, int mode, DevMember* mems, const int* list, int nmem, int C, double t, cudaStream_t s) {
+cudaError_t launch_any(int M, int mode, DevMember* mems, const int* list, int nmem, int C, double t, cudaStream_t s,
+                       int* queue = nullptr, int ngrid = 0) {
   switch (M) {
-    case 256: return hw_launch_256(mode, mems, list, nmem, C, t, s);
-    case 512: return hw_launch_512(mode, mems, list, nmem, C, t, s);
-    case 1024: return hw_launch_1024(mode, mems, list, nmem, C, t, s);
-    case 2048: return hw_launch_2048(mode, mems, list, nmem, C, t, s);
+    case 256: return hw_launch_256(mode, mems, list, nmem, C, t, s, queue, ngrid);
+    case 512: return hw_launch_512(mode, mems, list, nmem, C, t, s, queue, ngrid);
+    case 1024: return hw_launch_1024(mode, mems, list, nmem, C, t, s, queue, ngrid);
+    case 2048: return hw_launch_2048(mode, mems, list, nmem, C, t, s, queue, ngrid);
     default: return cudaErrorInvalidValue;
+  }
+}
+
+int max_clusters_any(int M, int C) {
+  switch (M) {
+    case 256: return hw_max_clusters_256(C);
+    case 512: return hw_max_clusters_512(C);
+    case 1024: return hw_max_clusters_1024(C);
+    case 2048: return hw_max_clusters_2048(C);
+    default: return 0;
   }
 }
 
@@ -494,6 +507,26 @@ bool hw_ctx::init(const std::vector<std::string>& dirs, const hw_opts* o, const 
     HW_CUDA(cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming));
     HW_CUDA(cudaEventCreate(&c.t_start));
     HW_CUDA(cudaEventCreate(&c.t_stop));
+    HW_CUDA(cudaMalloc(&c.d_queue, sizeof(int)));
+  }
+  // evolve grids: one cluster per member (resident == 0, the default: measured the
+  // fastest), or a persistent grid whose clusters pull members from the class's queue --
+  // at most `resident` clusters, or (resident < 0) the class's share of the resident
+  // clusters by grid points (members x CTAs), a quarter over so that a class that
+  // drains its queue early leaves its slots to the waiting clusters of the others
+  double total = 0.0;
+  for (const auto& c : classes) total += double(c.members.size()) * c.C;
+  for (auto& c : classes) {
+    const int nm = int(c.members.size());
+    if (opt.resident == 0) {
+      c.grid = 0;
+    } else if (opt.resident > 0) {
+      c.grid = std::min(nm, opt.resident);
+    } else {
+      const int maxc = max_clusters_any(c.M, c.C);
+      const double share = double(nm) * c.C / total;
+      c.grid = maxc > 0 ? std::min(nm, std::max(1, int(std::ceil(1.25 * maxc * share)))) : 0;
+    }
   }
   return true;
 }
@@ -534,7 +567,9 @@ bool hw_ctx::run(int i_stop_all, double t_end, bool by_time, const int* per_memb
     k_order_class<<<1, 256, size_t(nm) * (sizeof(long long) + sizeof(int)), c.stream>>>(d_mems, c.d_list, nm,
                                                                                       d_prev_rhs);
     HW_CUDA(cudaGetLastError());
-    cudaError_t e = launch_any(c.M, 0, d_mems, c.d_list, int(c.members.size()), c.C, 0.0, c.stream);
+    if (c.grid > 0) HW_CUDA(cudaMemsetAsync(c.d_queue, 0, sizeof(int), c.stream));
+    cudaError_t e = launch_any(c.M, 0, d_mems, c.d_list, int(c.members.size()), c.C, 0.0, c.stream,
+                               c.grid > 0 ? c.d_queue : nullptr, c.grid);
     if (e != cudaSuccess) { err = std::string("launch: ") + cudaGetErrorString(e); return false; }
     HW_CUDA(cudaEventRecord(c.t_stop, c.stream));
     HW_CUDA(cudaEventRecord(c.done, c.stream));
@@ -594,6 +629,7 @@ hw_ctx::~hw_ctx() {
   if (d_off) cudaFree(d_off);
   for (auto& c : classes) {
     if (c.d_list) cudaFree(c.d_list);
+    if (c.d_queue) cudaFree(c.d_queue);
     if (c.stream) cudaStreamDestroy(c.stream);
     if (c.done) cudaEventDestroy(c.done);
     if (c.t_start) cudaEventDestroy(c.t_start);

@@ -24,6 +24,7 @@ class HwOpts(ctypes.Structure):
         ("cluster", ctypes.c_int),
         ("device", ctypes.c_int),
         ("slice", ctypes.c_int),
+        ("resident", ctypes.c_int),
     ]
 
 
@@ -124,14 +125,18 @@ class Engine:
     (``Engine(["deck0", "deck1", ...])``) on one GPU."""
 
     def __init__(self, decks, eps_abs=0.0, eps_rel=0.0, h0=0.0, seed=0, nref=0, exact_sequence=False,
-                 cluster=0, device=0, slice=0, slices=None):
+                 cluster=0, device=0, slice=0, slices=None, resident=0):
         """slices: grid points per CTA per grid size ({Nx: points}, e.g. from
-        autotune.autotune_slices) or per member (a list); others use `slice`."""
+        autotune.autotune_slices) or per member (a list); others use `slice`.
+        resident: the evolve launches' grid (hw_opts.resident): 0 one cluster per
+        member, -1 a persistent grid of resident clusters pulling members from a
+        queue (sized to the class's share), n > 0 at most n such clusters per class."""
         L = load_library()
         if isinstance(decks, (str, os.PathLike)):
             decks = [decks]
         self.decks = [os.fspath(d) for d in decks]
-        opts = HwOpts(eps_abs, eps_rel, h0, seed, nref, int(bool(exact_sequence)), cluster, device, slice)
+        opts = HwOpts(eps_abs, eps_rel, h0, seed, nref, int(bool(exact_sequence)), cluster, device, slice,
+                      int(resident))
         arr = (ctypes.c_char_p * len(self.decks))(*[d.encode() for d in self.decks])
         if slices is None:
             self._h = L.hw_ensemble_create(arr, len(self.decks), ctypes.byref(opts))

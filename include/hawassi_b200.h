@@ -33,6 +33,12 @@ typedef struct hw_opts {
     int cluster;             /* CTAs per member, power of two (0 = automatic) */
     int device;              /* CUDA device ordinal */
     int slice;               /* grid points per CTA when cluster == 0 (0 = 2048) */
+    int resident;            /* evolve launches of an ensemble: 0 = one cluster per member
+                                (members started longest first); -1 = a persistent grid per
+                                grid-size class, its clusters pulling members (longest first)
+                                from a device queue, sized to the class's share of the
+                                resident clusters; n > 0 = a persistent grid of at most n
+                                clusters per class */
 } hw_opts;
 
 /* Replaces the reference's set-up (1d/main.cc:42-226): parse <workdir>/input.txt and
