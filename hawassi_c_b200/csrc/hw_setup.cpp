@@ -604,7 +604,7 @@ bool build_member(const std::string& dir, const SetupOptions& opt, Member& m, st
   m.has_influx = d.wavename != "zero";
   m.insig.assign(n, 0.0);
   m.insig_skew.assign(n, 0.0);
-  std::vector<double> ww;
+  std::vector<double> ww, kom, GV, ins_re, ins_im;   // modified_influx's kom, GVom, insig_hat
   if (m.has_influx) {
     // set_influx / nsqrspec (1d/functions.c:1256-1329): peak of the normalised spectrum
     std::vector<double> re(we), im(n, 0.0);
@@ -652,12 +652,23 @@ bool build_member(const std::string& dir, const SetupOptions& opt, Member& m, st
     double acc = 0;
     m.insig_skew[0] = 0;
     for (int i = 1; i < n; ++i) { acc = acc + 0.5 * m.dt * (m.insig[i - 1] + m.insig[i]); m.insig_skew[i] = acc; }
-    if (d.influxing == "Point") {
-      std::vector<double> GV(n);
+    if (d.influxing == "Point" || d.influxing == "AreaShort") {
+      kom.resize(n);
+      GV.resize(n);
       for (int i = 0; i < n; ++i) {
-        double kom = ww[i] == 0 ? 0 : invers_omega(ww[i], m.depthinf);
-        GV[i] = group_velocity_i(kom, m.depthinf);
+        kom[i] = ww[i] == 0 ? 0 : invers_omega(ww[i], m.depthinf);
+        GV[i] = group_velocity_i(kom[i], m.depthinf);
       }
+    }
+    if (d.influxing == "AreaShort") {
+      // the signal's spectrum (insig_hat) and the group velocity scaled to the long-wave
+      // speed at omega = 0, for x_space's division by the kernel's spectrum
+      ins_re = m.insig;
+      ins_im.assign(n, 0.0);
+      host_dft(ins_re, ins_im, -1);
+      const double g0 = GV[0];
+      for (int j = 0; j < n; ++j) GV[j] = GV[j] * std::sqrt(kG * m.depthinf) / g0;
+    } else if (d.influxing == "Point") {
       std::vector<double> a_re(m.insig), a_im(n, 0.0), s_re(m.insig_skew), s_im(n, 0.0);
       host_dft(a_re, a_im, -1);
       host_dft(s_re, s_im, -1);
@@ -722,12 +733,46 @@ bool build_member(const std::string& dir, const SetupOptions& opt, Member& m, st
       const int shift = int((m.Xinflux - d.Xstart) / m.dx);
       const int s = ((shift % Nx) + Nx) % Nx;
       for (int j = 0; j < Nx; ++j) sp[(j + s) % Nx] = re[j] / Nx;
+      if (d.influxing == "AreaShort") {
+        // 1d/x_space.c:64-78: the kernel under a Gaussian window of +-2 peak wavelengths
+        const double Lb = 2 * std::pow(0.4 * m.lambda_p, 2);
+        const int ind1 = closest(m.x, m.Xinflux - 2 * m.lambda_p), ind2 = closest(m.x, m.Xinflux + 2 * m.lambda_p);
+        std::vector<double> win(Nx, 0.0);
+        for (int i = ind1; i < ind2 + 1; ++i) win[i] = std::exp(-std::pow((m.x[i] - m.Xinflux), 2) / Lb);
+        for (int i = 0; i < Nx; ++i) sp[i] = sp[i] * win[i];
+      }
       std::vector<double> gr(sp), gi(Nx, 0.0);
       host_dft(gr, gi, -1);
       // scaling_influx (1d/functions.c:1747)
       for (int i = 0; i < Nx; ++i) { gr[i] = gr[i] * fact; gi[i] = gi[i] * fact; }
       const double scale = gr[0] * m.dx;
       for (int i = 0; i < Nx; ++i) { m.gamX_re[i] = gr[i] * cp / scale; m.gamX_im[i] = gi[i] * cp / scale; }
+      if (d.influxing == "AreaShort") {
+        // 1d/x_space.c:86-109: the signal's spectrum times the scaled group velocity over
+        // the kernel's spectral amplitude (a natural spline over the centred wavenumbers,
+        // its last value beyond them), back to time; its running integral again
+        const int n = m.n;
+        std::vector<double> ag(Nx), kt(Nx);
+        for (int i = 0; i < Nx / 2; ++i) {
+          ag[i] = std::sqrt(std::pow(m.gamX_re[Nx / 2 + i], 2) + std::pow(m.gamX_im[Nx / 2 + i], 2));
+          ag[Nx / 2 + i] = std::sqrt(std::pow(m.gamX_re[i], 2) + std::pow(m.gamX_im[i], 2));
+          kt[i] = m.k[Nx / 2 + i];
+          kt[Nx / 2 + i] = m.k[i];
+        }
+        const std::vector<double> cg = natural_spline_c(kt, ag);
+        std::vector<double> tr(n), ti(n);
+        for (int i = 0; i < n; ++i) {
+          const double gom = std::fabs(kom[i]) > std::fabs(kt[Nx - 1]) ? ag[Nx - 1]
+                                                                       : natural_spline_eval(kt, ag, cg, kom[i]);
+          tr[i] = ins_re[i] * GV[i] / gom / m.dx;
+          ti[i] = ins_im[i] * GV[i] / gom / m.dx;
+        }
+        host_dft(tr, ti, +1);
+        for (int j = 0; j < n; ++j) m.insig[j] = tr[j] / n;
+        double a = 0;
+        m.insig_skew[0] = 0;
+        for (int i = 1; i < n; ++i) { a = a + 0.5 * m.dt * (m.insig[i - 1] + m.insig[i]); m.insig_skew[i] = a; }
+      }
     }
     for (int i = 0; i < Nx; ++i) {
       m.gamXs_re[i] = -omega_i(m.k[i], m.depthinf) * m.gamX_im[i];

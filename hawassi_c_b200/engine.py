@@ -405,7 +405,7 @@ def jonswap_influx(specs, device=0):
 def deck_table(deck, name, seed=0, nref=0):
     """Host-side set-up table of a deck (no GPU involved)."""
     L = load_library()
-    opts = HwOpts(0.0, 0.0, 0.0, seed, nref, 0, 0, 0, 0)
+    opts = HwOpts(0.0, 0.0, 0.0, seed, nref, 0, 0, 0, 0, 0)
     n = L.hw_deck_table(os.fspath(deck).encode(), ctypes.byref(opts), name.encode(), None, 0)
     if n < 0:
         raise EngineError(L.hw_last_error(None).decode())

@@ -824,13 +824,43 @@ static int x_space(or_ctx* c) {
             double* spgam = (double*)malloc(sizeof(double) * (size_t)Nx);
             ifft_real_real(c->Ug, spgam, Nx);
             circshift(spgam, (int)((c->Xinflux - c->Xstart) / c->dx), Nx);
-            if (!strcmp(c->influxing, "AreaShort")) {
-                set_err("influxing AreaShort is not supported"); free(spgam); return -1;
+            const int area_short = !strcmp(c->influxing, "AreaShort");
+            if (area_short) {   /* 1d/x_space.c:64-78: the kernel under a Gaussian window */
+                double Lb = 2 * pow(0.4 * c->lambda_p, 2);
+                double* gaussInf = (double*)calloc((size_t)Nx, sizeof(double));
+                int ind1 = closest(c->x, c->Xinflux - 2 * c->lambda_p, Nx);
+                int ind2 = closest(c->x, c->Xinflux + 2 * c->lambda_p, Nx);
+                for (int i = ind1; i < ind2 + 1; i++) gaussInf[i] = exp(-pow((c->x[i] - c->Xinflux), 2) / Lb);
+                for (int i = 0; i < Nx; i++) spgam[i] = spgam[i] * gaussInf[i];
+                free(gaussInf);
             }
             fft_real_complex(spgam, c->gamX, Nx);
             scaling_influx(c->gamX, Nx, fact, c->dx, cp);
             ifft_complex_real(c->gamX, c->spatgamX, Nx);
             free(spgam);
+            if (area_short) {   /* 1d/x_space.c:86-109: the signal divided by the kernel's spectrum */
+                int n = c->n;
+                double* abs_gamX = (double*)malloc(sizeof(double) * (size_t)Nx);
+                double* ktemp = (double*)malloc(sizeof(double) * (size_t)Nx);
+                cpx* temp = (cpx*)malloc(sizeof(cpx) * (size_t)n);
+                for (int i = 0; i < Nx / 2; i++) {
+                    abs_gamX[i] = sqrt(pow(c->gamX[Nx / 2 + i].re, 2) + pow(c->gamX[Nx / 2 + i].im, 2));
+                    abs_gamX[Nx / 2 + i] = sqrt(pow(c->gamX[i].re, 2) + pow(c->gamX[i].im, 2));
+                    ktemp[i] = c->k[Nx / 2 + i];
+                    ktemp[Nx / 2 + i] = c->k[i];
+                }
+                cspline sg;
+                cspline_init(&sg, ktemp, abs_gamX, Nx);
+                for (int i = 0; i < n; i++) {
+                    double gamXom = fabs(c->kom[i]) > fabs(ktemp[Nx - 1]) ? abs_gamX[Nx - 1] : cspline_eval(&sg, c->kom[i]);
+                    temp[i].re = c->insig_hat[i].re * c->GVom[i] / gamXom / c->dx;
+                    temp[i].im = c->insig_hat[i].im * c->GVom[i] / gamXom / c->dx;
+                }
+                ifft_complex_real(temp, c->insig, n);
+                cumtrapz(c->insig, n, c->dt, c->insig_skew);
+                cspline_free(&sg);
+                free(abs_gamX); free(ktemp); free(temp);
+            }
         }
         for (int i = 0; i < Nx; i++) {
             c->gamX_skew[i].re = -omega_i(c->k[i], c->depthinf) * c->gamX[i].im;

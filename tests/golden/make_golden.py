@@ -20,10 +20,17 @@ Fixtures written (all are reference *outputs or inputs*, no reference code):
                              (gauge positions; all 5000 rows as printed with %f,
                              stored as integers of 1e-6)
   harmbar_constants.npz      x, t, depth, k, nu_peak of output/Constants_01.dat
+  reference_decks.tar.gz     the input decks (input.txt and the .dat files it names) of
+                             the reference's other 1D test cases that stay inside the
+                             hot path: flat and barred bottoms, HS2 and HS3, breaking,
+                             Area and AreaShort influx, an initial-value bore, one
+                             bidirectional breaking deck (REFERENCE_DECKS below)
 """
+import io
 import os
 import shutil
 import sys
+import tarfile
 
 import numpy as np
 
@@ -64,6 +71,27 @@ def main(ref):
     np.savez_compressed(os.path.join(HERE, "irslope_constants.npz"),
                         x=c["x"], depth=c["depth"], k=c["k"], nu_peak=c["nu_peak"])
     harmbar(ref)
+    reference_decks(ref)
+
+
+# 1d/Testcases decks (input files only) for the deck-by-deck parity test
+REFERENCE_DECKS = ("1dB003IrBar", "1dBBr002IrBar", "1dF001Foc", "1dF002Draup", "1dF003Irreg", "1dF006Bor",
+                   "1dFBr001Foc", "1dFBr002Foc", "1dFBr003Bi", "1dFBr004Ir")
+
+
+def reference_decks(ref):
+    out = os.path.join(HERE, "reference_decks.tar.gz")
+    with tarfile.open(out, "w:gz") as tar:
+        for name in REFERENCE_DECKS:
+            src = os.path.join(ref, "1d", "Testcases", name)
+            for f in sorted(os.listdir(src)):
+                if f == "input.txt" or f.endswith(".dat"):
+                    with open(os.path.join(src, f), "rb") as fi:
+                        data = fi.read()
+                    info = tarfile.TarInfo(f"{name}/{f}")
+                    info.size = len(data)
+                    info.mtime = 0
+                    tar.addfile(info, io.BytesIO(data))
 
 
 def read_gauge_text(path):

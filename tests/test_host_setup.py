@@ -80,3 +80,13 @@ def test_library_exports_every_declared_symbol():
     missing = [s for s in sorted(declared) if not hasattr(lib, s)]
     assert not missing, missing
     assert set(engine.EXPORTS) <= declared
+
+
+def test_reference_decks_setup(tmp_path):
+    """Every packed reference deck: the host set-up's tables equal the oracle's
+    (AreaShort and Area influx, user-defined bars, an initial-value bore)."""
+    from reference_decks import REFUSED, WINDOW, unpack
+    decks_ = unpack(tmp_path)
+    assert set(decks_) == set(WINDOW) | set(REFUSED)
+    for name, deck in decks_.items():
+        _compare(deck)
