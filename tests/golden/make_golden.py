@@ -23,8 +23,8 @@ Fixtures written (all are reference *outputs or inputs*, no reference code):
   reference_decks.tar.gz     the input decks (input.txt and the .dat files it names) of
                              the reference's other 1D test cases that stay inside the
                              hot path: flat and barred bottoms, HS2 and HS3, breaking,
-                             Area and AreaShort influx, an initial-value bore, one
-                             bidirectional breaking deck (REFERENCE_DECKS below)
+                             Area and AreaShort influx, an initial-value bore
+                             (REFERENCE_DECKS below)
 """
 import io
 import os

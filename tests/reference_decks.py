@@ -20,10 +20,9 @@ WINDOW = {
     "1dF006Bor": 20.0,        # HS2 flat, initial-value bore (initial.dat)
     "1dFBr001Foc": 10.0,      # HS3 flat with breaking enabled, Nx 8192
     "1dFBr002Foc": 20.0,      # HS3 flat with breaking enabled
+    "1dFBr003Bi": 20.0,       # HS3 flat, bichromatic group with breaking enabled, AreaShort
     "1dFBr004Ir": 20.0,       # HS2 flat, irregular waves with breaking enabled, AreaShort
 }
-# decks the device refuses, with the reason its set-up gives
-REFUSED = {"1dFBr003Bi": "bidirectional breaking"}
 
 
 def unpack(root):

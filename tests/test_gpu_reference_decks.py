@@ -4,8 +4,7 @@ decks a reference user already has.  Each deck runs through its output samples t
 reference_decks.WINDOW (up to a few thousand steps, inside the range where two
 roundings of the same arithmetic keep identical step sequences): identical accepted
 and rejected counts, eta and u within 1e-9, and on the breaking deck the same
-breaking.dat records.  The bidirectional breaking deck is refused by the device set-up
-with its reason."""
+breaking.dat records."""
 import concurrent.futures as cf
 
 import numpy as np
@@ -13,7 +12,7 @@ import pytest
 
 import oracle_lib as ol
 from decks_util import rel_l2
-from reference_decks import REFUSED, WINDOW, unpack
+from reference_decks import WINDOW, unpack
 
 pytestmark = pytest.mark.gpu
 
@@ -67,9 +66,3 @@ def test_reference_decks_match_oracle(tmp_path):
         e.close()
     assert any_breaking   # the barred breaking deck starts breaking inside its window
 
-
-@pytest.mark.parametrize("name", sorted(REFUSED))
-def test_reference_deck_refused_with_reason(tmp_path, name):
-    decks = unpack(tmp_path)
-    with pytest.raises(hw.EngineError, match=REFUSED[name]):
-        hw.Engine(decks[name])

@@ -85,8 +85,8 @@ def test_library_exports_every_declared_symbol():
 def test_reference_decks_setup(tmp_path):
     """Every packed reference deck: the host set-up's tables equal the oracle's
     (AreaShort and Area influx, user-defined bars, an initial-value bore)."""
-    from reference_decks import REFUSED, WINDOW, unpack
+    from reference_decks import WINDOW, unpack
     decks_ = unpack(tmp_path)
-    assert set(decks_) == set(WINDOW) | set(REFUSED)
+    assert set(decks_) == set(WINDOW)
     for name, deck in decks_.items():
         _compare(deck)
