@@ -18,7 +18,8 @@ LIB = os.path.join(LIBDIR, "libhawassi_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 SOURCES = ["hw_engine.cu", "hw_setup.cpp", "hw_inst_256.cu", "hw_inst_512.cu", "hw_inst_1024.cu",
-           "hw_inst_2048.cu", "hw_noalloc.cu", "hw_mlp.cu", "hw2d_engine.cu", "hw_kin.cu", "hw_influx.cu", "hw_peak.cu"]
+           "hw_inst_2048.cu", "hw_noalloc.cu", "hw_mlp.cu", "hw2d_engine.cu", "hw_kin.cu", "hw_influx.cu", "hw_peak.cu",
+           "hw2d_influx.cu"]
 HEADERS = ["hw_fft.cuh", "hw_device.cuh", "hw_rhs.cuh", "hw_stepper.cuh", "hw_breaking.cuh",
            "hw_kernels.cuh", "hw_kernels.h", "hw_setup.hpp", "hw_rhs_fast.cuh", "hw2d.cuh", "hw2d_var.cuh", "hw2d_brk.cuh", "hw2d_wall.cuh", "hw2d_out.cuh", "hw2d_hs3.cuh", "hw_output.cuh", "hw_kin.h"]
 

@@ -279,6 +279,43 @@ def directional_signals(y, t, Hs, Tp, gamma, s_spread, depth, n_freq, n_dir, see
     return z.real * r[None, :], z.imag * r[None, :]
 
 
+def reference_directional_components(t, Hs, Tp, gamma, s_spread, depth, seed):
+    """The spectral components of the 2D set-up's jonswap_influx (2d/functions.c:2226-2446)
+    for the time grid t: the first Nt/2 frequencies of freqspace over the time span, the
+    wavenumber of each at `depth` (exact dispersion), amplitudes sqrt(2 S dw) of
+    fun_jonswap's spectrum (normalised to Hs by the trapezoid m0), one direction each
+    drawn from the cos^2s distribution (s_spread; None or inf: long-crested) by
+    interpolating the inverse of its cumulative sum (natural cubic spline, as
+    gsl_spline_eval), and uniform phases.  The reference draws the uniforms from
+    srand(time(0)); here they come from the seeded splitmix64 stream (directions from
+    seed 2 seed + 1, phases from 2 seed + 2).  Returns (a, w, k, theta, phi)."""
+    from scipy.interpolate import CubicSpline
+    from .decks import splitmix64_uniform
+    nt = t.size
+    nh = nt // 2
+    ww = freqspace(float(t[-1] - t[0]), nt)[:nh]
+    wp = 2 * math.pi / Tp
+    fp = wp / (2 * math.pi)
+    JS = np.zeros(nh)
+    f = ww[1:] / (2 * math.pi)
+    sig = np.where(ww[1:] <= wp, 0.07, 0.09)
+    gp = np.exp(-0.5 * ((f / fp - 1) / sig) ** 2)
+    JS[1:] = 0.0081 * GRAV ** 2 * (2 * math.pi) ** -4 * f ** -5 * np.exp(-(5.0 / 4.0) * (f / fp) ** -4) * gamma ** gp
+    m0 = (np.sum(JS) - JS[0] / 2 - JS[-1] / 2) * (ww[1] - ww[0])
+    a = np.sqrt(2 * (Hs ** 2 / 16) * JS / m0 * (ww[1] - ww[0]))
+    th = -math.pi / 2 + np.arange(nh) * (math.pi / (nh - 1))
+    if s_spread is None or not np.isfinite(s_spread):
+        theta = np.zeros(nh)
+    else:
+        s = float(s_spread)
+        coef = math.gamma(s + 1.0) / (math.sqrt(math.pi) * math.gamma(s + 0.5))
+        cdf = np.cumsum(coef * np.cos(th) ** (2 * s))
+        cdf = cdf / cdf[-1] + math.exp(-12.0) / math.pi * th
+        theta = CubicSpline(cdf, th, bc_type="natural")(splitmix64_uniform(2 * seed + 1, nh))
+    phi = 2 * math.pi * splitmix64_uniform(2 * seed + 2, nh)
+    return a, ww, kappa_of_omega(ww, depth), theta, phi
+
+
 def two_depth_operator(depth, kx, ky, omega_p, U=0.0, mdir=0.0):
     """Tables of the two-reference-depth operator (funOprt_DispInterpolation_2p,
     2d/functions.c:1534-1626): on 101 depths between the shallowest and deepest
@@ -458,13 +495,17 @@ def shoal_bathymetry(x, y, deep=5.0, shallow=0.5, x1=100.0, x2=285.0, seed=0):
 def tables(nx=1024, ny=1024, Lx=300.0, Ly=300.0, depth=3.0, Hs=0.5, Tp=6.0, gamma=3.3, s_spread=10,
            n_freq=256, n_dir=64, t_end=300.0, dt=0.1, damp=30.0, x_line=45.0, nadj=1.0, model=2,
            propagation=0, seed=0, bathymetry="flat", shallow=0.5, walls=(), refl=0.5, breaking=False,
-           kbc=0.8, tc=0.2, tchar=0.5, ninterp=2) -> dict:
+           kbc=0.8, tc=0.2, tchar=0.5, ninterp=2, influx_model="lines", device=0) -> dict:
     """All tables of a 2D deck (vertical influx line at x_line).  bathymetry "flat":
     depth everywhere (rhs_AB2_2DF_uv); "shoal": `depth` offshore sloping to
     `shallow` with a seeded shoal, two reference depths (rhs_AB2_2DB_uv), or three
     with ninterp=3 (HSSgen_3depth).
     breaking=True adds the kinematic-breaking tables of parambreak
-    (2d/breaking.c:1-44) with the deck's KBC, TC, Tchar."""
+    (2d/breaking.c:1-44) with the deck's KBC, TC, Tchar.
+    influx_model "lines": n_freq x n_dir seeded components on the grids' Fourier lines
+    (directional_signals); "reference": jonswap_influx's own model, Nt/2 components with
+    one direction each (reference_directional_components), summed on the CUDA device
+    `device`."""
     x = np.linspace(0.0, Lx, nx)          # fun_intervaltovector (2d/functions1.c:204)
     y = np.linspace(0.0, Ly, ny)
     kx = freqspace(x[-1] - x[0], nx)
@@ -495,7 +536,16 @@ def tables(nx=1024, ny=1024, Lx=300.0, Ly=300.0, depth=3.0, Hs=0.5, Tp=6.0, gamm
     newgam, skewgam = area_kernels_vertical(x, y, kx, depth, x_line, damp, damp)
     nt = int(round(t_end / dt)) + 1
     tsig = np.arange(nt) * dt
-    sig, sigs = directional_signals(y, tsig, Hs, Tp, gamma, s_spread, depth, n_freq, n_dir, seed)
+    if influx_model == "reference":
+        # jonswap_influx's own model: Nt/2 components, one random direction each,
+        # summed for every sample and line point on the device
+        from .engine2d import directional_signal
+        comps = reference_directional_components(tsig, Hs, Tp, gamma, s_spread, depth, seed)
+        r = np.clip(tsig / 2.0, 0, 1)
+        sig, sigs = directional_signal(0.0, dt, nt, y, y[0], comps, ramp_t=0.5 * (1 - np.cos(math.pi * r)),
+                                       device=device)
+    else:
+        sig, sigs = directional_signals(y, tsig, Hs, Tp, gamma, s_spread, depth, n_freq, n_dir, seed)
     # The area kernel carries (2 pi)^2 / (dx dy) and integrates to that times dx along
     # x; scaling the elevation by dy / (2 pi)^2 makes the line generate the target
     # elevation (the reference reaches the same end by dividing the influx spectrum by

@@ -102,8 +102,27 @@ def _lib():
         L.hw2d_breaking_log_nodes.argtypes = [vp]
         L.hw2d_fields.argtypes = [vp, dp, dp, dp]
         L.hw2d_run_outputs.argtypes = [vp, ctypes.POINTER(Hw2dOutputs)]
+        L.hw2d_directional_influx.argtypes = [ctypes.c_int, dd, dd, ctypes.c_int, dp, dd, ctypes.c_int, dp, dp, dp,
+                                              dp, dp, dd, dp, dp, dp, dp, ctypes.c_int]
+        L.hw2d_influx_last_error.restype = ctypes.c_char_p
         _bound = True
     return L
+
+
+def directional_signal(t0, dt, nt, y, y0, comps, mdir=0.0, ramp_t=None, ramp_y=None, device=0):
+    """The directional line signal and its quadrature ([lines][nt] each) of the
+    components comps = (a, w, k, theta, phi) on the device (hw2d_directional_influx)."""
+    L = _lib()
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    a, w, k, th, ph = (np.ascontiguousarray(v, dtype=np.float64) for v in comps)
+    rt = np.ones(nt) if ramp_t is None else np.ascontiguousarray(ramp_t, dtype=np.float64)
+    ry = np.ones(y.size) if ramp_y is None else np.ascontiguousarray(ramp_y, dtype=np.float64)
+    eta, skew = np.empty((y.size, nt)), np.empty((y.size, nt))
+    if L.hw2d_directional_influx(int(nt), float(t0), float(dt), y.size, _ptr(y), float(y0), a.size, _ptr(a), _ptr(w),
+                                 _ptr(k), _ptr(th), _ptr(ph), float(mdir), _ptr(rt), _ptr(ry), _ptr(eta), _ptr(skew),
+                                 int(device)):
+        raise EngineError(L.hw2d_influx_last_error().decode())
+    return eta, skew
 
 
 def _ptr(a):

@@ -300,6 +300,23 @@ typedef struct hw2d_tables {
     const double* om2_k;        /* [K][ny*nx] Omega^2 of each reference depth   */
 } hw2d_tables;
 
+/* The directional JONSWAP line signal of the 2D set-up's jonswap_influx
+ * (2d/functions.c:2310-2446, vertical influx line) on the device: for the nt samples
+ * t0 + i dt and the nlines line points y[j],
+ *   eta[j*nt + i]  = ramp_t[i] ramp_y[j] sum_c a[c] cos(-w[c] t_i + phi[c] + k[c] sin(theta[c] + mdir) (y[j] - y0)),
+ *   skew[j*nt + i] = the same sum of sin (the quadrature the 2D source takes beside it),
+ * in the [line][sample] layout of hw2d_tables.sig / .sigskew.  The nc components (the
+ * reference draws nt/2 of them, one direction each, from srand(time(0)); the Python
+ * set-up draws them from a seeded stream, decks2d.reference_directional_components)
+ * are host arrays, as are the outputs; the call allocates and frees its device
+ * buffers and restores the caller's current device.  Returns 0, or 1 with the reason
+ * in hw2d_influx_last_error(). */
+int hw2d_directional_influx(int nt, double t0, double dt, int nlines, const double* y, double y0, int nc,
+                            const double* a, const double* w, const double* k, const double* theta,
+                            const double* phi, double mdir, const double* ramp_t, const double* ramp_y,
+                            double* eta, double* skew, int device);
+const char* hw2d_influx_last_error(void);
+
 /* opts: eps_abs/eps_rel (<= 0: the 2D reference's 1e-3 / 1e-2, 2d/main.c:196-197),
  * h0 (<= 0: dt/5 of the signal grid, 2d/fun_odesolver.c:2580), device. */
 hw2d_ctx*   hw2d_create(const hw2d_tables* tables, const hw_opts* opts);

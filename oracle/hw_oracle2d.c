@@ -1664,3 +1664,87 @@ done:
     free(eta); free(u); free(v); free(ix); free(iy);
     return ret;
 }
+
+/* ------------------------------------------------------------------------ */
+/* The directional JONSWAP influx (jonswap_influx, 2d/functions.c:2226-2446) */
+/* ------------------------------------------------------------------------ */
+static double kappa_exact(double w, double d) {   /* w^2 = g k tanh(k d), Newton to convergence */
+    double k = w / sqrt(GRAV * d);
+    for (int it = 0; it < 60; it++) {
+        double th = tanh(k * d);
+        k = k - (GRAV * k * th - w * w) / (GRAV * th + GRAV * k * d * (1 - th * th));
+    }
+    return k;
+}
+
+void or2d_jonswap_components(int nt, const double* t, double Hs, double Tp, double gamma, double s, double depth,
+                             const double* rn, const double* ru, double* a, double* w, double* k, double* theta,
+                             double* phi) {
+    const int Nhalf = nt / 2;
+    /* freqspace (2d/functions.c:1810-1832) of the time span, its first Nt/2 entries */
+    const double len = t[nt - 1] - t[0];
+    const double dom = 2 * M_PI / len, fmin = -0.5 * 2 * M_PI / (len / (nt - 1));
+    const double fmax = (nt / 2) * 2 == nt ? -fmin - dom : -fmin;
+    const double du = (fmax - fmin) / (nt - 1);
+    double* ww = malloc(sizeof(double) * (size_t)nt);
+    for (int i = 0; i < nt / 2; i++) ww[i] = fmin + (nt / 2 + i) * du;
+    for (int i = nt / 2, n = 0; i < nt; i++, n++) ww[i] = fmin + n * du;
+    ww[0] = 1e-10;
+    /* fun_jonswap (2d/functions.c:2226-2307, no SPcorrection.dat) */
+    const double omgp = 2 * M_PI / Tp, fp = omgp / (2 * M_PI), alpha = 0.0081;
+    double* JS = calloc((size_t)Nhalf, sizeof(double));
+    for (int i = 1; i < Nhalf; i++) {
+        double sig = ww[i] <= omgp ? 0.07 : 0.09;
+        double f = ww[i] / (2 * M_PI);
+        double gp = exp(-0.5 * pow(((f / fp - 1) / sig), 2));
+        JS[i] = alpha * pow(GRAV, 2) * pow((2 * M_PI), (-4)) * pow(f, (-5)) * exp(-(5.0 / 4.0) * pow((f / fp), (-4))) *
+                pow(gamma, gp);
+    }
+    double m0 = 0;   /* trapz (2d/functions1.c:236) */
+    for (int i = 0; i < Nhalf; i++) m0 += (i == 0 || i == Nhalf - 1) ? JS[i] / 2 : JS[i];
+    m0 *= ww[1] - ww[0];
+    const double domg = ww[1] - ww[0];
+    /* directions: the cos^2s inverse CDF at the given uniforms */
+    double* th = malloc(sizeof(double) * (size_t)Nhalf);
+    const double ds = M_PI / (Nhalf - 1);
+    for (int j = 0; j < Nhalf; j++) th[j] = -M_PI / 2.0 + j * ds;
+    if (s > 0) {
+        const double coef = tgamma(s + 1.0) / (sqrt(M_PI) * tgamma(s + 0.5));
+        double* cdf = malloc(sizeof(double) * (size_t)Nhalf);
+        double total = 0;
+        for (int j = 0; j < Nhalf; j++) { total = total + coef * pow(cos(th[j]), 2 * s); cdf[j] = total; }
+        for (int j = 0; j < Nhalf; j++) cdf[j] = cdf[j] / cdf[Nhalf - 1] + exp(-12.0) / M_PI * th[j];
+        double* cc = malloc(sizeof(double) * (size_t)Nhalf);
+        or_cspline_coeffs(Nhalf, cdf, th, cc);
+        for (int j = 0; j < Nhalf; j++) theta[j] = or_cspline_eval(Nhalf, cdf, th, cc, rn[j]);
+        free(cdf); free(cc);
+    } else {
+        for (int j = 0; j < Nhalf; j++) theta[j] = 0.0;
+    }
+    for (int j = 0; j < Nhalf; j++) {
+        const double js = (pow(Hs, 2) / 16) * JS[j] / m0;
+        a[j] = sqrt(2 * js * domg);
+        w[j] = ww[j];
+        k[j] = kappa_exact(ww[j], depth);
+        phi[j] = 2 * M_PI * ru[j];
+    }
+    free(ww); free(JS); free(th);
+}
+
+void or2d_directional_signal(int nt, const double* t, int nlines, const double* y, double y0, int nc,
+                             const double* a, const double* w, const double* k, const double* theta,
+                             const double* phi, double mdir, const double* ramp_t, const double* ramp_y,
+                             double* eta, double* skew) {
+    for (int j = 0; j < nlines; j++)
+        for (int i = 0; i < nt; i++) {
+            double sc = 0, ss = 0;
+            for (int c = 0; c < nc; c++) {
+                const double ph = -w[c] * t[i] + phi[c] + k[c] * sin(theta[c] + mdir) * (y[j] - y0);
+                sc += a[c] * cos(ph);
+                ss += a[c] * sin(ph);
+            }
+            const double r = ramp_t[i] * ramp_y[j];
+            eta[(size_t)j * nt + i] = sc * r;
+            skew[(size_t)j * nt + i] = ss * r;
+        }
+}

@@ -82,6 +82,25 @@ typedef struct or2d_tables {
 
 /* Copies every table.  eps <= 0 selects the reference's 2D values (abs 1e-3,
  * rel 1e-2, 2d/main.c:196-197).  Returns NULL on error (or2d_last_error). */
+/* The directional JONSWAP influx of jonswap_influx (2d/functions.c:2226-2446): the
+ * components of the Nt-sample time grid t (uniform) -- w = freqspace(t[Nt-1] - t[0], Nt)
+ * (2d/functions.c:1810) restricted to its first Nt/2 entries, k(w) at depth (exact
+ * dispersion by Newton), a = sqrt(2 S(w) dw) from fun_jonswap (Hs, Tp, gamma; JS[0] = 0,
+ * trapezoid m0), one direction each from the cos^2s distribution by inverse-CDF
+ * interpolation (GSL natural cspline) of the given uniforms rn (s <= 0: long-crested,
+ * every direction 0), phase 2 pi ru -- and the line signal they add up to along a
+ * vertical influx line,
+ *   eta[j][i] = ramp_t[i] ramp_y[j] sum_c a_c cos(-w_c t_i + phi_c + k_c sin(theta_c + mdir) (y_j - y0)),
+ * with skew[j][i] the same sum of sin (the quadrature the 2D source takes beside it).
+ * rn and ru hold nt / 2 uniforms each; the outputs a, w, k, theta, phi nt / 2 entries. */
+void or2d_jonswap_components(int nt, const double* t, double Hs, double Tp, double gamma, double s, double depth,
+                             const double* rn, const double* ru, double* a, double* w, double* k, double* theta,
+                             double* phi);
+void or2d_directional_signal(int nt, const double* t, int nlines, const double* y, double y0, int nc,
+                             const double* a, const double* w, const double* k, const double* theta,
+                             const double* phi, double mdir, const double* ramp_t, const double* ramp_y,
+                             double* eta, double* skew);
+
 or2d_ctx* or2d_create(const or2d_tables* tb, double eps_abs, double eps_rel);
 void or2d_destroy(or2d_ctx* c);
 const char* or2d_last_error(void);

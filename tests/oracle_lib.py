@@ -229,6 +229,33 @@ def mlp_loss_grad(params, records):
     return L, g
 
 
+def jonswap_components_2d(t, Hs, Tp, gamma, s, depth, rn, ru):
+    """or2d_jonswap_components: (a, w, k, theta, phi) of the 2D directional influx."""
+    L = lib()
+    nh = t.size // 2
+    out = [np.zeros(nh) for _ in range(5)]
+    t = np.ascontiguousarray(t, dtype=np.float64)
+    rn = np.ascontiguousarray(rn, dtype=np.float64)
+    ru = np.ascontiguousarray(ru, dtype=np.float64)
+    L.or2d_jonswap_components(t.size, _p(t), ctypes.c_double(Hs), ctypes.c_double(Tp), ctypes.c_double(gamma),
+                              ctypes.c_double(s), ctypes.c_double(depth), _p(rn), _p(ru), *[_p(o) for o in out])
+    return tuple(out)
+
+
+def directional_signal_2d(t, y, y0, comps, mdir=0.0, ramp_t=None, ramp_y=None):
+    """or2d_directional_signal: the direct sum, [lines][nt] elevation and quadrature."""
+    L = lib()
+    t = np.ascontiguousarray(t, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    a, w, k, th, ph = (np.ascontiguousarray(v, dtype=np.float64) for v in comps)
+    rt = np.ones(t.size) if ramp_t is None else np.ascontiguousarray(ramp_t, dtype=np.float64)
+    ry = np.ones(y.size) if ramp_y is None else np.ascontiguousarray(ramp_y, dtype=np.float64)
+    eta, skew = np.zeros((y.size, t.size)), np.zeros((y.size, t.size))
+    L.or2d_directional_signal(t.size, _p(t), y.size, _p(y), ctypes.c_double(y0), a.size, _p(a), _p(w), _p(k),
+                              _p(th), _p(ph), ctypes.c_double(mdir), _p(rt), _p(ry), _p(eta), _p(skew))
+    return eta, skew
+
+
 class Oracle2D:
     """The 2D flat-bottom restatement (oracle/hw_oracle2d.c) on a table dict."""
 

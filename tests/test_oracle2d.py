@@ -343,3 +343,25 @@ def test_k_reference_weights():
     w2 = decks2d.plain_k_operator(tb, 2)["gam_k"]
     assert np.abs(w2[0] - tb["gam_min"].ravel()).max() < 1e-4
     assert np.abs(w2[1] - tb["gam_plus"].ravel()).max() < 1e-4
+
+
+# ------------------------------------------------- the directional influx model
+@pytest.mark.parametrize("s_spread", [10.0, None])
+def test_reference_directional_components_match_oracle(s_spread):
+    """decks2d's components of jonswap_influx (seeded draws) equal the oracle's C
+    restatement given the same uniforms: amplitudes, frequencies, wavenumbers,
+    directions (the cos^2s inverse CDF) and phases."""
+    import math
+    import oracle_lib as ol
+    from hawassi_c_b200.decks import splitmix64_uniform
+    t = np.arange(601) * 0.1
+    got = decks2d.reference_directional_components(t, 0.5, 6.0, 3.3, s_spread, 4.0, seed=7)
+    nh = t.size // 2
+    ref = ol.jonswap_components_2d(t, 0.5, 6.0, 3.3, s_spread if s_spread else -1.0, 4.0,
+                                   splitmix64_uniform(15, nh), splitmix64_uniform(16, nh))
+    for g, r in zip(got, ref):
+        np.testing.assert_allclose(g, r, rtol=1e-12, atol=1e-14)
+    a, w = got[0], got[1]
+    assert np.sum(a ** 2) / 2 == pytest.approx((0.5 / 4) ** 2, rel=0.02)   # Hs from the amplitudes
+    if s_spread:
+        assert np.abs(got[3]).max() < math.pi / 2 and np.std(got[3]) > 0.1
