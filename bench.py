@@ -133,7 +133,7 @@ def sample_members(decks, n):
     return [decks[int(i * step)] for i in range(n)]
 
 
-LEARNED_MEMBERS = 16
+LEARNED_MEMBERS = 64   # the configuration's evaluation ensemble
 
 
 def learned_vs_plain(device):
