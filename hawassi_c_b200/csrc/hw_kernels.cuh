@@ -22,7 +22,9 @@ template <int M>
 __device__ __forceinline__ void evolve_member(DevMember* mems, int mi, int mode, DevMember& sd, double* red,
                                               double2* smem_buf, int C, int rank) {
   if (threadIdx.x == 0) sd = mems[mi];
-  __syncthreads();
+  // a cluster barrier, not only the CTA's: the RHS's first phase writes into the
+  // partner CTA's shared memory, which must be running
+  member_sync(C);
   Ctx<M> X = make_ctx<M>(sd, smem_buf, red, rank);
   Bufs B;
   B.y = sd.y;

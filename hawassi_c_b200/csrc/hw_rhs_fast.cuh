@@ -222,20 +222,55 @@ __device__ __noinline__ void rhs_hs2_flat(Ctx<M>& X, double t, double2* __restri
   };
   if (X.stg) {
     // during a step the stage input is formed here from y and the k's (and kept in
-    // zs for the assembly); the value at the partner wavenumber N - k is formed from
-    // the same global vectors, so no exchange between the CTAs is needed
+    // zs for the assembly).  Each Hermitian pair {k, N - k} is formed once, by one
+    // thread: CTA c takes the first half of its slice, i < M / 2, with the partners
+    // (CTA (C - c) mod C, index M - 1 - i, or (M - i) mod M in CTA 0), which lie in the
+    // partner CTA's second half; CTA 0's positions 0 and M / 2 are their own partners.
+    // The thread writes both packed values, the partner's into the partner CTA's slices
+    // (its shared memory through the cluster when that is another CTA).
     double2* zw = d.zs;
-    HW_FOREACH(X) {
-      const int pp = partner_pos(X, idx);
-      const double2 e = stage_val(*X.stg, p), w = stage_val(*X.stg, N + p);
-      const double2 ep = stage_val(*X.stg, pp), wp = stage_val(*X.stg, N + pp);
+    constexpr int T = Ctx<M>::T;
+    const int c = X.c, cq = (C - c) & (C - 1);
+    double2* Aq = A;
+    double2* Bq = Bf;
+    if (cq != c) {
+      cg::cluster_group cl = cg::this_cluster();
+      Aq = cl.map_shared_rank(A, cq);
+      Bq = cl.map_shared_rank(Bf, cq);
+    }
+    const StageSrc& st = *X.stg;
+    auto pair = [&](int i, int j) {
+      const int p = c * M + i, pp = cq * M + j;
+      const double2 e = stage_val(st, p), w = stage_val(st, N + p);
+      if (p == pp) {
+        zw[p] = e;
+        zw[N + p] = w;
+        double2 a, b;
+        packed(p, p, e, e, w, w, a, b);
+        A[pidx(i)] = a;
+        Bf[pidx(i)] = b;
+        return;
+      }
+      const double2 ep = stage_val(st, pp), wp = stage_val(st, N + pp);
       zw[p] = e;
       zw[N + p] = w;
+      zw[pp] = ep;
+      zw[N + pp] = wp;
       double2 a, b;
       packed(p, pp, e, ep, w, wp, a, b);
-      A[pidx(idx)] = a;
-      Bf[pidx(idx)] = b;
+      A[pidx(i)] = a;
+      Bf[pidx(i)] = b;
+      packed(pp, p, ep, e, wp, w, a, b);
+      Aq[pidx(j)] = a;
+      Bq[pidx(j)] = b;
+    };
+#pragma unroll
+    for (int u = 0; u < kPts / 2; ++u) {
+      const int i = X.tid + u * T;
+      pair(i, c == 0 ? ((M - i) & (M - 1)) : (M - 1 - i));
     }
+    if (c == 0 && X.tid == 0) pair(M / 2, M / 2);
+    if (C > 1) cg::this_cluster().sync();   // the partners' slices are written
   } else {
     // zs written by the caller: the partner values come through the slices
     HW_FOREACH(X) {
