@@ -117,3 +117,25 @@ def test_k_reference_weights_reproduce_the_peak_dispersion(tmp_path):
     blend_o = sum(g[q] * om(kap, D[q]) for q in range(K))
     assert np.max(np.abs(blend_c / cp2(kap, h) - 1)) < 1e-8
     assert np.max(np.abs(blend_o / om(kap, h) - 1)) < 1e-8
+
+
+def test_up3ip_weights_solve_the_three_depth_system(golden_dir, tmp_path):
+    """Up3IP's weights (1d/functions.c:2247-2340), checked independently of both
+    restatements: at every point the blend of the three reference depths' long-wave
+    speed, frequency and squared phase speed at the point's peak wavenumber gives the
+    point's own -- exactly at the 101 depth samples the reference solves at, to the
+    natural spline's interpolation error between them (measured below 3e-5)."""
+    from hawassi_c_b200.learned import kappa_linear
+    G = 9.80665
+    cp2 = lambda k, d: G * np.tanh(k * d) / k
+    om = lambda k, d: np.sqrt(G * k * np.tanh(k * d))
+    c0 = lambda d: np.sqrt(G * d)
+    for deck in (os.path.join(golden_dir, "harmbar"), small_deck(tmp_path, "v3", nx=1024, varying=True)):
+        h = engine.deck_table(deck, "depth")
+        nu = float(engine.deck_table(deck, "nu_peak")[0])
+        g = [engine.deck_table(deck, n) for n in ("gam_min", "gam_mid", "gam_plus")]
+        D = (h.min(), (h.min() + h.max()) / 2, h.max())
+        kap = kappa_linear(nu, h)
+        for f in (lambda d: c0(d), lambda d: om(kap, d), lambda d: cp2(kap, d)):
+            blend = sum(gj * f(Dj) for gj, Dj in zip(g, D))
+            assert np.max(np.abs(blend / f(h) - 1)) < 1e-4
