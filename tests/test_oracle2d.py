@@ -365,3 +365,51 @@ def test_reference_directional_components_match_oracle(s_spread):
     assert np.sum(a ** 2) / 2 == pytest.approx((0.5 / 4) ** 2, rel=0.02)   # Hs from the amplitudes
     if s_spread:
         assert np.abs(got[3]).max() < math.pi / 2 and np.std(got[3]) > 0.1
+
+
+@pytest.mark.parametrize("K", [4, 16])
+def test_hs3_terms_are_cubic_k_reference(K):
+    """The same homogeneity with the K-reference-depth operator (the plain 16-depth one
+    and the 4-depth form of the learned blend)."""
+    tb3 = decks2d.tables(nx=64, ny=32, Lx=57.6, Ly=28.8, depth=2.0, shallow=0.6, Hs=0.1, Tp=3.0, n_freq=24,
+                         n_dir=6, t_end=6.0, dt=0.1, damp=6.0, x_line=10.0, nadj=1.0, seed=2, bathymetry="shoal",
+                         model=3)
+    for k in ("newgam", "skewgam", "tsig", "sig", "sigskew"):
+        tb3[k] = None
+    tb3["nt"] = 0
+    tb3 = decks2d.plain_k_operator(tb3, K)
+    tb2 = dict(tb3, model=2)
+    n = tb3["nx"] * tb3["ny"]
+    o2, o3 = Oracle2D(tb2), Oracle2D(tb3)
+    rng = np.random.default_rng(13)
+    z = 0.02 * rng.standard_normal(6 * n) * np.tile(tb3["aal"].ravel(), 6) * np.sqrt(n)
+    d1 = o3.rhs(0.0, z) - o2.rhs(0.0, z)
+    d2 = o3.rhs(0.0, 2 * z) - o2.rhs(0.0, 2 * z)
+    assert np.linalg.norm(d1) > 1e-8 * np.linalg.norm(o2.rhs(0.0, z))
+    assert np.linalg.norm(d2 - 8 * d1) < 1e-8 * np.linalg.norm(d2)
+
+
+def test_k_reference_operator_with_idle_depths_is_the_two_depth_one():
+    """A flat 1.5 m bottom under 4 reference depths (1.5, 3, 6, 12 m): the K-depth
+    weights put every point wholly on the first depth, and the idle depths' terms are
+    exact zeros, so the K-reference RHS equals, bit for bit, the two-depth RHS with the
+    same weights (gam_min = 1, gam_plus = 0) -- which the test above relates to the flat
+    RHS."""
+    tb = decks2d.tables(nx=64, ny=32, Lx=57.6, Ly=28.8, depth=1.5, Hs=0.1, Tp=3.0, n_freq=24, n_dir=6, t_end=6.0,
+                        dt=0.1, damp=6.0, x_line=10.0, nadj=1.0, seed=2)
+    n = tb["nx"] * tb["ny"]
+    depth = np.full((tb["ny"], tb["nx"]), 1.5)
+    D = np.array([1.5, 3.0, 6.0, 12.0])
+    w = decks2d.k_reference_weights(depth, 2 * np.pi / 3.0, D)
+    assert np.allclose(w[0], 1.0, atol=1e-12) and np.allclose(w[1:], 0.0, atol=1e-12)
+    w = np.zeros_like(w)
+    w[0] = 1.0
+    kt = decks2d.with_k_operator(dict(tb, depth=depth), D, w)
+    two = dict(tb, gam_min=np.ones(n), gam_plus=np.zeros(n), csq_min=kt["csq_k"][0], csq_plus=kt["csq_k"][1],
+               om2_min=kt["om2_k"][0], om2_plus=kt["om2_k"][1])
+    rng = np.random.default_rng(14)
+    z = 0.02 * rng.standard_normal(6 * n) * np.tile(tb["aal"].ravel(), 6) * np.sqrt(n)
+    for model in (2, 3):
+        a = Oracle2D(dict(two, model=model)).rhs(0.4, z)
+        b = Oracle2D(dict(kt, model=model)).rhs(0.4, z)
+        assert np.array_equal(a, b), model
