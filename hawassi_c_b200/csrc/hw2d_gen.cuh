@@ -2,7 +2,9 @@
 // rhs_AB2_2DB_uv and rhs_AB3_2DB_uv (2d/fun_odesolver.c:4350-4402, 4542-4626,
 // 4735-4844) with their term functions fun_termshat_AB1/AB2/AB3_2DB_uv
 // (:2874-2960, 3327-3510, 4104-4296) and the two- or three-reference-depth
-// operator HSSgen_2depth / HSSgen_3depth (:500-697).
+// operator HSSgen_2depth / HSSgen_3depth (:500-697), or its sum over K reference depths
+// (the plain K-reference operator and the learned 4-depth blend, which the reference
+// does not have).
 //
 // Unlike the fused passes of hw2d_var.cuh (two reference depths, HS1/HS2 only),
 // this path runs the reference's sequence of whole-field operations one by one:
@@ -11,7 +13,7 @@
 // kernel, and every pointwise step is a grid-stride kernel over the field.  Its
 // fields are full complex N = Nx Ny arrays in the reference's row-major order, in
 // one pool owned by the engine.  It serves the combinations the fused passes do
-// not cover (three reference depths; HS3 on the varying bottom) at the
+// not cover (three or K reference depths; HS3 on the varying bottom) at the
 // reference's own transform count.
 #pragma once
 
